@@ -1,0 +1,106 @@
+"""Seeded small 2.5D cases shared by the golden-vector generator and the parity tests.
+
+Every case is raw arrays (mesh nodes and cells, electrode positions, ABMN rows, a
+conductivity model, a measurement cotangent and a conductivity direction), so the reference,
+the oracle and the CUDA path all start from identical inputs.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def structured_section(xs, depths, triangles: bool = True):
+    """Nodes and cells of a flat-topped section; ``depths`` are positive, increasing from 0.
+
+    Quads are ``[a, b, c, d]`` counter-clockwise from the upper-left node; triangle meshes split
+    each quad as ``[a, d, b], [b, d, c]``.
+    """
+
+    xs, zs = np.asarray(xs, dtype=float), -np.asarray(depths, dtype=float)
+    grid_x, grid_z = np.meshgrid(xs, zs)
+    nodes = np.column_stack((grid_x.ravel(), grid_z.ravel()))
+    index = np.arange(nodes.shape[0]).reshape(len(zs), len(xs))
+    a = index[:-1, :-1].ravel()
+    b = index[:-1, 1:].ravel()
+    c = index[1:, 1:].ravel()
+    d = index[1:, :-1].ravel()
+    if triangles:
+        cells = np.stack((np.stack((a, d, b), 1), np.stack((b, d, c), 1)), 1).reshape(-1, 3)
+    else:
+        cells = np.stack((d, c, b, a), 1)
+    return nodes, cells
+
+
+def dipole_dipole(count: int, max_a: int, max_n: int) -> np.ndarray:
+    rows = [
+        (i, i + a, i + a * (n + 1), i + a * (n + 2))
+        for a in range(1, max_a + 1)
+        for n in range(1, max_n + 1)
+        for i in range(count)
+        if i + a * (n + 2) < count
+    ]
+    return np.asarray(rows, dtype=np.int64)
+
+
+def _centroids(nodes, cells):
+    return nodes[cells].mean(axis=1)
+
+
+def layered_model(nodes, cells, rng) -> np.ndarray:
+    """Conductivity of a three-layer section with one Gaussian anomaly (seeded)."""
+
+    centers = _centroids(nodes, cells)
+    depth = -centers[:, 1]
+    depth_span = float(depth.max())
+    interfaces = np.sort(rng.uniform(0.1, 0.7, 2)) * depth_span
+    layer_rho = 10.0 ** rng.uniform(1.0, 3.0, 3)
+    rho = np.where(depth < interfaces[0], layer_rho[0], np.where(depth < interfaces[1], layer_rho[1], layer_rho[2]))
+    x0 = rng.uniform(centers[:, 0].min(), centers[:, 0].max())
+    z0 = -rng.uniform(0.1, 0.5) * depth_span
+    radius = rng.uniform(0.1, 0.25) * depth_span
+    contrast = 10.0 ** rng.uniform(-1.0, 1.0)
+    r2 = (centers[:, 0] - x0) ** 2 + (centers[:, 1] - z0) ** 2
+    rho = rho * contrast ** np.exp(-r2 / (2.0 * radius * radius))
+    return 1.0 / rho
+
+
+CASES = {
+    # Flat P1 triangles, dipole-dipole, exercised with every derivative.
+    "tri_flat": {"mesh": "tri", "exact_jacobian": True, "parameters": True, "seed": 3},
+    # Flat bilinear quadrilaterals (the reference's own test meshes are quad strips).
+    "quad_flat": {"mesh": "quad", "exact_jacobian": False, "parameters": False, "seed": 4},
+    # Triangles with remote electrodes: pole-dipole (B remote) and dipole-pole (N remote).
+    "tri_pole": {"mesh": "tri", "poles": True, "exact_jacobian": False, "parameters": False, "seed": 5},
+}
+
+
+def case_inputs(name: str) -> dict:
+    spec = CASES[name]
+    rng = np.random.default_rng(spec["seed"])
+    xs = np.arange(0.0, 45.0 + 1e-9, 1.5)
+    depths = np.concatenate(([0.0], np.cumsum(np.concatenate((np.full(4, 0.75), np.geomspace(1.0, 4.0, 5))))))
+    nodes, cells = structured_section(xs, depths, triangles=spec["mesh"] == "tri")
+    count = 12
+    electrodes = np.column_stack((6.0 + 3.0 * np.arange(count), np.zeros(count)))
+    measurements = dipole_dipole(count, 2, 4)
+    if spec.get("poles"):
+        extra = [(i, -1, i + 2, i + 3) for i in range(0, count - 3, 2)]
+        extra += [(i, i + 1, i + 3, -1) for i in range(1, count - 3, 3)]
+        measurements = np.concatenate((measurements, np.asarray(extra, dtype=np.int64)))
+    sigma = layered_model(nodes, cells, rng)
+    out = {
+        "nodes": nodes,
+        "cells": cells.astype(np.int64),
+        "electrodes": electrodes,
+        "measurements": measurements,
+        "sigma": sigma,
+        "cotangent": rng.standard_normal(measurements.shape[0]),
+        "direction": rng.standard_normal(cells.shape[0]) * sigma * 1e-2,
+    }
+    if spec.get("parameters"):
+        ids = np.full(cells.shape[0], -1, dtype=np.int64)
+        half = cells.shape[0] // 2
+        ids[:half] = np.arange(half) // 3
+        out["parameter_ids"] = ids
+    return out
