@@ -1,0 +1,31 @@
+"""adtlert_b200: B200 (sm_100a) forward-and-sensitivity path of AD-TLERT's 2.5D ERT operator.
+
+Drop-in for ``adtlert.forward``'s ``ERTForward2p5D`` and ``apparent_resistivity_autograd``; the
+heavy work runs in ``libadtlert_b200.so`` (CUDA kernels behind a C ABI, ``include/adtlert_b200.h``).
+"""
+
+from .autograd import (
+    ERT2p5DApparentResistivityFunction,
+    ERT3DApparentResistivityFunction,
+    ERTApparentResistivityFunction,
+    apparent_resistivity_autograd,
+)
+from .ert2p5d import Discretization, ERTForward2p5D, ForwardResponse
+from .fem import inverse_cosine_weights, wavenumber_bounds
+from .geometry import Mesh, Survey
+from .inputs import FLOAT_DTYPE
+
+__all__ = [
+    "Discretization",
+    "ERT2p5DApparentResistivityFunction",
+    "ERT3DApparentResistivityFunction",
+    "ERTApparentResistivityFunction",
+    "ERTForward2p5D",
+    "FLOAT_DTYPE",
+    "ForwardResponse",
+    "Mesh",
+    "Survey",
+    "apparent_resistivity_autograd",
+    "inverse_cosine_weights",
+    "wavenumber_bounds",
+]

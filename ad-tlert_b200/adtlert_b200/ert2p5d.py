@@ -1,0 +1,611 @@
+"""2.5D multi-wavenumber ERT operator on the B200 kernels of ``libadtlert_b200``.
+
+Drop-in for ``adtlert.forward.ERTForward2p5D`` (adtlert/forward/ert2p5d.py:108-1121): same
+constructor, methods, keyword arguments, defaults, exceptions and return devices (results on
+the CPU). Every wavenumber is solved with the secondary-field formulation
+
+    A(sigma) u_s = A(1) u_p - A(sigma) (rho_src u_p),    u = u_s + rho_src u_p,
+
+with the analytic half-space primary field of each electrode. The host builds the element
+templates and boundary terms once; assembly, the batched direct solve, quadrature, the ABMN
+gathers and every derivative run as CUDA kernels on the caller's current stream.
+"""
+
+from __future__ import annotations
+
+import contextlib
+import ctypes
+import hashlib
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native
+from .fem import (
+    analytic_primary,
+    boundary_mass,
+    inverse_cosine_weights,
+    quad_templates,
+    robin_coefficients,
+    triangle_templates,
+    wavenumber_bounds,
+)
+from .field_cache import FieldCache, factorization_name, newest_batches_first
+from .geometry import Mesh, Survey, geometric_factors, locate_points
+from .inputs import (
+    FLOAT_DTYPE,
+    cell_vector,
+    check_finite,
+    conductivity_model,
+    conductivity_series,
+    cotangent_series,
+    measurement_vector,
+    option,
+    parameter_targets,
+)
+
+Tensor = torch.Tensor
+
+
+@dataclass(frozen=True)
+class ForwardResponse:
+    """Result of a 2.5D ERT forward solve (CPU tensors)."""
+
+    apparent_resistivity: Tensor
+    resistance: Tensor
+    electrode_potentials: Tensor
+    integrated_potentials: Tensor
+    wavenumbers: Tensor
+    weights: Tensor
+
+
+@dataclass(frozen=True)
+class Discretization:
+    """Element space of the operator (the input mesh for flat surfaces)."""
+
+    name: str
+    parent_cell_ids: np.ndarray
+    dof_nodes: np.ndarray
+    cell_dofs: np.ndarray
+    boundary_dofs: np.ndarray
+    boundary_cells: np.ndarray
+    stiffness: np.ndarray
+    mass: np.ndarray
+    boundary_mass: np.ndarray
+    boundary_geometries: np.ndarray
+    electrode_matrix: np.ndarray
+    nnz: int
+    spd: bool = True
+
+    @property
+    def dof_count(self) -> int:
+        return int(self.dof_nodes.shape[0])
+
+
+@dataclass
+class _Fields:
+    """Total fields (W, N, E) of one model on the GPU, dofs in the plan's solver order."""
+
+    total: Tensor
+
+    def on(self, device) -> Tensor:
+        return self.total.to(device)
+
+
+class _Slots:
+    """Factor slots of the plan, keyed by batch size, each remembering which models it holds.
+
+    Mirrors the naming contract of the reference's BatchedSolver (adtlert/forward/cudss.py:63-122):
+    a slot is reused only when the requested factorization name equals the recorded one; any
+    unnamed factorization forgets the record.
+    """
+
+    def __init__(self) -> None:
+        self.slots: dict[int, dict] = {}
+        self.factorizations = 0
+
+    def lookup(self, models: int) -> dict:
+        if models not in self.slots:
+            self.slots[models] = {"slot": len(self.slots), "name": None}
+        return self.slots[models]
+
+    def holds(self, models: int, name) -> bool:
+        entry = self.slots.get(models)
+        return entry is not None and name is not None and entry["name"] == name
+
+    def close(self) -> None:
+        for entry in self.slots.values():
+            entry["name"] = None
+
+
+@dataclass
+class ProblemArrays:
+    """Host arrays of one 2.5D plan (what ``adt_plan_create`` copies), built without a GPU."""
+
+    arrays: dict
+    wavenumbers: np.ndarray
+    weights: np.ndarray
+    stiffness: np.ndarray
+    mass: np.ndarray
+    boundary_mass: np.ndarray
+    robin: np.ndarray
+    electrode_matrix: np.ndarray
+    source_nodes: np.ndarray
+    source_cells: np.ndarray
+    counts: dict
+
+    def struct(self) -> _native.Problem:
+        a, c = self.arrays, self.counts
+        h = _native.host_ptr
+        return _native.Problem(
+            dof_count=c["N"], dim=2, dof_coordinates=h(a["coords"]), cell_count=c["C"], local_dofs=c["K"],
+            cell_dofs=h(a["cell_dofs"]), stiffness=h(a["stiffness"]), mass=h(a["mass"]), parent_cells=None,
+            model_cell_count=c["C"], boundary_count=c["Nb"], boundary_local=2, boundary_dofs=h(a["bdofs"]),
+            boundary_cells=h(a["bcells"]), boundary_mass=h(a["bmass"]), boundary_coefficients=h(a["bcoef"]),
+            wavenumber_count=c["W"], wavenumbers=h(a["k"]), weights=h(a["w"]), electrode_count=c["E"],
+            receiver_width=c["K"], receiver_dofs=h(a["rdofs"]), receiver_weights=h(a["rw"]),
+            measurement_count=c["D"], abmn=h(a["abmn"]), source_cell_ptr=h(a["sptr"]), source_cells=h(a["scells"]),
+        )
+
+
+def build_problem(mesh: Mesh, survey: Survey, quadrature_order: int = 2) -> ProblemArrays:
+    """Quadrature, element templates, mixed-boundary coefficients, electrode interpolation and
+    source-resistivity cells of a flat-surface operator (``build_discretization("native")``,
+    adtlert/forward/discretization.py:485-575, and ert2p5d.py:158-216)."""
+
+    positions = survey.electrode_positions[:, :2]
+    k, w = inverse_cosine_weights(*wavenumber_bounds(survey.electrode_positions))
+    nodes, cells = mesh.nodes, mesh.cells
+    if cells.shape[1] == 3:
+        stiffness, mass = triangle_templates(nodes, cells, quadrature_order)
+    else:
+        stiffness, mass = quad_templates(nodes, cells)
+    bmass = boundary_mass(mesh.boundary_edge_lengths)
+    robin = robin_coefficients(mesh.boundary_edge_centers, mesh.boundary_edge_normals, mesh.surface_edge_mask,
+                               mesh.surface_reference_level, positions.mean(axis=0), k)
+    cell_ids, interp = locate_points(nodes, cells, positions)
+    E, N, K = survey.electrode_count, mesh.node_count, cells.shape[1]
+    receiver_dofs = cells[cell_ids].astype(np.int32)
+    electrode_matrix = np.zeros((E, N))
+    np.add.at(electrode_matrix, (np.repeat(np.arange(E), K), receiver_dofs.reshape(-1)), interp.reshape(-1))
+    distance = np.linalg.norm(nodes[None] - positions[:, None], axis=2)
+    nearest = np.argmin(distance, axis=1)
+    source_nodes = np.where(distance[np.arange(E), nearest] <= 1e-2, nearest, -1)
+    ptr, lists = [0], []
+    for e, node in enumerate(source_nodes):
+        around = np.flatnonzero((cells == node).any(axis=1)) if node >= 0 else np.asarray([cell_ids[e]])
+        lists.append(around)
+        ptr.append(ptr[-1] + len(around))
+    arrays = {
+        "coords": np.ascontiguousarray(nodes, dtype=np.float64),
+        "cell_dofs": np.ascontiguousarray(cells, dtype=np.int32),
+        "stiffness": np.ascontiguousarray(stiffness, dtype=np.float64),
+        "mass": np.ascontiguousarray(mass, dtype=np.float64),
+        "bdofs": np.ascontiguousarray(mesh.boundary_edges, dtype=np.int32),
+        "bcells": np.ascontiguousarray(mesh.boundary_edge_cells, dtype=np.int32),
+        "bmass": np.ascontiguousarray(bmass, dtype=np.float64),
+        "bcoef": np.ascontiguousarray(robin, dtype=np.float64),
+        "k": np.ascontiguousarray(k, dtype=np.float64),
+        "w": np.ascontiguousarray(w, dtype=np.float64),
+        "rdofs": np.ascontiguousarray(receiver_dofs, dtype=np.int32),
+        "rw": np.ascontiguousarray(interp, dtype=np.float64),
+        "abmn": np.ascontiguousarray(survey.measurement_slots(), dtype=np.int32),
+        "sptr": np.asarray(ptr, dtype=np.int32),
+        "scells": np.ascontiguousarray(np.concatenate(lists), dtype=np.int32),
+    }
+    counts = {"N": N, "C": mesh.cell_count, "K": K, "Nb": len(mesh.boundary_edges), "W": len(k), "E": E,
+              "D": survey.measurement_count}
+    return ProblemArrays(arrays, k, w, stiffness, mass, bmass, robin, electrode_matrix, source_nodes, cell_ids, counts)
+
+
+def _to_host(tensor: Tensor) -> Tensor:
+    """Device tensor -> CPU tensor in page-locked memory (torch's caching host allocator), so the
+    copy runs at full link bandwidth."""
+
+    out = torch.empty(tensor.shape, dtype=tensor.dtype, pin_memory=True)
+    out.copy_(tensor, non_blocking=True)
+    torch.cuda.current_stream(tensor.device).synchronize()
+    return out
+
+
+def _mesh_arrays(mesh) -> Mesh:
+    """Our Mesh for the reference's or our own mesh object."""
+
+    if isinstance(mesh, Mesh):
+        return mesh
+    surface = getattr(mesh, "surface_node_ids", None)
+    return Mesh.from_arrays(mesh.nodes, mesh.cells, surface_node_ids=surface)
+
+
+def _survey_arrays(survey) -> Survey:
+    if isinstance(survey, Survey):
+        return survey
+    return Survey.from_arrays(survey.electrode_positions, survey.measurements)
+
+
+class ERTForward2p5D:
+    """2.5D ERT forward operator (flat surfaces, analytic primary field) on B200 kernels."""
+
+    def __init__(
+        self,
+        mesh,
+        survey,
+        *,
+        quadrature_order: int = 2,
+        numerical_h2_refined: bool = True,
+        numerical_p2_refined: bool = True,
+        topographic_geometric_factor_mode: str = "analytic",
+        terrain_cache_dir=None,
+        normal_field_cache_max_entries: int = 8,
+        series_batch_steps: int = 8,
+    ) -> None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("ADTLERT requires an NVIDIA GPU with CUDA (B200 kernels)")
+        gf_mode = option(topographic_geometric_factor_mode, ("analytic", "numerical"), "topographic_geometric_factor_mode")
+        if int(normal_field_cache_max_entries) < 0:
+            raise ValueError("normal_field_cache_max_entries must be non-negative")
+        if int(series_batch_steps) < 1:
+            raise ValueError("series_batch_steps must be >= 1")
+        self.source_mesh, self.source_survey = mesh, survey
+        self.mesh = _mesh_arrays(mesh)
+        self.survey = _survey_arrays(survey)
+        if not self.mesh.is_flat_surface:
+            raise NotImplementedError("terrain surfaces (numerical primary field) are not supported by this build")
+        self.numerical_h2_refined = bool(numerical_h2_refined)
+        self.numerical_p2_refined = bool(numerical_p2_refined)
+        self.topographic_geometric_factor_mode = gf_mode
+        self.terrain_cache_dir = terrain_cache_dir
+        self.normal_field_cache_max_entries = int(normal_field_cache_max_entries)
+        self.series_batch_steps = int(series_batch_steps)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self._lib = _native.load_library()
+        self._cache: dict = {}
+        self._field_cache = FieldCache(self.normal_field_cache_max_entries)
+        self._solver = _Slots()
+        self._plan = None
+        self._build(int(quadrature_order))
+
+    @classmethod
+    def from_mesh_survey(cls, mesh, survey, quadrature_order: int = 2, numerical_h2_refined: bool = True,
+                         numerical_p2_refined: bool = True, topographic_geometric_factor_mode: str = "analytic",
+                         terrain_cache_dir=None, normal_field_cache_max_entries: int = 8,
+                         series_batch_steps: int = 8) -> ERTForward2p5D:
+        return cls(
+            mesh,
+            survey,
+            quadrature_order=quadrature_order,
+            numerical_h2_refined=numerical_h2_refined,
+            numerical_p2_refined=numerical_p2_refined,
+            topographic_geometric_factor_mode=topographic_geometric_factor_mode,
+            terrain_cache_dir=terrain_cache_dir,
+            normal_field_cache_max_entries=normal_field_cache_max_entries,
+            series_batch_steps=series_batch_steps,
+        )
+
+    # ------------------------------------------------------------------ set-up
+    def _build(self, quadrature_order: int) -> None:
+        problem = build_problem(self.mesh, self.survey, quadrature_order)
+        self._problem = problem
+        k, w = problem.wavenumbers, problem.weights
+        self.wavenumbers = torch.as_tensor(k, dtype=FLOAT_DTYPE)
+        self.weights = torch.as_tensor(w, dtype=FLOAT_DTYPE)
+        self.source_node_ids = torch.as_tensor(problem.source_nodes, dtype=torch.long)
+        self.source_cell_ids = torch.as_tensor(problem.source_cells, dtype=torch.long)
+        mesh, survey = self.mesh, self.survey
+        nodes, cells = mesh.nodes, mesh.cells
+        E, N = survey.electrode_count, mesh.node_count
+        arrays = problem.arrays
+        problem = problem.struct()
+        plan = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _native.check(self._lib.adt_plan_create(ctypes.byref(problem), ctypes.byref(plan)), None, "adt_plan_create")
+        self._plan = plan
+        info = _native.PlanInfo()
+        self._lib.adt_plan_get_info(plan, ctypes.byref(info))
+        self.plan_info = {name: getattr(info, name) for name, _ in _native.PlanInfo._fields_}
+        order = np.empty(N, dtype=np.int32)
+        self._lib.adt_plan_dof_order(plan, _native.host_ptr(order))
+        self._dof_order = order
+        pa = self._problem
+        self.discretization = Discretization(
+            name="native", parent_cell_ids=np.arange(mesh.cell_count), dof_nodes=nodes, cell_dofs=cells,
+            boundary_dofs=mesh.boundary_edges, boundary_cells=mesh.boundary_edge_cells, stiffness=pa.stiffness,
+            mass=pa.mass, boundary_mass=pa.boundary_mass, boundary_geometries=pa.robin,
+            electrode_matrix=pa.electrode_matrix, nnz=int(info.nnz),
+        )
+        primary = np.ascontiguousarray(
+            analytic_primary(nodes, cells, survey.electrode_positions[:, :2], pa.source_nodes, k), dtype=np.float64
+        )
+        with torch.cuda.device(self.device):
+            _native.check(self._lib.adt_set_primary(plan, _native.host_ptr(primary), self._stream()), plan, "adt_set_primary")
+        self._geometric = torch.as_tensor(geometric_factors(survey.electrode_positions, survey.measurements), dtype=FLOAT_DTYPE)
+        self.W, self.E, self.N, self.D = len(k), E, N, survey.measurement_count
+        self.C = mesh.cell_count
+
+    # ------------------------------------------------------------------ helpers
+    def _stream(self):
+        return _native.stream_handle(self.device)
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return FLOAT_DTYPE
+
+    @property
+    def use_numerical_primary(self) -> bool:
+        return False
+
+    @property
+    def use_numerical_geometric_factors(self) -> bool:
+        return False
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.adt_kernel_launches(self._plan))
+
+    def _sigma(self, conductivity) -> Tensor:
+        return conductivity_model(conductivity, self.C)
+
+    def _series(self, conductivities) -> Tensor:
+        return conductivity_series(conductivities, self.C)
+
+    def _geometric_factors(self) -> Tensor:
+        return self._geometric
+
+    def _call(self, name: str, *args) -> None:
+        _native.check(getattr(self._lib, name)(self._plan, *args), self._plan, name)
+
+    def _factorize(self, sigmas: Tensor, name) -> int:
+        """Slot holding the factorization of ``sigmas`` (device float32, (B, C)); refactorizes
+        unless the slot of this batch size already holds the named factorization."""
+
+        batch = int(sigmas.shape[0])
+        entry = self._solver.lookup(batch)
+        if not self._solver.holds(batch, name):
+            self._call("adt_factorize", entry["slot"], _native.ptr(sigmas), batch, self._stream())
+            entry["name"] = name
+            self._solver.factorizations += 1
+        return entry["slot"]
+
+    # ------------------------------------------------------------------ fields
+    def _solve_fields(self, sigmas: Tensor, name) -> list[_Fields]:
+        batch = int(sigmas.shape[0])
+        sig = sigmas.to(self.device, torch.float32).contiguous()
+        entry = self._solver.lookup(batch)
+        self._call("adt_factorize", entry["slot"], _native.ptr(sig), batch, self._stream())
+        entry["name"] = name
+        self._solver.factorizations += 1
+        total = torch.empty((batch, self.W, self.N, self.E), dtype=torch.float32, device=self.device)
+        self._call("adt_solve_fields", entry["slot"], _native.ptr(sig), batch, _native.ptr(total), self._stream())
+        check_finite(total, "total fields")
+        return [_Fields(total[i]) for i in range(batch)]
+
+    def _fields_series(self, models: Tensor):
+        return self._field_cache.solve_series(models, self.series_batch_steps, self._solve_fields)
+
+    def _fields(self, conductivity) -> _Fields:
+        return self._fields_series(self._sigma(conductivity)[None])[0][0]
+
+    def normal_field_cache_info(self) -> dict[str, int]:
+        return self._field_cache.info()
+
+    def _stack(self, fields: list[_Fields]) -> Tensor:
+        if len(fields) == 1:
+            return fields[0].total[None]
+        return torch.stack([f.total for f in fields]).contiguous()
+
+    def _transfers(self, totals: Tensor, potentials: bool = False):
+        """Normal and reciprocal transfers (S, D) float64 on the device (+ (S, E, E) potentials)."""
+
+        S = int(totals.shape[0])
+        normal = torch.empty((S, self.D), dtype=torch.float64, device=self.device)
+        reciprocal = torch.empty_like(normal)
+        pot = torch.empty((S, self.E, self.E), dtype=torch.float64, device=self.device) if potentials else None
+        self._call("adt_measure", _native.ptr(totals), S, _native.ptr(normal), _native.ptr(reciprocal), _native.ptr(pot), self._stream())
+        return normal, reciprocal, pot
+
+    @staticmethod
+    def _combine(normal: Tensor, reciprocal: Tensor) -> Tensor:
+        return torch.sign(normal) * torch.sqrt(torch.abs(normal * reciprocal))
+
+    def _measure(self, conductivity):
+        fields = self._fields(conductivity)
+        normal, reciprocal, _ = self._transfers(fields.total[None])
+        return fields, normal[0], reciprocal[0]
+
+    # ------------------------------------------------------------------ forward API
+    def solve(self, conductivity, currents=1.0) -> ForwardResponse:
+        fields = self._fields(conductivity)
+        normal, reciprocal, potentials = self._transfers(fields.total[None], potentials=True)
+        return self._response(fields, normal[0], reciprocal[0], potentials[0], currents)
+
+    def _response(self, fields, normal, reciprocal, potentials, currents) -> ForwardResponse:
+        integrated = torch.empty((self.E, self.N), dtype=torch.float32, device=self.device)
+        self._call("adt_integrated_potentials", _native.ptr(fields.total), _native.ptr(integrated), self._stream())
+        check_finite(integrated, "integrated potentials")
+        resistance = self._combine(normal.cpu(), reciprocal.cpu()).to(FLOAT_DTYPE)
+        current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
+        if potentials is None:
+            _, _, pot = self._transfers(fields.total[None], potentials=True)
+            potentials = pot[0]
+        return ForwardResponse(
+            apparent_resistivity=self._geometric * resistance / current,
+            resistance=resistance,
+            electrode_potentials=potentials.cpu().to(FLOAT_DTYPE),
+            integrated_potentials=integrated.cpu(),
+            wavenumbers=self.wavenumbers,
+            weights=self.weights,
+        )
+
+    def resistance(self, conductivity) -> Tensor:
+        _, normal, reciprocal = self._measure(conductivity)
+        return self._combine(normal.cpu(), reciprocal.cpu()).to(FLOAT_DTYPE)
+
+    def apparent_resistivity_values(self, conductivity, currents=1.0) -> Tensor:
+        current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
+        return self._geometric * self.resistance(conductivity) / current
+
+    def resistance_series(self, conductivities) -> Tensor:
+        fields, _ = self._fields_series(self._series(conductivities))
+        normal, reciprocal, _ = self._transfers(self._stack(fields))
+        return self._combine(normal.cpu(), reciprocal.cpu()).to(FLOAT_DTYPE)
+
+    def apparent_resistivity_series(self, conductivities, currents=1.0) -> Tensor:
+        current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
+        return self._geometric * self.resistance_series(conductivities) / current
+
+    def prepare(self, conductivity=None, *, include_solver_state: bool = True) -> None:
+        """Populate solver and field caches before timed solves (the set-up is done at construction)."""
+
+        if include_solver_state:
+            self._fields(torch.ones(self.C) if conductivity is None else conductivity)
+
+    # ------------------------------------------------------------------ derivatives
+    def _columns(self, cell_parameter_ids=None, parameter_count=None):
+        """(key, columns, ptr, cells) of the aggregation into parameters, or None for identity."""
+
+        ids, count = parameter_targets(cell_parameter_ids, parameter_count, self.C)
+        if cell_parameter_ids is None:
+            return None
+        digest = hashlib.blake2b(ids.tobytes(), digest_size=16).digest()
+        key = ("columns", digest, count)
+        if key not in self._cache:
+            active = np.flatnonzero(ids >= 0)
+            order = active[np.argsort(ids[active], kind="stable")]
+            ptr = np.concatenate(([0], np.cumsum(np.bincount(ids[active], minlength=count)))).astype(np.int32)
+            self._cache[key] = (len(self._cache) + 1, count, ptr, np.ascontiguousarray(order, dtype=np.int32))
+        return self._cache[key]
+
+    def _aggregate(self, values: Tensor, columns) -> Tensor:
+        if columns is None:
+            return values
+        key, count, ptr, cells = columns
+        rows = int(values.shape[0])
+        out = torch.empty((rows, count), dtype=torch.float32, device=self.device)
+        self._call("adt_aggregate_columns", key, count, _native.host_ptr(ptr), _native.host_ptr(cells),
+                   _native.ptr(values.contiguous()), rows, int(values.shape[1]), _native.ptr(out), self._stream())
+        return out
+
+    def _batch_size(self, batch_size, direct: bool) -> int:
+        if batch_size is None:
+            if not direct:
+                return 8
+            return min(self.D, 64) if self.C >= 4096 else self.D
+        if batch_size < 1:
+            raise ValueError("batch_size must be >= 1")
+        return int(batch_size)
+
+    def _jacobian_device(self, fields: _Fields, columns=None) -> Tensor:
+        """Normal-quadrupole Jacobian (D, C or P) on the device; every row in one launch."""
+
+        J = torch.empty((self.D, self.C), dtype=torch.float32, device=self.device)
+        self._call("adt_normal_jacobian", _native.ptr(fields.total), 0, self.D, _native.ptr(J), self._stream())
+        return self._aggregate(J, columns)
+
+    def solve_with_jacobian(self, conductivity, currents=1.0, *, batch_size=None,
+                            include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
+                            jacobian_cell_parameter_ids=None, jacobian_parameter_count=None):
+        fields, normal, reciprocal = self._measure(conductivity)
+        direct = normal_sensitivity and not include_robin_boundary_derivative
+        batch = self._batch_size(batch_size, direct)
+        if direct:
+            columns = self._columns(jacobian_cell_parameter_ids, jacobian_parameter_count)
+            jacobian = _to_host(self._jacobian_device(fields, columns))
+        else:
+            key = self._field_cache.key(self._sigma(conductivity))
+            slot = self._factorize(self._sigma(conductivity).to(self.device)[None].contiguous(), factorization_name([key]))
+            rows = []
+            for start in range(0, self.D, batch):
+                count = min(batch, self.D - start)
+                out = torch.empty((count, self.C), dtype=torch.float32, device=self.device)
+                self._call("adt_adjoint_jacobian", slot, _native.ptr(fields.total), _native.ptr(normal), _native.ptr(reciprocal),
+                           start, count, int(include_robin_boundary_derivative), int(normal_sensitivity), _native.ptr(out), self._stream())
+                rows.append(out)
+            jacobian = _to_host(torch.cat(rows))
+        check_finite(jacobian, "jacobian")
+        return self._response(fields, normal, reciprocal, None, currents), jacobian
+
+    def jacobian(self, conductivity, *, batch_size=None, include_robin_boundary_derivative: bool = False,
+                 normal_sensitivity: bool = True) -> Tensor:
+        return self.solve_with_jacobian(conductivity, batch_size=batch_size,
+                                        include_robin_boundary_derivative=include_robin_boundary_derivative,
+                                        normal_sensitivity=normal_sensitivity)[1]
+
+    def jacobian_columnwise(self, conductivity) -> Tensor:
+        basis = torch.eye(self.C, dtype=FLOAT_DTYPE)
+        return torch.stack([self.jvp(conductivity, column) for column in basis], dim=1)
+
+    def vjp(self, conductivity, cotangent) -> Tensor:
+        cotangent = measurement_vector(cotangent, self.D, FLOAT_DTYPE)
+        return self.vjp_series(self._sigma(conductivity)[None], cotangent[None])[0]
+
+    def vjp_series(self, conductivities, cotangents) -> Tensor:
+        models = self._series(conductivities)
+        cotangents = cotangent_series(cotangents, models.shape[0], self.D)
+        fields, keys = self._fields_series(models)
+        gradients: dict[int, Tensor] = {}
+        for batch in newest_batches_first(len(fields), self.series_batch_steps):
+            totals = self._stack([fields[step] for step in batch])
+            normal, reciprocal, _ = self._transfers(totals)
+            slot = self._factorize(models[batch].to(self.device, torch.float32).contiguous(),
+                                   factorization_name([keys[step] for step in batch]))
+            cot = cotangents[batch].to(self.device, torch.float64).contiguous()
+            grad = torch.empty((len(batch), self.C), dtype=torch.float32, device=self.device)
+            self._call("adt_vjp", slot, _native.ptr(totals), _native.ptr(normal), _native.ptr(reciprocal),
+                       _native.ptr(cot), len(batch), _native.ptr(grad), self._stream())
+            for i, step in enumerate(batch):
+                gradients[step] = grad[i]
+        gradient = torch.stack([gradients[step] for step in range(len(fields))]).cpu()
+        check_finite(gradient, "conductivity gradient")
+        return gradient
+
+    def jvp(self, conductivity, delta_conductivity) -> Tensor:
+        sigma = self._sigma(conductivity)
+        fields, normal, reciprocal = self._measure(sigma)
+        direction = cell_vector(delta_conductivity, self.C).to(self.device, torch.float32).contiguous()
+        slot = self._factorize(sigma.to(self.device)[None].contiguous(), factorization_name([self._field_cache.key(sigma)]))
+        out = torch.empty(self.D, dtype=torch.float64, device=self.device)
+        self._call("adt_jvp", slot, _native.ptr(fields.total), _native.ptr(normal), _native.ptr(reciprocal),
+                   _native.ptr(direction), _native.ptr(out), self._stream())
+        check_finite(out, "tangent fields")
+        return out.cpu().to(FLOAT_DTYPE)
+
+    def normal_vjp(self, conductivity, cotangent, *, cell_parameter_ids=None, parameter_count=None) -> Tensor:
+        columns = self._columns(cell_parameter_ids, parameter_count)
+        fields = self._fields(conductivity)
+        weights = measurement_vector(cotangent, self.D, torch.float64).to(self.device).contiguous()
+        grad = torch.empty((1, self.C), dtype=torch.float32, device=self.device)
+        self._call("adt_normal_vjp", _native.ptr(fields.total), _native.ptr(weights), _native.ptr(grad), self._stream())
+        gradient = self._aggregate(grad, columns)[0].cpu()
+        check_finite(gradient, "normal sensitivity vjp")
+        return gradient
+
+    def normal_vjp_series(self, conductivities, cotangents, *, cell_parameter_ids=None, parameter_count=None) -> Tensor:
+        models = self._series(conductivities)
+        cotangents = cotangent_series(cotangents, models.shape[0], self.D)
+        return torch.stack([
+            self.normal_vjp(m, c, cell_parameter_ids=cell_parameter_ids, parameter_count=parameter_count)
+            for m, c in zip(models, cotangents, strict=True)
+        ])
+
+    def normal_jvp(self, conductivity, delta_conductivity) -> Tensor:
+        fields = self._fields(conductivity)
+        direction = cell_vector(delta_conductivity, self.C).to(self.device, torch.float32).contiguous()
+        out = torch.empty(self.D, dtype=torch.float64, device=self.device)
+        self._call("adt_normal_jvp", _native.ptr(fields.total), _native.ptr(direction), _native.ptr(out), self._stream())
+        result = out.cpu().to(FLOAT_DTYPE)
+        check_finite(result, "normal sensitivity jvp")
+        return result
+
+    # ------------------------------------------------------------------ lifetime
+    def close(self) -> None:
+        """Drop cached fields and forget held factorizations (the operator keeps working)."""
+
+        self._field_cache.clear()
+        self._solver.close()
+
+    def __del__(self) -> None:
+        with contextlib.suppress(Exception):
+            if self._plan is not None:
+                torch.cuda.synchronize(self.device)
+                self._lib.adt_plan_destroy(self._plan)
+                self._plan = None

@@ -1,0 +1,103 @@
+// Internal declarations shared by the adtlert_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "adtlert_b200.h"
+#include "plan_host.h"
+
+namespace adt {
+
+// Threads of the solver kernels.
+constexpr int kSolverThreads = 256;
+
+struct Slot {
+  int systems = 0;          // systems currently factorized (models * W)
+  size_t capacity = 0;      // systems allocated
+  double* values = nullptr; // [systems][nnz]
+  double* factors = nullptr;// [systems][factor_stride]
+};
+
+struct Aggregation {
+  int key = -1, columns = 0;
+  int* ptr = nullptr;
+  int* cells = nullptr;
+};
+
+}  // namespace adt
+
+struct adt_plan {
+  // sizes
+  int N = 0, dim = 2, C = 0, K = 0, Cm = 0, Nb = 0, BL = 0, W = 0, E = 0, D = 0, RW = 0;
+  int nnz = 0, nb = 0, max_m = 0, levels = 0;
+  int64_t contributions = 0;
+  int64_t factor_stride = 0;
+  int RS = 0;  // stiffness features per wavenumber
+  int R = 0;   // all features per wavenumber (stiffness + mass)
+  std::vector<int> perm;  // position -> original dof
+  std::vector<int> iperm; // original dof -> position
+  std::vector<int> level_begin;  // task ranges per level (root is the last level)
+  // device geometry
+  int* csr_ptr = nullptr;
+  int* csr_col = nullptr;
+  int* csr_row = nullptr;
+  int* contrib_ptr = nullptr;
+  int* contrib = nullptr;
+  double* stiffness = nullptr;  // [C][K*K]
+  double* mass = nullptr;       // [C][K*K]
+  double* bmass = nullptr;      // [Nb][BL*BL]
+  double* bcoef = nullptr;      // [W][Nb]
+  int* cell_dofs = nullptr;     // [C][K] solver order
+  int* parent = nullptr;        // [C] or null
+  int* bcells = nullptr;        // [Nb]
+  int* bdofs = nullptr;         // [Nb][BL] solver order
+  int* cell_bptr = nullptr;     // [C+1] boundary elements of each cell
+  int* cell_blist = nullptr;
+  double* k2 = nullptr;         // [W]
+  double* weights = nullptr;    // [W]
+  int* abmn = nullptr;          // [D][4]
+  int* rcv_dofs = nullptr;      // [E][RW] solver order
+  double* rcv_w = nullptr;      // [E][RW]
+  int* src_ptr = nullptr;       // [E+1]
+  int* src_cells = nullptr;
+  float* features = nullptr;    // [C][R][K]
+  float* fscale = nullptr;      // [W][R]
+  int* model_ptr = nullptr;     // [Cm+1] discretization cells of each model cell
+  int* model_list = nullptr;
+  int* pair_ptr = nullptr;      // [(E+1)^2+1] routed pair-cotangent scatter
+  int* pair_list = nullptr;
+  int* rdof_ptr = nullptr;      // receiver dofs of the adjoint right-hand side
+  int* rdof_rcv = nullptr;
+  double* rdof_w = nullptr;
+  int* rdof_dof = nullptr;
+  int rdofs = 0;
+  int64_t* tasks = nullptr;
+  int64_t* pulls = nullptr;
+  // primary field
+  double* primary = nullptr;    // [W][N][E] solver order
+  double* refrhs = nullptr;     // [W][N][E]
+  bool has_primary = false;
+  // slots and workspace
+  std::vector<adt::Slot> slots;
+  std::vector<adt::Aggregation> aggregations;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  std::string error;
+  int64_t launches = 0;
+  int device = 0;
+};
+
+namespace adt {
+
+// Record an error on the plan and return `status`.
+adt_status fail(adt_plan* plan, adt_status status, const std::string& message);
+// Check the launch status of the last kernel.
+adt_status check_launch(adt_plan* plan, const char* what);
+// Grow the plan's scratch to `bytes`; returns nullptr on failure.
+void* scratch(adt_plan* plan, size_t bytes);
+
+}  // namespace adt

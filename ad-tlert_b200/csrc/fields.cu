@@ -1,0 +1,254 @@
+// Assembly, right-hand sides, total fields and measurement gathers of the 2.5D operator.
+//
+// All reductions run over precomputed lists in a fixed order (no atomics), so every result is
+// bitwise repeatable. Fields are node-major, [system][dof][electrode], with dofs in the plan's
+// solver order: the electrode axis is contiguous, so a warp reading one dof row of all
+// electrodes is one coalesced transaction.
+#include "adt_internal.h"
+#include "kernels.h"
+
+namespace adt {
+
+// values[t][slot] = sum over the slot's routed contributions of
+//   sigma_parent(cell) * (K + k_w^2 M)[cell][ij]        (volume)
+//   sigma_parent(cell(b)) * alpha_w[b] * Mb[b][ij]       (mixed boundary, if robin)
+// for systems t = model * W + w. Replaces _assemble + GroupSum (adtlert/forward/ert2p5d.py:275-314,
+// adtlert/forward/kernels.py:30-85).
+__global__ void assemble_kernel(AssembleArgs a) {
+  const int64_t total = (int64_t)a.systems * a.nnz;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int t = (int)(idx / a.nnz), slot = (int)(idx - (int64_t)t * a.nnz);
+    const int w = t % a.W, s = t / a.W;
+    const float* sig = a.sigma + (int64_t)s * a.Cm;
+    const double k2 = a.k2[w];
+    const int volume = a.C * a.K2;
+    double acc = 0.0;
+    for (int c = a.contrib_ptr[slot]; c < a.contrib_ptr[slot + 1]; ++c) {
+      const int code = a.contrib[c];
+      if (code < volume) {
+        const int cell = code / a.K2;
+        const double sigma = sig[a.parent ? a.parent[cell] : cell];
+        acc += sigma * (a.stiffness[code] + k2 * a.mass[code]);
+      } else if (a.robin) {
+        const int bc = code - volume, b = bc / a.BL2;
+        const int cell = a.bcells[b];
+        const double sigma = sig[a.parent ? a.parent[cell] : cell];
+        acc += sigma * a.bcoef[(int64_t)w * a.Nb + b] * a.bmass[bc];
+      }
+    }
+    a.values[idx] = acc;
+  }
+}
+
+// rho[s][e] = exp(-(1/n) sum log sigma) over the cells around electrode e's node, or 1/sigma of its
+// cell (a list of one). Replaces _source_resistivities (ert2p5d.py:480-511).
+__global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
+                                  const int* ptr, const int* cells, double* rho) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= models * E) return;
+  const int s = idx / E, e = idx % E;
+  double acc = 0.0;
+  for (int i = ptr[e]; i < ptr[e + 1]; ++i) acc -= log((double)sigma[(int64_t)s * Cm + cells[i]]);
+  const int n = ptr[e + 1] - ptr[e];
+  rho[idx] = n > 0 ? exp(acc / n) : 1.0;
+}
+
+// out[t][n][e] = base[w][n][e] + coef(t,e) * sum_{slot in row n} values[t][slot] x[src(t)][col][e]
+// where coef(t,e) = scale * (rho ? rho[model(t)][e] : 1). `x_per_model` selects whether x is indexed
+// by system (fields of each system) or by wavenumber (the primary field shared by all models).
+__global__ void spmm_kernel(SpmmArgs a) {
+  const int64_t total = (int64_t)a.systems * a.N * a.E;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(idx % a.E);
+    const int64_t rest = idx / a.E;
+    const int n = (int)(rest % a.N), t = (int)(rest / a.N);
+    const int w = t % a.W, s = t / a.W;
+    const double* v = a.values + (int64_t)(a.values_per_wavenumber ? w : t) * a.nnz;
+    const int64_t xo = (int64_t)(a.x_per_system ? t : w) * a.N * a.E;
+    double acc = 0.0;
+    if (a.x_double) {
+      const double* x = (const double*)a.x + xo;
+      for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
+        acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E + e];
+    } else {
+      const float* x = (const float*)a.x + xo;
+      for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
+        acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E + e];
+    }
+    double coef = a.scale;
+    if (a.rho) coef *= a.rho[s * a.E + e];
+    double out = coef * acc;
+    if (a.base) out += a.base[((int64_t)w * a.N + n) * a.E + e];
+    a.out[idx] = out;
+  }
+}
+
+// fields[t][n][e] = x[t][n][e] + rho[s][e] * primary[w][n][e]
+__global__ void total_kernel(const double* x, const double* primary, const double* rho, int W,
+                             int N, int E, int systems, float* fields) {
+  const int64_t total = (int64_t)systems * N * E;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(idx % E);
+    const int64_t rest = idx / E;
+    const int n = (int)(rest % N), t = (int)(rest / N);
+    const int w = t % W, s = t / W;
+    fields[idx] = (float)(x[idx] + rho[s * E + e] * primary[((int64_t)w * N + n) * E + e]);
+  }
+}
+
+// One block per model: electrode potentials P[e][r] = sum_k wr_k sum_w weight_w u_w[dof_rk][e]
+// in shared memory (slot E is the zero remote row/column), then the normal and reciprocal
+// transfers of every ABMN row. Replaces _integrate + _normal_reciprocal (ert2p5d.py:560-589).
+__global__ void measure_kernel(MeasureArgs a) {
+  extern __shared__ double pot[];
+  const int E1 = a.E + 1;
+  const int s = blockIdx.x;
+  const int64_t fo = (int64_t)s * a.W * a.N * a.E;
+  auto field = [&](int64_t i) -> double {
+    return a.f_double ? ((const double*)a.fields)[fo + i] : (double)((const float*)a.fields)[fo + i];
+  };
+  for (int idx = threadIdx.x; idx < E1 * E1; idx += blockDim.x) pot[idx] = 0.0;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < a.E * a.E; idx += blockDim.x) {
+    const int r = idx / a.E, e = idx % a.E;  // e fastest: coalesced field reads
+    double acc = 0.0;
+    for (int k = 0; k < a.RW; ++k) {
+      const int dof = a.rcv_dofs[r * a.RW + k];
+      if (dof < 0) continue;
+      double integ = 0.0;
+      for (int w = 0; w < a.W; ++w)
+        integ += a.weights[w] * field(((int64_t)w * a.N + dof) * a.E + e);
+      acc += a.rcv_w[r * a.RW + k] * integ;
+    }
+    pot[e * E1 + r] = acc;
+    if (a.potentials) a.potentials[((int64_t)s * a.E + e) * a.E + r] = acc;
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < a.D; d += blockDim.x) {
+    const int A = a.abmn[4 * d], B = a.abmn[4 * d + 1], M = a.abmn[4 * d + 2], N = a.abmn[4 * d + 3];
+    const double n = (pot[A * E1 + M] - pot[A * E1 + N]) - (pot[B * E1 + M] - pot[B * E1 + N]);
+    const double r = (pot[M * E1 + A] - pot[M * E1 + B]) - (pot[N * E1 + A] - pot[N * E1 + B]);
+    if (a.combine) {
+      // tangent of sign(n) sqrt|n r|: 0.5 sign(r) (dn r + n dr) / max(sqrt|n r|, 1e-30)
+      const double n0 = a.base_normal[(int64_t)s * a.D + d], r0 = a.base_recip[(int64_t)s * a.D + d];
+      const double scale = fmax(sqrt(fabs(n0 * r0)), 1e-30);
+      const double sign = (r0 > 0.0) - (r0 < 0.0);
+      a.normal[(int64_t)s * a.D + d] = 0.5 * sign * (n * r0 + n0 * r) / scale;
+    } else {
+      a.normal[(int64_t)s * a.D + d] = n;
+      a.reciprocal[(int64_t)s * a.D + d] = r;
+    }
+  }
+}
+
+// pairs[q][e][f] (e, f < E) = sum over the (e, f) entry's routed list of +-coef, where each entry
+// names a row d and whether it carries the normal or the reciprocal cotangent.
+// Replaces _pair_cotangent (ert2p5d.py:591-629).
+__global__ void pair_kernel(PairArgs a) {
+  const int64_t total = (int64_t)a.count * a.E * a.E;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(idx / (a.E * a.E));
+    const int ef = (int)(idx - (int64_t)q * a.E * a.E);
+    const int e = ef / a.E, f = ef % a.E;
+    const int slot = e * (a.E + 1) + f;
+    double acc = 0.0;
+    for (int i = a.pair_ptr[slot]; i < a.pair_ptr[slot + 1]; ++i) {
+      const int code = a.pair_list[i];
+      const int d = code >> 2, kind = code & 3;
+      if (kind >= 2 && a.normal_only) continue;
+      double coef;
+      if (a.unit) {
+        coef = (d == a.row_begin + q) ? 1.0 : 0.0;
+        if (coef == 0.0) continue;
+      } else {
+        coef = a.cot[(int64_t)q * a.D + d];
+      }
+      if (!a.normal_only) {
+        // exact derivative of sign(n) sqrt|n r|: common * r for normal, common * n for reciprocal
+        const int64_t md = (int64_t)(a.model_of_count ? q : 0) * a.D + d;
+        const double n0 = a.normal[md], r0 = a.recip[md];
+        const double scale = fmax(sqrt(fabs(n0 * r0)), 1e-30);
+        const double sign = (r0 > 0.0) - (r0 < 0.0);
+        coef *= 0.5 * sign / scale * (kind < 2 ? r0 : n0);
+      }
+      acc += (kind & 1) ? -coef : coef;
+    }
+    a.pairs[idx] = acc;
+  }
+}
+
+// Adjoint right-hand sides rhs[t][n][col] with t = model * W + w, col = q_local * E + e:
+// weight_w * sum_r pairs[q][e][r] Pel[r][n], nonzero only at receiver dofs (routed list).
+// Replaces _adjoint_rhs (ert2p5d.py:631-639).
+__global__ void adjoint_rhs_kernel(AdjointRhsArgs a) {
+  const int ncol = a.q_per_model * a.E;
+  const int64_t total = (int64_t)a.systems * a.rdofs * ncol;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int col = (int)(idx % ncol);
+    const int64_t rest = idx / ncol;
+    const int i = (int)(rest % a.rdofs), t = (int)(rest / a.rdofs);
+    const int w = t % a.W, s = t / a.W;
+    const int ql = col / a.E, e = col % a.E;
+    const int q = s * a.q_per_model + ql;
+    const double* pr = a.pairs + ((int64_t)q * a.E + e) * a.E;
+    double acc = 0.0;
+    for (int j = a.rdof_ptr[i]; j < a.rdof_ptr[i + 1]; ++j) acc += pr[a.rdof_rcv[j]] * a.rdof_w[j];
+    a.rhs[((int64_t)t * a.N + a.rdof_dof[i]) * ncol + col] = a.weights[w] * acc;
+  }
+}
+
+// Partial Gram sums for normal_jvp: partial[b][e][f] = sum over this block's slice of (w, n) of
+// weight_w * phi[w][n][e] * y[w][n][f]; a second pass sums the partials in block order.
+__global__ void gram_partial_kernel(const float* phi, const double* y, const double* weights,
+                                    int W, int N, int E, int chunk, double* partial) {
+  extern __shared__ double rows[];
+  const int64_t total = (int64_t)W * N;
+  const int64_t begin = (int64_t)blockIdx.x * chunk;
+  const int64_t end = begin + chunk < total ? begin + chunk : total;
+  double* out = partial + (int64_t)blockIdx.x * E * E;
+  for (int ef = threadIdx.x; ef < E * E; ef += blockDim.x) {
+    const int e = ef / E, f = ef % E;
+    double acc = 0.0;
+    for (int64_t wn = begin; wn < end; ++wn) {
+      const int w = (int)(wn / N);
+      acc += weights[w] * (double)phi[wn * E + e] * y[wn * E + f];
+    }
+    out[ef] = acc;
+  }
+}
+
+__global__ void gram_gather_kernel(const double* partial, int blocks, int E, int D,
+                                   const int* abmn, double* out) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= D) return;
+  const int A = abmn[4 * d], B = abmn[4 * d + 1], M = abmn[4 * d + 2], N = abmn[4 * d + 3];
+  auto gram = [&](int i, int j) -> double {
+    if (i >= E || j >= E) return 0.0;
+    double acc = 0.0;
+    for (int b = 0; b < blocks; ++b) acc += partial[((int64_t)b * E + i) * E + j];
+    return -acc;
+  };
+  out[d] = gram(M, A) - gram(M, B) - gram(N, A) + gram(N, B);
+}
+
+// integrated[e][orig] = sum_w weight_w fields[w][pos(orig)][e]
+__global__ void integrated_kernel(const float* fields, const double* weights, const int* iperm,
+                                  int W, int N, int E, float* integrated) {
+  const int64_t total = (int64_t)N * E;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(idx / N), orig = (int)(idx % N);
+    const int n = iperm[orig];
+    double acc = 0.0;
+    for (int w = 0; w < W; ++w) acc += weights[w] * (double)fields[((int64_t)w * N + n) * E + e];
+    integrated[idx] = (float)acc;
+  }
+}
+
+
+}  // namespace adt

@@ -1,0 +1,47 @@
+// Host-side plan construction of adtlert_b200 (no CUDA): sparse pattern, level-set elimination
+// order, assembly routing, block cyclic reduction schedule, per-cell template factors and the
+// measurement routings. The device plan uploads these arrays unchanged.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "adtlert_b200.h"
+
+namespace adt {
+
+constexpr int kMaxBlock = 64;  // largest elimination block the solver kernels accept
+
+// Fields of one elimination task (one row of the int64 task table).
+enum TaskField : int {
+  T_J = 0, T_MJ, T_OFFJ, T_LOFF,
+  T_P, T_MP, T_OFFP, T_UOFF, T_LINKP,
+  T_Q, T_MQ, T_OFFQ, T_VOFF, T_LINKQ,
+  T_FILL, T_PULL0, T_PULL1,
+  T_FIELDS
+};
+// Fields of one pull (a Schur-complement contribution of an earlier elimination).
+enum PullField : int { P_TYPE = 0, P_OFF, P_ME, P_EOFF, P_FIELDS };
+
+struct HostPlan {
+  int N = 0, dim = 2, C = 0, K = 0, Cm = 0, Nb = 0, BL = 0, W = 0, E = 0, D = 0, RW = 0;
+  int nnz = 0, nb = 0, max_m = 0, levels = 0, RS = 0, R = 0, rdofs = 0;
+  int64_t contributions = 0, factor_stride = 0;
+  std::vector<int> perm, iperm, level_begin;
+  std::vector<int> csr_ptr, csr_col, csr_row, contrib_ptr, contrib;
+  std::vector<int64_t> task_rows, pulls;
+  std::vector<float> features, fscale;
+  std::vector<int> pair_ptr, pair_list, rcv_dofs;
+  std::vector<double> rcv_w;
+  std::vector<int> rdof_ptr, rdof_rcv, rdof_dof;
+  std::vector<double> rdof_w;
+  std::vector<int> cdofs, bd, cell_bptr, cell_blist, model_ptr, model_list;
+  std::vector<double> k2;
+};
+
+// Validates `pr` and builds every host array of its plan; on failure returns the status and
+// sets `err`.
+adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err);
+
+}  // namespace adt

@@ -1,0 +1,238 @@
+// Sensitivity contractions: the normal-quadrupole Jacobian and the per-cell adjoint gradients.
+//
+// Jacobian. For every discretization cell c, the unit templates factor as K_c = Ls^T Ls and
+// M_c = Lm^T Lm (computed once on the host), so with per-wavenumber features
+//   F_w[e] = ( sqrt(w_w) Ls x_we ; sqrt(w_w) k_w Lm x_we ),   x_we = fields_w[dofs(c)][e],
+// the electrode Gram G_c[e][f] = sum_w F_w[e] . F_w[f] = sum_w w_w x_we^T (K_c + k_w^2 M_c) x_wf,
+// and every ABMN row is four Gram entries:
+//   J[d][c] = -(G[M][A] - G[M][B] - G[N][A] + G[N][B])      (slot E = remote = 0).
+// A block owns `cells_per_block` cells; each thread accumulates 4x4 tiles of the upper triangle
+// of some cells' Grams in registers (fixed wavenumber/feature order: bitwise repeatable), the
+// packed Grams go to shared memory, and the rows are gathered so that a warp writes contiguous
+// cells of one row. This replaces the per-entry serial contraction of the reference kernel
+// (adtlert/forward/kernels.py:132-178), whose result it equals up to rounding.
+#include "adt_internal.h"
+#include "kernels.h"
+
+namespace adt {
+
+constexpr int kJacThreads = 256;
+constexpr int kJacJobs = 5;  // 4x4 Gram tiles per thread
+
+// Dynamic shared memory of jacobian_kernel for `cells` cells per block.
+size_t jacobian_smem(int cells, int R, int E) {
+  const int E4 = (E + 3) & ~3;
+  return sizeof(float) * ((size_t)cells * R * E4 + (size_t)cells * E * (E + 1) / 2);
+}
+
+__device__ __forceinline__ int packed_index(int i, int j, int E) {
+  // i <= j < E, row-major upper triangle
+  return i * E - (i * (i - 1)) / 2 + (j - i);
+}
+
+__global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a) {
+  extern __shared__ float jsm[];
+  const int CT = a.cells_per_block;
+  const int E4 = (a.E + 3) & ~3;
+  const int nt4 = E4 / 4;
+  const int NT = nt4 * (nt4 + 1) / 2;
+  const int P = a.E * (a.E + 1) / 2;
+  float* feat = jsm;                    // [CT][R][E4]
+  float* gram = jsm + CT * a.R * E4;    // [CT][P]
+  const int c0 = blockIdx.x * CT;
+  const int tid = threadIdx.x;
+
+  int job_cell[kJacJobs], job_ti[kJacJobs], job_tj[kJacJobs];
+#pragma unroll
+  for (int j = 0; j < kJacJobs; ++j) {
+    const int job = tid + j * kJacThreads;
+    job_cell[j] = -1;
+    job_ti[j] = job_tj[j] = 0;
+    if (job < CT * NT) {
+      job_cell[j] = job / NT;
+      int t = job % NT, ti = 0, len = nt4;
+      while (t >= len) { t -= len; ++ti; --len; }
+      job_ti[j] = ti;
+      job_tj[j] = ti + t;
+    }
+  }
+  float acc[kJacJobs][16];
+#pragma unroll
+  for (int j = 0; j < kJacJobs; ++j)
+#pragma unroll
+    for (int r = 0; r < 16; ++r) acc[j][r] = 0.f;
+
+  for (int w = 0; w < a.W; ++w) {
+    __syncthreads();
+    const float* fw = a.fields + (int64_t)w * a.N * a.E;
+    for (int idx = tid; idx < CT * E4; idx += kJacThreads) {
+      const int ci = idx / E4, e = idx - ci * E4;
+      const int c = c0 + ci;
+      float x[16];
+      const bool live = c < a.C && e < a.E;
+      if (live) {
+        for (int k = 0; k < a.K; ++k) x[k] = fw[(int64_t)a.cell_dofs[c * a.K + k] * a.E + e];
+      }
+      for (int f = 0; f < a.R; ++f) {
+        float v = 0.f;
+        if (live) {
+          const float* lf = a.features + ((int64_t)c * a.R + f) * a.K;
+          for (int k = 0; k < a.K; ++k) v = fmaf(lf[k], x[k], v);
+          v *= a.fscale[w * a.R + f];
+        }
+        feat[(ci * a.R + f) * E4 + e] = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kJacJobs; ++j) {
+      if (job_cell[j] < 0) continue;
+      const float* base = feat + job_cell[j] * a.R * E4;
+      for (int f = 0; f < a.R; ++f) {
+        const float4 u = *reinterpret_cast<const float4*>(base + f * E4 + 4 * job_ti[j]);
+        const float4 v = *reinterpret_cast<const float4*>(base + f * E4 + 4 * job_tj[j]);
+        const float ua[4] = {u.x, u.y, u.z, u.w};
+        const float va[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) acc[j][r * 4 + s] = fmaf(ua[r], va[s], acc[j][r * 4 + s]);
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kJacJobs; ++j) {
+    if (job_cell[j] < 0) continue;
+    float* g = gram + job_cell[j] * P;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int i = 4 * job_ti[j] + r, k = 4 * job_tj[j] + s;
+        if (i <= k && k < a.E) g[packed_index(i, k, a.E)] = acc[j][r * 4 + s];
+      }
+  }
+  __syncthreads();
+  const int ncells = min(CT, a.C - c0);
+  for (int idx = tid; idx < a.rows * CT; idx += kJacThreads) {
+    const int dl = idx / CT, ci = idx - dl * CT;
+    if (ci >= ncells) continue;
+    const int* q = a.abmn + 4 * (a.row_begin + dl);
+    const float* g = gram + ci * P;
+    auto G = [&](int i, int k) -> float {
+      if (i >= a.E || k >= a.E) return 0.f;
+      return i <= k ? g[packed_index(i, k, a.E)] : g[packed_index(k, i, a.E)];
+    };
+    const int A = q[0], B = q[1], M = q[2], N = q[3];
+    const float v = (G(M, A) - G(M, B)) - (G(N, A) - G(N, B));
+    a.out[(int64_t)dl * a.C + c0 + ci] = -v;
+  }
+}
+
+// One warp per (cotangent q, cell): g[q][c] = -sum_w sum_e x_we^T (K + k_w^2 M) y_we over the
+// cell's dofs (x scaled by x_scale[w], y by y_scale[w]), plus the mixed-boundary term
+// -sum_w sum_e x^T (alpha_w[b] Mb) y over the cell's boundary elements when `robin`.
+// Lanes own electrodes; the lane sums are combined by a fixed shuffle tree.
+// Replaces _cell_gradient (adtlert/forward/ert2p5d.py:765-825).
+__global__ void cell_gradient_kernel(CellGradientArgs a) {
+  const int warps = blockDim.x / 32;
+  const int64_t warp_id = (int64_t)blockIdx.x * warps + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  const int64_t count = (int64_t)a.models * a.q_per_model;
+  if (warp_id >= count * a.C) return;
+  const int q = (int)(warp_id / a.C), c = (int)(warp_id % a.C);
+  const int s = q / a.q_per_model, ql = q % a.q_per_model;
+  const int K = a.K, K2 = K * K;
+  const int* dofs = a.cell_dofs + (int64_t)c * K;
+  double acc = 0.0;
+  for (int w = 0; w < a.W; ++w) {
+    const int64_t t = (int64_t)s * a.W + w;
+    const double xs = a.x_scale ? a.x_scale[w] : 1.0;
+    const double ys = a.y_scale ? a.y_scale[w] : 1.0;
+    const double k2 = a.k2[w];
+    for (int e = lane; e < a.E; e += 32) {
+      double xv[16], yv[16];
+      for (int k = 0; k < K; ++k) {
+        const int64_t xi = (t * a.N + dofs[k]) * a.x_cols + (int64_t)ql * a.E + e;
+        const int64_t yi = (t * a.N + dofs[k]) * a.E + e;
+        xv[k] = xs * (a.x_double ? ((const double*)a.x)[xi] : (double)((const float*)a.x)[xi]);
+        yv[k] = ys * (a.y_double ? ((const double*)a.y)[yi] : (double)((const float*)a.y)[yi]);
+      }
+      const double* st = a.stiffness + (int64_t)c * K2;
+      const double* ms = a.mass + (int64_t)c * K2;
+      double sum = 0.0;
+      for (int i = 0; i < K; ++i) {
+        double row = 0.0;
+        for (int j = 0; j < K; ++j) row += (st[i * K + j] + k2 * ms[i * K + j]) * yv[j];
+        sum += xv[i] * row;
+      }
+      if (a.robin) {
+        for (int bi = a.cell_bptr[c]; bi < a.cell_bptr[c + 1]; ++bi) {
+          const int b = a.cell_blist[bi];
+          const double alpha = a.bcoef[(int64_t)w * a.Nb + b];
+          const int* bd = a.bdofs + (int64_t)b * a.BL;
+          const double* bm = a.bmass + (int64_t)b * a.BL * a.BL;
+          for (int i = 0; i < a.BL; ++i) {
+            const int64_t xi = (t * a.N + bd[i]) * a.x_cols + (int64_t)ql * a.E + e;
+            const double xb = xs * (a.x_double ? ((const double*)a.x)[xi] : (double)((const float*)a.x)[xi]);
+            double row = 0.0;
+            for (int j = 0; j < a.BL; ++j) {
+              const int64_t yi = (t * a.N + bd[j]) * a.E + e;
+              const double yb = ys * (a.y_double ? ((const double*)a.y)[yi] : (double)((const float*)a.y)[yi]);
+              row += alpha * bm[i * a.BL + j] * yb;
+            }
+            sum += xb * row;
+          }
+        }
+      }
+      acc += sum;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if (lane == 0) a.out[(int64_t)q * a.C + c] = -acc;
+}
+
+// current[w][n][e] = sum_f pairs[f][e] phi[w][n][f] (the "current" fields of normal_vjp,
+// adtlert/forward/ert2p5d.py:907-908).
+__global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, int E,
+                           double* current) {
+  const int64_t total = (int64_t)W * N * E;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(idx % E);
+    const int64_t row = idx / E;
+    const float* x = phi + row * E;
+    double acc = 0.0;
+    for (int f = 0; f < E; ++f) acc += pairs[f * E + e] * (double)x[f];
+    current[idx] = acc;
+  }
+}
+
+// out[r][col] = sum over the column's cells (fixed order) of in[r][cell].
+__global__ void aggregate_kernel(const double* in, int rows, int C, int columns, const int* ptr,
+                                 const int* cells, float* out, int64_t in_stride) {
+  const int64_t total = (int64_t)rows * columns;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / columns), col = (int)(idx % columns);
+    double acc = 0.0;
+    for (int i = ptr[col]; i < ptr[col + 1]; ++i) acc += in[(int64_t)r * in_stride + cells[i]];
+    out[idx] = (float)acc;
+  }
+}
+
+__global__ void aggregate_float_kernel(const float* in, int rows, int C, int columns,
+                                       const int* ptr, const int* cells, float* out) {
+  const int64_t total = (int64_t)rows * columns;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / columns), col = (int)(idx % columns);
+    float acc = 0.f;
+    for (int i = ptr[col]; i < ptr[col + 1]; ++i) acc += in[(int64_t)r * C + cells[i]];
+    out[idx] = acc;
+  }
+}
+
+}  // namespace adt

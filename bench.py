@@ -1,0 +1,406 @@
+"""Benchmark: Jacobian entries per second of the flat 2.5D ERT operator on B200.
+
+Workload (one "step"): ``jacobian()`` of a fresh seeded model on the flat section (120 m x 40 m,
+4961 nodes, 9600 P1 triangles, 48 electrodes, 1232 dipole-dipole rows, 17 wavenumbers):
+assembly of 17 operators, their factorization, the secondary-field solve for 48 sources,
+quadrature + ABMN measurement, and the 1232 x 9600 normal-quadrupole Jacobian.
+
+* ``value``: D*C / step time with the models already in HBM and J left in HBM, timed per step
+  with CUDA events on the launching stream; L2 is flushed (256 MiB write) between steps,
+  outside the timed events.
+* ``e2e``: the same metric through the public API, ``ERTForward2p5D.jacobian(sigma)`` with the
+  model in pinned host memory and J returned to the host, wall-clock per call.
+* ``--impl reference``: the reference's CPU path (FP64 oracle fields + the C restatement of the
+  reference kernel on all host threads), one model per step.
+
+Multi-GPU (torchrun): every rank runs its own models (time-lapse steps are independent), no
+collective on the data path; value = all ranks' entries / max-over-ranks time ("weak").
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "ad-tlert_b200"))
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=5)
+    parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    parser.add_argument("--e2e-steps", type=int, default=None)
+    parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
+    return parser.parse_args()
+
+
+def workload(max_n: int):
+    from adtlert_b200 import synthetic
+
+    nodes, cells, electrodes, rows = synthetic.flat_section(max_n)
+    return nodes, cells, electrodes, rows
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return rank, world
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        handle, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(handle)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL,
+            )
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        finally:
+            Path(self.path).unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({name for r in rows for name, flag in zip(names, r[5:9]) if flag.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return {"hbm_gbs": data["hbm_gbs"], "bf16_tflops": data["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def ncu_traffic() -> dict:
+    path = ROOT / "profiles" / "traffic.json"
+    return json.loads(path.read_text()) if path.exists() else {}
+
+
+def run_reference(args, rank: int, world: int) -> dict:
+    """The reference's CPU path on the host cores, one full model per step (bounded sample)."""
+
+    sys.path.insert(0, str(ROOT))
+    from adtlert_b200 import synthetic
+    from oracle import baseline
+    from oracle.ert2p5d import Oracle2p5D
+
+    nodes, cells, electrodes, rows = workload(args.max_n)
+    oracle = Oracle2p5D(nodes, cells, electrodes, rows)
+    D, C = len(rows), len(cells)
+    threads = baseline.host_threads()
+    baseline.build()
+    for i in range(args.warmup):
+        baseline.jacobian(oracle, synthetic.layered_model(nodes, cells, 10_000 + i), threads)
+    times = []
+    for i in range(args.steps):
+        sigma = synthetic.layered_model(nodes, cells, i)
+        start = time.perf_counter()
+        baseline.jacobian(oracle, sigma, threads)
+        times.append(time.perf_counter() - start)
+    total = sum(times)
+    value = D * C * args.steps / total
+    sample = f"{args.steps} models x full jacobian ({D} x {C}): SuperLU fields + C contraction"
+    return {
+        "metric": "jacobian_entries_per_second",
+        "value": value,
+        "unit": "entries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "impl": "reference",
+        "config": config(D, C, 17, 48, world),
+        "cpu_baseline": {"value": value, "unit": "entries/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def config(D, C, W, E, world) -> dict:
+    return {
+        "workload": f"2.5D flat jacobian(): {C} P1 triangles, 4961 nodes, {E} electrodes, {D} dipole-dipole rows, {W} wavenumbers; fresh model per step",
+        "rows": D,
+        "cells": C,
+        "wavenumbers": W,
+        "electrodes": E,
+        "l2": "flushed between steps (256 MiB write, outside the timed events)",
+        "parallelism": f"replicas x{world} (independent models per rank)",
+    }
+
+
+def run_b200(args, rank: int, world: int) -> dict | None:
+    from adtlert_b200 import ERTForward2p5D, Mesh, Survey, synthetic
+    from adtlert_b200 import _native
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    nodes, cells, electrodes, rows = workload(args.max_n)
+    forward = ERTForward2p5D.from_mesh_survey(Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, rows))
+    lib, plan = forward._lib, forward._plan
+    W, N, E, D, C = forward.W, forward.N, forward.E, forward.D, forward.C
+    stream = torch.cuda.current_stream(device)
+    handle = _native.stream_handle(device)
+    total_models = args.warmup + args.steps
+    models = torch.as_tensor(
+        np.stack([synthetic.layered_model(nodes, cells, 1000 * rank + i) for i in range(total_models)]), device=device
+    )
+    fields = torch.empty((1, W, N, E), dtype=torch.float32, device=device)
+    normal = torch.empty((1, D), dtype=torch.float64, device=device)
+    recip = torch.empty_like(normal)
+    J = torch.empty((D, C), dtype=torch.float32, device=device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    slot = 15
+
+    def call(name, *a):
+        _native.check(getattr(lib, name)(plan, *a), plan, name)
+
+    def factorize(i):
+        call("adt_factorize", slot, _native.ptr(models[i]), 1, handle)
+
+    def solve(i):
+        call("adt_solve_fields", slot, _native.ptr(models[i]), 1, _native.ptr(fields), handle)
+
+    def measure(i):
+        call("adt_measure", _native.ptr(fields), 1, _native.ptr(normal), _native.ptr(recip), None, handle)
+
+    def sensitivity(i):
+        call("adt_normal_jacobian", _native.ptr(fields), 0, D, _native.ptr(J), handle)
+
+    stages = (("factorize", factorize), ("solve_fields", solve), ("measure", measure), ("normal_jacobian", sensitivity))
+
+    def step(i):
+        for _, fn in stages:
+            fn(i)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = forward.kernel_launches()
+    with ClockSampler(device.index) as clocks:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            events[k][0].record(stream)
+            step(args.warmup + k)
+            events[k][1].record(stream)
+        torch.cuda.synchronize(device)
+    launches = forward.kernel_launches() - launches0
+    barrier(world)
+    torch.cuda.synchronize(device)
+    elapsed = sum(a.elapsed_time(b) for a, b in events) / 1e3
+    elapsed_max = max_over_ranks(elapsed, world)
+    value = world * D * C * args.steps / elapsed_max
+    clock = clocks.summary()
+
+    # per-stage breakdown (same workload, L2 flushed, after the timed region)
+    stage_ms = {}
+    reps = max(3, min(args.steps, 10))
+    for name, fn in stages:
+        total = 0.0
+        for k in range(reps):
+            i = args.warmup + (k % args.steps)
+            for other_name, other in stages:  # rebuild the inputs each stage needs
+                if other_name == name:
+                    break
+                other(i)
+            flush.fill_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn(i)
+            b.record(stream)
+            torch.cuda.synchronize(device)
+            total += a.elapsed_time(b)
+        stage_ms[name] = total / reps
+    info = forward.plan_info
+    K, R = cells.shape[1], info["features"]
+    algorithmic = {
+        # J write + fields read + cell dofs + per-cell template factors + ABMN
+        "normal_jacobian": 4 * D * C + 4 * W * N * E + 4 * K * C + 4 * R * K * C + 16 * D,
+        # CSR values read, dense factors written (float64)
+        "factorize": 8 * W * info["nnz"] + 8 * W * info["factor_doubles_per_system"],
+        # factors read twice (forward + backward), rhs/solution, primary, fields written
+        "solve_fields": 2 * 8 * W * info["factor_doubles_per_system"] + 3 * 8 * W * N * E + 4 * W * N * E,
+        "measure": 4 * W * E * E * 3 + 16 * D,
+    }
+    dominant = max(stage_ms, key=stage_ms.get)
+    peaks = measured_peaks()
+    launches_per_stage = {"normal_jacobian": 1, "measure": 1, "factorize": info["levels"] + 1,
+                          "solve_fields": 2 * info["levels"] + 1}
+    def roofline(name):
+        per_launch_bytes = algorithmic[name] / launches_per_stage[name]
+        per_launch_s = stage_ms[name] / 1e3 / launches_per_stage[name]
+        achieved = per_launch_bytes / per_launch_s / 1e9
+        traffic = ncu_traffic().get(name)
+        return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": name,
+                "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": per_launch_s * 1e3,
+                "peak_source": peaks["source"]}
+
+    # end to end through the public API: pinned host model in, J on the host out
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
+    host_models = [torch.as_tensor(synthetic.layered_model(nodes, cells, 50_000 + 1000 * rank + i)).pin_memory() for i in range(e2e_steps + 2)]
+    for i in range(2):
+        forward.jacobian(host_models[i])
+    torch.cuda.synchronize(device)
+    barrier(world)
+    start = time.perf_counter()
+    for i in range(e2e_steps):
+        out = forward.jacobian(host_models[2 + i])
+    torch.cuda.synchronize(device)
+    e2e_time = max_over_ranks(time.perf_counter() - start, world)
+    e2e = {
+        "value": world * D * C * e2e_steps / e2e_time,
+        "unit": "entries/s",
+        "h2d_bytes_per_step": 4 * C,
+        "d2h_bytes_per_step": 4 * D * C + 2 * 8 * D + 8 * E * E + 4 * E * N,
+        "ms_per_step": 1e3 * e2e_time / e2e_steps,
+    }
+    assert out.shape == (D, C)
+
+    if rank != 0:
+        return None
+    result = {
+        "metric": "jacobian_entries_per_second",
+        "value": value,
+        "unit": "entries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 fields / f64 factorization",
+        "data": "synthetic (seeded layered models with Gaussian anomalies)",
+        "config": config(D, C, W, E, world),
+        "roofline": roofline(dominant),
+        "sensitivity_roofline": roofline("normal_jacobian"),
+        "stages_ms": stage_ms,
+        "clocks": clock,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+    }
+    if world == 1:
+        result["cpu_baseline"] = cpu_baseline(args, nodes, cells, electrodes, rows)
+    return result
+
+
+def cpu_baseline(args, nodes, cells, electrodes, rows) -> dict:
+    sys.path.insert(0, str(ROOT))
+    from adtlert_b200 import synthetic
+    from oracle import baseline
+    from oracle.ert2p5d import Oracle2p5D
+
+    oracle = Oracle2p5D(nodes, cells, electrodes, rows)
+    threads = baseline.host_threads()
+    baseline.build()
+    count, total = 0, 0.0
+    while count < 3 or (total < 10.0 and count < 10):
+        sigma = synthetic.layered_model(nodes, cells, 90_000 + count)
+        start = time.perf_counter()
+        baseline.jacobian(oracle, sigma, threads)
+        total += time.perf_counter() - start
+        count += 1
+    D, C = len(rows), len(cells)
+    return {"value": D * C * count / total, "unit": "entries/s", "cores": threads, "kind": "port",
+            "sample": f"{count} models x full jacobian ({D} x {C}): FP64 SuperLU fields + C contraction, {total:.1f} s"}
+
+
+def main():
+    args = parse_args()
+    rank, world = dist_setup(args)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world)), flush=True)
+    else:
+        result = run_b200(args, rank, world)
+        if result is not None:
+            print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,181 @@
+/*
+ * adtlert_b200 -- C ABI of the B200 (sm_100a) forward-and-sensitivity path of AD-TLERT's
+ * 2.5D DC-resistivity operator.
+ *
+ * One plan per discretization (mesh + survey + wavenumber quadrature). Geometry, element
+ * templates, the sparse pattern, its assembly routing and the block elimination schedule of
+ * the direct solver are host arrays copied into the plan once; the plan owns that device
+ * memory. Every other array crossing this boundary is a caller-owned DEVICE pointer (for
+ * example a PyTorch CUDA tensor); work is enqueued on the caller's stream and the entry points
+ * return without synchronizing unless stated. Entry points are not thread-safe per plan.
+ *
+ * Layouts (row-major, C order):
+ *   sigma      [S][model_cells]                       float32 (conductivity, S models)
+ *   fields     [S][W][dofs][E]                        float32 (total potentials; the dof axis
+ *                                                      is the plan's solver order, see
+ *                                                      adt_plan_dof_order)
+ *   normal, reciprocal   [S][D]                       float64 (transfer resistances)
+ *   jacobian   [rows][columns]                        float32
+ *
+ * ABMN rows use electrode slots; slot E is the remote electrode, whose potential is zero.
+ *
+ * Status codes map onto the reference's Python exceptions: INVALID_ARG -> ValueError,
+ * NONFINITE -> FloatingPointError, SOLVER_FAIL -> FloatingPointError (non-positive pivot),
+ * OOM -> MemoryError, CUDA_ERROR / TIMEOUT -> RuntimeError.
+ */
+#ifndef ADTLERT_B200_H
+#define ADTLERT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  ADT_OK = 0,
+  ADT_INVALID_ARG = 1,
+  ADT_NONFINITE = 2,
+  ADT_SOLVER_FAIL = 3,
+  ADT_OOM = 4,
+  ADT_TIMEOUT = 5,
+  ADT_CUDA_ERROR = 6
+} adt_status;
+
+typedef struct adt_plan adt_plan;
+typedef void* adt_stream; /* a cudaStream_t; NULL is the legacy default stream */
+
+/* Discretization of one 2.5D operator (host arrays, copied by adt_plan_create).
+ * Mirrors adtlert/forward/discretization.py:128-156 (Discretization) plus the quadrature of
+ * adtlert/forward/integration.py:32-49 and the survey slots of adtlert/survey/core.py:77-85. */
+typedef struct {
+  int32_t dof_count;              /* N */
+  int32_t dim;                    /* coordinate dimension of dof_coordinates (2 or 3) */
+  const double* dof_coordinates;  /* N*dim, used to choose the elimination order */
+  int32_t cell_count;             /* C: discretization cells */
+  int32_t local_dofs;             /* K: dofs per cell (3 P1 triangle, 4 Q1 quad, ...) */
+  const int32_t* cell_dofs;       /* C*K */
+  const double* stiffness;        /* C*K*K unit-conductivity stiffness templates */
+  const double* mass;             /* C*K*K unit mass templates */
+  const int32_t* parent_cells;    /* C: model cell of each discretization cell, NULL = identity */
+  int32_t model_cell_count;       /* number of model (conductivity) cells */
+  int32_t boundary_count;         /* Nb Robin boundary elements */
+  int32_t boundary_local;         /* dofs per boundary element */
+  const int32_t* boundary_dofs;   /* Nb*boundary_local */
+  const int32_t* boundary_cells;  /* Nb: owning discretization cell */
+  const double* boundary_mass;    /* Nb*boundary_local^2 unit boundary-mass templates */
+  const double* boundary_coefficients; /* W*Nb mixed-boundary geometry per wavenumber */
+  int32_t wavenumber_count;       /* W */
+  const double* wavenumbers;      /* W */
+  const double* weights;          /* W inverse cosine-transform weights */
+  int32_t electrode_count;        /* E: source electrodes == field rows per wavenumber */
+  int32_t receiver_width;         /* nonzeros per electrode interpolation row */
+  const int32_t* receiver_dofs;   /* E*receiver_width (-1 pads) */
+  const double* receiver_weights; /* E*receiver_width */
+  int32_t measurement_count;      /* D */
+  const int32_t* abmn;            /* D*4 electrode slots, E = remote */
+  const int32_t* source_cell_ptr; /* E+1: model cells averaged for each source resistivity */
+  const int32_t* source_cells;    /* source_cell_ptr[E] model cell ids */
+} adt_problem;
+
+/* Summary of a plan (sizes, elimination schedule). */
+typedef struct {
+  int32_t dof_count, nnz, block_count, max_block, levels;
+  int32_t features;                  /* Gram features per cell and wavenumber */
+  int64_t factor_doubles_per_system; /* dense factor storage of one system */
+  int64_t contributions;             /* routed assembly contributions */
+} adt_plan_info;
+
+/* Replaces: ERTForward2p5D.from_mesh_survey geometry set-up (adtlert/forward/ert2p5d.py:133-216),
+ * sparse_pattern (adtlert/forward/discretization.py:100-125), the GroupSum routing of
+ * _assemble (ert2p5d.py:275-314) and the cuDSS analysis/plan (adtlert/forward/cudss.py:24-45). */
+adt_status adt_plan_create(const adt_problem* problem, adt_plan** plan);
+adt_status adt_plan_destroy(adt_plan* plan);
+adt_status adt_plan_get_info(const adt_plan* plan, adt_plan_info* info);
+/* Copies the solver dof order (N int32: position -> original dof) to host memory. */
+adt_status adt_plan_dof_order(const adt_plan* plan, int32_t* order);
+/* Copies the last error message of the plan (or of a failed create, when plan is NULL). */
+adt_status adt_last_error(const adt_plan* plan, char* buffer, size_t size);
+
+/* Unit-resistivity primary field, host array [W][E][N] in original dof order; computes the
+ * conductivity-independent right-hand side A(1) u_p on the device.
+ * Replaces: _unit_primary / _reference_rhs (adtlert/forward/ert2p5d.py:418-478). */
+adt_status adt_set_primary(adt_plan* plan, const double* primary, adt_stream stream);
+
+/* Assembles A_w(sigma_s) for S models (S*W systems) into factor slot `slot` and factorizes
+ * them. Replaces: _assemble (ert2p5d.py:275-314) + BatchedSolver.solve factorization
+ * (adtlert/forward/cudss.py:63-122). */
+adt_status adt_factorize(adt_plan* plan, int32_t slot, const float* sigma, int32_t models,
+                         adt_stream stream);
+
+/* Secondary-field solve with the slot's factorization of the same models, writing total
+ * fields u = u_s + rho_src u_p. Replaces: _solve_fields (ert2p5d.py:532-553). */
+adt_status adt_solve_fields(adt_plan* plan, int32_t slot, const float* sigma, int32_t models,
+                            float* fields, adt_stream stream);
+
+/* Normal and reciprocal transfer resistances of S models (and, if not NULL, the E*E electrode
+ * potentials per model). Replaces: _integrate + _normal_reciprocal (ert2p5d.py:560-589). */
+adt_status adt_measure(adt_plan* plan, const float* fields, int32_t models, double* normal,
+                       double* reciprocal, double* potentials, adt_stream stream);
+
+/* Integrated potentials [E][N] in original dof order of one model (ForwardResponse field). */
+adt_status adt_integrated_potentials(adt_plan* plan, const float* fields, float* integrated,
+                                     adt_stream stream);
+
+/* Normal-quadrupole sensitivity rows [row_begin, row_begin+row_count) of one model,
+ * out[d][c] = -sum_w w_w (u_M - u_N)^T (K_c + k_w^2 M_c) (u_A - u_B) over discretization cells.
+ * Replaces: normal_sensitivity (adtlert/forward/kernels.py:132-268) as called by
+ * _normal_jacobian (ert2p5d.py:984-1010). */
+adt_status adt_normal_jacobian(adt_plan* plan, const float* fields, int32_t row_begin,
+                               int32_t row_count, float* jacobian, adt_stream stream);
+
+/* Sums the `in_columns` columns of values [rows][in_columns] into `columns` outputs:
+ * column_ptr[columns+1] / column_cells[] list the input columns of every output column in
+ * summation order (host arrays, cached in the plan under `key`; inputs listed nowhere are
+ * dropped). Replaces CellAggregation.columns (adtlert/forward/kernels.py:88-113). */
+adt_status adt_aggregate_columns(adt_plan* plan, int32_t key, int32_t columns,
+                                 const int32_t* column_ptr, const int32_t* column_cells,
+                                 const float* values, int32_t rows, int32_t in_columns,
+                                 float* out, adt_stream stream);
+
+/* Exact VJP of the reciprocity-averaged resistance for S models factorized in `slot`:
+ * cotangents [S][D] (float64) -> gradients [S][model_cells] (float32). With `robin` the mixed
+ * boundary derivative is included. Replaces: vjp_series (ert2p5d.py:835-871) with
+ * _pair_cotangent/_adjoint_rhs/_cell_gradient (591-639, 765-825). */
+adt_status adt_vjp(adt_plan* plan, int32_t slot, const float* fields, const double* normal,
+                   const double* reciprocal, const double* cotangents, int32_t models,
+                   float* gradient, adt_stream stream);
+
+/* Exact-derivative Jacobian rows of one model factorized in `slot` (model 0 of the slot),
+ * rows [row_begin, row_begin+row_count), each the VJP of a unit cotangent; with
+ * `normal_only` the cotangent acts on the normal reading only (the normal-quadrupole
+ * convention) and `robin` adds the boundary term. Replaces _adjoint_jacobian
+ * (ert2p5d.py:1012-1050). */
+adt_status adt_adjoint_jacobian(adt_plan* plan, int32_t slot, const float* fields,
+                                const double* normal, const double* reciprocal,
+                                int32_t row_begin, int32_t row_count, int32_t robin,
+                                int32_t normal_only, float* jacobian, adt_stream stream);
+
+/* JVP of one model factorized in `slot`: direction [model_cells] -> [D] resistance tangent.
+ * Replaces: jvp (ert2p5d.py:873-890). */
+adt_status adt_jvp(adt_plan* plan, int32_t slot, const float* fields, const double* normal,
+                   const double* reciprocal, const float* direction, double* out,
+                   adt_stream stream);
+
+/* Normal-convention products without a solve. normal_vjp: cotangent [D] -> [model_cells]
+ * (before parameter aggregation); normal_jvp: direction [model_cells] -> [D].
+ * Replaces: normal_vjp / normal_jvp (ert2p5d.py:892-943). */
+adt_status adt_normal_vjp(adt_plan* plan, const float* fields, const double* cotangent,
+                          float* gradient, adt_stream stream);
+adt_status adt_normal_jvp(adt_plan* plan, const float* fields, const float* direction,
+                          double* out, adt_stream stream);
+
+/* Number of kernels this library has launched since the plan was created. */
+int64_t adt_kernel_launches(const adt_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADTLERT_B200_H */
