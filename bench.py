@@ -46,6 +46,7 @@ def parse_args():
     parser.add_argument("--impl", choices=("b200", "reference"), default="b200")
     parser.add_argument("--e2e-steps", type=int, default=None)
     parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
+    parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg (profiling runs)")
     return parser.parse_args()
 
 
@@ -359,7 +360,7 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "e2e": e2e,
         "gpu_launches": int(launches),
     }
-    if world == 1:
+    if world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(args, nodes, cells, electrodes, rows)
     return result
 
