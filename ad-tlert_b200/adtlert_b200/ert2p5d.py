@@ -521,7 +521,6 @@ class ERTForward2p5D:
                            start, count, int(include_robin_boundary_derivative), int(normal_sensitivity), _native.ptr(out), self._stream())
                 rows.append(out)
             jacobian = _to_host(torch.cat(rows))
-        check_finite(jacobian, "jacobian")
         return self._response(fields, normal, reciprocal, None, currents), jacobian
 
     def jacobian(self, conductivity, *, batch_size=None, include_robin_boundary_derivative: bool = False,

@@ -84,6 +84,8 @@ struct adt_plan {
   // slots and workspace
   std::vector<adt::Slot> slots;
   std::vector<adt::Aggregation> aggregations;
+  double* pot = nullptr;        // potential tables of the measurement kernels
+  size_t pot_count = 0;
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
   std::string error;

@@ -99,47 +99,57 @@ __global__ void total_kernel(const double* x, const double* primary, const doubl
   }
 }
 
-// One block per model: electrode potentials P[e][r] = sum_k wr_k sum_w weight_w u_w[dof_rk][e]
-// in shared memory (slot E is the zero remote row/column), then the normal and reciprocal
-// transfers of every ABMN row. Replaces _integrate + _normal_reciprocal (ert2p5d.py:560-589).
-__global__ void measure_kernel(MeasureArgs a) {
-  extern __shared__ double pot[];
+// Electrode potentials pot[s][e][r] = sum_k wr_k sum_w weight_w u_w[dof_rk][e] of every model into
+// a padded (E+1) x (E+1) table (slot E: the zero remote row and column), one thread per entry.
+// Replaces _integrate + the electrode product of _normal_reciprocal (ert2p5d.py:560-582).
+__global__ void potentials_kernel(MeasureArgs a, int models, double* pot) {
   const int E1 = a.E + 1;
-  const int s = blockIdx.x;
-  const int64_t fo = (int64_t)s * a.W * a.N * a.E;
-  auto field = [&](int64_t i) -> double {
-    return a.f_double ? ((const double*)a.fields)[fo + i] : (double)((const float*)a.fields)[fo + i];
-  };
-  for (int idx = threadIdx.x; idx < E1 * E1; idx += blockDim.x) pot[idx] = 0.0;
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < a.E * a.E; idx += blockDim.x) {
-    const int r = idx / a.E, e = idx % a.E;  // e fastest: coalesced field reads
+  const int64_t total = (int64_t)models * E1 * E1;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(idx / (E1 * E1));
+    const int rem = (int)(idx - (int64_t)s * E1 * E1);
+    const int r = rem / E1, e = rem - r * E1;  // pot[s][e][r] stored at [s][r][e]: e fastest
     double acc = 0.0;
-    for (int k = 0; k < a.RW; ++k) {
-      const int dof = a.rcv_dofs[r * a.RW + k];
-      if (dof < 0) continue;
-      double integ = 0.0;
-      for (int w = 0; w < a.W; ++w)
-        integ += a.weights[w] * field(((int64_t)w * a.N + dof) * a.E + e);
-      acc += a.rcv_w[r * a.RW + k] * integ;
+    if (r < a.E && e < a.E) {
+      const int64_t fo = (int64_t)s * a.W * a.N * a.E;
+      for (int k = 0; k < a.RW; ++k) {
+        const int dof = a.rcv_dofs[r * a.RW + k];
+        if (dof < 0) continue;
+        double integ = 0.0;
+        for (int w = 0; w < a.W; ++w) {
+          const int64_t i = fo + ((int64_t)w * a.N + dof) * a.E + e;
+          integ += a.weights[w] * (a.f_double ? ((const double*)a.fields)[i] : (double)((const float*)a.fields)[i]);
+        }
+        acc += a.rcv_w[r * a.RW + k] * integ;
+      }
+      if (a.potentials) a.potentials[((int64_t)s * a.E + e) * a.E + r] = acc;
     }
-    pot[e * E1 + r] = acc;
-    if (a.potentials) a.potentials[((int64_t)s * a.E + e) * a.E + r] = acc;
+    pot[idx] = acc;
   }
-  __syncthreads();
-  for (int d = threadIdx.x; d < a.D; d += blockDim.x) {
+}
+
+// Normal and reciprocal transfers of every (model, row) from the potential table; in combine
+// mode the tangent of sign(n) sqrt|n r| instead (ert2p5d.py:584-589, 647-655, 886-890).
+__global__ void transfers_kernel(MeasureArgs a, int models, const double* pot) {
+  const int E1 = a.E + 1;
+  const int64_t total = (int64_t)models * a.D;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(idx / a.D), d = (int)(idx - (int64_t)s * a.D);
+    const double* P = pot + (int64_t)s * E1 * E1;
+    auto at = [&](int src, int rcv) { return P[rcv * E1 + src]; };
     const int A = a.abmn[4 * d], B = a.abmn[4 * d + 1], M = a.abmn[4 * d + 2], N = a.abmn[4 * d + 3];
-    const double n = (pot[A * E1 + M] - pot[A * E1 + N]) - (pot[B * E1 + M] - pot[B * E1 + N]);
-    const double r = (pot[M * E1 + A] - pot[M * E1 + B]) - (pot[N * E1 + A] - pot[N * E1 + B]);
+    const double n = (at(A, M) - at(A, N)) - (at(B, M) - at(B, N));
+    const double r = (at(M, A) - at(M, B)) - (at(N, A) - at(N, B));
     if (a.combine) {
-      // tangent of sign(n) sqrt|n r|: 0.5 sign(r) (dn r + n dr) / max(sqrt|n r|, 1e-30)
-      const double n0 = a.base_normal[(int64_t)s * a.D + d], r0 = a.base_recip[(int64_t)s * a.D + d];
+      const double n0 = a.base_normal[idx], r0 = a.base_recip[idx];
       const double scale = fmax(sqrt(fabs(n0 * r0)), 1e-30);
       const double sign = (r0 > 0.0) - (r0 < 0.0);
-      a.normal[(int64_t)s * a.D + d] = 0.5 * sign * (n * r0 + n0 * r) / scale;
+      a.normal[idx] = 0.5 * sign * (n * r0 + n0 * r) / scale;
     } else {
-      a.normal[(int64_t)s * a.D + d] = n;
-      a.reciprocal[(int64_t)s * a.D + d] = r;
+      a.normal[idx] = n;
+      a.reciprocal[idx] = r;
     }
   }
 }

@@ -103,7 +103,8 @@ __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
 __global__ void spmm_kernel(SpmmArgs a);
 __global__ void total_kernel(const double* x, const double* primary, const double* rho, int W,
                              int N, int E, int systems, float* fields);
-__global__ void measure_kernel(MeasureArgs a);
+__global__ void potentials_kernel(MeasureArgs a, int models, double* pot);
+__global__ void transfers_kernel(MeasureArgs a, int models, const double* pot);
 __global__ void pair_kernel(PairArgs a);
 __global__ void adjoint_rhs_kernel(AdjointRhsArgs a);
 __global__ void gram_partial_kernel(const float* phi, const double* y, const double* weights,
@@ -114,7 +115,7 @@ __global__ void integrated_kernel(const float* fields, const double* weights, co
                                   int W, int N, int E, float* integrated);
 __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, int E,
                            double* current);
-__global__ void jacobian_kernel(JacobianArgs a);
+cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s);
 __global__ void cell_gradient_kernel(CellGradientArgs a);
 __global__ void aggregate_kernel(const double* in, int rows, int C, int columns, const int* ptr,
                                  const int* cells, float* out, int64_t in_stride);

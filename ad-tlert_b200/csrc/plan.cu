@@ -181,11 +181,17 @@ void launch_measure(adt_plan* p, const TF* fields, int models, double* normal, d
   a.RW = p->RW;
   a.D = p->D;
   a.combine = base_n ? 1 : 0;
-  const size_t smem = (size_t)(p->E + 1) * (p->E + 1) * sizeof(double);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(measure_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  measure_kernel<<<models, 256, smem, s>>>(a);
-  p->launches++;
+  const size_t need = (size_t)models * (p->E + 1) * (p->E + 1);
+  if (need > p->pot_count) {
+    if (p->pot) cudaFree(p->pot);
+    p->pot = nullptr;
+    p->pot_count = 0;
+    if (cudaMalloc(&p->pot, need * sizeof(double)) != cudaSuccess) return;
+    p->pot_count = need;
+  }
+  potentials_kernel<<<grid_for((int64_t)need), 256, 0, s>>>(a, models, p->pot);
+  transfers_kernel<<<grid_for((int64_t)models * p->D), 256, 0, s>>>(a, models, p->pot);
+  p->launches += 2;
 }
 
 void launch_pairs(adt_plan* p, const double* cot, const double* normal, const double* recip,
@@ -354,7 +360,7 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->cell_bptr, p->cell_blist, p->k2, p->weights, p->abmn, p->rcv_dofs,
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
-                  p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch};
+                  p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& s : p->slots) {
@@ -504,9 +510,10 @@ adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_beg
   const int E4 = (p->E + 3) & ~3;
   const int nt4 = E4 / 4, NT = nt4 * (nt4 + 1) / 2;
   int cells = std::max(1, std::min(32, (256 * 5) / NT));
-  while (cells > 1 && jacobian_smem(cells, p->R, p->E) > 110 * 1024) --cells;
+  const int E4c = (p->E + 3) & ~3;
+  while (cells > 1 && (jacobian_smem(cells, p->R, p->E) > 110 * 1024 || cells * E4c > 256 * 4)) --cells;
   const size_t smem = jacobian_smem(cells, p->R, p->E);
-  if (smem > 220 * 1024 || NT > 256 * 5)
+  if (smem > 220 * 1024 || NT > 256 * 5 || cells * E4c > 256 * 4)
     return fail(p, ADT_INVALID_ARG, "too many electrodes for the sensitivity kernel");
   JacobianArgs a;
   a.fields = fields;
@@ -524,8 +531,7 @@ adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_beg
   a.row_begin = row_begin;
   a.rows = row_count;
   a.cells_per_block = cells;
-  cudaFuncSetAttribute(jacobian_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  jacobian_kernel<<<(p->C + cells - 1) / cells, 256, smem, (cudaStream_t)stream>>>(a);
+  launch_jacobian(a, smem, (cudaStream_t)stream);
   p->launches++;
   return check_launch(p, "normal jacobian");
 }

@@ -17,12 +17,14 @@
 namespace adt {
 
 constexpr int kJacThreads = 256;
-constexpr int kJacJobs = 5;  // 4x4 Gram tiles per thread
+constexpr int kJacJobs = 5;   // 4x4 Gram tiles per thread
+constexpr int kJacItems = 4;  // feature items (cell, electrode) per thread and wavenumber
 
-// Dynamic shared memory of jacobian_kernel for `cells` cells per block.
+// Dynamic shared memory of jacobian_kernel for `cells` cells per block: two feature buffers
+// (wavenumbers w and w+1) and the packed upper-triangular Grams.
 size_t jacobian_smem(int cells, int R, int E) {
   const int E4 = (E + 3) & ~3;
-  return sizeof(float) * ((size_t)cells * R * E4 + (size_t)cells * E * (E + 1) / 2);
+  return sizeof(float) * (2 * (size_t)cells * R * E4 + (size_t)cells * E * (E + 1) / 2);
 }
 
 __device__ __forceinline__ int packed_index(int i, int j, int E) {
@@ -30,31 +32,44 @@ __device__ __forceinline__ int packed_index(int i, int j, int E) {
   return i * E - (i * (i - 1)) / 2 + (j - i);
 }
 
+// K local dofs and R features per cell and wavenumber are compile-time (K = R = 0: runtime).
+template <int KC, int RC>
 __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a) {
   extern __shared__ float jsm[];
+  const int K = KC > 0 ? KC : a.K;
+  const int R = RC > 0 ? RC : a.R;
+  constexpr int KMAX = KC > 0 ? KC : 16;
   const int CT = a.cells_per_block;
-  const int E4 = (a.E + 3) & ~3;
+  const int E = a.E, E4 = (E + 3) & ~3;
   const int nt4 = E4 / 4;
   const int NT = nt4 * (nt4 + 1) / 2;
-  const int P = a.E * (a.E + 1) / 2;
-  float* feat = jsm;                    // [CT][R][E4]
-  float* gram = jsm + CT * a.R * E4;    // [CT][P]
+  const int P = E * (E + 1) / 2;
+  const int fsize = CT * R * E4;
+  float* gram = jsm + 2 * fsize;  // [CT][P]
   const int c0 = blockIdx.x * CT;
   const int tid = threadIdx.x;
 
-  int job_cell[kJacJobs], job_ti[kJacJobs], job_tj[kJacJobs];
+  // this thread's Gram tiles: smem offsets of the two 4-electrode strips they multiply (-1: none)
+  int off_u[kJacJobs], off_v[kJacJobs];
 #pragma unroll
   for (int j = 0; j < kJacJobs; ++j) {
     const int job = tid + j * kJacThreads;
-    job_cell[j] = -1;
-    job_ti[j] = job_tj[j] = 0;
+    off_u[j] = off_v[j] = -1;
     if (job < CT * NT) {
-      job_cell[j] = job / NT;
-      int t = job % NT, ti = 0, len = nt4;
+      const int cell = job / NT;
+      int t = job - cell * NT, ti = 0, len = nt4;
       while (t >= len) { t -= len; ++ti; --len; }
-      job_ti[j] = ti;
-      job_tj[j] = ti + t;
+      off_u[j] = cell * R * E4 + 4 * ti;
+      off_v[j] = cell * R * E4 + 4 * (ti + t);
     }
+  }
+  // this thread's feature items (cell, electrode)
+  int item_cell[kJacItems], item_e[kJacItems];
+#pragma unroll
+  for (int it = 0; it < kJacItems; ++it) {
+    const int idx = tid + it * kJacThreads;
+    item_cell[it] = idx < CT * E4 ? idx / E4 : -1;
+    item_e[it] = idx < CT * E4 ? idx - (idx / E4) * E4 : 0;
   }
   float acc[kJacJobs][16];
 #pragma unroll
@@ -62,35 +77,57 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
 #pragma unroll
     for (int r = 0; r < 16; ++r) acc[j][r] = 0.f;
 
-  for (int w = 0; w < a.W; ++w) {
-    __syncthreads();
-    const float* fw = a.fields + (int64_t)w * a.N * a.E;
-    for (int idx = tid; idx < CT * E4; idx += kJacThreads) {
-      const int ci = idx / E4, e = idx - ci * E4;
-      const int c = c0 + ci;
-      float x[16];
-      const bool live = c < a.C && e < a.E;
-      if (live) {
-        for (int k = 0; k < a.K; ++k) x[k] = fw[(int64_t)a.cell_dofs[c * a.K + k] * a.E + e];
-      }
-      for (int f = 0; f < a.R; ++f) {
+  float xv[kJacItems][KMAX];
+  auto fetch = [&](int w) {
+    const float* fw = a.fields + (int64_t)w * a.N * E;
+#pragma unroll
+    for (int it = 0; it < kJacItems; ++it) {
+      const int c = c0 + item_cell[it];
+      const bool live = item_cell[it] >= 0 && c < a.C && item_e[it] < E;
+#pragma unroll
+      for (int k = 0; k < KMAX; ++k) {
         float v = 0.f;
-        if (live) {
-          const float* lf = a.features + ((int64_t)c * a.R + f) * a.K;
-          for (int k = 0; k < a.K; ++k) v = fmaf(lf[k], x[k], v);
-          v *= a.fscale[w * a.R + f];
-        }
-        feat[(ci * a.R + f) * E4 + e] = v;
+        if (live && (KC > 0 || k < K)) v = __ldg(fw + (int64_t)__ldg(a.cell_dofs + c * K + k) * E + item_e[it]);
+        xv[it][k] = v;
       }
     }
-    __syncthreads();
+  };
+  auto features = [&](int w, float* buf) {
+#pragma unroll
+    for (int it = 0; it < kJacItems; ++it) {
+      const int ci = item_cell[it];
+      if (ci < 0) continue;
+      const int c = min(c0 + ci, a.C - 1);
+      const float* lf = a.features + (int64_t)c * R * K;
+      const float* sc = a.fscale + w * R;
+#pragma unroll
+      for (int f = 0; f < (RC > 0 ? RC : 32); ++f) {
+        if (RC == 0 && f >= R) break;
+        float v = 0.f;
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k)
+          if (KC > 0 || k < K) v = fmaf(__ldg(lf + f * K + k), xv[it][k], v);
+        buf[(ci * R + f) * E4 + item_e[it]] = v * __ldg(sc + f);
+      }
+    }
+  };
+
+  fetch(0);
+  features(0, jsm);
+  __syncthreads();
+  for (int w = 0; w < a.W; ++w) {
+    const float* cur = jsm + (w & 1) * fsize;
+    if (w + 1 < a.W) fetch(w + 1);  // loads in flight during the tile products
 #pragma unroll
     for (int j = 0; j < kJacJobs; ++j) {
-      if (job_cell[j] < 0) continue;
-      const float* base = feat + job_cell[j] * a.R * E4;
-      for (int f = 0; f < a.R; ++f) {
-        const float4 u = *reinterpret_cast<const float4*>(base + f * E4 + 4 * job_ti[j]);
-        const float4 v = *reinterpret_cast<const float4*>(base + f * E4 + 4 * job_tj[j]);
+      if (off_u[j] < 0) continue;
+      const float* pu = cur + off_u[j];
+      const float* pv = cur + off_v[j];
+#pragma unroll
+      for (int f = 0; f < (RC > 0 ? RC : 32); ++f) {
+        if (RC == 0 && f >= R) break;
+        const float4 u = *reinterpret_cast<const float4*>(pu + f * E4);
+        const float4 v = *reinterpret_cast<const float4*>(pv + f * E4);
         const float ua[4] = {u.x, u.y, u.z, u.w};
         const float va[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
@@ -99,35 +136,64 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
           for (int s = 0; s < 4; ++s) acc[j][r * 4 + s] = fmaf(ua[r], va[s], acc[j][r * 4 + s]);
       }
     }
+    if (w + 1 < a.W) features(w + 1, jsm + ((w + 1) & 1) * fsize);
+    __syncthreads();
   }
-  __syncthreads();
 #pragma unroll
   for (int j = 0; j < kJacJobs; ++j) {
-    if (job_cell[j] < 0) continue;
-    float* g = gram + job_cell[j] * P;
+    if (off_u[j] < 0) continue;
+    const int job = tid + j * kJacThreads;
+    const int cell = job / NT;
+    int t = job - cell * NT, ti = 0, len = nt4;
+    while (t >= len) { t -= len; ++ti; --len; }
+    float* g = gram + cell * P;
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
-        const int i = 4 * job_ti[j] + r, k = 4 * job_tj[j] + s;
-        if (i <= k && k < a.E) g[packed_index(i, k, a.E)] = acc[j][r * 4 + s];
+        const int i = 4 * ti + r, k = 4 * (ti + t) + s;
+        if (i <= k && k < E) g[packed_index(i, k, E)] = acc[j][r * 4 + s];
       }
   }
   __syncthreads();
+  // one thread per row: four Gram entries per cell, contiguous cells written together
   const int ncells = min(CT, a.C - c0);
-  for (int idx = tid; idx < a.rows * CT; idx += kJacThreads) {
-    const int dl = idx / CT, ci = idx - dl * CT;
-    if (ci >= ncells) continue;
-    const int* q = a.abmn + 4 * (a.row_begin + dl);
-    const float* g = gram + ci * P;
-    auto G = [&](int i, int k) -> float {
-      if (i >= a.E || k >= a.E) return 0.f;
-      return i <= k ? g[packed_index(i, k, a.E)] : g[packed_index(k, i, a.E)];
+  for (int dl = tid; dl < a.rows; dl += kJacThreads) {
+    const int4 q = *reinterpret_cast<const int4*>(a.abmn + 4 * (a.row_begin + dl));
+    auto index = [&](int i, int k) -> int {
+      if (i >= E || k >= E) return -1;
+      return i <= k ? packed_index(i, k, E) : packed_index(k, i, E);
     };
-    const int A = q[0], B = q[1], M = q[2], N = q[3];
-    const float v = (G(M, A) - G(M, B)) - (G(N, A) - G(N, B));
-    a.out[(int64_t)dl * a.C + c0 + ci] = -v;
+    const int ima = index(q.z, q.x), imb = index(q.z, q.y), ina = index(q.w, q.x), inb = index(q.w, q.y);
+    float* out = a.out + (int64_t)dl * a.C + c0;
+    for (int ci = 0; ci < ncells; ++ci) {
+      const float* g = gram + ci * P;
+      const float ma = ima >= 0 ? g[ima] : 0.f, mb = imb >= 0 ? g[imb] : 0.f;
+      const float na = ina >= 0 ? g[ina] : 0.f, nb = inb >= 0 ? g[inb] : 0.f;
+      out[ci] = -((ma - mb) - (na - nb));
+    }
   }
+}
+
+template __global__ void jacobian_kernel<3, 5>(JacobianArgs);
+template __global__ void jacobian_kernel<3, 6>(JacobianArgs);
+template __global__ void jacobian_kernel<4, 7>(JacobianArgs);
+template __global__ void jacobian_kernel<4, 8>(JacobianArgs);
+template __global__ void jacobian_kernel<0, 0>(JacobianArgs);
+
+// Launch the instantiation matching the plan's (K, R).
+cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s) {
+  const int blocks = (a.C + a.cells_per_block - 1) / a.cells_per_block;
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<blocks, kJacThreads, smem, s>>>(a);
+    return cudaGetLastError();
+  };
+  if (a.K == 3 && a.R == 5) return go(jacobian_kernel<3, 5>);
+  if (a.K == 3 && a.R == 6) return go(jacobian_kernel<3, 6>);
+  if (a.K == 4 && a.R == 7) return go(jacobian_kernel<4, 7>);
+  if (a.K == 4 && a.R == 8) return go(jacobian_kernel<4, 8>);
+  return go(jacobian_kernel<0, 0>);
 }
 
 // One warp per (cotangent q, cell): g[q][c] = -sum_w sum_e x_we^T (K + k_w^2 M) y_we over the
