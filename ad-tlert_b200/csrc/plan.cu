@@ -20,7 +20,7 @@ adt_status factorize_systems(adt_plan* p, int systems, const double* values, dou
 adt_status solve_systems(adt_plan* p, int systems, int nrhs, const double* factors,
                          double* rhs, cudaStream_t s);
 void configure_solver_kernels();
-size_t jacobian_smem(int cells, int R, int E);
+size_t jacobian_smem(int cells, int R, int E, int K);
 
 namespace {
 
@@ -509,11 +509,15 @@ adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_beg
   if (row_count == 0) return ADT_OK;
   const int E4 = (p->E + 3) & ~3;
   const int nt4 = E4 / 4, NT = nt4 * (nt4 + 1) / 2;
-  int cells = std::max(1, std::min(32, (256 * 5) / NT));
+  // cells per block: a power of two (threads split evenly over cells), at most 5 Gram tiles and
+  // 4 feature items per thread, and shared memory for two blocks per SM
   const int E4c = (p->E + 3) & ~3;
-  while (cells > 1 && (jacobian_smem(cells, p->R, p->E) > 110 * 1024 || cells * E4c > 256 * 4)) --cells;
-  const size_t smem = jacobian_smem(cells, p->R, p->E);
-  if (smem > 220 * 1024 || NT > 256 * 5 || cells * E4c > 256 * 4)
+  int cells = 32;
+  while (cells > 1 && (cells * NT > 256 * 5 || cells * E4c > 256 * 4 ||
+                       jacobian_smem(cells, p->R, p->E, p->K) > 110 * 1024))
+    cells /= 2;
+  const size_t smem = jacobian_smem(cells, p->R, p->E, p->K);
+  if (smem > 220 * 1024 || cells * NT > 256 * 5 || cells * E4c > 256 * 4)
     return fail(p, ADT_INVALID_ARG, "too many electrodes for the sensitivity kernel");
   JacobianArgs a;
   a.fields = fields;

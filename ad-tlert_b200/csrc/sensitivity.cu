@@ -22,9 +22,10 @@ constexpr int kJacItems = 4;  // feature items (cell, electrode) per thread and 
 
 // Dynamic shared memory of jacobian_kernel for `cells` cells per block: two feature buffers
 // (wavenumbers w and w+1) and the packed upper-triangular Grams.
-size_t jacobian_smem(int cells, int R, int E) {
+size_t jacobian_smem(int cells, int R, int E, int K) {
   const int E4 = (E + 3) & ~3;
-  return sizeof(float) * (2 * (size_t)cells * R * E4 + (size_t)cells * E * (E + 1) / 2);
+  return sizeof(float) * (2 * (size_t)cells * R * E4 + (size_t)cells * E * (E + 1) / 2 +
+                          (size_t)cells * R * K + (size_t)cells * K);
 }
 
 __device__ __forceinline__ int packed_index(int i, int j, int E) {
@@ -63,51 +64,59 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
       off_v[j] = cell * R * E4 + 4 * (ti + t);
     }
   }
-  // this thread's feature items (cell, electrode)
-  int item_cell[kJacItems], item_e[kJacItems];
-#pragma unroll
-  for (int it = 0; it < kJacItems; ++it) {
-    const int idx = tid + it * kJacThreads;
-    item_cell[it] = idx < CT * E4 ? idx / E4 : -1;
-    item_e[it] = idx < CT * E4 ? idx - (idx / E4) * E4 : 0;
+  // feature stage: threads are cell-major (TPC threads per cell, strided electrodes); the block's
+  // template factors and cell dofs are staged in shared memory once
+  float* coef = gram + CT * P;                           // [CT][R][K]
+  int* dofs = reinterpret_cast<int*>(coef + CT * R * K);  // [CT][K]
+  for (int i = tid; i < CT * R * K; i += kJacThreads) {
+    const int c = min(c0 + i / (R * K), a.C - 1);
+    coef[i] = a.features[(int64_t)c * R * K + i % (R * K)];
   }
+  for (int i = tid; i < CT * K; i += kJacThreads) {
+    const int c = c0 + i / K;
+    dofs[i] = c < a.C ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
+  }
+  const int TPC = kJacThreads / CT;
+  const int my_cell = tid / TPC, my_eg = tid - my_cell * TPC;
   float acc[kJacJobs][16];
 #pragma unroll
   for (int j = 0; j < kJacJobs; ++j)
 #pragma unroll
     for (int r = 0; r < 16; ++r) acc[j][r] = 0.f;
+  __syncthreads();
 
   float xv[kJacItems][KMAX];
   auto fetch = [&](int w) {
     const float* fw = a.fields + (int64_t)w * a.N * E;
 #pragma unroll
     for (int it = 0; it < kJacItems; ++it) {
-      const int c = c0 + item_cell[it];
-      const bool live = item_cell[it] >= 0 && c < a.C && item_e[it] < E;
+      const int e = my_eg + it * TPC;
 #pragma unroll
       for (int k = 0; k < KMAX; ++k) {
         float v = 0.f;
-        if (live && (KC > 0 || k < K)) v = __ldg(fw + (int64_t)__ldg(a.cell_dofs + c * K + k) * E + item_e[it]);
+        if (KC > 0 || k < K) {
+          const int dof = dofs[my_cell * K + k];
+          if (dof >= 0 && e < E) v = __ldg(fw + (int64_t)dof * E + e);
+        }
         xv[it][k] = v;
       }
     }
   };
   auto features = [&](int w, float* buf) {
+    const float* cf = coef + my_cell * R * K;
+    const float* sc = a.fscale + w * R;
 #pragma unroll
     for (int it = 0; it < kJacItems; ++it) {
-      const int ci = item_cell[it];
-      if (ci < 0) continue;
-      const int c = min(c0 + ci, a.C - 1);
-      const float* lf = a.features + (int64_t)c * R * K;
-      const float* sc = a.fscale + w * R;
+      const int e = my_eg + it * TPC;
+      if (e >= E4) continue;
 #pragma unroll
       for (int f = 0; f < (RC > 0 ? RC : 32); ++f) {
         if (RC == 0 && f >= R) break;
         float v = 0.f;
 #pragma unroll
         for (int k = 0; k < KMAX; ++k)
-          if (KC > 0 || k < K) v = fmaf(__ldg(lf + f * K + k), xv[it][k], v);
-        buf[(ci * R + f) * E4 + item_e[it]] = v * __ldg(sc + f);
+          if (KC > 0 || k < K) v = fmaf(cf[f * K + k], xv[it][k], v);
+        buf[(my_cell * R + f) * E4 + e] = v * __ldg(sc + f);
       }
     }
   };

@@ -14,9 +14,10 @@
 // Forward: y_j = L_j^-1 (b_j - sum pulls); backward: x_j = L_j^-T (y_j - U_p x_p - V_q^T x_q).
 //
 // Dense block work runs on shared-memory tiles of MAXM rows (32, 48 or 64, chosen from the
-// plan's widest level): Cholesky and triangular solves are blocked by 8 (the 8x8 diagonal part in
-// registers, the rest as register-tiled updates), so a block of m rows needs about 3 m/8
-// barriers instead of 2-3 per row.
+// plan's widest level). The pulled updates of a block accumulate in per-thread 4x4 register
+// tiles while the next pull's operands stream into shared memory with cp.async (one barrier per
+// pull); Cholesky and triangular solves are blocked by 8 (the diagonal part in registers, the
+// rest as register-tiled updates) and multiply by reciprocal diagonals.
 #include "adt_internal.h"
 
 namespace adt {
@@ -26,11 +27,104 @@ constexpr int kB = 8;  // diagonal block of the blocked Cholesky / triangular so
 
 __device__ __forceinline__ double quiet_nan() { return __longlong_as_double(0x7ff8000000000000ULL); }
 
-// C[i][j] += alpha * sum_p opA(i,p) opB(p,j) for i < m, j < n, p < k, where
-// opA(i,p) = A_T ? A[p*lda+i] : A[i*lda+p] and opB(p,j) = B_T ? B[j*ldb+p] : B[p*ldb+j].
-// Every operand tile is zero beyond its logical size up to a multiple of 4, so the 4x4
-// micro-tiles (rows ti + r*mt, columns tj + s*nt: conflict-free, broadcast-friendly) read
-// without bounds checks; only the stores are predicated.
+// ---- asynchronous global -> shared copies (8-byte cp.async) --------------------------------
+__device__ __forceinline__ void async_copy8(double* dst, const double* src) {
+  const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(addr), "l"(src));
+}
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// rows x cols dense block at src -> tile with leading dimension ld
+__device__ __forceinline__ void async_tile(double* dst, int ld, const double* src, int rows, int cols) {
+  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+    const int r = i / cols, c = i - r * cols;
+    async_copy8(dst + r * ld + c, src + i);
+  }
+}
+
+// rows x cols slice of a right-hand-side array (row stride `stride`) -> tile
+__device__ __forceinline__ void async_rows(double* dst, int ld, const double* src, int64_t stride, int rows, int cols) {
+  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+    const int r = i / cols, c = i - r * cols;
+    async_copy8(dst + r * ld + c, src + r * stride + c);
+  }
+}
+
+// ---- register-tiled products ---------------------------------------------------------------
+// Output m x n is covered by 4x4 micro-tiles with rows ti + r*mt and columns tj + s*nt
+// (conflict-free, broadcast-friendly shared-memory reads). Rows/columns past m/n read whatever
+// the tile holds there and only feed accumulators that are never stored; the reduction index p
+// is always exact.
+struct Micro {
+  int mt, nt, tile, part, nsplit, ti, tj;
+  bool active;
+  __device__ Micro(int m, int n) {
+    mt = (m + 3) >> 2;
+    nt = (n + 3) >> 2;
+    const int tiles = mt * nt;
+    nsplit = tiles <= (int)blockDim.x / 2 ? 2 : 1;  // small outputs: two threads split the reduction
+    const int per = blockDim.x / nsplit;
+    tile = threadIdx.x % per;
+    part = threadIdx.x / per;
+    active = tile < tiles;
+    ti = active ? tile / nt : 0;
+    tj = active ? tile - ti * nt : 0;
+  }
+};
+
+template <bool A_T, bool B_T>
+__device__ __forceinline__ void accumulate(double (&acc)[4][4], const Micro& u, const double* A, int lda,
+                                           const double* B, int ldb, int k) {
+  if (!u.active) return;
+  for (int p = u.part; p < k; p += u.nsplit) {
+    double a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = u.ti + r * u.mt;
+      a[r] = A_T ? A[p * lda + i] : A[i * lda + p];
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int j = u.tj + s * u.nt;
+      b[s] = B_T ? B[j * ldb + p] : B[p * ldb + j];
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) acc[r][s] = fma(a[r], b[s], acc[r][s]);
+  }
+}
+
+// Combine the split halves (through `scratch`, >= 128 x 16 doubles) and subtract from C (m x n).
+// Must be entered by all threads after the operands' last use; ends with a barrier.
+__device__ void subtract_tile(double (&acc)[4][4], const Micro& u, double* C, int ldc, int m, int n,
+                              double* scratch) {
+  if (u.nsplit == 2) {
+    if (u.part == 1 && u.active)
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) scratch[u.tile * 16 + r * 4 + s] = acc[r][s];
+    __syncthreads();
+  }
+  if (u.part == 0 && u.active) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = u.ti + r * u.mt;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int j = u.tj + s * u.nt;
+        double v = acc[r][s];
+        if (u.nsplit == 2) v += scratch[u.tile * 16 + r * 4 + s];
+        if (i < m && j < n) C[i * ldc + j] -= v;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// C[i][j] += alpha * sum_p opA(i,p) opB(p,j) for i < m, j < n, p < k (one call, no split).
 template <bool A_T, bool B_T>
 __device__ void tile_gemm(double* C, int ldc, const double* A, int lda, const double* B, int ldb,
                           int m, int n, int k, double alpha) {
@@ -73,15 +167,15 @@ __device__ void tile_gemm(double* C, int ldc, const double* A, int lda, const do
   }
 }
 
-template <int LD>
-__device__ void zero(double* a, int rows) {
-  for (int i = threadIdx.x; i < rows * LD; i += blockDim.x) a[i] = 0.0;
+__device__ __forceinline__ void zero_rows(double* a, int ld, int rows) {
+  for (int i = threadIdx.x; i < rows * ld; i += blockDim.x) a[i] = 0.0;
 }
 
-// In-place lower Cholesky of the m x m tile `a` (leading dimension LD, zero-padded). A
-// non-positive pivot becomes NaN, which propagates to every result of the system.
+// In-place lower Cholesky of the m x m tile `a` (leading dimension LD); rinv[i] = 1 / L[i][i].
+// A non-positive pivot becomes NaN, which propagates to every result of the system. Only the
+// lower triangle is read; the strict upper triangle is zeroed on exit.
 template <int LD>
-__device__ void cholesky(double* a, int m) {
+__device__ void cholesky(double* a, int m, double* rinv) {
   for (int kb = 0; kb < m; kb += kB) {
     const int nb = min(kB, m - kb);
     if (threadIdx.x < 32) {  // diagonal block in registers: lane r owns row r
@@ -94,8 +188,10 @@ __device__ void cholesky(double* a, int m) {
         if (k < nb) {
           const double pivot = __shfl_sync(0xffffffffu, row[k], k);
           const double d = pivot > 0.0 ? sqrt(pivot) : quiet_nan();
+          const double inv = 1.0 / d;
           if (r == k) row[k] = d;
-          else if (r > k) row[k] /= d;
+          else if (r > k) row[k] *= inv;
+          if (r == 0) rinv[kb + k] = inv;
 #pragma unroll
           for (int c = k + 1; c < kB; ++c) {
             const double lck = __shfl_sync(0xffffffffu, row[k], c);
@@ -118,7 +214,7 @@ __device__ void cholesky(double* a, int m) {
           double v = a[i * LD + kb + c];
 #pragma unroll
           for (int s = 0; s < c; ++s) v = fma(-x[s], a[(kb + c) * LD + kb + s], v);
-          x[c] = v / a[(kb + c) * LD + kb + c];
+          x[c] = v * rinv[kb + c];
           a[i * LD + kb + c] = x[c];
         }
       }
@@ -138,9 +234,14 @@ __device__ void cholesky(double* a, int m) {
   __syncthreads();
 }
 
-// Solve L X = B in place (L: m x m lower, leading dimension LDL; B: m x n, leading dimension LDB).
-template <int LDL, int LDB>
-__device__ void lower_solve(const double* l, double* b, int m, int n) {
+// rinv[i] = 1 / l[i][i] for a loaded factor tile; ends with a barrier.
+__device__ void reciprocal_diagonal(const double* l, int ldl, int m, double* rinv) {
+  for (int i = threadIdx.x; i < m; i += blockDim.x) rinv[i] = 1.0 / l[i * ldl + i];
+  __syncthreads();
+}
+
+// Solve L X = B in place (L: m x m lower; B: m x n).
+__device__ void lower_solve(const double* l, int ldl, const double* rinv, double* b, int ldb, int m, int n) {
   for (int kb = 0; kb < m; kb += kB) {
     const int nb = min(kB, m - kb);
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
@@ -148,26 +249,25 @@ __device__ void lower_solve(const double* l, double* b, int m, int n) {
 #pragma unroll
       for (int r = 0; r < kB; ++r) {
         if (r < nb) {
-          double v = b[(kb + r) * LDB + c];
+          double v = b[(kb + r) * ldb + c];
 #pragma unroll
-          for (int s = 0; s < r; ++s) v = fma(-l[(kb + r) * LDL + kb + s], x[s], v);
-          x[r] = v / l[(kb + r) * LDL + kb + r];
-          b[(kb + r) * LDB + c] = x[r];
+          for (int s = 0; s < r; ++s) v = fma(-l[(kb + r) * ldl + kb + s], x[s], v);
+          x[r] = v * rinv[kb + r];
+          b[(kb + r) * ldb + c] = x[r];
         }
       }
     }
     __syncthreads();
     const int rest = m - kb - nb;
     if (rest > 0)
-      tile_gemm<false, false>(b + (kb + nb) * LDB, LDB, l + (kb + nb) * LDL + kb, LDL, b + kb * LDB, LDB,
+      tile_gemm<false, false>(b + (kb + nb) * ldb, ldb, l + (kb + nb) * ldl + kb, ldl, b + kb * ldb, ldb,
                               rest, n, nb, -1.0);
     __syncthreads();
   }
 }
 
 // Solve L^T X = B in place.
-template <int LDL, int LDB>
-__device__ void upper_solve(const double* l, double* b, int m, int n) {
+__device__ void upper_solve(const double* l, int ldl, const double* rinv, double* b, int ldb, int m, int n) {
   const int last = ((m - 1) / kB) * kB;
   for (int kb = last; kb >= 0; kb -= kB) {
     const int nb = min(kB, m - kb);
@@ -176,29 +276,28 @@ __device__ void upper_solve(const double* l, double* b, int m, int n) {
 #pragma unroll
       for (int r = kB - 1; r >= 0; --r) {
         if (r < nb) {
-          double v = b[(kb + r) * LDB + c];
+          double v = b[(kb + r) * ldb + c];
 #pragma unroll
           for (int s = r + 1; s < kB; ++s)
-            if (s < nb) v = fma(-l[(kb + s) * LDL + kb + r], x[s], v);
-          x[r] = v / l[(kb + r) * LDL + kb + r];
-          b[(kb + r) * LDB + c] = x[r];
+            if (s < nb) v = fma(-l[(kb + s) * ldl + kb + r], x[s], v);
+          x[r] = v * rinv[kb + r];
+          b[(kb + r) * ldb + c] = x[r];
         }
       }
     }
     __syncthreads();
     if (kb > 0)
-      tile_gemm<true, false>(b, LDB, l + kb * LDL, LDL, b + kb * LDB, LDB, kb, n, nb, -1.0);
+      tile_gemm<true, false>(b, ldb, l + kb * ldl, ldl, b + kb * ldb, ldb, kb, n, nb, -1.0);
     __syncthreads();
   }
 }
 
-template <int LD>
-__device__ void load_tile(double* dst, const double* src, int rows, int cols) {
-  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-    const int r = i / cols, c = i - r * cols;
-    dst[r * LD + c] = src[i];
-  }
-}
+template <int MAXM>
+constexpr size_t factor_smem() { return sizeof(double) * ((size_t)MAXM * (MAXM + 1) + (size_t)MAXM * (2 * MAXM + 2) + MAXM); }
+template <int MAXM>
+constexpr size_t forward_smem() { return sizeof(double) * (4 * (size_t)MAXM * (MAXM + 1) + MAXM); }
+template <int MAXM>
+constexpr size_t backward_smem() { return sizeof(double) * (6 * (size_t)MAXM * (MAXM + 1) + MAXM); }
 
 template <int MAXM>
 __global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 3 : 1)
@@ -207,11 +306,11 @@ factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict
                     const int* __restrict__ csr_row, const int* __restrict__ csr_col, int nnz,
                     const double* __restrict__ values, double* __restrict__ factors,
                     int64_t stride) {
-  constexpr int LD = MAXM + 1, LDB = 2 * MAXM + 1;
+  constexpr int LD = MAXM + 1, LDB = 2 * MAXM + 2;
   extern __shared__ double sm[];
-  double* dm = sm;                 // D_j -> L_j                       (MAXM x LD)
-  double* bt = dm + MAXM * LD;     // [A[j,p] | A[q,j]^T] -> [U_p | V_q^T]  (MAXM x LDB)
-  double* ws = bt + MAXM * LDB;    // pull staging / fill              (MAXM x LD)
+  double* dm = sm;                // D_j -> L_j -> fill                        (MAXM x LD)
+  double* bt = dm + MAXM * LD;    // pull buffers, then [A[j,p] | A[q,j]^T] -> [U_p | V_q^T]
+  double* rinv = bt + MAXM * LDB;
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* val = values + (int64_t)blockIdx.y * nnz;
   double* f = factors + (int64_t)blockIdx.y * stride;
@@ -219,25 +318,55 @@ factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict
   const int p = (int)t[T_P], mp = p >= 0 ? (int)t[T_MP] : 0, offp = (int)t[T_OFFP];
   const int q = (int)t[T_Q], mq = q >= 0 ? (int)t[T_MQ] : 0, offq = (int)t[T_OFFQ];
   const bool p_csr = p >= 0 && t[T_LINKP] < 0, q_csr = q >= 0 && t[T_LINKQ] < 0;
-
-  zero<LD>(dm, MAXM);
-  zero<LDB>(bt, MAXM);
-  __syncthreads();
-  // original couplings of block j's rows, straight from the assembled CSR values
   const int s0 = csr_ptr[offj], s1 = csr_ptr[offj + mj];
+  const int64_t u0 = t[T_PULL0], u1 = t[T_PULL1];
+  auto issue = [&](int64_t u, double* dst) {
+    const int64_t* pl = pulls + u * P_FIELDS;
+    const int me = (int)pl[P_ME];
+    if (pl[P_TYPE] == 0) async_tile(dst, LD, f + pl[P_OFF], me, mj);  // U (me x mj)
+    else async_tile(dst, LD, f + pl[P_OFF], mj, me);                  // V (mj x me)
+    async_commit();
+  };
+  if (u0 < u1) issue(u0, bt);
+
+  // 1. the original diagonal block D_j from the assembled CSR values
+  zero_rows(dm, LD, mj);
+  __syncthreads();
+  for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+    const int c = csr_col[s];
+    if (c >= offj && c < offj + mj) dm[(csr_row[s] - offj) * LD + (c - offj)] = val[s];
+  }
+  // 2. Schur-complement updates of blocks eliminated next to j at earlier levels:
+  //    D -= sum U^T U (left-eliminated) / V V^T (right-eliminated), accumulated in registers
+  const Micro mu(mj, mj);
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc[r][s] = 0.0;
+  for (int64_t u = u0; u < u1; ++u) {
+    async_wait_all();
+    __syncthreads();
+    if (u + 1 < u1) issue(u + 1, bt + ((u + 1 - u0) & 1) * MAXM * LD);
+    const double* cur = bt + ((u - u0) & 1) * MAXM * LD;
+    const int me = (int)pulls[u * P_FIELDS + P_ME];
+    if (pulls[u * P_FIELDS + P_TYPE] == 0) accumulate<true, false>(acc, mu, cur, LD, cur, LD, me);
+    else accumulate<false, true>(acc, mu, cur, LD, cur, LD, me);
+  }
+  __syncthreads();
+  if (u0 < u1) subtract_tile(acc, mu, dm, LD, mj, mj, bt);
+
+  // 3. couplings to the chain neighbours: [A[j,p] | A[q,j]^T]
+  zero_rows(bt, LDB, mj);
+  __syncthreads();
   for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
     const int r = csr_row[s] - offj, c = csr_col[s];
-    const double v = val[s];
-    if (c >= offj && c < offj + mj) dm[r * LD + (c - offj)] = v;
-    else if (p_csr && c >= offp && c < offp + mp) bt[r * LDB + (c - offp)] = v;
-    else if (q_csr && c >= offq && c < offq + mq) bt[r * LDB + mp + (c - offq)] = v;
+    if (p_csr && c >= offp && c < offp + mp) bt[r * LDB + (c - offp)] = val[s];
+    else if (q_csr && c >= offq && c < offq + mq) bt[r * LDB + mp + (c - offq)] = val[s];
   }
-  if (p >= 0 && !p_csr) {  // A[j,p] (mj x mp) from the previous level's fill
-    const double* src = f + t[T_LINKP];
-    for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
-      const int r = i / mp, c = i - r * mp;
-      bt[r * LDB + c] = src[i];
-    }
+  if (p >= 0 && !p_csr) {  // A[j,p] (mj x mp): the previous level's fill
+    async_tile(bt, LDB, f + t[T_LINKP], mj, mp);
+    async_commit();
   }
   if (q >= 0 && !q_csr) {  // A[q,j] (mq x mj), stored transposed next to A[j,p]
     const double* src = f + t[T_LINKQ];
@@ -246,22 +375,11 @@ factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict
       bt[k * LDB + mp + r] = src[i];
     }
   }
+  async_wait_all();
   __syncthreads();
 
-  // Schur-complement updates from blocks eliminated next to j at earlier levels
-  for (int64_t u = t[T_PULL0]; u < t[T_PULL1]; ++u) {
-    const int64_t* pl = pulls + u * P_FIELDS;
-    const int type = (int)pl[P_TYPE], me = (int)pl[P_ME];
-    zero<LD>(ws, MAXM);
-    __syncthreads();
-    if (type == 0) load_tile<LD>(ws, f + pl[P_OFF], me, mj);  // U (me x mj): D -= U^T U
-    else load_tile<LD>(ws, f + pl[P_OFF], mj, me);            // V (mj x me): D -= V V^T
-    __syncthreads();
-    if (type == 0) tile_gemm<true, false>(dm, LD, ws, LD, ws, LD, mj, mj, me, -1.0);
-    else tile_gemm<false, true>(dm, LD, ws, LD, ws, LD, mj, mj, me, -1.0);
-    __syncthreads();
-  }
-  cholesky<LD>(dm, mj);
+  // 4. L_j, then [U_p | V_q^T] = L_j^-1 [A[j,p] | A[q,j]^T]
+  cholesky<LD>(dm, mj, rinv);
   {
     double* out = f + t[T_LOFF];
     for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
@@ -269,31 +387,30 @@ factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict
       out[i] = dm[r * LD + c];
     }
   }
-  if (mp + mq > 0) {
-    lower_solve<LD, LDB>(dm, bt, mj, mp + mq);  // [U_p | V_q^T]
-    double* up = f + t[T_UOFF];
-    for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
-      const int r = i / mp, c = i - r * mp;
-      up[i] = bt[r * LDB + c];
-    }
-    if (q >= 0) {
-      double* vq = f + t[T_VOFF];
-      for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
-        const int r = i / mj, k = i - r * mj;
-        vq[i] = bt[k * LDB + mp + r];
-      }
-    }
-    if (p >= 0 && q >= 0) {  // fill A[q,p] = -V_q U_p = -(V_q^T)^T U_p
-      zero<LD>(ws, MAXM);
-      __syncthreads();
-      tile_gemm<true, false>(ws, LD, bt + mp, LDB, bt, LDB, mq, mp, mj, -1.0);
-      __syncthreads();
-      double* out = f + t[T_FILL];
-      for (int i = threadIdx.x; i < mq * mp; i += blockDim.x) {
-        const int r = i / mp, c = i - r * mp;
-        out[i] = ws[r * LD + c];
-      }
-    }
+  if (mp + mq == 0) return;
+  lower_solve(dm, LD, rinv, bt, LDB, mj, mp + mq);
+  double* up = f + t[T_UOFF];
+  for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
+    const int r = i / mp, c = i - r * mp;
+    up[i] = bt[r * LDB + c];
+  }
+  if (q < 0) return;
+  double* vq = f + t[T_VOFF];
+  for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
+    const int r = i / mj, k = i - r * mj;
+    vq[i] = bt[k * LDB + mp + r];
+  }
+  if (p < 0) return;
+  // 5. fill A[q,p] = -V_q U_p, built in the L_j tile (already stored)
+  __syncthreads();
+  zero_rows(dm, LD, mq);
+  __syncthreads();
+  tile_gemm<true, false>(dm, LD, bt + mp, LDB, bt, LDB, mq, mp, mj, -1.0);
+  __syncthreads();
+  double* out = f + t[T_FILL];
+  for (int i = threadIdx.x; i < mq * mp; i += blockDim.x) {
+    const int r = i / mp, c = i - r * mp;
+    out[i] = dm[r * LD + c];
   }
 }
 
@@ -305,99 +422,113 @@ forward_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restric
                      double* __restrict__ rhs, int64_t rhs_stride, int nrhs, int root) {
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
-  double* lt = sm;
-  double* bt = lt + MAXM * LD;
-  double* mt = bt + MAXM * LD;
-  double* yt = mt + MAXM * LD;
+  auto tile = [&](int i) { return sm + i * MAXM * LD; };
+  double* rinv = sm + 4 * MAXM * LD;
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* f = factors + (int64_t)blockIdx.y * stride;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
   const int c0 = blockIdx.z * MAXM;
   const int nc = min(MAXM, nrhs - c0);
   const int mj = (int)t[T_MJ], offj = (int)t[T_OFFJ];
-
-  zero<LD>(bt, MAXM);
-  zero<LD>(lt, MAXM);
-  __syncthreads();
-  for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
-    const int r = i / nc, c = i - r * nc;
-    bt[r * LD + c] = x[(int64_t)(offj + r) * nrhs + c0 + c];
-  }
-  for (int64_t u = t[T_PULL0]; u < t[T_PULL1]; ++u) {
+  const int64_t u0 = t[T_PULL0], u1 = t[T_PULL1];
+  // pairs (tile[0], tile[1]) and (tile[2], tile[3]) alternate between pulls; the pair free
+  // during the last pull receives b_j and L_j
+  auto issue_pull = [&](int64_t u, int pair) {
     const int64_t* pl = pulls + u * P_FIELDS;
-    const int type = (int)pl[P_TYPE], me = (int)pl[P_ME], eoff = (int)pl[P_EOFF];
-    zero<LD>(mt, MAXM);
-    zero<LD>(yt, MAXM);
+    const int me = (int)pl[P_ME];
+    if (pl[P_TYPE] == 0) async_tile(tile(2 * pair), LD, f + pl[P_OFF], me, mj);
+    else async_tile(tile(2 * pair), LD, f + pl[P_OFF], mj, me);
+    async_rows(tile(2 * pair + 1), LD, x + (int64_t)pl[P_EOFF] * nrhs + c0, nrhs, me, nc);
+    async_commit();
+  };
+  auto issue_final = [&](int pair) {
+    async_rows(tile(2 * pair), LD, x + (int64_t)offj * nrhs + c0, nrhs, mj, nc);
+    async_tile(tile(2 * pair + 1), LD, f + t[T_LOFF], mj, mj);
+    async_commit();
+  };
+  int final_pair = 0;
+  if (u0 == u1) issue_final(0);
+  else issue_pull(u0, 0);
+  const Micro mu(mj, nc);
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc[r][s] = 0.0;
+  for (int64_t u = u0; u < u1; ++u) {
+    async_wait_all();
     __syncthreads();
-    if (type == 0) load_tile<LD>(mt, f + pl[P_OFF], me, mj);
-    else load_tile<LD>(mt, f + pl[P_OFF], mj, me);
-    for (int i = threadIdx.x; i < me * nc; i += blockDim.x) {
-      const int r = i / nc, c = i - r * nc;
-      yt[r * LD + c] = x[(int64_t)(eoff + r) * nrhs + c0 + c];
-    }
-    __syncthreads();
-    if (type == 0) tile_gemm<true, false>(bt, LD, mt, LD, yt, LD, mj, nc, me, -1.0);
-    else tile_gemm<false, false>(bt, LD, mt, LD, yt, LD, mj, nc, me, -1.0);
-    __syncthreads();
+    const int cur = (int)((u - u0) & 1), nxt = cur ^ 1;
+    if (u + 1 < u1) issue_pull(u + 1, nxt);
+    else { issue_final(nxt); final_pair = nxt; }
+    const double* M = tile(2 * cur);
+    const double* Y = tile(2 * cur + 1);
+    const int me = (int)pulls[u * P_FIELDS + P_ME];
+    if (pulls[u * P_FIELDS + P_TYPE] == 0) accumulate<true, false>(acc, mu, M, LD, Y, LD, me);   // U^T y
+    else accumulate<false, false>(acc, mu, M, LD, Y, LD, me);                                     // V y
   }
-  load_tile<LD>(lt, f + t[T_LOFF], mj, mj);
+  async_wait_all();
   __syncthreads();
-  lower_solve<LD, LD>(lt, bt, mj, nc);
-  if (root) upper_solve<LD, LD>(lt, bt, mj, nc);
+  double* bt = tile(2 * final_pair);
+  double* lt = tile(2 * final_pair + 1);
+  if (u0 < u1) subtract_tile(acc, mu, bt, LD, mj, nc, tile(2 * (final_pair ^ 1)));
+  reciprocal_diagonal(lt, LD, mj, rinv);
+  lower_solve(lt, LD, rinv, bt, LD, mj, nc);
+  if (root) upper_solve(lt, LD, rinv, bt, LD, mj, nc);
   for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
     const int r = i / nc, c = i - r * nc;
     x[(int64_t)(offj + r) * nrhs + c0 + c] = bt[r * LD + c];
   }
 }
 
-// Backward level: x_j = L_j^-T (y_j - U_p x_p - V_q^T x_q).
+// Backward level: x_j = L_j^-T (y_j - U_p x_p - V_q^T x_q), every operand prefetched at once.
 template <int MAXM>
-__global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 3 : 1)
+__global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
 backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
                       const double* __restrict__ factors, int64_t stride,
                       double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
-  double* lt = sm;
-  double* bt = lt + MAXM * LD;
-  double* mt = bt + MAXM * LD;
-  double* yt = mt + MAXM * LD;
+  double* ut = sm;                 // U_p (mj x mp)
+  double* xp = ut + MAXM * LD;     // x_p (mp x nc)
+  double* vt = xp + MAXM * LD;     // V_q (mq x mj)
+  double* xq = vt + MAXM * LD;     // x_q (mq x nc)
+  double* bt = xq + MAXM * LD;     // y_j -> x_j
+  double* lt = bt + MAXM * LD;     // L_j
+  double* rinv = lt + MAXM * LD;
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* f = factors + (int64_t)blockIdx.y * stride;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
   const int c0 = blockIdx.z * MAXM;
   const int nc = min(MAXM, nrhs - c0);
   const int mj = (int)t[T_MJ], offj = (int)t[T_OFFJ];
-
-  zero<LD>(bt, MAXM);
-  zero<LD>(lt, MAXM);
-  __syncthreads();
-  for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
-    const int r = i / nc, c = i - r * nc;
-    bt[r * LD + c] = x[(int64_t)(offj + r) * nrhs + c0 + c];
+  const int p = (int)t[T_P], q = (int)t[T_Q];
+  const int mp = p >= 0 ? (int)t[T_MP] : 0, mq = q >= 0 ? (int)t[T_MQ] : 0;
+  if (p >= 0) {
+    async_tile(ut, LD, f + t[T_UOFF], mj, mp);
+    async_rows(xp, LD, x + t[T_OFFP] * nrhs + c0, nrhs, mp, nc);
   }
-  for (int side = 0; side < 2; ++side) {
-    const int nb = side == 0 ? (int)t[T_P] : (int)t[T_Q];
-    if (nb < 0) continue;
-    const int me = side == 0 ? (int)t[T_MP] : (int)t[T_MQ];
-    const int eoff = side == 0 ? (int)t[T_OFFP] : (int)t[T_OFFQ];
-    zero<LD>(mt, MAXM);
-    zero<LD>(yt, MAXM);
-    __syncthreads();
-    if (side == 0) load_tile<LD>(mt, f + t[T_UOFF], mj, me);  // U_p (mj x mp)
-    else load_tile<LD>(mt, f + t[T_VOFF], me, mj);            // V_q (mq x mj)
-    for (int i = threadIdx.x; i < me * nc; i += blockDim.x) {
-      const int r = i / nc, c = i - r * nc;
-      yt[r * LD + c] = x[(int64_t)(eoff + r) * nrhs + c0 + c];
-    }
-    __syncthreads();
-    if (side == 0) tile_gemm<false, false>(bt, LD, mt, LD, yt, LD, mj, nc, me, -1.0);
-    else tile_gemm<true, false>(bt, LD, mt, LD, yt, LD, mj, nc, me, -1.0);
-    __syncthreads();
+  if (q >= 0) {
+    async_tile(vt, LD, f + t[T_VOFF], mq, mj);
+    async_rows(xq, LD, x + t[T_OFFQ] * nrhs + c0, nrhs, mq, nc);
   }
-  load_tile<LD>(lt, f + t[T_LOFF], mj, mj);
+  async_rows(bt, LD, x + (int64_t)offj * nrhs + c0, nrhs, mj, nc);
+  async_tile(lt, LD, f + t[T_LOFF], mj, mj);
+  async_commit();
+  async_wait_all();
   __syncthreads();
-  upper_solve<LD, LD>(lt, bt, mj, nc);
+  const Micro mu(mj, nc);
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc[r][s] = 0.0;
+  if (p >= 0) accumulate<false, false>(acc, mu, ut, LD, xp, LD, mp);
+  if (q >= 0) accumulate<true, false>(acc, mu, vt, LD, xq, LD, mq);
+  __syncthreads();
+  if (p >= 0 || q >= 0) subtract_tile(acc, mu, bt, LD, mj, nc, ut);
+  reciprocal_diagonal(lt, LD, mj, rinv);
+  upper_solve(lt, LD, rinv, bt, LD, mj, nc);
   for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
     const int r = i / nc, c = i - r * nc;
     x[(int64_t)(offj + r) * nrhs + c0 + c] = bt[r * LD + c];
@@ -405,15 +536,10 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
 }
 
 template <int MAXM>
-constexpr size_t factor_smem() { return sizeof(double) * ((size_t)MAXM * (MAXM + 1) * 2 + (size_t)MAXM * (2 * MAXM + 1)); }
-template <int MAXM>
-constexpr size_t solve_smem() { return sizeof(double) * 4 * (size_t)MAXM * (MAXM + 1); }
-
-template <int MAXM>
 void configure() {
   cudaFuncSetAttribute(factor_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem<MAXM>());
-  cudaFuncSetAttribute(forward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem<MAXM>());
-  cudaFuncSetAttribute(backward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem<MAXM>());
+  cudaFuncSetAttribute(forward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<MAXM>());
+  cudaFuncSetAttribute(backward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)backward_smem<MAXM>());
 }
 
 template <int MAXM>
@@ -435,14 +561,14 @@ void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, dou
   for (int level = 0; level < p->levels; ++level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
     dim3 grid(t1 - t0, systems, tiles);
-    forward_level_kernel<MAXM><<<grid, kSolverThreads, solve_smem<MAXM>(), s>>>(
+    forward_level_kernel<MAXM><<<grid, kSolverThreads, forward_smem<MAXM>(), s>>>(
         p->tasks, p->pulls, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs, level == p->levels - 1);
     p->launches++;
   }
   for (int level = p->levels - 2; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
     dim3 grid(t1 - t0, systems, tiles);
-    backward_level_kernel<MAXM><<<grid, kSolverThreads, solve_smem<MAXM>(), s>>>(
+    backward_level_kernel<MAXM><<<grid, kSolverThreads, backward_smem<MAXM>(), s>>>(
         p->tasks, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs);
     p->launches++;
   }
