@@ -34,6 +34,7 @@ SYMBOLS = (
     "adt_jvp",
     "adt_normal_vjp",
     "adt_normal_jvp",
+    "adt_measure_static",
     "adt_kernel_launches",
 )
 
@@ -123,6 +124,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_jvp": (status, [_p, _i32, _p, _p, _p, _p, _p, _p]),
         "adt_normal_vjp": (status, [_p, _p, _p, _p, _p]),
         "adt_normal_jvp": (status, [_p, _p, _p, _p, _p]),
+        "adt_measure_static": (status, [_p, _p, _i32, _p, _p, _p]),
         "adt_kernel_launches": (_i64, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():

@@ -171,6 +171,17 @@ adt_status adt_normal_vjp(adt_plan* plan, const float* fields, const double* cot
 adt_status adt_normal_jvp(adt_plan* plan, const float* fields, const float* direction,
                           double* out, adt_stream stream);
 
+/* adt_measure without any device allocation: no counterpart in the reference. For callers that
+ * may not call cudaMalloc while running (GPU memory fully reserved by another allocator, or
+ * loops that must not block on the driver's allocator); adt_measure grows a plan-owned table
+ * with cudaMalloc instead. The potential table lives in a fixed array compiled into the library:
+ * 65,536 doubles (512 KiB) per device, held until exit, so models * (E+1)^2 must not exceed
+ * 65,536 (larger requests return ADT_INVALID_ARG). All calls share that array: calls that overlap
+ * on the GPU race and must be ordered by the caller. The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress), so make it before any stream capture. */
+adt_status adt_measure_static(adt_plan* plan, const float* fields, int32_t models, double* normal,
+                              double* reciprocal, adt_stream stream);
+
 /* Number of kernels this library has launched since the plan was created. */
 int64_t adt_kernel_launches(const adt_plan* plan);
 
