@@ -24,7 +24,8 @@ constexpr int kJacItems = 4;  // feature items (cell, electrode) per thread and 
 // (wavenumbers w and w+1) and the packed upper-triangular Grams.
 size_t jacobian_smem(int cells, int R, int E, int K) {
   const int E4 = (E + 3) & ~3;
-  return sizeof(float) * (2 * (size_t)cells * R * E4 + (size_t)cells * E * (E + 1) / 2 +
+  const size_t gram = (size_t)(E * (E + 1) / 2) | 1;  // odd stride: conflict-free across cells
+  return sizeof(float) * (2 * (size_t)cells * R * E4 + (size_t)cells * gram +
                           (size_t)cells * R * K + (size_t)cells * K);
 }
 
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
   const int E = a.E, E4 = (E + 3) & ~3;
   const int nt4 = E4 / 4;
   const int NT = nt4 * (nt4 + 1) / 2;
-  const int P = E * (E + 1) / 2;
+  const int P = (E * (E + 1) / 2) | 1;  // packed Gram stride (odd: cells hit distinct banks)
   const int fsize = CT * R * E4;
   float* gram = jsm + 2 * fsize;  // [CT][P]
   const int c0 = blockIdx.x * CT;
@@ -165,21 +166,22 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
       }
   }
   __syncthreads();
-  // one thread per row: four Gram entries per cell, contiguous cells written together
+  // rows go to groups of CT threads (CT is a power of two <= 32); thread ci of a group reads cell
+  // ci's four Gram entries, so a group stores CT contiguous floats of one row
   const int ncells = min(CT, a.C - c0);
-  for (int dl = tid; dl < a.rows; dl += kJacThreads) {
+  const int ci = tid % CT;
+  for (int dl = tid / CT; dl < a.rows; dl += kJacThreads / CT) {
     const int4 q = *reinterpret_cast<const int4*>(a.abmn + 4 * (a.row_begin + dl));
     auto index = [&](int i, int k) -> int {
       if (i >= E || k >= E) return -1;
       return i <= k ? packed_index(i, k, E) : packed_index(k, i, E);
     };
     const int ima = index(q.z, q.x), imb = index(q.z, q.y), ina = index(q.w, q.x), inb = index(q.w, q.y);
-    float* out = a.out + (int64_t)dl * a.C + c0;
-    for (int ci = 0; ci < ncells; ++ci) {
+    if (ci < ncells) {
       const float* g = gram + ci * P;
       const float ma = ima >= 0 ? g[ima] : 0.f, mb = imb >= 0 ? g[imb] : 0.f;
       const float na = ina >= 0 ? g[ina] : 0.f, nb = inb >= 0 ? g[inb] : 0.f;
-      out[ci] = -((ma - mb) - (na - nb));
+      a.out[(int64_t)dl * a.C + c0 + ci] = -((ma - mb) - (na - nb));
     }
   }
 }
