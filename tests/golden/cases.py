@@ -104,3 +104,63 @@ def case_inputs(name: str) -> dict:
         ids[:half] = np.arange(half) // 3
         out["parameter_ids"] = ids
     return out
+
+
+def box_tetrahedra(nx: int = 6, ny: int = 6, nz: int = 4, relief: float = 0.0):
+    """Box 12 m x 12 m x 8 m of hexahedra split into six tetrahedra around the main diagonal;
+    ``relief`` bends the top surface (z' = z + relief * depth fraction * sin(x / 4))."""
+
+    xs, ys, zs = np.linspace(0, 12, nx + 1), np.linspace(0, 12, ny + 1), np.linspace(-8, 0, nz + 1)
+    gx, gy, gz = np.meshgrid(xs, ys, zs, indexing="ij")
+    gz = gz + relief * (gz - gz.min()) / (gz.max() - gz.min()) * np.sin(gx / 4.0)
+    nodes = np.column_stack((gx.ravel(), gy.ravel(), gz.ravel()))
+    index = np.arange(nodes.shape[0]).reshape(nx + 1, ny + 1, nz + 1)
+    corners = np.stack([
+        index[:-1, :-1, :-1], index[1:, :-1, :-1], index[1:, 1:, :-1], index[:-1, 1:, :-1],
+        index[:-1, :-1, 1:], index[1:, :-1, 1:], index[1:, 1:, 1:], index[:-1, 1:, 1:],
+    ], axis=-1).reshape(-1, 8)
+    fans = ((1, 2, 6), (2, 3, 6), (3, 7, 6), (7, 4, 6), (4, 5, 6), (5, 1, 6))
+    tets = np.stack([corners[:, [0, a, b, c]] for a, b, c in fans], axis=1).reshape(-1, 4)
+    return nodes, tets.astype(np.int64)
+
+
+CASES3D = {
+    # flat box, mixed far-field boundary, analytic singularity removal and geometric factors
+    "tet_mixed": {"relief": 0.0, "boundary": "mixed", "seed": 11},
+    # flat box, homogeneous Dirichlet far field
+    "tet_dirichlet": {"relief": 0.0, "boundary": "dirichlet", "seed": 12},
+    # bent top surface: point sources and numerical geometric factors
+    "tet_relief": {"relief": 1.0, "boundary": "mixed", "seed": 13},
+}
+
+
+def case3d_inputs(name: str) -> dict:
+    spec = CASES3D[name]
+    rng = np.random.default_rng(spec["seed"])
+    nodes, cells = box_tetrahedra(nx=12, relief=spec["relief"])
+    top = nodes[:, 2] >= nodes[:, 2].max() - 1e-9 if spec["relief"] == 0.0 else None
+    line = np.flatnonzero(np.isclose(nodes[:, 1], 6.0) & (np.isclose(nodes[:, 2], nodes[:, 2].max()) if top is None else top))
+    if spec["relief"] != 0.0:
+        # surface nodes of the bent box: the highest node of every (x, y) column on y = 6
+        columns = np.flatnonzero(np.isclose(nodes[:, 1], 6.0))
+        line = np.asarray([c[np.argmax(nodes[c, 2])] for c in np.split(columns, len(columns) // 5)])
+    line = line[np.argsort(nodes[line, 0])]
+    electrodes = nodes[line]
+    count = len(electrodes)
+    rows = [(i, i + 1, i + 1 + n, i + 2 + n) for n in range(1, 4) for i in range(count) if i + 2 + n < count]
+    rows += [(i, -1, i + 2, i + 3) for i in range(0, count - 3, 2)]
+    measurements = np.asarray(rows, dtype=np.int64)
+    centers = nodes[cells].mean(axis=1)
+    sigma = np.full(len(cells), 0.01)
+    r2 = (centers[:, 0] - 6.0) ** 2 + (centers[:, 1] - 6.0) ** 2 + (centers[:, 2] + 3.0) ** 2
+    sigma = sigma * (1.0 + 2.0 * np.exp(-r2 / 8.0)) * np.exp(0.1 * rng.standard_normal(len(cells)))
+    return {
+        "nodes": nodes,
+        "cells": cells,
+        "electrodes": electrodes,
+        "measurements": measurements,
+        "sigma": sigma,
+        "cotangent": rng.standard_normal(len(measurements)),
+        "direction": rng.standard_normal(len(cells)) * sigma * 1e-2,
+        "boundary": spec["boundary"],
+    }

@@ -29,7 +29,7 @@ HERE = Path(__file__).resolve().parent
 REFERENCE = Path("/root/reference")
 
 sys.path.insert(0, str(HERE))
-from cases import CASES, case_inputs  # noqa: E402
+from cases import CASES, CASES3D, case3d_inputs, case_inputs  # noqa: E402
 
 
 def _stub_meshio(directory: Path) -> None:
@@ -140,11 +140,45 @@ def _run_2p5d(name: str, spec: dict, precision: str) -> dict:
     return out
 
 
+def _run_3d(name: str, precision: str) -> dict:
+    import numpy as np
+    import torch
+
+    _, e3 = _patch_reference()
+    from adtlert.mesh import Mesh3D
+    from adtlert.survey import Survey
+
+    inputs = case3d_inputs(name)
+    mesh = Mesh3D.from_arrays(inputs["nodes"], inputs["cells"])
+    survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
+    forward = e3.ERTForward3D.from_mesh_survey(mesh, survey, boundary_mode=inputs["boundary"])
+    sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float64)
+    cotangent = torch.as_tensor(inputs["cotangent"], dtype=torch.float64)
+    direction = torch.as_tensor(inputs["direction"], dtype=torch.float64)
+    response = forward.solve(sigma)
+    out = {
+        "geometric_factors": forward._geometric_factors().numpy(),
+        "apparent_resistivity": response.apparent_resistivity.numpy(),
+        "resistance": response.resistance.numpy(),
+        "node_potentials": response.node_potentials.numpy(),
+        "jacobian": forward.jacobian(sigma).numpy(),
+        "jacobian_robin": forward.jacobian(sigma, include_robin_boundary_derivative=True).numpy(),
+        "vjp": forward.vjp(sigma, cotangent).numpy(),
+        "jvp": forward.jvp(sigma, direction).numpy(),
+        "normal_vjp": forward.normal_vjp(sigma, cotangent).numpy(),
+        "normal_jvp": forward.normal_jvp(sigma, direction).numpy(),
+        "homogeneous_apparent_resistivity": forward.apparent_resistivity_values(
+            torch.full((mesh.cell_count,), 0.01, dtype=torch.float64)
+        ).numpy(),
+    }
+    return out
+
+
 def _child(name: str, precision: str, target: str) -> None:
     import numpy as np
 
     sys.path.insert(0, str(REFERENCE))
-    out = _run_2p5d(name, CASES[name], precision)
+    out = _run_3d(name, precision) if name in CASES3D else _run_2p5d(name, CASES[name], precision)
     np.savez_compressed(target, **out)
 
 
@@ -155,7 +189,10 @@ def main() -> None:
         return
     with tempfile.TemporaryDirectory() as stub:
         _stub_meshio(Path(stub))
-        for name in CASES:
+        only = sys.argv[1:]
+        for name in [*CASES, *CASES3D]:
+            if only and name not in only:
+                continue
             for precision in ("float64", "float32"):
                 target = HERE / f"{name}_{precision}.npz"
                 env = dict(os.environ)
