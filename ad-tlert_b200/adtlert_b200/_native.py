@@ -23,6 +23,7 @@ SYMBOLS = (
     "adt_plan_dof_order",
     "adt_last_error",
     "adt_set_primary",
+    "adt_set_static_rhs",
     "adt_factorize",
     "adt_solve_fields",
     "adt_measure",
@@ -34,6 +35,7 @@ SYMBOLS = (
     "adt_jvp",
     "adt_normal_vjp",
     "adt_normal_jvp",
+    "adt_boundary_jacobian",
     "adt_measure_static",
     "adt_kernel_launches",
 )
@@ -74,6 +76,8 @@ class Problem(ctypes.Structure):
         ("abmn", _p),
         ("source_cell_ptr", _p),
         ("source_cells", _p),
+        ("fixed_count", _i32),
+        ("fixed_dofs", _p),
     ]
 
 
@@ -113,6 +117,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_plan_dof_order": (status, [_p, _p]),
         "adt_last_error": (status, [_p, ctypes.c_char_p, ctypes.c_size_t]),
         "adt_set_primary": (status, [_p, _p, _p]),
+        "adt_set_static_rhs": (status, [_p, _p, _p, _p]),
         "adt_factorize": (status, [_p, _i32, _p, _i32, _p]),
         "adt_solve_fields": (status, [_p, _i32, _p, _i32, _p, _p]),
         "adt_measure": (status, [_p, _p, _i32, _p, _p, _p, _p]),
@@ -122,8 +127,9 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_vjp": (status, [_p, _i32, _p, _p, _p, _p, _i32, _p, _p]),
         "adt_adjoint_jacobian": (status, [_p, _i32, _p, _p, _p, _i32, _i32, _i32, _i32, _p, _p]),
         "adt_jvp": (status, [_p, _i32, _p, _p, _p, _p, _p, _p]),
-        "adt_normal_vjp": (status, [_p, _p, _p, _p, _p]),
-        "adt_normal_jvp": (status, [_p, _p, _p, _p, _p]),
+        "adt_normal_vjp": (status, [_p, _p, _p, _i32, _p, _p]),
+        "adt_normal_jvp": (status, [_p, _p, _p, _i32, _p, _p]),
+        "adt_boundary_jacobian": (status, [_p, _p, _i32, _i32, _p, _p]),
         "adt_measure_static": (status, [_p, _p, _i32, _p, _p, _p]),
         "adt_kernel_launches": (_i64, [_p]),
     }

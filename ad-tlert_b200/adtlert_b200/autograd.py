@@ -14,11 +14,12 @@ import torch
 from torch.autograd.function import once_differentiable
 
 from .ert2p5d import ERTForward2p5D
+from .ert3d import ERTForward3D
 from .inputs import FLOAT_DTYPE
 
 
 def _operators():
-    return (ERTForward2p5D,)
+    return (ERTForward2p5D, ERTForward3D)
 
 
 def _validate_inputs(conductivity, currents, forward_operator) -> None:

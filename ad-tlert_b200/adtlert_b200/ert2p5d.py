@@ -573,7 +573,7 @@ class ERTForward2p5D:
         fields = self._fields(conductivity)
         weights = measurement_vector(cotangent, self.D, torch.float64).to(self.device).contiguous()
         grad = torch.empty((1, self.C), dtype=torch.float32, device=self.device)
-        self._call("adt_normal_vjp", _native.ptr(fields.total), _native.ptr(weights), _native.ptr(grad), self._stream())
+        self._call("adt_normal_vjp", _native.ptr(fields.total), _native.ptr(weights), 0, _native.ptr(grad), self._stream())
         gradient = self._aggregate(grad, columns)[0].cpu()
         check_finite(gradient, "normal sensitivity vjp")
         return gradient
@@ -590,7 +590,7 @@ class ERTForward2p5D:
         fields = self._fields(conductivity)
         direction = cell_vector(delta_conductivity, self.C).to(self.device, torch.float32).contiguous()
         out = torch.empty(self.D, dtype=torch.float64, device=self.device)
-        self._call("adt_normal_jvp", _native.ptr(fields.total), _native.ptr(direction), _native.ptr(out), self._stream())
+        self._call("adt_normal_jvp", _native.ptr(fields.total), _native.ptr(direction), 0, _native.ptr(out), self._stream())
         result = out.cpu().to(FLOAT_DTYPE)
         check_finite(result, "normal sensitivity jvp")
         return result

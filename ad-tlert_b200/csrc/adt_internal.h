@@ -77,10 +77,15 @@ struct adt_plan {
   int rdofs = 0;
   int64_t* tasks = nullptr;
   int64_t* pulls = nullptr;
+  int* fixed = nullptr;         // fixed (Dirichlet) dofs, solver order
+  int nfixed = 0;
+  int* owners = nullptr;        // cells owning boundary elements
+  int nowners = 0;
   // primary field
   double* primary = nullptr;    // [W][N][E] solver order
   double* refrhs = nullptr;     // [W][N][E]
   bool has_primary = false;
+  bool static_rhs = false;      // refrhs is the whole right-hand side (no primary correction)
   // slots and workspace
   std::vector<adt::Slot> slots;
   std::vector<adt::Aggregation> aggregations;

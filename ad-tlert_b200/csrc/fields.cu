@@ -26,7 +26,9 @@ __global__ void assemble_kernel(AssembleArgs a) {
     double acc = 0.0;
     for (int c = a.contrib_ptr[slot]; c < a.contrib_ptr[slot + 1]; ++c) {
       const int code = a.contrib[c];
-      if (code < volume) {
+      if (code < 0) {
+        if (a.identity) acc += 1.0;
+      } else if (code < volume) {
         const int cell = code / a.K2;
         const double sigma = sig[a.parent ? a.parent[cell] : cell];
         acc += sigma * (a.stiffness[code] + k2 * a.mass[code]);
@@ -95,7 +97,8 @@ __global__ void total_kernel(const double* x, const double* primary, const doubl
     const int64_t rest = idx / E;
     const int n = (int)(rest % N), t = (int)(rest / N);
     const int w = t % W, s = t / W;
-    fields[idx] = (float)(x[idx] + rho[s * E + e] * primary[((int64_t)w * N + n) * E + e]);
+    fields[idx] = primary ? (float)(x[idx] + rho[s * E + e] * primary[((int64_t)w * N + n) * E + e])
+                          : (float)x[idx];
   }
 }
 

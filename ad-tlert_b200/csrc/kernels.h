@@ -20,6 +20,7 @@ struct AssembleArgs {
   const double* k2;
   double* values;  // [systems][nnz]
   int systems, nnz, W, C, Cm, K2, BL2, Nb, robin;
+  int identity;    // add the unit diagonal of fixed dofs (system matrices, not derivatives)
 };
 
 struct SpmmArgs {
@@ -97,6 +98,20 @@ struct CellGradientArgs {
   int models, W, N, E, C, K, BL, Nb, robin, x_cols, q_per_model;
 };
 
+struct BoundaryJacobianArgs {
+  const float* fields;     // [W][N][E] one model
+  const double* weights;   // [W]
+  const double* bcoef;     // [W][Nb]
+  const double* bmass;     // [Nb][BL][BL]
+  const int* bdofs;        // [Nb][BL] solver order
+  const int* cell_bptr;    // [C+1]
+  const int* cell_blist;
+  const int* owners;       // cells owning boundary elements
+  const int* abmn;         // [D][4]
+  float* out;              // [rows][C]
+  int W, N, E, C, Nb, BL, owner_count, row_begin, rows;
+};
+
 __global__ void assemble_kernel(AssembleArgs a);
 __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models, const int* ptr,
                                   const int* cells, double* rho);
@@ -117,6 +132,9 @@ __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, 
                            double* current);
 cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s);
 __global__ void cell_gradient_kernel(CellGradientArgs a);
+__global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a);
+__global__ void add_kernel(double* y, const double* x, int64_t count);
+__global__ void zero_rows_kernel(double* x, const int* rows, int count, int W, int N, int E);
 __global__ void aggregate_kernel(const double* in, int rows, int C, int columns, const int* ptr,
                                  const int* cells, float* out, int64_t in_stride);
 __global__ void aggregate_float_kernel(const float* in, int rows, int C, int columns,

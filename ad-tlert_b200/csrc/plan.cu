@@ -102,7 +102,7 @@ adt_status ensure_slot(adt_plan* p, int slot, int systems) {
 }
 
 AssembleArgs assemble_args(adt_plan* p, const float* sigma, int systems, double* values,
-                           bool robin) {
+                           bool robin, bool identity) {
   AssembleArgs a;
   a.sigma = sigma;
   a.parent = p->parent;
@@ -124,12 +124,14 @@ AssembleArgs assemble_args(adt_plan* p, const float* sigma, int systems, double*
   a.BL2 = p->BL * p->BL;
   a.Nb = p->Nb;
   a.robin = robin ? 1 : 0;
+  a.identity = identity ? 1 : 0;
   return a;
 }
 
+// System matrices (identity = true: unit diagonals on fixed dofs) or their sigma-derivatives.
 void launch_assemble(adt_plan* p, const float* sigma, int systems, double* values, bool robin,
-                     cudaStream_t s) {
-  AssembleArgs a = assemble_args(p, sigma, systems, values, robin);
+                     bool identity, cudaStream_t s) {
+  AssembleArgs a = assemble_args(p, sigma, systems, values, robin, identity);
   assemble_kernel<<<grid_for((int64_t)systems * p->nnz), 256, 0, s>>>(a);
   p->launches++;
 }
@@ -348,6 +350,10 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   ADT_UP(&p->rdof_rcv, hp.rdof_rcv);
   ADT_UP(&p->rdof_w, hp.rdof_w);
   ADT_UP(&p->rdof_dof, hp.rdof_dof);
+  ADT_UP(&p->fixed, hp.fixed);
+  ADT_UP(&p->owners, hp.bowners);
+  p->nfixed = (int)hp.fixed.size();
+  p->nowners = (int)hp.bowners.size();
 #undef ADT_UP
   *out = p;
   return ADT_OK;
@@ -360,7 +366,8 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->cell_bptr, p->cell_blist, p->k2, p->weights, p->abmn, p->rcv_dofs,
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
-                  p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot};
+                  p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
+                  p->fixed, p->owners};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& s : p->slots) {
@@ -403,6 +410,7 @@ adt_status adt_last_error(const adt_plan* p, char* buffer, size_t size) {
 
 adt_status adt_set_primary(adt_plan* p, const double* primary, adt_stream stream) {
   if (!p || !primary) return ADT_INVALID_ARG;
+  if (p->static_rhs) return fail(p, ADT_INVALID_ARG, "the plan already holds a static right-hand side");
   cudaStream_t s = (cudaStream_t)stream;
   const size_t count = (size_t)p->W * p->N * p->E;
   std::vector<double> host(count);
@@ -424,12 +432,66 @@ adt_status adt_set_primary(adt_plan* p, const double* primary, adt_stream stream
   float* ones = (float*)(base + cv.offsets[is]);
   std::vector<float> h1(p->Cm, 1.0f);
   cudaMemcpyAsync(ones, h1.data(), h1.size() * sizeof(float), cudaMemcpyHostToDevice, s);
-  launch_assemble(p, ones, p->W, values, true, s);
+  launch_assemble(p, ones, p->W, values, true, true, s);
   // A(1) u_p for every wavenumber
   launch_spmm<double>(p, values, false, p->primary, false, nullptr, nullptr, 1.0, p->W, p->refrhs, s);
   cudaStreamSynchronize(s);
   p->has_primary = true;
   return check_launch(p, "reference right-hand side");
+}
+
+adt_status adt_set_static_rhs(adt_plan* p, const double* unit_primary, const double* direct,
+                              adt_stream stream) {
+  if (!p) return ADT_INVALID_ARG;
+  if (p->primary) return fail(p, ADT_INVALID_ARG, "the plan already holds a primary field");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t count = (size_t)p->W * p->N * p->E;
+  // host [W][E][N] original order -> [W][N][E] solver order
+  auto permuted = [&](const double* src) {
+    std::vector<double> host(count);
+    for (int w = 0; w < p->W; ++w)
+      for (int e = 0; e < p->E; ++e)
+        for (int n = 0; n < p->N; ++n)
+          host[((size_t)w * p->N + p->iperm[n]) * p->E + e] = src[((size_t)w * p->E + e) * p->N + n];
+    return host;
+  };
+  if (!p->refrhs && cudaMalloc(&p->refrhs, count * sizeof(double)) != cudaSuccess)
+    return fail(p, ADT_OOM, "right-hand side allocation failed");
+  Carve cv;
+  const size_t iv = cv.add((size_t)p->W * p->nnz * sizeof(double));
+  const size_t is = cv.add((size_t)p->Cm * sizeof(float));
+  const size_t ix = cv.add(count * sizeof(double));
+  char* base = (char*)scratch(p, cv.total);
+  if (!base) return fail(p, ADT_OOM, "scratch allocation failed");
+  double* values = (double*)(base + cv.offsets[iv]);
+  float* ones = (float*)(base + cv.offsets[is]);
+  double* x = (double*)(base + cv.offsets[ix]);
+  cudaMemsetAsync(p->refrhs, 0, count * sizeof(double), s);
+  if (unit_primary) {
+    const std::vector<double> host = permuted(unit_primary);
+    cudaMemcpyAsync(x, host.data(), count * sizeof(double), cudaMemcpyHostToDevice, s);
+    std::vector<float> h1(p->Cm, 1.0f);
+    cudaMemcpyAsync(ones, h1.data(), h1.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    launch_assemble(p, ones, p->W, values, true, true, s);
+    launch_spmm<double>(p, values, false, x, false, nullptr, nullptr, 1.0, p->W, p->refrhs, s);
+    cudaStreamSynchronize(s);  // the host staging buffers go out of scope
+  }
+  if (direct) {
+    const std::vector<double> host = permuted(direct);
+    cudaMemcpyAsync(x, host.data(), count * sizeof(double), cudaMemcpyHostToDevice, s);
+    add_kernel<<<grid_for((int64_t)count), 256, 0, s>>>(p->refrhs, x, (int64_t)count);
+    p->launches++;
+    cudaStreamSynchronize(s);
+  }
+  if (p->nfixed > 0) {
+    zero_rows_kernel<<<grid_for((int64_t)p->W * p->nfixed * p->E), 256, 0, s>>>(
+        p->refrhs, p->fixed, p->nfixed, p->W, p->N, p->E);
+    p->launches++;
+  }
+  cudaStreamSynchronize(s);
+  p->has_primary = true;
+  p->static_rhs = true;
+  return check_launch(p, "static right-hand side");
 }
 
 adt_status adt_factorize(adt_plan* p, int32_t slot, const float* sigma, int32_t models,
@@ -440,7 +502,7 @@ adt_status adt_factorize(adt_plan* p, int32_t slot, const float* sigma, int32_t 
   adt_status st = ensure_slot(p, slot, systems);
   if (st != ADT_OK) return st;
   Slot& sl = p->slots[slot];
-  launch_assemble(p, sigma, systems, sl.values, true, s);
+  launch_assemble(p, sigma, systems, sl.values, true, true, s);
   st = factorize_systems(p, systems, sl.values, sl.factors, s);
   sl.systems = systems;
   return st;
@@ -449,7 +511,8 @@ adt_status adt_factorize(adt_plan* p, int32_t slot, const float* sigma, int32_t 
 adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32_t models,
                             float* fields, adt_stream stream) {
   if (!p || !sigma || !fields || models <= 0) return fail(p, ADT_INVALID_ARG, "invalid solve arguments");
-  if (!p->has_primary) return fail(p, ADT_INVALID_ARG, "adt_set_primary must be called first");
+  if (!p->has_primary)
+    return fail(p, ADT_INVALID_ARG, "adt_set_primary or adt_set_static_rhs must be called first");
   if (slot < 0 || slot >= (int)p->slots.size() || p->slots[slot].systems < models * p->W)
     return fail(p, ADT_INVALID_ARG, "slot does not hold a factorization of these models");
   cudaStream_t s = (cudaStream_t)stream;
@@ -461,6 +524,18 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
   if (!base) return fail(p, ADT_OOM, "scratch allocation failed");
   double* rho = (double*)(base + cv.offsets[ir]);
   double* x = (double*)(base + cv.offsets[ix]);
+  if (p->static_rhs) {
+    const size_t per_model = (size_t)p->W * p->N * p->E;
+    for (int m = 0; m < models; ++m)
+      cudaMemcpyAsync(x + m * per_model, p->refrhs, per_model * sizeof(double),
+                      cudaMemcpyDeviceToDevice, s);
+    adt_status st = solve_systems(p, systems, p->E, p->slots[slot].factors, x, s);
+    if (st != ADT_OK) return st;
+    total_kernel<<<grid_for((int64_t)systems * p->N * p->E), 256, 0, s>>>(x, nullptr, nullptr, p->W,
+                                                                           p->N, p->E, systems, fields);
+    p->launches++;
+    return check_launch(p, "field solve");
+  }
   source_rho_kernel<<<grid_for((int64_t)models * p->E), 256, 0, s>>>(sigma, p->Cm, p->E, models,
                                                                       p->src_ptr, p->src_cells, rho);
   p->launches++;
@@ -641,7 +716,7 @@ adt_status adt_jvp(adt_plan* p, int32_t slot, const float* fields, const double*
   if (!base) return fail(p, ADT_OOM, "scratch allocation failed");
   double* values = (double*)(base + cv.offsets[iv]);
   double* x = (double*)(base + cv.offsets[ix]);
-  launch_assemble(p, direction, p->W, values, true, s);
+  launch_assemble(p, direction, p->W, values, true, false, s);
   launch_spmm<float>(p, values, false, fields, true, nullptr, nullptr, -1.0, p->W, x, s);
   adt_status st = solve_systems(p, p->W, p->E, p->slots[slot].factors, x, s);
   if (st != ADT_OK) return st;
@@ -650,7 +725,7 @@ adt_status adt_jvp(adt_plan* p, int32_t slot, const float* fields, const double*
 }
 
 adt_status adt_normal_vjp(adt_plan* p, const float* fields, const double* cotangent,
-                          float* gradient, adt_stream stream) {
+                          int32_t robin, float* gradient, adt_stream stream) {
   if (!p || !fields || !cotangent || !gradient) return fail(p, ADT_INVALID_ARG, "invalid normal_vjp arguments");
   cudaStream_t s = (cudaStream_t)stream;
   Carve cv;
@@ -665,13 +740,13 @@ adt_status adt_normal_vjp(adt_plan* p, const float* fields, const double* cotang
   launch_pairs(p, cotangent, nullptr, nullptr, 1, true, false, 0, false, pairs, s);
   mix_kernel<<<grid_for((int64_t)p->W * p->N * p->E), 256, 0, s>>>(pairs, fields, p->W, p->N, p->E, current);
   p->launches++;
-  launch_cell_gradient(p, current, true, p->E, nullptr, fields, false, p->weights, 1, 1, false, g, s);
+  launch_cell_gradient(p, current, true, p->E, nullptr, fields, false, p->weights, 1, 1, robin != 0, g, s);
   launch_to_model_cells(p, g, 1, gradient, s);
   return check_launch(p, "normal vjp");
 }
 
-adt_status adt_normal_jvp(adt_plan* p, const float* fields, const float* direction, double* out,
-                          adt_stream stream) {
+adt_status adt_normal_jvp(adt_plan* p, const float* fields, const float* direction,
+                          int32_t robin, double* out, adt_stream stream) {
   if (!p || !fields || !direction || !out) return fail(p, ADT_INVALID_ARG, "invalid normal_jvp arguments");
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t rows = (int64_t)p->W * p->N;
@@ -686,13 +761,43 @@ adt_status adt_normal_jvp(adt_plan* p, const float* fields, const float* directi
   double* values = (double*)(base + cv.offsets[iv]);
   double* y = (double*)(base + cv.offsets[iy]);
   double* partial = (double*)(base + cv.offsets[ip]);
-  launch_assemble(p, direction, p->W, values, false, s);
+  launch_assemble(p, direction, p->W, values, robin != 0, false, s);
   launch_spmm<float>(p, values, false, fields, true, nullptr, nullptr, 1.0, p->W, y, s);
   gram_partial_kernel<<<blocks, 256, 0, s>>>(fields, y, p->weights, p->W, p->N, p->E, chunk, partial);
   p->launches++;
   gram_gather_kernel<<<(p->D + 255) / 256, 256, 0, s>>>(partial, blocks, p->E, p->D, p->abmn, out);
   p->launches++;
   return check_launch(p, "normal jvp");
+}
+
+adt_status adt_boundary_jacobian(adt_plan* p, const float* fields, int32_t row_begin,
+                                 int32_t row_count, float* jacobian, adt_stream stream) {
+  if (!p || !fields || !jacobian || row_begin < 0 || row_count < 0 || row_begin + row_count > p->D)
+    return fail(p, ADT_INVALID_ARG, "invalid boundary jacobian arguments");
+  if (row_count == 0 || p->nowners == 0) return ADT_OK;
+  BoundaryJacobianArgs a;
+  a.fields = fields;
+  a.weights = p->weights;
+  a.bcoef = p->bcoef;
+  a.bmass = p->bmass;
+  a.bdofs = p->bdofs;
+  a.cell_bptr = p->cell_bptr;
+  a.cell_blist = p->cell_blist;
+  a.owners = p->owners;
+  a.abmn = p->abmn;
+  a.out = jacobian;
+  a.W = p->W;
+  a.N = p->N;
+  a.E = p->E;
+  a.C = p->C;
+  a.Nb = p->Nb;
+  a.BL = p->BL;
+  a.owner_count = p->nowners;
+  a.row_begin = row_begin;
+  a.rows = row_count;
+  boundary_jacobian_kernel<<<grid_for((int64_t)row_count * p->nowners), 256, 0, (cudaStream_t)stream>>>(a);
+  p->launches++;
+  return check_launch(p, "boundary jacobian");
 }
 
 int64_t adt_kernel_launches(const adt_plan* p) { return p ? p->launches : 0; }

@@ -140,6 +140,14 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
       { err = "boundary cells out of range"; return ADT_INVALID_ARG; }
   if (!pr->parent_cells && pr->model_cell_count != C)
     { err = "model_cell_count must equal cell_count without parents"; return ADT_INVALID_ARG; }
+  if (pr->fixed_count < 0 || pr->fixed_count > N || (pr->fixed_count > 0 && !pr->fixed_dofs))
+    { err = "invalid fixed dofs"; return ADT_INVALID_ARG; }
+  std::vector<char> fixed(N, 0);
+  for (int i = 0; i < pr->fixed_count; ++i) {
+    if (pr->fixed_dofs[i] < 0 || pr->fixed_dofs[i] >= N)
+      { err = "fixed dofs out of range"; return ADT_INVALID_ARG; }
+    fixed[pr->fixed_dofs[i]] = 1;
+  }
 
   hp.N = N; hp.dim = pr->dim; hp.C = C; hp.K = K; hp.Cm = pr->model_cell_count;
   hp.Nb = Nb; hp.BL = BL; hp.W = W; hp.E = E; hp.D = D; hp.RW = RW;
@@ -247,15 +255,22 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
   std::vector<int> ccount(hp.nnz + 1, 0);
   std::vector<std::pair<int, int>> routed;  // (slot, code)
   routed.reserve(keys.size());
+  // pairs touching a fixed dof are not routed (they stay explicit zeros of the pattern, so the
+  // elimination order does not depend on the boundary mode); a fixed diagonal gets the unit code
   for (int c = 0; c < C; ++c)
     for (int i = 0; i < K; ++i)
-      for (int j = 0; j < K; ++j)
-        routed.push_back({slot_of(pr->cell_dofs[c * K + i], pr->cell_dofs[c * K + j]), c * K * K + i * K + j});
+      for (int j = 0; j < K; ++j) {
+        const int r = pr->cell_dofs[c * K + i], q = pr->cell_dofs[c * K + j];
+        if (!fixed[r] && !fixed[q]) routed.push_back({slot_of(r, q), c * K * K + i * K + j});
+      }
   for (int b = 0; b < Nb; ++b)
     for (int i = 0; i < BL; ++i)
-      for (int j = 0; j < BL; ++j)
-        routed.push_back({slot_of(pr->boundary_dofs[b * BL + i], pr->boundary_dofs[b * BL + j]),
-                          C * K * K + b * BL * BL + i * BL + j});
+      for (int j = 0; j < BL; ++j) {
+        const int r = pr->boundary_dofs[b * BL + i], q = pr->boundary_dofs[b * BL + j];
+        if (!fixed[r] && !fixed[q]) routed.push_back({slot_of(r, q), C * K * K + b * BL * BL + i * BL + j});
+      }
+  for (int n = 0; n < N; ++n)
+    if (fixed[n]) routed.push_back({slot_of(n, n), kUnitCode});
   std::stable_sort(routed.begin(), routed.end());
   std::vector<int> contrib_ptr(hp.nnz + 1, 0), contrib(routed.size());
   for (size_t i = 0; i < routed.size(); ++i) {
@@ -381,8 +396,11 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
     for (double v : svals[c]) { lo = std::min(lo, v); hi = std::max(hi, std::fabs(v)); }
     if (lo > 1e-9 * hi) rs = K;
   }
+  // mass features only when some wavenumber is non-zero (a 3D operator has none)
+  bool any_mass = false;
+  for (int w = 0; w < W; ++w) any_mass = any_mass || pr->wavenumbers[w] != 0.0;
   hp.RS = rs;
-  hp.R = rs + K;
+  hp.R = rs + (any_mass ? K : 0);
   std::vector<float> features((size_t)C * hp.R * K);
   for (int c = 0; c < C; ++c) {
     std::vector<int> order(K);
@@ -457,6 +475,11 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
   }
   std::vector<double> k2(W);
   for (int w = 0; w < W; ++w) k2[w] = pr->wavenumbers[w] * pr->wavenumbers[w];
+  std::vector<int> bowners, fixed_solver;
+  for (int c = 0; c < C; ++c)
+    if (cell_bptr[c + 1] > cell_bptr[c]) bowners.push_back(c);
+  for (int n = 0; n < N; ++n)
+    if (fixed[hp.perm[n]]) fixed_solver.push_back(n);
 
   hp.csr_ptr = std::move(csr_ptr);
   hp.csr_col = std::move(csr_col);
@@ -482,6 +505,8 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
   hp.model_ptr = std::move(model_ptr);
   hp.model_list = std::move(model_list);
   hp.k2 = std::move(k2);
+  hp.bowners = std::move(bowners);
+  hp.fixed = std::move(fixed_solver);
   return ADT_OK;
 }
 

@@ -12,6 +12,7 @@
 namespace adt {
 
 constexpr int kMaxBlock = 64;  // largest elimination block the solver kernels accept
+constexpr int kUnitCode = -1;  // assembly contribution of constant 1 (a fixed dof's diagonal)
 
 // Fields of one elimination task (one row of the int64 task table).
 enum TaskField : int {
@@ -38,6 +39,8 @@ struct HostPlan {
   std::vector<double> rdof_w;
   std::vector<int> cdofs, bd, cell_bptr, cell_blist, model_ptr, model_list;
   std::vector<double> k2;
+  std::vector<int> bowners;  // cells owning at least one boundary element, ascending
+  std::vector<int> fixed;    // fixed dofs in solver order, ascending
 };
 
 // Validates `pr` and builds every host array of its plan; on failure returns the status and

@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
 }
 
 template __global__ void jacobian_kernel<3, 5>(JacobianArgs);
+template __global__ void jacobian_kernel<4, 3>(JacobianArgs);
 template __global__ void jacobian_kernel<3, 6>(JacobianArgs);
 template __global__ void jacobian_kernel<4, 7>(JacobianArgs);
 template __global__ void jacobian_kernel<4, 8>(JacobianArgs);
@@ -201,6 +202,7 @@ cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s) 
     return cudaGetLastError();
   };
   if (a.K == 3 && a.R == 5) return go(jacobian_kernel<3, 5>);
+  if (a.K == 4 && a.R == 3) return go(jacobian_kernel<4, 3>);
   if (a.K == 3 && a.R == 6) return go(jacobian_kernel<3, 6>);
   if (a.K == 4 && a.R == 7) return go(jacobian_kernel<4, 7>);
   if (a.K == 4 && a.R == 8) return go(jacobian_kernel<4, 8>);
@@ -269,6 +271,60 @@ __global__ void cell_gradient_kernel(CellGradientArgs a) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
   if (lane == 0) a.out[(int64_t)q * a.C + c] = -acc;
+}
+
+// Mixed-boundary part of the Jacobian, added to rows already holding the volume part: one thread
+// per (row, boundary-owning cell) sums, over the cell's boundary elements in list order,
+//   sum_w weight_w alpha_w[b] (u_M - u_N)_b^T Mb[b] (u_A - u_B)_b          (slot E = remote = 0)
+// and subtracts it from out[row][cell]. This is the Robin template of the reference's cell
+// templates (adtlert/forward/ert3d.py:224-256, used by jacobian at 867-927).
+__global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a) {
+  const int64_t total = (int64_t)a.rows * a.owner_count;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int dl = (int)(idx / a.owner_count), c = a.owners[idx % a.owner_count];
+    const int* q = a.abmn + 4 * (a.row_begin + dl);
+    const int A = q[0], B = q[1], M = q[2], Nn = q[3];
+    double acc = 0.0;
+    for (int w = 0; w < a.W; ++w) {
+      const float* f = a.fields + (int64_t)w * a.N * a.E;
+      auto at = [&](int dof, int e) -> double { return e < a.E ? (double)f[(int64_t)dof * a.E + e] : 0.0; };
+      for (int bi = a.cell_bptr[c]; bi < a.cell_bptr[c + 1]; ++bi) {
+        const int b = a.cell_blist[bi];
+        const int* bd = a.bdofs + (int64_t)b * a.BL;
+        const double* bm = a.bmass + (int64_t)b * a.BL * a.BL;
+        double sum = 0.0;
+        for (int i = 0; i < a.BL; ++i) {
+          const double v = at(bd[i], M) - at(bd[i], Nn);
+          double row = 0.0;
+          for (int j = 0; j < a.BL; ++j) row += bm[i * a.BL + j] * (at(bd[j], A) - at(bd[j], B));
+          sum += v * row;
+        }
+        acc += a.weights[w] * a.bcoef[(int64_t)w * a.Nb + b] * sum;
+      }
+    }
+    float* o = a.out + (int64_t)dl * a.C + c;
+    *o = (float)((double)*o - acc);
+  }
+}
+
+// y += x elementwise.
+__global__ void add_kernel(double* y, const double* x, int64_t count) {
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
+       idx += (int64_t)gridDim.x * blockDim.x)
+    y[idx] += x[idx];
+}
+
+// x[w][row][e] = 0 for the listed rows (the fixed dofs of a Dirichlet boundary).
+__global__ void zero_rows_kernel(double* x, const int* rows, int count, int W, int N, int E) {
+  const int64_t total = (int64_t)W * count * E;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(idx % E);
+    const int64_t rest = idx / E;
+    const int i = (int)(rest % count), w = (int)(rest / count);
+    x[((int64_t)w * N + rows[i]) * E + e] = 0.0;
+  }
 }
 
 // current[w][n][e] = sum_f pairs[f][e] phi[w][n][f] (the "current" fields of normal_vjp,

@@ -1,8 +1,9 @@
 /*
  * adtlert_b200 -- C ABI of the B200 (sm_100a) forward-and-sensitivity path of AD-TLERT's
- * 2.5D DC-resistivity operator.
+ * 2.5D and 3D DC-resistivity operators.
  *
- * One plan per discretization (mesh + survey + wavenumber quadrature). Geometry, element
+ * One plan per discretization (mesh + survey + wavenumber quadrature; a 3D operator is one
+ * system per model: a single wavenumber 0 of weight 1). Geometry, element
  * templates, the sparse pattern, its assembly routing and the block elimination schedule of
  * the direct solver are host arrays copied into the plan once; the plan owns that device
  * memory. Every other array crossing this boundary is a caller-owned DEVICE pointer (for
@@ -46,9 +47,11 @@ typedef enum {
 typedef struct adt_plan adt_plan;
 typedef void* adt_stream; /* a cudaStream_t; NULL is the legacy default stream */
 
-/* Discretization of one 2.5D operator (host arrays, copied by adt_plan_create).
+/* Discretization of one operator (host arrays, copied by adt_plan_create).
  * Mirrors adtlert/forward/discretization.py:128-156 (Discretization) plus the quadrature of
- * adtlert/forward/integration.py:32-49 and the survey slots of adtlert/survey/core.py:77-85. */
+ * adtlert/forward/integration.py:32-49 and the survey slots of adtlert/survey/core.py:77-85;
+ * for 3D, the tetrahedral templates, Robin faces and Dirichlet dofs of
+ * adtlert/forward/ert3d.py:224-351. */
 typedef struct {
   int32_t dof_count;              /* N */
   int32_t dim;                    /* coordinate dimension of dof_coordinates (2 or 3) */
@@ -77,6 +80,8 @@ typedef struct {
   const int32_t* abmn;            /* D*4 electrode slots, E = remote */
   const int32_t* source_cell_ptr; /* E+1: model cells averaged for each source resistivity */
   const int32_t* source_cells;    /* source_cell_ptr[E] model cell ids */
+  int32_t fixed_count;            /* Dirichlet dofs: identity rows, no couplings, zero fields */
+  const int32_t* fixed_dofs;      /* fixed_count dof ids (NULL when fixed_count is 0) */
 } adt_problem;
 
 /* Summary of a plan (sizes, elimination schedule). */
@@ -102,6 +107,15 @@ adt_status adt_last_error(const adt_plan* plan, char* buffer, size_t size);
  * conductivity-independent right-hand side A(1) u_p on the device.
  * Replaces: _unit_primary / _reference_rhs (adtlert/forward/ert2p5d.py:418-478). */
 adt_status adt_set_primary(adt_plan* plan, const double* primary, adt_stream stream);
+
+/* Conductivity-independent right-hand sides of fields solved without a primary-field
+ * correction (the 3D operator): rhs = A(1) unit_primary + direct, zeroed on the fixed dofs;
+ * both host arrays are [W][E][N] in original dof order and either may be NULL. Afterwards
+ * adt_solve_fields solves A(sigma) u = rhs and writes u (sigma only selects the factorization).
+ * Replaces: _build_unit_operator, _build_source_rhs and _build_receiver_rhs
+ * (adtlert/forward/ert3d.py:353-413). */
+adt_status adt_set_static_rhs(adt_plan* plan, const double* unit_primary, const double* direct,
+                              adt_stream stream);
 
 /* Assembles A_w(sigma_s) for S models (S*W systems) into factor slot `slot` and factorizes
  * them. Replaces: _assemble (ert2p5d.py:275-314) + BatchedSolver.solve factorization
@@ -164,12 +178,23 @@ adt_status adt_jvp(adt_plan* plan, int32_t slot, const float* fields, const doub
                    adt_stream stream);
 
 /* Normal-convention products without a solve. normal_vjp: cotangent [D] -> [model_cells]
- * (before parameter aggregation); normal_jvp: direction [model_cells] -> [D].
- * Replaces: normal_vjp / normal_jvp (ert2p5d.py:892-943). */
+ * (before parameter aggregation); normal_jvp: direction [model_cells] -> [D]. With `robin`
+ * the operator derivative includes the mixed-boundary terms: for a 3D operator, whose
+ * receiver fields are field columns of their own, these are the exact vjp and jvp.
+ * Replaces: normal_vjp / normal_jvp (ert2p5d.py:892-943); vjp, jvp, normal_vjp and
+ * normal_jvp of ERTForward3D (adtlert/forward/ert3d.py:736-865). */
 adt_status adt_normal_vjp(adt_plan* plan, const float* fields, const double* cotangent,
-                          float* gradient, adt_stream stream);
+                          int32_t robin, float* gradient, adt_stream stream);
 adt_status adt_normal_jvp(adt_plan* plan, const float* fields, const float* direction,
-                          double* out, adt_stream stream);
+                          int32_t robin, double* out, adt_stream stream);
+
+/* Adds the mixed-boundary derivative to Jacobian rows [row_begin, row_begin+row_count) of one
+ * model written by adt_normal_jacobian (same layout, discretization-cell columns):
+ * J[d][c] += -sum_w w_w sum_{b owned by c} alpha_wb (u_M - u_N)_b^T Mb_b (u_A - u_B)_b.
+ * Replaces: the Robin templates of ERTForward3D.jacobian(include_robin_boundary_derivative=True)
+ * (adtlert/forward/ert3d.py:867-927). */
+adt_status adt_boundary_jacobian(adt_plan* plan, const float* fields, int32_t row_begin,
+                                 int32_t row_count, float* jacobian, adt_stream stream);
 
 /* adt_measure without any device allocation: no counterpart in the reference. For callers that
  * may not call cudaMalloc while running (GPU memory fully reserved by another allocator, or

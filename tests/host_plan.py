@@ -65,7 +65,7 @@ class HostPlan:
             for name in ("perm", "iperm", "level_begin", "csr_ptr", "csr_col", "csr_row", "contrib_ptr", "contrib",
                          "task_rows", "pulls", "features", "fscale", "pair_ptr", "pair_list", "rcv_dofs", "rcv_w",
                          "rdof_ptr", "rdof_rcv", "rdof_dof", "rdof_w", "cdofs", "bd", "cell_bptr", "cell_blist",
-                         "model_ptr", "model_list", "k2"):
+                         "model_ptr", "model_list", "k2", "bowners", "fixed"):
                 size = lib.shim_table(handle, name.encode(), None)
                 out = np.empty(size, dtype=_TYPES.get(name, np.int32))
                 lib.shim_table(handle, name.encode(), out.ctypes.data_as(ctypes.c_void_p))
@@ -80,7 +80,8 @@ class HostPlan:
             pass
 
 
-def replay_assembly(hp: HostPlan, sigma, stiffness, mass, bmass, bcoef, bcells, k2_w, robin=True) -> np.ndarray:
+def replay_assembly(hp: HostPlan, sigma, stiffness, mass, bmass, bcoef, bcells, k2_w, robin=True,
+                    identity=True) -> np.ndarray:
     """CSR values of one system as assemble_kernel computes them (solver order)."""
 
     C, K2 = stiffness.shape[0], stiffness.shape[1] * stiffness.shape[2]
@@ -90,7 +91,9 @@ def replay_assembly(hp: HostPlan, sigma, stiffness, mass, bmass, bcoef, bcells, 
     for slot in range(hp.nnz):
         acc = 0.0
         for code in hp.contrib[hp.contrib_ptr[slot]:hp.contrib_ptr[slot + 1]]:
-            if code < C * K2:
+            if code < 0:
+                acc += 1.0 if identity else 0.0
+            elif code < C * K2:
                 acc += sigma[code // K2] * (s_flat[code] + k2_w * m_flat[code])
             elif robin:
                 bc = code - C * K2
