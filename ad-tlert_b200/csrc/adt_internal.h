@@ -81,6 +81,10 @@ struct adt_plan {
   int nfixed = 0;
   int* owners = nullptr;        // cells owning boundary elements
   int nowners = 0;
+  // tiled solver (blocks wider than kMaxBlock): device work items, host ranges
+  bool tiled = false;
+  int* titems = nullptr;
+  std::vector<int> tranges, panel_ptr;
   // primary field
   double* primary = nullptr;    // [W][N][E] solver order
   double* refrhs = nullptr;     // [W][N][E]

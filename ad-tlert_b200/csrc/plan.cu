@@ -351,6 +351,10 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   ADT_UP(&p->rdof_w, hp.rdof_w);
   ADT_UP(&p->rdof_dof, hp.rdof_dof);
   ADT_UP(&p->fixed, hp.fixed);
+  ADT_UP(&p->titems, hp.titems);
+  p->tiled = hp.tiled;
+  p->tranges = hp.tranges;
+  p->panel_ptr = hp.panel_ptr;
   ADT_UP(&p->owners, hp.bowners);
   p->nfixed = (int)hp.fixed.size();
   p->nowners = (int)hp.bowners.size();
@@ -367,7 +371,7 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
                   p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
-                  p->fixed, p->owners};
+                  p->fixed, p->owners, p->titems};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& s : p->slots) {

@@ -97,6 +97,52 @@ int pseudo_peripheral(const std::vector<int>& ptr, const std::vector<int>& adj, 
   return root;
 }
 
+int tiles_of(int64_t m) { return (int)((m + kTile - 1) / kTile); }
+
+// Work items of the tiled solver from the task table (see HostPlan).
+void build_tile_items(HostPlan& hp, const std::vector<int64_t>& task_rows) {
+  const int L = hp.levels;
+  std::vector<std::vector<int>> groups(3 * L);
+  std::vector<std::vector<std::vector<int>>> panels(L);
+  for (int l = 0; l < L; ++l) {
+    int max_panels = 0;
+    for (int t = hp.level_begin[l]; t < hp.level_begin[l + 1]; ++t)
+      max_panels = std::max(max_panels, tiles_of(task_rows[(int64_t)t * T_FIELDS + T_MJ]));
+    panels[l].assign(max_panels, {});
+    for (int t = hp.level_begin[l]; t < hp.level_begin[l + 1]; ++t) {
+      const int64_t* row = &task_rows[(int64_t)t * T_FIELDS];
+      const int mj = (int)row[T_MJ];
+      const int tj = tiles_of(mj);
+      const int tp = row[T_P] >= 0 ? tiles_of(row[T_MP]) : 0;
+      const int tq = row[T_Q] >= 0 ? tiles_of(row[T_MQ]) : 0;
+      for (int r0 = 0; r0 < mj; r0 += kScatterRows)
+        groups[l].insert(groups[l].end(), {t, r0, std::min(kScatterRows, mj - r0), 0});
+      for (int qi = 0; qi < tq && tp > 0; ++qi)
+        for (int pi = 0; pi < tp; ++pi) groups[L + l].insert(groups[L + l].end(), {t, qi, pi, 0});
+      for (int i = 0; i < tj; ++i) groups[2 * L + l].insert(groups[2 * L + l].end(), {t, i, 0, 0});
+      for (int k = 0; k < tj; ++k) {
+        auto& g = panels[l][k];
+        for (int i = k; i < tj; ++i) g.insert(g.end(), {t, SEG_J, i, 0});
+        for (int i = 0; i < tp; ++i) g.insert(g.end(), {t, SEG_P, i, 0});
+        for (int i = 0; i < tq; ++i) g.insert(g.end(), {t, SEG_Q, i, 0});
+      }
+    }
+  }
+  hp.titems.clear();
+  hp.tranges.clear();
+  auto add_range = [&](const std::vector<int>& items) {
+    hp.tranges.push_back((int)(hp.titems.size() / 4));
+    hp.titems.insert(hp.titems.end(), items.begin(), items.end());
+    hp.tranges.push_back((int)(hp.titems.size() / 4));
+  };
+  for (auto& g : groups) add_range(g);
+  hp.panel_ptr.assign(1, 0);
+  for (int l = 0; l < L; ++l) {
+    for (auto& g : panels[l]) add_range(g);
+    hp.panel_ptr.push_back(hp.panel_ptr.back() + (int)panels[l].size());
+  }
+}
+
 }  // namespace
 
 adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err) {
@@ -209,20 +255,21 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
     }
     const bool ok = width <= kMaxBlock;
     const bool best_ok = best_width > 0 && best_width <= kMaxBlock;
-    if (best.empty() || (ok && !best_ok) || (ok == best_ok && (ok ? cost < best_cost : width < best_width))) {
+    if (best.empty() || (ok && !best_ok) || (ok == best_ok && cost < best_cost)) {
       best = lv;
       best_cost = cost;
       best_width = width;
     }
   }
-  if (best_width > kMaxBlock) {
+  if (best_width > kMaxTiledBlock) {
     char msg[256];
     std::snprintf(msg, sizeof msg,
                   "the narrowest level-set ordering has %d dofs per level; the solver accepts at most %d",
-                  best_width, kMaxBlock);
+                  best_width, kMaxTiledBlock);
     err = msg;
     return ADT_INVALID_ARG;
   }
+  hp.tiled = best_width > kMaxBlock;
   hp.nb = (int)best.size();
   hp.max_m = best_width;
   std::vector<int> bm(hp.nb), boff(hp.nb + 1, 0);
@@ -383,6 +430,8 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
     }
     task_rows[t * T_FIELDS + T_PULL1] = (int64_t)pulls.size() / P_FIELDS;
   }
+
+  if (hp.tiled) build_tile_items(hp, task_rows);
 
   // ---- per-cell template factors (features of the sensitivity Gram) ----
   std::vector<std::vector<double>> svals(C), svecs(C), mvals(C), mvecs(C);

@@ -11,7 +11,10 @@
 
 namespace adt {
 
-constexpr int kMaxBlock = 64;  // largest elimination block the solver kernels accept
+constexpr int kMaxBlock = 64;  // largest block of the shared-memory solver kernels
+constexpr int kMaxTiledBlock = 4096;  // largest block of the tiled (global-memory) solver
+constexpr int kTile = 64;       // tile edge of the tiled solver
+constexpr int kScatterRows = 32;  // block rows per scatter item of the tiled solver
 constexpr int kUnitCode = -1;  // assembly contribution of constant 1 (a fixed dof's diagonal)
 
 // Fields of one elimination task (one row of the int64 task table).
@@ -22,6 +25,9 @@ enum TaskField : int {
   T_FILL, T_PULL0, T_PULL1,
   T_FIELDS
 };
+// Row segments of a tiled elimination: the eliminated block j and its chain neighbours p, q.
+enum TileSegment : int { SEG_J = 0, SEG_P = 1, SEG_Q = 2 };
+
 // Fields of one pull (a Schur-complement contribution of an earlier elimination).
 enum PullField : int { P_TYPE = 0, P_OFF, P_ME, P_EOFF, P_FIELDS };
 
@@ -41,6 +47,12 @@ struct HostPlan {
   std::vector<double> k2;
   std::vector<int> bowners;  // cells owning at least one boundary element, ascending
   std::vector<int> fixed;    // fixed dofs in solver order, ascending
+  // tiled solver (blocks wider than kMaxBlock): work items of 4 ints and [begin, end) ranges.
+  // Range r: scatter items of level r (task, row0, rows, -); r = L + l: fill tiles of level l
+  // (task, qi, pi, -); r = 2L + l: row tiles of the eliminated blocks of level l (task, i, -, -);
+  // r = 3L + panel_ptr[l] + k: panel k of level l (task, segment, tile row, -).
+  bool tiled = false;
+  std::vector<int> titems, tranges, panel_ptr;
 };
 
 // Validates `pr` and builds every host array of its plan; on failure returns the status and

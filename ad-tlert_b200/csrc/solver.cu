@@ -535,6 +535,472 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
   }
 }
 
+// ============================================================================================
+// Tiled solver for blocks wider than kMaxBlock. The same elimination (same storage of L_j, U_p,
+// V_q and fills) runs on 64 x 64 tiles in global memory, several launches per level:
+//   scatter   D_j (lower), [A[j,p]] -> U_p, [A[q,j]] -> V_q from the CSR values or earlier fills
+//   panel k   (a) update: tile (i, k) of the stacked rows [j; p; q] -= sum_{c < 64k} row_i(c)
+//                 row_k(c) (and, for rows of j, the Schur pulls of earlier eliminations); the
+//                 item of the diagonal tile (k, k) then factors it (no other item of the launch
+//                 reads it: they read columns < 64k and write their own tiles);
+//             (b) triangular solve of every tile below the diagonal with L_kk. Rows p and q of
+//                 the stacked factor are U_p^T and V_q.
+//   fill      A[q,p] = -V_q U_p
+// A block's pulls and its own left-looking columns are summed in fixed order (bitwise
+// repeatable). Solves: forward = pull update of b_j, then a left-looking substitution per
+// (task, 64-column strip); backward = coupling update, then the transposed substitution.
+// ============================================================================================
+constexpr int kTT = kSolverThreads;  // threads of the tiled kernels (16 x 16 micro-tile grid)
+constexpr int kKC = 16;              // reduction depth staged per step
+constexpr int kTLD = kTile + 1;      // leading dimension of the shared tiles
+
+// Element (a, c) of a strided operand: base[a * rs + c * cs].
+struct Operand {
+  const double* base;
+  int64_t rs, cs;
+};
+
+__device__ __forceinline__ Operand operand(const double* base, int64_t rs, int64_t cs) {
+  Operand o;
+  o.base = base;
+  o.rs = rs;
+  o.cs = cs;
+  return o;
+}
+
+template <int N>
+__device__ __forceinline__ void async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Stage depth chunk [c0, c0 + kKC) of rows [0, rows) of `op` as tile[c][a] (zero outside).
+__device__ __forceinline__ void stage(double* tile, const Operand& op, int rows, int depth, int c0) {
+  const bool depth_fast = op.cs == 1;
+  for (int idx = threadIdx.x; idx < kKC * kTile; idx += blockDim.x) {
+    const int a = depth_fast ? idx / kKC : idx % kTile;
+    const int c = depth_fast ? idx % kKC : idx / kTile;
+    double* dst = tile + c * kTLD + a;
+    if (a < rows && c0 + c < depth) async_copy8(dst, op.base + a * op.rs + (int64_t)(c0 + c) * op.cs);
+    else *dst = 0.0;
+  }
+}
+
+// acc[r][s] += sum_{c < depth} A(ty + 16 r, c) B(tx + 16 s, c) for A rows < ra, B rows < rb.
+// `sm` holds 4 * kKC * kTLD doubles; entered and left by all threads (ends with a barrier).
+__device__ void gemm_nt(double (&acc)[4][4], const Operand& A, int ra, const Operand& B, int rb,
+                        int depth, double* sm) {
+  if (depth <= 0) return;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int chunks = (depth + kKC - 1) / kKC;
+  auto a_tile = [&](int b) { return sm + b * 2 * kKC * kTLD; };
+  auto b_tile = [&](int b) { return sm + b * 2 * kKC * kTLD + kKC * kTLD; };
+  stage(a_tile(0), A, ra, depth, 0);
+  stage(b_tile(0), B, rb, depth, 0);
+  async_commit();
+  for (int ch = 0; ch < chunks; ++ch) {
+    if (ch + 1 < chunks) {
+      stage(a_tile((ch + 1) & 1), A, ra, depth, (ch + 1) * kKC);
+      stage(b_tile((ch + 1) & 1), B, rb, depth, (ch + 1) * kKC);
+      async_commit();
+      async_wait<1>();
+    } else {
+      async_wait<0>();
+    }
+    __syncthreads();
+    const double* at = a_tile(ch & 1);
+    const double* bt = b_tile(ch & 1);
+#pragma unroll 4
+    for (int c = 0; c < kKC; ++c) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) a[r] = at[c * kTLD + ty + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) b[q] = bt[c * kTLD + tx + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void zero_acc(double (&acc)[4][4]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+}
+
+// C(a, b) = C(a, b) - acc (subtract) or -acc (store) for a < rows, b < cols (and b <= a when
+// `lower`), C(a, b) at c[a * rs + b * cs].
+__device__ __forceinline__ void put_acc(const double (&acc)[4][4], double* c, int64_t rs, int64_t cs,
+                                        int rows, int cols, bool subtract, bool lower) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int a = ty + 16 * r;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int b = tx + 16 * q;
+      if (a < rows && b < cols && (!lower || b <= a)) {
+        double* dst = c + a * rs + b * cs;
+        *dst = subtract ? *dst - acc[r][q] : -acc[r][q];
+      }
+    }
+  }
+}
+
+struct TaskView {
+  int mj, offj, p, mp, offp, q, mq, offq;
+  int64_t loff, uoff, voff, fill, linkp, linkq, pull0, pull1;
+  __device__ explicit TaskView(const int64_t* t) {
+    mj = (int)t[T_MJ];
+    offj = (int)t[T_OFFJ];
+    loff = t[T_LOFF];
+    p = (int)t[T_P];
+    mp = p >= 0 ? (int)t[T_MP] : 0;
+    offp = (int)t[T_OFFP];
+    uoff = t[T_UOFF];
+    linkp = t[T_LINKP];
+    q = (int)t[T_Q];
+    mq = q >= 0 ? (int)t[T_MQ] : 0;
+    offq = (int)t[T_OFFQ];
+    voff = t[T_VOFF];
+    linkq = t[T_LINKQ];
+    fill = t[T_FILL];
+    pull0 = t[T_PULL0];
+    pull1 = t[T_PULL1];
+  }
+  // element (r, c) of segment `seg` of the stacked factor: rows of L_j, U_p^T or V_q
+  __device__ Operand segment(double* f, int seg, int r, int c) const {
+    if (seg == SEG_J) return operand(f + loff + (int64_t)r * mj + c, mj, 1);
+    if (seg == SEG_P) return operand(f + uoff + (int64_t)c * mp + r, 1, mp);
+    return operand(f + voff + (int64_t)r * mj + c, mj, 1);
+  }
+  __device__ int rows(int seg) const { return seg == SEG_J ? mj : (seg == SEG_P ? mp : mq); }
+};
+
+__global__ void __launch_bounds__(kTT)
+tiled_scatter_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
+                     const int* __restrict__ csr_ptr, const int* __restrict__ csr_row,
+                     const int* __restrict__ csr_col, int nnz, const double* __restrict__ values,
+                     double* __restrict__ factors, int64_t stride) {
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  const int r0 = it[1], rows = it[2];
+  const double* val = values + (int64_t)blockIdx.y * nnz;
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  const bool p_csr = v.p >= 0 && v.linkp < 0, q_csr = v.q >= 0 && v.linkq < 0;
+  for (int64_t i = threadIdx.x; i < (int64_t)rows * v.mj; i += blockDim.x)
+    f[v.loff + (int64_t)r0 * v.mj + i] = 0.0;
+  for (int64_t i = threadIdx.x; i < (int64_t)rows * v.mp; i += blockDim.x)
+    f[v.uoff + (int64_t)r0 * v.mp + i] = p_csr ? 0.0 : f[v.linkp + (int64_t)r0 * v.mp + i];
+  for (int64_t i = threadIdx.x; i < (int64_t)rows * v.mq; i += blockDim.x) {
+    const int qr = (int)(i / rows), r = r0 + (int)(i - (int64_t)qr * rows);
+    f[v.voff + (int64_t)qr * v.mj + r] = q_csr ? 0.0 : f[v.linkq + (int64_t)qr * v.mj + r];
+  }
+  __syncthreads();
+  const int s0 = csr_ptr[v.offj + r0], s1 = csr_ptr[v.offj + r0 + rows];
+  for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+    const int r = csr_row[s] - v.offj, c = csr_col[s];
+    if (c >= v.offj && c < v.offj + v.mj) {
+      if (c - v.offj <= r) f[v.loff + (int64_t)r * v.mj + (c - v.offj)] = val[s];
+    } else if (p_csr && c >= v.offp && c < v.offp + v.mp) {
+      f[v.uoff + (int64_t)r * v.mp + (c - v.offp)] = val[s];
+    } else if (q_csr && c >= v.offq && c < v.offq + v.mq) {
+      f[v.voff + (int64_t)(c - v.offq) * v.mj + r] = val[s];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTT)
+tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
+                    const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride) {
+  extern __shared__ double sm[];
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  const int seg = it[1], i = it[2];
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  const int ni = min(kTile, v.rows(seg) - kTile * i), mk = min(kTile, v.mj - kTile * k);
+  double acc[4][4];
+  zero_acc(acc);
+  if (k > 0)
+    gemm_nt(acc, v.segment(f, seg, kTile * i, 0), ni, v.segment(f, SEG_J, kTile * k, 0), mk, kTile * k, sm);
+  if (seg == SEG_J) {
+    for (int64_t u = v.pull0; u < v.pull1; ++u) {
+      const int64_t* pl = pulls + u * P_FIELDS;
+      const int me = (int)pl[P_ME];
+      const double* x = f + pl[P_OFF];
+      if (pl[P_TYPE] == 0)  // U_e (me x mj): (U^T U)[a][b] = sum_r U[r][a] U[r][b]
+        gemm_nt(acc, operand(x + kTile * i, 1, v.mj), ni, operand(x + kTile * k, 1, v.mj), mk, me, sm);
+      else  // V_e (mj x me): (V V^T)[a][b] = sum_r V[a][r] V[b][r]
+        gemm_nt(acc, operand(x + (int64_t)kTile * i * me, me, 1), ni,
+                operand(x + (int64_t)kTile * k * me, me, 1), mk, me, sm);
+    }
+  }
+  const Operand c = v.segment(f, seg, kTile * i, kTile * k);
+  const bool diagonal = seg == SEG_J && i == k;
+  put_acc(acc, const_cast<double*>(c.base), c.rs, c.cs, ni, mk, true, diagonal);
+  if (!diagonal) return;
+  // factor the updated diagonal tile in shared memory (after the staging buffers' last use)
+  double* dm = sm + 4 * kKC * kTLD;
+  double* rinv = dm + kTile * kTLD;
+  double* diag = const_cast<double*>(c.base);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
+    const int r = idx / mk, col = idx - r * mk;
+    dm[r * kTLD + col] = diag[(int64_t)r * v.mj + col];
+  }
+  __syncthreads();
+  cholesky<kTLD>(dm, mk, rinv);
+  for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
+    const int r = idx / mk, col = idx - r * mk;
+    diag[(int64_t)r * v.mj + col] = dm[r * kTLD + col];
+  }
+}
+
+__global__ void __launch_bounds__(kTT)
+tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
+                    double* __restrict__ factors, int64_t stride) {
+  extern __shared__ double sm[];
+  double* dm = sm;                // diagonal tile -> L_kk
+  double* tt = dm + kTile * kTLD; // transposed tile below
+  double* rinv = tt + kTile * kTLD;
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  const int seg = it[1], i = it[2];
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  if (seg == SEG_J && i == k) return;  // factored by the update launch
+  const int mk = min(kTile, v.mj - kTile * k);
+  const double* diag = f + v.loff + (int64_t)kTile * k * v.mj + kTile * k;
+  for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
+    const int r = idx / mk, c = idx - r * mk;
+    dm[r * kTLD + c] = diag[(int64_t)r * v.mj + c];
+  }
+  __syncthreads();
+  reciprocal_diagonal(dm, kTLD, mk, rinv);
+  const int ni = min(kTile, v.rows(seg) - kTile * i);
+  const Operand t = v.segment(f, seg, kTile * i, kTile * k);
+  double* tb = const_cast<double*>(t.base);
+  for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
+    const int a = idx / mk, c = idx - a * mk;
+    tt[c * kTLD + a] = tb[a * t.rs + c * t.cs];
+  }
+  __syncthreads();
+  lower_solve(dm, kTLD, rinv, tt, kTLD, mk, ni);  // L_kk X^T = T^T
+  for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
+    const int a = idx / mk, c = idx - a * mk;
+    tb[a * t.rs + c * t.cs] = tt[c * kTLD + a];
+  }
+}
+
+__global__ void __launch_bounds__(kTT)
+tiled_fill_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
+                  double* __restrict__ factors, int64_t stride) {
+  extern __shared__ double sm[];
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  const int qi = it[1], pi = it[2];
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  const int nq = min(kTile, v.mq - kTile * qi), np = min(kTile, v.mp - kTile * pi);
+  double acc[4][4];
+  zero_acc(acc);
+  // A[q,p] = -V_q U_p: sum_c V[a][c] U[c][b]
+  gemm_nt(acc, operand(f + v.voff + (int64_t)kTile * qi * v.mj, v.mj, 1), nq,
+          operand(f + v.uoff + kTile * pi, 1, v.mp), np, v.mj, sm);
+  put_acc(acc, f + v.fill + (int64_t)kTile * qi * v.mp + kTile * pi, v.mp, 1, nq, np, false, false);
+}
+
+// b_j -= sum of the pulls (U_e^T y_e or V_e y_e) on tile rows i of j, columns [c0, c0 + 64).
+__global__ void __launch_bounds__(kTT)
+tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
+                            const int64_t* __restrict__ pulls, const double* __restrict__ factors,
+                            int64_t stride, double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
+  extern __shared__ double sm[];
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  if (v.pull0 == v.pull1) return;
+  const int i = it[1];
+  const double* f = factors + (int64_t)blockIdx.y * stride;
+  double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
+  const int c0 = blockIdx.z * kTile, nc = min(kTile, nrhs - c0);
+  const int ni = min(kTile, v.mj - kTile * i);
+  double acc[4][4];
+  zero_acc(acc);
+  for (int64_t u = v.pull0; u < v.pull1; ++u) {
+    const int64_t* pl = pulls + u * P_FIELDS;
+    const int me = (int)pl[P_ME];
+    const double* m = f + pl[P_OFF];
+    const Operand y = operand(x + pl[P_EOFF] * nrhs + c0, 1, nrhs);
+    if (pl[P_TYPE] == 0) gemm_nt(acc, operand(m + kTile * i, 1, v.mj), ni, y, nc, me, sm);
+    else gemm_nt(acc, operand(m + (int64_t)kTile * i * me, me, 1), ni, y, nc, me, sm);
+  }
+  put_acc(acc, x + (int64_t)(v.offj + kTile * i) * nrhs + c0, nrhs, 1, ni, nc, true, false);
+}
+
+// y_j -= U_p x_p + V_q^T x_q on tile rows i of j, columns [c0, c0 + 64).
+__global__ void __launch_bounds__(kTT)
+tiled_backward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
+                             const double* __restrict__ factors, int64_t stride,
+                             double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
+  extern __shared__ double sm[];
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  if (v.p < 0 && v.q < 0) return;
+  const int i = it[1];
+  const double* f = factors + (int64_t)blockIdx.y * stride;
+  double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
+  const int c0 = blockIdx.z * kTile, nc = min(kTile, nrhs - c0);
+  const int ni = min(kTile, v.mj - kTile * i);
+  double acc[4][4];
+  zero_acc(acc);
+  if (v.p >= 0)
+    gemm_nt(acc, operand(f + v.uoff + (int64_t)kTile * i * v.mp, v.mp, 1), ni,
+            operand(x + (int64_t)v.offp * nrhs + c0, 1, nrhs), nc, v.mp, sm);
+  if (v.q >= 0)
+    gemm_nt(acc, operand(f + v.voff + kTile * i, 1, v.mj), ni,
+            operand(x + (int64_t)v.offq * nrhs + c0, 1, nrhs), nc, v.mq, sm);
+  put_acc(acc, x + (int64_t)(v.offj + kTile * i) * nrhs + c0, nrhs, 1, ni, nc, true, false);
+}
+
+// Substitutions with L_j on columns [c0, c0 + 64) of one task: forward (L y = b, left-looking
+// over tile rows), and backward (L^T x = y) when `backward`; `forward` may be off.
+__global__ void __launch_bounds__(kTT)
+tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
+                        const double* __restrict__ factors, int64_t stride, double* __restrict__ rhs,
+                        int64_t rhs_stride, int nrhs, int forward, int backward) {
+  extern __shared__ double sm[];
+  double* dm = sm;                 // L_rr
+  double* bt = dm + kTile * kTLD;  // right-hand-side rows of tile r
+  double* rinv = bt + kTile * kTLD;
+  double* gs = rinv + kTile;       // gemm staging
+  const TaskView v(tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS);
+  const double* f = factors + (int64_t)blockIdx.y * stride;
+  const double* l = f + v.loff;
+  double* x = rhs + (int64_t)blockIdx.y * rhs_stride + (int64_t)v.offj * nrhs;
+  const int c0 = blockIdx.z * kTile, nc = min(kTile, nrhs - c0);
+  const int tiles = (v.mj + kTile - 1) / kTile;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  auto load_diag = [&](int r, int nr) {
+    for (int idx = threadIdx.x; idx < nr * nr; idx += blockDim.x) {
+      const int a = idx / nr, b = idx - a * nr;
+      dm[a * kTLD + b] = l[(int64_t)(kTile * r + a) * v.mj + kTile * r + b];
+    }
+  };
+  // bt = x rows of tile r minus acc
+  auto load_rows = [&](int r, int nr, const double (&acc)[4][4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int a = ty + 16 * i;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int b = tx + 16 * q;
+        if (a < nr && b < nc) bt[a * kTLD + b] = x[(int64_t)(kTile * r + a) * nrhs + c0 + b] - acc[i][q];
+      }
+    }
+  };
+  auto store_rows = [&](int r, int nr) {
+    for (int idx = threadIdx.x; idx < nr * nc; idx += blockDim.x) {
+      const int a = idx / nc, b = idx - a * nc;
+      x[(int64_t)(kTile * r + a) * nrhs + c0 + b] = bt[a * kTLD + b];
+    }
+  };
+  double acc[4][4];
+  if (forward) {
+    for (int r = 0; r < tiles; ++r) {
+      const int nr = min(kTile, v.mj - kTile * r);
+      zero_acc(acc);
+      gemm_nt(acc, operand(l + (int64_t)kTile * r * v.mj, v.mj, 1), nr, operand(x + c0, 1, nrhs), nc,
+              kTile * r, gs);
+      load_diag(r, nr);
+      load_rows(r, nr, acc);
+      __syncthreads();
+      reciprocal_diagonal(dm, kTLD, nr, rinv);
+      lower_solve(dm, kTLD, rinv, bt, kTLD, nr, nc);
+      store_rows(r, nr);
+      __syncthreads();
+    }
+  }
+  if (backward) {
+    for (int r = tiles - 1; r >= 0; --r) {
+      const int nr = min(kTile, v.mj - kTile * r);
+      const int below = kTile * (r + 1);
+      zero_acc(acc);
+      if (below < v.mj)  // sum_c L[below + c][64 r + a] x[below + c]
+        gemm_nt(acc, operand(l + (int64_t)below * v.mj + kTile * r, 1, v.mj), nr,
+                operand(x + (int64_t)below * nrhs + c0, 1, nrhs), nc, v.mj - below, gs);
+      load_diag(r, nr);
+      load_rows(r, nr, acc);
+      __syncthreads();
+      reciprocal_diagonal(dm, kTLD, nr, rinv);
+      upper_solve(dm, kTLD, rinv, bt, kTLD, nr, nc);
+      store_rows(r, nr);
+      __syncthreads();
+    }
+  }
+}
+
+constexpr size_t kGemmSmem = sizeof(double) * 4 * kKC * kTLD;
+constexpr size_t kUpdateSmem = kGemmSmem + sizeof(double) * (kTile * kTLD + kTile);
+constexpr size_t kFactorSmem = sizeof(double) * (2 * kTile * kTLD + kTile);
+constexpr size_t kSubstituteSmem = sizeof(double) * (2 * kTile * kTLD + kTile) + kGemmSmem;
+
+void configure_tiled() {
+  cudaFuncSetAttribute(tiled_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
+  cudaFuncSetAttribute(tiled_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
+  cudaFuncSetAttribute(tiled_substitute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubstituteSmem);
+}
+
+void factor_tiled(adt_plan* p, int systems, const double* values, double* factors, cudaStream_t s) {
+  const int L = p->levels;
+  auto range = [&](int r) { return std::make_pair(p->tranges[2 * r], p->tranges[2 * r + 1]); };
+  for (int level = 0; level < L; ++level) {
+    auto [b, e] = range(level);
+    tiled_scatter_kernel<<<dim3(e - b, systems), kTT, 0, s>>>(p->titems, b, p->tasks, p->csr_ptr, p->csr_row,
+                                                             p->csr_col, p->nnz, values, factors, p->factor_stride);
+    p->launches++;
+    for (int k = 0; k < p->panel_ptr[level + 1] - p->panel_ptr[level]; ++k) {
+      auto [pb, pe] = range(3 * L + p->panel_ptr[level] + k);
+      if (pe == pb) continue;
+      tiled_update_kernel<<<dim3(pe - pb, systems), kTT, kUpdateSmem, s>>>(p->titems, pb, k, p->tasks, p->pulls,
+                                                                         factors, p->factor_stride);
+      tiled_factor_kernel<<<dim3(pe - pb, systems), kTT, kFactorSmem, s>>>(p->titems, pb, k, p->tasks, factors,
+                                                                           p->factor_stride);
+      p->launches += 2;
+    }
+    auto [fb, fe] = range(L + level);
+    if (fe > fb) {
+      tiled_fill_kernel<<<dim3(fe - fb, systems), kTT, kGemmSmem, s>>>(p->titems, fb, p->tasks, factors,
+                                                                       p->factor_stride);
+      p->launches++;
+    }
+  }
+}
+
+void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s) {
+  const int L = p->levels;
+  const int64_t rhs_stride = (int64_t)p->N * nrhs;
+  const int strips = (nrhs + kTile - 1) / kTile;
+  auto range = [&](int r) { return std::make_pair(p->tranges[2 * r], p->tranges[2 * r + 1]); };
+  for (int level = 0; level < L; ++level) {
+    auto [b, e] = range(2 * L + level);
+    tiled_forward_update_kernel<<<dim3(e - b, systems, strips), kTT, kGemmSmem, s>>>(
+        p->titems, b, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
+    tiled_substitute_kernel<<<dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s>>>(
+        t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 1, level == L - 1);
+    p->launches += 2;
+  }
+  for (int level = L - 2; level >= 0; --level) {
+    auto [b, e] = range(2 * L + level);
+    tiled_backward_update_kernel<<<dim3(e - b, systems, strips), kTT, kGemmSmem, s>>>(
+        p->titems, b, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
+    tiled_substitute_kernel<<<dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s>>>(
+        t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 0, 1);
+    p->launches += 2;
+  }
+}
+
 template <int MAXM>
 void configure() {
   cudaFuncSetAttribute(factor_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem<MAXM>());
@@ -578,6 +1044,7 @@ void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, dou
 
 // Opt the solver kernels in to their dynamic shared memory on the current device.
 void configure_solver_kernels() {
+  configure_tiled();
   configure<32>();
   configure<48>();
   configure<64>();
@@ -585,7 +1052,8 @@ void configure_solver_kernels() {
 
 adt_status factorize_systems(adt_plan* p, int systems, const double* values, double* factors,
                              cudaStream_t s) {
-  if (p->max_m <= 32) factor_levels<32>(p, systems, values, factors, s);
+  if (p->tiled) factor_tiled(p, systems, values, factors, s);
+  else if (p->max_m <= 32) factor_levels<32>(p, systems, values, factors, s);
   else if (p->max_m <= 48) factor_levels<48>(p, systems, values, factors, s);
   else factor_levels<64>(p, systems, values, factors, s);
   return check_launch(p, "factorization");
@@ -593,7 +1061,8 @@ adt_status factorize_systems(adt_plan* p, int systems, const double* values, dou
 
 adt_status solve_systems(adt_plan* p, int systems, int nrhs, const double* factors,
                          double* rhs, cudaStream_t s) {
-  if (p->max_m <= 32) solve_levels<32>(p, systems, nrhs, factors, rhs, s);
+  if (p->tiled) solve_tiled(p, systems, nrhs, factors, rhs, s);
+  else if (p->max_m <= 32) solve_levels<32>(p, systems, nrhs, factors, rhs, s);
   else if (p->max_m <= 48) solve_levels<48>(p, systems, nrhs, factors, rhs, s);
   else solve_levels<64>(p, systems, nrhs, factors, rhs, s);
   return check_launch(p, "solve");

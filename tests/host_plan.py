@@ -60,12 +60,13 @@ class HostPlan:
         self.error = lib.shim_error(handle).decode()
         self._lib, self._h = lib, handle
         if self.status == 0:
-            for name in ("N", "nnz", "nb", "max_m", "levels", "RS", "R", "rdofs", "factor_stride", "contributions"):
+            for name in ("N", "nnz", "nb", "max_m", "levels", "RS", "R", "rdofs", "factor_stride", "contributions",
+                         "tiled"):
                 setattr(self, name, int(lib.shim_scalar(handle, name.encode())))
             for name in ("perm", "iperm", "level_begin", "csr_ptr", "csr_col", "csr_row", "contrib_ptr", "contrib",
                          "task_rows", "pulls", "features", "fscale", "pair_ptr", "pair_list", "rcv_dofs", "rcv_w",
                          "rdof_ptr", "rdof_rcv", "rdof_dof", "rdof_w", "cdofs", "bd", "cell_bptr", "cell_blist",
-                         "model_ptr", "model_list", "k2", "bowners", "fixed"):
+                         "model_ptr", "model_list", "k2", "bowners", "fixed", "titems", "tranges", "panel_ptr"):
                 size = lib.shim_table(handle, name.encode(), None)
                 out = np.empty(size, dtype=_TYPES.get(name, np.int32))
                 lib.shim_table(handle, name.encode(), out.ctypes.data_as(ctypes.c_void_p))
@@ -204,4 +205,223 @@ def replay_solve(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarray:
                 mq, offq = int(row[T_MQ]), int(row[T_OFFQ])
                 y -= block(int(row[T_VOFF]), mq, mj).T @ x[offq:offq + mq]
             x[offj:offj + mj] = sla.solve_triangular(block(int(row[T_LOFF]), mj, mj).T, y, lower=False)
+    return x
+
+
+# ---- tiled solver (blocks wider than 64) -------------------------------------------------------
+TILE = 64
+SEG_J, SEG_P, SEG_Q = range(3)
+
+
+def _strided(buf, base, rs, cs, rows, cols, what):
+    """rows x cols operand with element (a, c) at buf[base + a*rs + c*cs] (bounds-checked)."""
+
+    if rows <= 0 or cols <= 0:
+        return np.zeros((max(rows, 0), max(cols, 0)))
+    idx = base + np.arange(rows)[:, None] * rs + np.arange(cols)[None, :] * cs
+    assert idx.min() >= 0 and idx.max() < buf.size, f"{what}: access out of range"
+    return idx
+
+
+class _Launch:
+    """Read and write sets of the items of one launch: an item may write only what no other item
+    of the launch reads or writes (the kernels rely on it; nothing orders CTAs)."""
+
+    def __init__(self, name):
+        self.name, self.items = name, []
+
+    def item(self, reads, writes):
+        cat = lambda xs: np.unique(np.concatenate([np.ravel(x) for x in xs])) if xs else np.zeros(0, int)
+        self.items.append((cat(reads), cat(writes)))
+
+    def check(self):
+        owner = {}
+        for n, (_, writes) in enumerate(self.items):
+            for w in writes.tolist():
+                assert owner.setdefault(w, n) == n, f"{self.name}: two items write one entry"
+        for n, (reads, _) in enumerate(self.items):
+            for r in reads.tolist():
+                assert owner.get(r, n) == n, f"{self.name}: an item reads what another writes"
+
+
+class _Task:
+    def __init__(self, row):
+        self.mj, self.offj, self.loff = int(row[T_MJ]), int(row[T_OFFJ]), int(row[T_LOFF])
+        self.p = int(row[T_P])
+        self.mp = int(row[T_MP]) if self.p >= 0 else 0
+        self.offp, self.uoff, self.linkp = int(row[T_OFFP]), int(row[T_UOFF]), int(row[T_LINKP])
+        self.q = int(row[T_Q])
+        self.mq = int(row[T_MQ]) if self.q >= 0 else 0
+        self.offq, self.voff, self.linkq = int(row[T_OFFQ]), int(row[T_VOFF]), int(row[T_LINKQ])
+        self.fill, self.pull0, self.pull1 = int(row[T_FILL]), int(row[T_PULL0]), int(row[T_PULL1])
+
+    def segment(self, seg, r, c):
+        if seg == SEG_J:
+            return self.loff + r * self.mj + c, self.mj, 1
+        if seg == SEG_P:
+            return self.uoff + c * self.mp + r, 1, self.mp
+        return self.voff + r * self.mj + c, self.mj, 1
+
+    def rows(self, seg):
+        return (self.mj, self.mp, self.mq)[seg]
+
+
+def _items(hp, r):
+    b, e = hp.tranges[2 * r], hp.tranges[2 * r + 1]
+    return hp.titems.reshape(-1, 4)[b:e]
+
+
+def replay_factor_tiled(hp: HostPlan, values: np.ndarray) -> np.ndarray:
+    """Factor storage of one system as the tiled kernels write it (items, tiles and offsets as
+    the device indexes them)."""
+
+    f = np.full(hp.factor_stride, np.nan)
+    L = hp.levels
+    tasks = [_Task(r) for r in hp.tasks]
+    for level in range(L):
+        launch = _Launch("scatter")
+        for t, r0, rows, _ in _items(hp, level):
+            v = tasks[t]
+            writes = [_strided(f, v.loff + r0 * v.mj, v.mj, 1, rows, v.mj, "L rows")]
+            reads = []
+            if v.p >= 0:
+                writes.append(_strided(f, v.uoff + r0 * v.mp, v.mp, 1, rows, v.mp, "U rows"))
+                if v.linkp >= 0:
+                    reads.append(_strided(f, v.linkp + r0 * v.mp, v.mp, 1, rows, v.mp, "fill p"))
+            if v.q >= 0:
+                writes.append(_strided(f, v.voff + r0, 1, v.mj, rows, v.mq, "V cols"))
+                if v.linkq >= 0:
+                    reads.append(_strided(f, v.linkq + r0, 1, v.mj, rows, v.mq, "fill q"))
+            launch.item(reads, writes)
+        launch.check()
+        for t, r0, rows, _ in _items(hp, level):  # scatter
+            v = tasks[t]
+            f[_strided(f, v.loff + r0 * v.mj, v.mj, 1, rows, v.mj, "L rows")] = 0.0
+            if v.p >= 0:
+                dst = _strided(f, v.uoff + r0 * v.mp, v.mp, 1, rows, v.mp, "U rows")
+                f[dst] = 0.0 if v.linkp < 0 else f[_strided(f, v.linkp + r0 * v.mp, v.mp, 1, rows, v.mp, "fill p")]
+            if v.q >= 0:
+                dst = _strided(f, v.voff + r0, 1, v.mj, rows, v.mq, "V cols")
+                f[dst] = 0.0 if v.linkq < 0 else f[_strided(f, v.linkq + r0, 1, v.mj, rows, v.mq, "fill q")]
+            for s in range(hp.csr_ptr[v.offj + r0], hp.csr_ptr[v.offj + r0 + rows]):
+                r, c = hp.csr_row[s] - v.offj, hp.csr_col[s]
+                if v.offj <= c < v.offj + v.mj:
+                    if c - v.offj <= r:
+                        f[v.loff + r * v.mj + c - v.offj] = values[s]
+                elif v.p >= 0 and v.linkp < 0 and v.offp <= c < v.offp + v.mp:
+                    f[v.uoff + r * v.mp + c - v.offp] = values[s]
+                elif v.q >= 0 and v.linkq < 0 and v.offq <= c < v.offq + v.mq:
+                    f[v.voff + (c - v.offq) * v.mj + r] = values[s]
+        panels = hp.panel_ptr[level + 1] - hp.panel_ptr[level]
+        for k in range(panels):
+            items = _items(hp, 3 * L + hp.panel_ptr[level] + k)
+            launch = _Launch("update")
+            updates = []
+            for t, seg, i, _ in items:  # update launch: reads, then the item's own tile
+                v = tasks[t]
+                ni, mk = min(TILE, v.rows(seg) - TILE * i), min(TILE, v.mj - TILE * k)
+                assert ni > 0 and mk > 0
+                acc = np.zeros((ni, mk))
+                reads = []
+                if k > 0:
+                    ia = _strided(f, *v.segment(seg, TILE * i, 0), ni, TILE * k, "A rows")
+                    ib = _strided(f, *v.segment(SEG_J, TILE * k, 0), mk, TILE * k, "B rows")
+                    acc += f[ia] @ f[ib].T
+                    reads += [ia, ib]
+                if seg == SEG_J:
+                    for u in range(v.pull0, v.pull1):
+                        typ, off, me, _ = hp.pull_table[u]
+                        if typ == 0:
+                            ia = _strided(f, off + TILE * i, 1, v.mj, ni, me, "pull U")
+                            ib = _strided(f, off + TILE * k, 1, v.mj, mk, me, "pull U")
+                        else:
+                            ia = _strided(f, off + TILE * i * me, me, 1, ni, me, "pull V")
+                            ib = _strided(f, off + TILE * k * me, me, 1, mk, me, "pull V")
+                        acc += f[ia] @ f[ib].T
+                        reads += [ia, ib]
+                idx = _strided(f, *v.segment(seg, TILE * i, TILE * k), ni, mk, "C tile")
+                launch.item(reads, [idx])
+                updates.append((v, seg, i, idx, acc))
+            launch.check()
+            for v, seg, i, idx, acc in updates:
+                if seg == SEG_J and i == k:  # lower part, then the in-place Cholesky of the tile
+                    mask = np.tril(np.ones(acc.shape, bool))
+                    f[idx[mask]] -= acc[mask]
+                    f[idx] = np.linalg.cholesky(np.where(mask, f[idx], f[idx].T))
+                else:
+                    f[idx] -= acc
+            launch = _Launch("triangular solve")
+            solves = []
+            for t, seg, i, _ in items:
+                v = tasks[t]
+                if seg == SEG_J and i == k:
+                    continue
+                mk = min(TILE, v.mj - TILE * k)
+                didx = _strided(f, v.loff + TILE * k * v.mj + TILE * k, v.mj, 1, mk, mk, "diag")
+                ni = min(TILE, v.rows(seg) - TILE * i)
+                idx = _strided(f, *v.segment(seg, TILE * i, TILE * k), ni, mk, "tile")
+                launch.item([didx], [idx])
+                solves.append((didx, idx))
+            launch.check()
+            for didx, idx in solves:
+                f[idx] = sla.solve_triangular(np.tril(f[didx]), f[idx].T, lower=True).T
+        launch = _Launch("fill")
+        fills = []
+        for t, qi, pi, _ in _items(hp, L + level):
+            v = tasks[t]
+            nq, npp = min(TILE, v.mq - TILE * qi), min(TILE, v.mp - TILE * pi)
+            ia = _strided(f, v.voff + TILE * qi * v.mj, v.mj, 1, nq, v.mj, "fill V")
+            ib = _strided(f, v.uoff + TILE * pi, 1, v.mp, npp, v.mj, "fill U")
+            io = _strided(f, v.fill + TILE * qi * v.mp + TILE * pi, v.mp, 1, nq, npp, "fill")
+            launch.item([ia, ib], [io])
+            fills.append((ia, ib, io))
+        launch.check()
+        for ia, ib, io in fills:
+            f[io] = -(f[ia] @ f[ib].T)
+    return f
+
+
+def replay_solve_tiled(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+    """Forward and backward substitution of the tiled kernels on rhs [N][ncols] (solver order)."""
+
+    x = np.array(rhs, dtype=float)
+    L = hp.levels
+    tasks = [_Task(r) for r in hp.tasks]
+
+    def lj(v):
+        return f[_strided(f, v.loff, v.mj, 1, v.mj, v.mj, "L_j")]
+
+    for level in range(L):
+        for t, i, _, _ in _items(hp, 2 * L + level):
+            v = tasks[t]
+            ni = min(TILE, v.mj - TILE * i)
+            rows = slice(v.offj + TILE * i, v.offj + TILE * i + ni)
+            for u in range(v.pull0, v.pull1):
+                typ, off, me, eoff = hp.pull_table[u]
+                if typ == 0:
+                    a = f[_strided(f, off + TILE * i, 1, v.mj, ni, me, "pull U")]
+                else:
+                    a = f[_strided(f, off + TILE * i * me, me, 1, ni, me, "pull V")]
+                x[rows] -= a @ x[eoff:eoff + me]
+        for t in range(hp.level_begin[level], hp.level_begin[level + 1]):
+            v = tasks[t]
+            block = slice(v.offj, v.offj + v.mj)
+            x[block] = sla.solve_triangular(lj(v), x[block], lower=True)
+            if level == L - 1:
+                x[block] = sla.solve_triangular(lj(v).T, x[block], lower=False)
+    for level in range(L - 2, -1, -1):
+        for t, i, _, _ in _items(hp, 2 * L + level):
+            v = tasks[t]
+            ni = min(TILE, v.mj - TILE * i)
+            rows = slice(v.offj + TILE * i, v.offj + TILE * i + ni)
+            if v.p >= 0:
+                a = f[_strided(f, v.uoff + TILE * i * v.mp, v.mp, 1, ni, v.mp, "U_p")]
+                x[rows] -= a @ x[v.offp:v.offp + v.mp]
+            if v.q >= 0:
+                a = f[_strided(f, v.voff + TILE * i, 1, v.mj, ni, v.mq, "V_q")]
+                x[rows] -= a @ x[v.offq:v.offq + v.mq]
+        for t in range(hp.level_begin[level], hp.level_begin[level + 1]):
+            v = tasks[t]
+            block = slice(v.offj, v.offj + v.mj)
+            x[block] = sla.solve_triangular(lj(v).T, x[block], lower=False)
     return x
