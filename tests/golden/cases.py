@@ -65,6 +65,52 @@ def layered_model(nodes, cells, rng) -> np.ndarray:
     return 1.0 / rho
 
 
+def terrain_quads(nx: int = 30, nz: int = 12, dx: float = 2.0):
+    """Terrain-following quadrilateral strips (the reference's own terrain test geometry): top
+    row of nodes first, cells ``[top-left, top-right, bottom-right, bottom-left]``; the surface
+    rises with a slope of 0.03 plus a 0.05 sinusoidal ripple per column."""
+
+    x = np.arange(nx + 1) * dx
+    slope = 0.03 + 0.05 * np.sin(np.arange(nx))
+    z_top = np.concatenate(([0.0], np.cumsum(slope * dx)))
+    offsets = np.concatenate(([0.0], -np.cumsum(np.linspace(0.5, 2.0, nz))))
+    nodes = np.asarray([[xi, zt + off] for off in offsets for xi, zt in zip(x, z_top)])
+    width = nx + 1
+    cells = np.asarray([
+        [layer * width + c, layer * width + c + 1, (layer + 1) * width + c + 1, (layer + 1) * width + c]
+        for layer in range(nz) for c in range(nx)
+    ], dtype=np.int64)
+    return nodes, cells, np.arange(width)
+
+
+def terrain_triangles(nx: int = 36, nz: int = 10, dx: float = 1.5, seed: int = 21):
+    """Triangles on a jittered terrain-following grid (columns deliberately not aligned, so the
+    mesh is not a columnar strip mesh); surface elevation is a sum of three sinusoids."""
+
+    rng = np.random.default_rng(seed)
+    x0 = np.arange(nx + 1) * dx
+    depths = np.concatenate(([0.0], np.cumsum(np.linspace(0.6, 2.5, nz))))
+
+    def top(x):
+        return 1.2 * np.sin(x / 7.0) + 0.6 * np.sin(x / 3.1 + 1.0) + 0.3 * np.sin(x / 1.7 + 2.0)
+
+    nodes = []
+    for d in depths:
+        jitter = np.zeros(nx + 1)
+        jitter[1:-1] = rng.uniform(-0.2, 0.2, nx - 1) * dx
+        x = x0 + jitter
+        nodes += [[xi, top(xi) - d] for xi in x]
+    nodes = np.asarray(nodes)
+    width = nx + 1
+    cells = []
+    for k in range(nz):
+        for i in range(nx):
+            a, b = k * width + i, k * width + i + 1
+            c, d = (k + 1) * width + i + 1, (k + 1) * width + i
+            cells += [[a, d, b], [b, d, c]] if (i + k) % 2 == 0 else [[a, d, c], [a, c, b]]
+    return nodes, np.asarray(cells, dtype=np.int64), np.arange(width)
+
+
 CASES = {
     # Flat P1 triangles, dipole-dipole, exercised with every derivative.
     "tri_flat": {"mesh": "tri", "exact_jacobian": True, "parameters": True, "seed": 3},
@@ -72,12 +118,52 @@ CASES = {
     "quad_flat": {"mesh": "quad", "exact_jacobian": False, "parameters": False, "seed": 4},
     # Triangles with remote electrodes: pole-dipole (B remote) and dipole-pole (N remote).
     "tri_pole": {"mesh": "tri", "poles": True, "exact_jacobian": False, "parameters": False, "seed": 5},
+    # Terrain quadrilateral strips: H2-refined Q1 fields, serendipity-Q2 numerical primary field.
+    "quad_terrain": {"mesh": "terrain_quad", "exact_jacobian": True, "parameters": True, "seed": 6},
+    # The same geometry with numerical (FEM) geometric factors.
+    "quad_terrain_gf": {"mesh": "terrain_quad", "gf_mode": "numerical", "exact_jacobian": False,
+                        "parameters": False, "seed": 7},
+    # Unstructured-column terrain triangles: H2-refined P1 fields, P2 numerical primary field.
+    "tri_terrain": {"mesh": "terrain_tri", "exact_jacobian": False, "parameters": False, "seed": 8},
 }
+
+
+FLAT_CASES = [name for name, spec in CASES.items() if not spec["mesh"].startswith("terrain")]
+TERRAIN_CASES = [name for name, spec in CASES.items() if spec["mesh"].startswith("terrain")]
+
+
+def _terrain_inputs(spec: dict, rng) -> dict:
+    if spec["mesh"] == "terrain_quad":
+        nodes, cells, surface = terrain_quads()
+    else:
+        nodes, cells, surface = terrain_triangles()
+    electrodes = nodes[surface[2:-2:2]]
+    measurements = dipole_dipole(len(electrodes), 2, 4)
+    sigma = layered_model(nodes - np.asarray([0.0, nodes[:, 1].max()]), cells, rng)
+    return {
+        "nodes": nodes,
+        "cells": cells,
+        "surface_node_ids": surface,
+        "electrodes": electrodes,
+        "measurements": measurements,
+        "sigma": sigma,
+        "cotangent": rng.standard_normal(measurements.shape[0]),
+        "direction": rng.standard_normal(cells.shape[0]) * sigma * 1e-2,
+        "gf_mode": spec.get("gf_mode", "analytic"),
+    }
 
 
 def case_inputs(name: str) -> dict:
     spec = CASES[name]
     rng = np.random.default_rng(spec["seed"])
+    if spec["mesh"].startswith("terrain"):
+        out = _terrain_inputs(spec, rng)
+        if spec.get("parameters"):
+            ids = np.full(out["cells"].shape[0], -1, dtype=np.int64)
+            half = out["cells"].shape[0] // 2
+            ids[:half] = np.arange(half) // 3
+            out["parameter_ids"] = ids
+        return out
     xs = np.arange(0.0, 45.0 + 1e-9, 1.5)
     depths = np.concatenate(([0.0], np.cumsum(np.concatenate((np.full(4, 0.75), np.geomspace(1.0, 4.0, 5))))))
     nodes, cells = structured_section(xs, depths, triangles=spec["mesh"] == "tri")

@@ -93,9 +93,11 @@ def _run_2p5d(name: str, spec: dict, precision: str) -> dict:
     from adtlert.survey import Survey
 
     inputs = case_inputs(name)
-    mesh = Mesh.from_arrays(inputs["nodes"], inputs["cells"])
+    mesh = Mesh.from_arrays(inputs["nodes"], inputs["cells"], surface_node_ids=inputs.get("surface_node_ids"))
     survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
-    forward = e2.ERTForward2p5D.from_mesh_survey(mesh, survey)
+    forward = e2.ERTForward2p5D.from_mesh_survey(
+        mesh, survey, topographic_geometric_factor_mode=inputs.get("gf_mode", "analytic")
+    )
     dtype = forward.dtype
     sigma = torch.as_tensor(inputs["sigma"], dtype=dtype)
     cotangent = torch.as_tensor(inputs["cotangent"], dtype=dtype)
@@ -119,8 +121,11 @@ def _run_2p5d(name: str, spec: dict, precision: str) -> dict:
             torch.full((mesh.cell_count,), 0.01, dtype=dtype)
         ).numpy(),
     }
-    if precision == "float64":
+    if precision == "float64" and not forward.use_numerical_primary:
         out["total_fields"] = fields.numpy()
+    if forward.use_numerical_primary:
+        out["integrated_potentials"] = response.integrated_potentials.numpy()
+        out["discretization_nodes"] = np.asarray(forward.discretization.dof_nodes, dtype=np.float64)
     chunked = forward.jacobian(sigma, batch_size=5).numpy()
     assert np.allclose(chunked, out["jacobian"], rtol=1e-5, atol=1e-6 * np.abs(chunked).max())
     if spec.get("exact_jacobian"):

@@ -12,7 +12,7 @@ import pytest
 import torch
 
 from adtlert_b200 import ERTForward2p5D, Mesh, Survey, apparent_resistivity_autograd, synthetic
-from cases import CASES, case_inputs
+from cases import FLAT_CASES, case_inputs
 from conftest import ROOT, assert_close
 from oracle.ert2p5d import Oracle2p5D
 
@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-4  # float32 parity bar (max-norm relative)
 
 
-@pytest.fixture(scope="module", params=list(CASES))
+@pytest.fixture(scope="module", params=FLAT_CASES)
 def case(request):
     name = request.param
     inputs = case_inputs(name)

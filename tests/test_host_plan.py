@@ -11,7 +11,7 @@ import scipy.sparse.linalg as spl
 
 from adtlert_b200 import Mesh, Survey, synthetic
 from adtlert_b200.ert2p5d import build_problem
-from cases import CASES, case_inputs
+from cases import FLAT_CASES, case_inputs
 from conftest import assert_close
 from host_plan import HostPlan, replay_assembly, replay_factor, replay_solve
 from oracle.ert2p5d import Oracle2p5D
@@ -26,7 +26,7 @@ def _plan(nodes, cells, electrodes, measurements):
     return mesh, survey, problem, hp
 
 
-@pytest.fixture(scope="module", params=list(CASES))
+@pytest.fixture(scope="module", params=FLAT_CASES)
 def case(request):
     inputs = case_inputs(request.param)
     mesh, survey, problem, hp = _plan(inputs["nodes"], inputs["cells"], inputs["electrodes"], inputs["measurements"])

@@ -3,7 +3,7 @@
 import numpy as np
 import pytest
 
-from cases import CASES, case_inputs
+from cases import FLAT_CASES, case_inputs
 from conftest import ROOT, assert_close
 from oracle import baseline
 from oracle.ert2p5d import Oracle2p5D, inverse_cosine_weights, wavenumber_bounds
@@ -11,7 +11,7 @@ from oracle.ert2p5d import Oracle2p5D, inverse_cosine_weights, wavenumber_bounds
 GOLDEN = ROOT / "tests" / "golden"
 
 
-@pytest.fixture(scope="module", params=list(CASES))
+@pytest.fixture(scope="module", params=FLAT_CASES)
 def pinned(request):
     name = request.param
     inputs = case_inputs(name)
