@@ -1,4 +1,5 @@
-"""Host-side set-up of the 2.5D discretization: quadrature, element templates, boundary terms.
+"""Host-side set-up of the 2.5D discretizations: quadrature, P1/Q1/P2/serendipity element
+templates, boundary terms.
 
 All of this runs once per operator (float64 NumPy/SciPy); the per-model work is on the GPU.
 Formulas follow the reference's element math (cited per function).
@@ -83,6 +84,90 @@ def quad_templates(nodes: np.ndarray, cells: np.ndarray):
     stiffness = np.einsum("cqid,cqjd,cq->cij", grads, grads, wdet)
     mass = np.einsum("qi,qj,cq->cij", values, values, wdet)
     return stiffness, mass
+
+
+# Six-point degree-4 rule on the reference triangle (Dunavant's published rule; weights sum to
+# the reference area 1/2), as adtlert/fem/triangle.py:21-31 tabulates it.
+_DEGREE4_POINTS = np.array([
+    [0.445948490915965, 0.445948490915965], [0.445948490915965, 0.108103018168070],
+    [0.108103018168070, 0.445948490915965], [0.091576213509771, 0.091576213509771],
+    [0.091576213509771, 0.816847572980459], [0.816847572980459, 0.091576213509771],
+])
+_DEGREE4_WEIGHTS = np.array([0.1116907948390055] * 3 + [0.0549758718276610] * 3)
+
+
+def p2_triangle_templates(nodes: np.ndarray, cells: np.ndarray):
+    """Unit P2 stiffness and mass of 6-node triangles (vertices, then midpoints 01, 12, 20) with
+    the degree-4 rule (adtlert/fem/triangle.py:140-255)."""
+
+    pts, wts = _DEGREE4_POINTS, _DEGREE4_WEIGHTS
+    l2, l3 = pts[:, 0], pts[:, 1]
+    l1 = 1.0 - l2 - l3
+    values = np.stack((l1 * (2 * l1 - 1), l2 * (2 * l2 - 1), l3 * (2 * l3 - 1), 4 * l1 * l2, 4 * l2 * l3, 4 * l3 * l1), -1)
+    g1, g2, g3 = np.array([-1.0, -1.0]), np.array([1.0, 0.0]), np.array([0.0, 1.0])
+    L1, L2, L3 = (x[:, None] for x in (l1, l2, l3))
+    reference = np.stack((
+        (4 * L1 - 1) * g1, (4 * L2 - 1) * g2, (4 * L3 - 1) * g3,
+        4 * (L1 * g2 + L2 * g1), 4 * (L2 * g3 + L3 * g2), 4 * (L3 * g1 + L1 * g3),
+    ), axis=-2)  # (q, 6, 2)
+    p = nodes[cells[:, :3]]
+    jac = np.stack((p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), axis=-1)
+    area = 0.5 * np.abs(np.linalg.det(jac))
+    grads = np.einsum("eij,qnj->eqni", np.linalg.inv(jac).transpose(0, 2, 1), reference)
+    weights = 2.0 * area[:, None] * wts[None, :]
+    stiffness = np.einsum("eqid,eqjd,eq->eij", grads, grads, weights)
+    mass = np.einsum("qi,qj,eq->eij", values, values, weights)
+    return stiffness, mass
+
+
+def _serendipity(points: np.ndarray):
+    xi, eta = points[:, 0], points[:, 1]
+    values = np.stack((
+        -0.25 * (1 - xi) * (1 - eta) * (1 + xi + eta), -0.25 * (1 + xi) * (1 - eta) * (1 - xi + eta),
+        -0.25 * (1 + xi) * (1 + eta) * (1 - xi - eta), -0.25 * (1 - xi) * (1 + eta) * (1 + xi - eta),
+        0.5 * (1 - xi * xi) * (1 - eta), 0.5 * (1 + xi) * (1 - eta * eta),
+        0.5 * (1 - xi * xi) * (1 + eta), 0.5 * (1 - xi) * (1 - eta * eta),
+    ), axis=-1)
+    d_xi = np.stack((
+        0.25 * (1 - eta) * (2 * xi + eta), 0.25 * (1 - eta) * (2 * xi - eta),
+        0.25 * (1 + eta) * (2 * xi + eta), 0.25 * (1 + eta) * (2 * xi - eta),
+        -xi * (1 - eta), 0.5 * (1 - eta * eta), -xi * (1 + eta), -0.5 * (1 - eta * eta),
+    ), axis=-1)
+    d_eta = np.stack((
+        0.25 * (1 - xi) * (xi + 2 * eta), 0.25 * (1 + xi) * (-xi + 2 * eta),
+        0.25 * (1 + xi) * (xi + 2 * eta), 0.25 * (1 - xi) * (-xi + 2 * eta),
+        -0.5 * (1 - xi * xi), -(1 + xi) * eta, 0.5 * (1 - xi * xi), -(1 - xi) * eta,
+    ), axis=-1)
+    return values, np.stack((d_xi, d_eta), axis=-1)
+
+
+def serendipity_templates(nodes: np.ndarray, quads: np.ndarray):
+    """Unit 8-node serendipity stiffness and mass on bilinear quadrilateral geometry, 3x3 Gauss
+    rule (adtlert/forward/discretization.py:159-267, quadratic branch); ``quads`` are the 4
+    geometry corners."""
+
+    g, gw = np.polynomial.legendre.leggauss(3)
+    pts = np.asarray([[x, y] for y in g for x in g])
+    wts = np.asarray([wx * wy for wy in gw for wx in gw])
+    xi, eta = pts[:, 0], pts[:, 1]
+    geometry = 0.25 * np.stack(
+        (np.stack((-(1 - eta), 1 - eta, 1 + eta, -(1 + eta)), -1), np.stack((-(1 - xi), -(1 + xi), 1 + xi, 1 - xi), -1)),
+        axis=-1,
+    )  # (q, 4, 2)
+    values, reference = _serendipity(pts)
+    jac = np.einsum("cid,qia->cqda", nodes[quads], geometry)
+    grads = np.einsum("qia,cqab->cqib", reference, np.linalg.inv(jac))
+    wdet = np.abs(np.linalg.det(jac)) * wts
+    stiffness = np.einsum("cqid,cqjd,cq->cij", grads, grads, wdet)
+    mass = np.einsum("qi,qj,cq->cij", values, values, wdet)
+    return stiffness, mass
+
+
+def boundary_mass_p2(lengths: np.ndarray) -> np.ndarray:
+    """Quadratic edge mass L/30 [[4, 2, -1], [2, 16, 2], [-1, 2, 4]] for (end, midpoint, end)
+    dofs (adtlert/fem/boundary.py:37-40)."""
+
+    return lengths[:, None, None] * (np.array([[4.0, 2.0, -1.0], [2.0, 16.0, 2.0], [-1.0, 2.0, 4.0]]) / 30.0)[None]
 
 
 def boundary_mass(lengths: np.ndarray) -> np.ndarray:

@@ -1,4 +1,5 @@
-"""2D meshes and ABMN surveys with the metadata the 2.5D operator needs.
+"""2D meshes and ABMN surveys with the metadata the 2.5D operator needs, plus the mesh
+operations of the terrain discretizations (H2 refinement, columnar expansion, P2 topology).
 
 ``Mesh.from_arrays`` / ``Survey.from_arrays`` mirror the reference constructors
 (adtlert/mesh/core.py:576-630, adtlert/survey/core.py:34-61): same validation, same boundary
@@ -145,8 +146,146 @@ class Mesh:
     def is_flat_surface(self) -> bool:
         return bool(self.flat_surface)
 
+    @property
+    def cell_node_count(self) -> int:
+        return int(self.cells.shape[1])
+
+    @property
+    def is_triangle_mesh(self) -> bool:
+        return self.cell_node_count == 3
+
+    @property
+    def is_quadrilateral_mesh(self) -> bool:
+        return self.cell_node_count == 4
+
+    @property
+    def surface_nodes(self) -> np.ndarray:
+        return self.nodes[self.surface_node_ids]
+
     def locate_points(self, points, tol: float = 1e-4) -> tuple[np.ndarray, np.ndarray]:
         return locate_points(self.nodes, self.cells, _as_numpy(points, float), tol)
+
+    def _require_triangles(self, operation: str) -> None:
+        if not self.is_triangle_mesh:
+            raise ValueError(f"{operation} is currently implemented for triangle meshes only")
+
+    def refine_uniform(self) -> tuple[Mesh, np.ndarray]:
+        """Split every triangle into four through its edge midpoints (H2); returns the refined
+        mesh and the parent cell of each child (adtlert/mesh/core.py:326-337, 689-698)."""
+
+        self._require_triangles("uniform refinement")
+        points, midpoint, _ = edge_midpoint_builder(self.nodes)
+        cells, parents = [], []
+        for parent, (n0, n1, n2) in enumerate(self.cells.tolist()):
+            m01, m12, m20 = midpoint(n0, n1), midpoint(n1, n2), midpoint(n2, n0)
+            cells += [[n0, m01, m20], [n1, m12, m01], [n2, m20, m12], [m01, m12, m20]]
+            parents += [parent] * 4
+        surface = self.surface_node_ids.tolist()
+        refined_surface = [surface[0]]
+        for a, b in zip(surface[:-1], surface[1:]):
+            refined_surface += [midpoint(a, b), b]
+        refined = Mesh.from_arrays(np.asarray(points), np.asarray(cells), surface_node_ids=np.asarray(refined_surface))
+        return refined, np.asarray(parents, dtype=np.int64)
+
+    def expand_columnar_cells(self, tol: float = 1e-6) -> tuple[Mesh, np.ndarray] | None:
+        """Complete single-triangle terrain strips into triangulated quads, or ``None`` when the
+        mesh is not such a structure (adtlert/mesh/core.py:466-540, 723-736)."""
+
+        if not self.is_triangle_mesh:
+            return None
+        expanded = expand_columnar_triangles(self.nodes, self.cells, tol)
+        if expanded is None:
+            return None
+        nodes, cells, parents = expanded
+        return Mesh.from_arrays(nodes, cells, surface_node_ids=self.surface_node_ids), parents
+
+    def build_quadratic_topology(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Shared-edge P2 nodes, cells ``(v0, v1, v2, m01, m12, m20)`` and boundary edges
+        ``(a, b, m_ab)`` (adtlert/mesh/core.py:543-555, 738-744)."""
+
+        self._require_triangles("quadratic topology")
+        points, midpoint, _ = edge_midpoint_builder(self.nodes)
+        cells = [[n0, n1, n2, midpoint(n0, n1), midpoint(n1, n2), midpoint(n2, n0)] for n0, n1, n2 in self.cells.tolist()]
+        boundary = [[a, b, midpoint(a, b)] for a, b in self.boundary_edges.tolist()]
+        return np.asarray(points), np.asarray(cells, dtype=np.int64), np.asarray(boundary, dtype=np.int64)
+
+
+def edge_midpoint_builder(nodes):
+    """A growing node list and ``midpoint(a, b)``, which appends each edge's midpoint once
+    (adtlert/mesh/core.py:27-44)."""
+
+    points = [np.asarray(p, dtype=float) for p in np.asarray(nodes, dtype=float)]
+    index: dict[tuple[int, int], int] = {}
+
+    def midpoint(a: int, b: int) -> int:
+        key = (a, b) if a < b else (b, a)
+        if key not in index:
+            index[key] = len(points)
+            points.append(0.5 * (points[key[0]] + points[key[1]]))
+        return index[key]
+
+    return points, midpoint, index
+
+
+def _orient_ccw(nodes, triangle: list[int]) -> list[int]:
+    p0, p1, p2 = (np.asarray(nodes[n], dtype=float) for n in triangle)
+    e1, e2 = p1 - p0, p2 - p0
+    return triangle if e1[0] * e2[1] - e1[1] * e2[0] > 0.0 else [triangle[0], triangle[2], triangle[1]]
+
+
+def expand_columnar_triangles(nodes, cells, tol: float = 1e-6):
+    """For meshes whose cells each span two adjacent node columns (a node pair in one column,
+    one node in the next), add the missing half of every strip quad, creating a bottom node where
+    a column is one node short; ``None`` for any other mesh (adtlert/mesh/core.py:466-540)."""
+
+    nodes, cells = np.asarray(nodes, dtype=float), np.asarray(cells, dtype=np.int64)
+    if nodes.shape[0] == 0 or cells.shape[0] == 0:
+        return None
+    columns: list[list[int]] = []
+    for node in np.argsort(nodes[:, 0], kind="mergesort").tolist():
+        if columns and abs(nodes[node, 0] - nodes[columns[-1][0], 0]) <= tol:
+            columns[-1].append(node)
+        else:
+            columns.append([node])
+    sizes = [len(c) for c in columns]
+    if len(columns) < 10 or min(sizes) < 2 or max(sizes) - min(sizes) > 1:
+        return None
+    column_of = np.full(nodes.shape[0], -1, dtype=np.int64)
+    row_of = np.full(nodes.shape[0], -1, dtype=np.int64)
+    for column_id, column in enumerate(columns):
+        column.sort(key=lambda n: (-nodes[n, 1], nodes[n, 0]))
+        for row, node in enumerate(column):
+            column_of[node], row_of[node] = column_id, row
+    expanded_nodes = nodes.tolist()
+    expanded, parents = [], []
+    for parent, cell in enumerate(cells):
+        column_ids, rows = column_of[cell], row_of[cell]
+        unique, counts = np.unique(column_ids, return_counts=True)
+        if unique.shape[0] != 2 or unique[1] != unique[0] + 1 or sorted(counts.tolist()) != [1, 2]:
+            return None
+        pair_column, lone_column = int(unique[np.argmax(counts)]), int(unique[np.argmin(counts)])
+        pair = column_ids == pair_column
+        order = np.argsort(rows[pair])
+        pair_nodes, pair_rows = cell[pair][order], rows[pair][order]
+        if pair_rows[1] != pair_rows[0] + 1:
+            return None
+        lone_row = int(rows[~pair][0])
+        if lone_row not in pair_rows:
+            return None
+        missing_row = int(pair_rows[1] if lone_row == pair_rows[0] else pair_rows[0])
+        lone = columns[lone_column]
+        if missing_row >= len(lone):
+            if missing_row != len(lone) or len(lone) + 1 != max(sizes):
+                return None
+            depth = nodes[int(pair_nodes[1]), 1] - nodes[columns[pair_column][0], 1]
+            expanded_nodes.append([float(nodes[lone[0], 0]), float(nodes[lone[0], 1] + depth)])
+            lone.append(len(expanded_nodes) - 1)
+        missing = int(lone[missing_row])
+        if missing in cell.tolist():
+            return None
+        expanded += [cell.tolist(), _orient_ccw(expanded_nodes, [missing, int(pair_nodes[0]), int(pair_nodes[1])])]
+        parents += [parent, parent]
+    return np.asarray(expanded_nodes), np.asarray(expanded, dtype=np.int64), np.asarray(parents, dtype=np.int64)
 
 
 def locate_points(nodes, cells, points, tol: float = 1e-4) -> tuple[np.ndarray, np.ndarray]:
