@@ -26,6 +26,8 @@ SYMBOLS = (
     "adt_set_static_rhs",
     "adt_factorize",
     "adt_solve_fields",
+    "adt_solve",
+    "adt_factorize_wavenumbers",
     "adt_measure",
     "adt_integrated_potentials",
     "adt_normal_jacobian",
@@ -120,6 +122,8 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_set_static_rhs": (status, [_p, _p, _p, _p]),
         "adt_factorize": (status, [_p, _i32, _p, _i32, _p]),
         "adt_solve_fields": (status, [_p, _i32, _p, _i32, _p, _p]),
+        "adt_solve": (status, [_p, _i32, _i32, _i32, _p, _p]),
+        "adt_factorize_wavenumbers": (status, [_p, _i32, _p, _i32, _i32, _p]),
         "adt_measure": (status, [_p, _p, _i32, _p, _p, _p, _p]),
         "adt_integrated_potentials": (status, [_p, _p, _p, _p]),
         "adt_normal_jacobian": (status, [_p, _p, _i32, _i32, _p, _p]),

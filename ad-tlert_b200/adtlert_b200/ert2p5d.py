@@ -6,9 +6,12 @@ the CPU). Every wavenumber is solved with the secondary-field formulation
 
     A(sigma) u_s = A(1) u_p - A(sigma) (rho_src u_p),    u = u_s + rho_src u_p,
 
-with the analytic half-space primary field of each electrode. The host builds the element
-templates and boundary terms once; assembly, the batched direct solve, quadrature, the ABMN
-gathers and every derivative run as CUDA kernels on the caller's current stream.
+with the analytic half-space primary field of each electrode on flat surfaces. On terrain the
+fields live on an H2-refined auxiliary mesh and u_p is the numerical unit-conductivity potential
+of a quadratic auxiliary discretization (solved once on the GPU, optionally cached on disk);
+geometric factors may come from the same kind of solve. The host builds the element templates
+and boundary terms once; assembly, the batched direct solves, quadrature, the ABMN gathers and
+every derivative run as CUDA kernels on the caller's current stream.
 """
 
 from __future__ import annotations
@@ -16,7 +19,9 @@ from __future__ import annotations
 import contextlib
 import ctypes
 import hashlib
-from dataclasses import dataclass, field
+import os
+from dataclasses import dataclass
+from pathlib import Path
 
 import numpy as np
 import torch
@@ -31,6 +36,7 @@ from .fem import (
     triangle_templates,
     wavenumber_bounds,
 )
+from .discretization import Discretization, build_discretization, exact_node_indices
 from .field_cache import FieldCache, factorization_name, newest_batches_first
 from .geometry import Mesh, Survey, geometric_factors, locate_points
 from .inputs import (
@@ -58,29 +64,6 @@ class ForwardResponse:
     integrated_potentials: Tensor
     wavenumbers: Tensor
     weights: Tensor
-
-
-@dataclass(frozen=True)
-class Discretization:
-    """Element space of the operator (the input mesh for flat surfaces)."""
-
-    name: str
-    parent_cell_ids: np.ndarray
-    dof_nodes: np.ndarray
-    cell_dofs: np.ndarray
-    boundary_dofs: np.ndarray
-    boundary_cells: np.ndarray
-    stiffness: np.ndarray
-    mass: np.ndarray
-    boundary_mass: np.ndarray
-    boundary_geometries: np.ndarray
-    electrode_matrix: np.ndarray
-    nnz: int
-    spd: bool = True
-
-    @property
-    def dof_count(self) -> int:
-        return int(self.dof_nodes.shape[0])
 
 
 @dataclass
@@ -140,11 +123,12 @@ class ProblemArrays:
         h = _native.host_ptr
         return _native.Problem(
             dof_count=c["N"], dim=2, dof_coordinates=h(a["coords"]), cell_count=c["C"], local_dofs=c["K"],
-            cell_dofs=h(a["cell_dofs"]), stiffness=h(a["stiffness"]), mass=h(a["mass"]), parent_cells=None,
-            model_cell_count=c["C"], boundary_count=c["Nb"], boundary_local=2, boundary_dofs=h(a["bdofs"]),
-            boundary_cells=h(a["bcells"]), boundary_mass=h(a["bmass"]), boundary_coefficients=h(a["bcoef"]),
-            wavenumber_count=c["W"], wavenumbers=h(a["k"]), weights=h(a["w"]), electrode_count=c["E"],
-            receiver_width=c["K"], receiver_dofs=h(a["rdofs"]), receiver_weights=h(a["rw"]),
+            cell_dofs=h(a["cell_dofs"]), stiffness=h(a["stiffness"]), mass=h(a["mass"]),
+            parent_cells=h(a.get("parents")), model_cell_count=c.get("Cm", c["C"]), boundary_count=c["Nb"],
+            boundary_local=c.get("BL", 2), boundary_dofs=h(a["bdofs"]), boundary_cells=h(a["bcells"]),
+            boundary_mass=h(a["bmass"]), boundary_coefficients=h(a["bcoef"]), wavenumber_count=c["W"],
+            wavenumbers=h(a["k"]), weights=h(a["w"]), electrode_count=c["E"],
+            receiver_width=c.get("RW", c["K"]), receiver_dofs=h(a["rdofs"]), receiver_weights=h(a["rw"]),
             measurement_count=c["D"], abmn=h(a["abmn"]), source_cell_ptr=h(a["sptr"]), source_cells=h(a["scells"]),
         )
 
@@ -199,6 +183,74 @@ def build_problem(mesh: Mesh, survey: Survey, quadrature_order: int = 2) -> Prob
     return ProblemArrays(arrays, k, w, stiffness, mass, bmass, robin, electrode_matrix, source_nodes, cell_ids, counts)
 
 
+def source_cells(mesh: Mesh, survey: Survey):
+    """Source node of every electrode (an input-mesh node within 1e-2, else -1) and the model
+    cells whose conductivities set its source resistivity: the cells around that node, else the
+    containing cell (ert2p5d.py:185-193, 480-511). Returns (nodes, containing cells, ptr, cells)."""
+
+    positions = survey.electrode_positions[:, :2]
+    cell_ids, _ = locate_points(mesh.nodes, mesh.cells, positions)
+    distance = np.linalg.norm(mesh.nodes[None] - positions[:, None], axis=2)
+    nearest = np.argmin(distance, axis=1)
+    nodes = np.where(distance[np.arange(len(positions)), nearest] <= 1e-2, nearest, -1)
+    ptr, lists = [0], []
+    for e, node in enumerate(nodes):
+        around = np.flatnonzero((mesh.cells == node).any(axis=1)) if node >= 0 else np.asarray([cell_ids[e]])
+        lists.append(around)
+        ptr.append(ptr[-1] + len(around))
+    return nodes, cell_ids, np.asarray(ptr, dtype=np.int32), np.ascontiguousarray(np.concatenate(lists), dtype=np.int32)
+
+
+def space_problem(d: Discretization, mesh: Mesh, survey: Survey, k: np.ndarray, w: np.ndarray) -> ProblemArrays:
+    """Plan arrays of any discretization (terrain auxiliary spaces: parent cells, quadratic
+    elements, dense electrode rows turned into receiver lists)."""
+
+    rows = d.electrode_matrix
+    width = max(int(np.max(np.count_nonzero(rows, axis=1))), 1)
+    rdofs = np.full((rows.shape[0], width), -1, dtype=np.int32)
+    rw = np.zeros((rows.shape[0], width))
+    for e, row in enumerate(rows):
+        nz = np.flatnonzero(row)
+        rdofs[e, :len(nz)], rw[e, :len(nz)] = nz, row[nz]
+    src_nodes, src_cells, sptr, scells = source_cells(mesh, survey)
+    K, BL = d.cell_dofs.shape[1], d.boundary_dofs.shape[1]
+    arrays = {
+        "coords": np.ascontiguousarray(d.dof_nodes, dtype=np.float64),
+        "cell_dofs": np.ascontiguousarray(d.cell_dofs, dtype=np.int32),
+        "stiffness": np.ascontiguousarray(d.stiffness, dtype=np.float64),
+        "mass": np.ascontiguousarray(d.mass, dtype=np.float64),
+        "parents": np.ascontiguousarray(d.parent_cell_ids, dtype=np.int32),
+        "bdofs": np.ascontiguousarray(d.boundary_dofs, dtype=np.int32),
+        "bcells": np.ascontiguousarray(d.boundary_cells, dtype=np.int32),
+        "bmass": np.ascontiguousarray(d.boundary_mass, dtype=np.float64),
+        "bcoef": np.ascontiguousarray(d.boundary_geometries, dtype=np.float64),
+        "k": np.ascontiguousarray(k, dtype=np.float64),
+        "w": np.ascontiguousarray(w, dtype=np.float64),
+        "rdofs": rdofs,
+        "rw": rw,
+        "abmn": np.ascontiguousarray(survey.measurement_slots(), dtype=np.int32),
+        "sptr": sptr,
+        "scells": scells,
+    }
+    counts = {"N": d.dof_count, "C": len(d.cell_dofs), "Cm": mesh.cell_count, "K": K, "BL": BL, "RW": width,
+              "Nb": len(d.boundary_dofs), "W": len(k), "E": survey.electrode_count, "D": survey.measurement_count}
+    return ProblemArrays(arrays, k, w, d.stiffness, d.mass, d.boundary_mass, d.boundary_geometries,
+                         d.electrode_matrix, src_nodes, src_cells, counts)
+
+
+TERRAIN_CACHE_VERSION = "b200_terrain_unit_potentials_v1"
+
+
+def _terrain_cache_dir(value) -> Path | None:
+    """Folder of the terrain unit-potential cache: the argument, else ``ADTLERT_TERRAIN_CACHE_DIR``
+    (unset or empty: no disk cache) (adtlert/forward/ert2p5d.py:1135-1145)."""
+
+    if value is not None:
+        return Path(value).expanduser()
+    env = os.environ.get("ADTLERT_TERRAIN_CACHE_DIR", "").strip()
+    return Path(env).expanduser() if env else None
+
+
 def _to_host(tensor: Tensor) -> Tensor:
     """Device tensor -> CPU tensor in page-locked memory (torch's caching host allocator), so the
     copy runs at full link bandwidth."""
@@ -225,7 +277,8 @@ def _survey_arrays(survey) -> Survey:
 
 
 class ERTForward2p5D:
-    """2.5D ERT forward operator (flat surfaces, analytic primary field) on B200 kernels."""
+    """2.5D ERT forward operator (analytic primary field on flat surfaces, numerical primary
+    field on terrain) on B200 kernels."""
 
     def __init__(
         self,
@@ -250,12 +303,11 @@ class ERTForward2p5D:
         self.source_mesh, self.source_survey = mesh, survey
         self.mesh = _mesh_arrays(mesh)
         self.survey = _survey_arrays(survey)
-        if not self.mesh.is_flat_surface:
-            raise NotImplementedError("terrain surfaces (numerical primary field) are not supported by this build")
         self.numerical_h2_refined = bool(numerical_h2_refined)
         self.numerical_p2_refined = bool(numerical_p2_refined)
         self.topographic_geometric_factor_mode = gf_mode
-        self.terrain_cache_dir = terrain_cache_dir
+        self.terrain_cache_dir = _terrain_cache_dir(terrain_cache_dir)
+        self._terrain = not self.mesh.is_flat_surface
         self.normal_field_cache_max_entries = int(normal_field_cache_max_entries)
         self.series_batch_steps = int(series_batch_steps)
         self.device = torch.device("cuda", torch.cuda.current_device())
@@ -285,43 +337,158 @@ class ERTForward2p5D:
 
     # ------------------------------------------------------------------ set-up
     def _build(self, quadrature_order: int) -> None:
-        problem = build_problem(self.mesh, self.survey, quadrature_order)
+        mesh, survey = self.mesh, self.survey
+        E, D = survey.electrode_count, survey.measurement_count
+        if self._terrain:
+            k, w = inverse_cosine_weights(*wavenumber_bounds(survey.electrode_positions))
+            refine = self.numerical_h2_refined
+
+            def build(name, **options):
+                return build_discretization(name, mesh, survey, k, auxiliary=True, refine=refine,
+                                            quadrature_order=quadrature_order, **options)
+
+            self.discretization = build("primary")
+            self.primary_potential_discretization = build("primary_potential", quadratic=True)
+            self.geometric_discretization = None
+            if self.topographic_geometric_factor_mode == "numerical":
+                self.geometric_discretization = build("geometric", quadratic=self.numerical_p2_refined)
+            problem = space_problem(self.discretization, mesh, survey, k, w)
+        else:
+            problem = build_problem(mesh, survey, quadrature_order)
+            k, w = problem.wavenumbers, problem.weights
+            self.primary_potential_discretization = self.geometric_discretization = None
         self._problem = problem
-        k, w = problem.wavenumbers, problem.weights
         self.wavenumbers = torch.as_tensor(k, dtype=FLOAT_DTYPE)
         self.weights = torch.as_tensor(w, dtype=FLOAT_DTYPE)
         self.source_node_ids = torch.as_tensor(problem.source_nodes, dtype=torch.long)
         self.source_cell_ids = torch.as_tensor(problem.source_cells, dtype=torch.long)
-        mesh, survey = self.mesh, self.survey
-        nodes, cells = mesh.nodes, mesh.cells
-        E, N = survey.electrode_count, mesh.node_count
-        arrays = problem.arrays
-        problem = problem.struct()
-        plan = ctypes.c_void_p()
-        with torch.cuda.device(self.device):
-            _native.check(self._lib.adt_plan_create(ctypes.byref(problem), ctypes.byref(plan)), None, "adt_plan_create")
+        self.W, self.E, self.D, self.C = len(k), E, D, mesh.cell_count
+        plan, info, order = self._create_plan(problem)
         self._plan = plan
-        info = _native.PlanInfo()
-        self._lib.adt_plan_get_info(plan, ctypes.byref(info))
-        self.plan_info = {name: getattr(info, name) for name, _ in _native.PlanInfo._fields_}
-        order = np.empty(N, dtype=np.int32)
-        self._lib.adt_plan_dof_order(plan, _native.host_ptr(order))
+        self.plan_info = info
         self._dof_order = order
-        pa = self._problem
-        self.discretization = Discretization(
-            name="native", parent_cell_ids=np.arange(mesh.cell_count), dof_nodes=nodes, cell_dofs=cells,
-            boundary_dofs=mesh.boundary_edges, boundary_cells=mesh.boundary_edge_cells, stiffness=pa.stiffness,
-            mass=pa.mass, boundary_mass=pa.boundary_mass, boundary_geometries=pa.robin,
-            electrode_matrix=pa.electrode_matrix, nnz=int(info.nnz),
-        )
-        primary = np.ascontiguousarray(
-            analytic_primary(nodes, cells, survey.electrode_positions[:, :2], pa.source_nodes, k), dtype=np.float64
-        )
+        self.N = int(problem.counts["N"])
+        self.Cd = int(problem.counts["C"])
+        pa = problem
+        if not self._terrain:
+            self.discretization = Discretization(
+                name="native", geometry=mesh, parent_cell_ids=np.arange(mesh.cell_count), dof_nodes=mesh.nodes,
+                cell_dofs=mesh.cells, boundary_dofs=mesh.boundary_edges, stiffness=pa.stiffness, mass=pa.mass,
+                boundary_mass=pa.boundary_mass, boundary_geometries=pa.robin, electrode_matrix=pa.electrode_matrix,
+                spd=True,
+            )
+            primary = analytic_primary(mesh.nodes, mesh.cells, survey.electrode_positions[:, :2], pa.source_nodes, k)
+            self._geometric = torch.as_tensor(geometric_factors(survey.electrode_positions, survey.measurements),
+                                              dtype=FLOAT_DTYPE)
+        else:
+            potential = self.primary_potential_discretization
+            selection = exact_node_indices(potential.dof_nodes, self.discretization.dof_nodes)
+            primary = self._unit_potentials(potential)[..., selection]
+            self._geometric = None
+        primary = np.ascontiguousarray(primary, dtype=np.float64)
         with torch.cuda.device(self.device):
             _native.check(self._lib.adt_set_primary(plan, _native.host_ptr(primary), self._stream()), plan, "adt_set_primary")
-        self._geometric = torch.as_tensor(geometric_factors(survey.electrode_positions, survey.measurements), dtype=FLOAT_DTYPE)
-        self.W, self.E, self.N, self.D = len(k), E, N, survey.measurement_count
-        self.C = mesh.cell_count
+
+    def _create_plan(self, problem: ProblemArrays):
+        struct = problem.struct()
+        plan = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _native.check(self._lib.adt_plan_create(ctypes.byref(struct), ctypes.byref(plan)), None, "adt_plan_create")
+        info = _native.PlanInfo()
+        self._lib.adt_plan_get_info(plan, ctypes.byref(info))
+        order = np.empty(problem.counts["N"], dtype=np.int32)
+        self._lib.adt_plan_dof_order(plan, _native.host_ptr(order))
+        return plan, {name: getattr(info, name) for name, _ in _native.PlanInfo._fields_}, order
+
+    # ------------------------------------------------------------------ terrain set-up
+    def _disk_path(self, name: str, d: Discretization) -> Path | None:
+        if self.terrain_cache_dir is None:
+            return None
+        digest = hashlib.sha256()
+        for label, value in (("version", TERRAIN_CACHE_VERSION), ("name", name),
+                             ("options", (self.numerical_h2_refined, self.numerical_p2_refined,
+                                          self.topographic_geometric_factor_mode))):
+            digest.update(f"{label}={value!r};".encode())
+        for array in (self.mesh.nodes, self.mesh.cells, self.mesh.surface_node_ids, self.survey.electrode_positions,
+                      self.survey.measurements, self.wavenumbers, self.weights, d.parent_cell_ids, d.dof_nodes,
+                      d.cell_dofs, d.boundary_dofs, d.electrode_matrix, d.stiffness, d.mass, d.boundary_mass,
+                      d.boundary_geometries):
+            array = np.ascontiguousarray(np.asarray(array))
+            digest.update(f"{array.dtype}{array.shape}".encode())
+            digest.update(array.tobytes())
+        return self.terrain_cache_dir / f"{digest.hexdigest()}.npz"
+
+    def _unit_potentials(self, d: Discretization) -> np.ndarray:
+        """Unit-conductivity potentials (W, E, dofs) of every electrode on ``d``: A_w(1) u = Pel
+        for every wavenumber, float64, a few wavenumbers per factorization; cached per
+        discretization in memory and, with a cache folder, on disk (ert2p5d.py:349-416)."""
+
+        key = ("unit_potentials", d.name)
+        if key in self._cache:
+            return self._cache[key]
+        shape = (self.W, self.E, d.dof_count)
+        path = self._disk_path(f"{d.name}_unit_potentials", d)
+        value = None
+        if path is not None and path.exists():
+            with contextlib.suppress(Exception):
+                with np.load(path) as stored:
+                    value = stored["value"] if stored["value"].shape == shape else None
+        if value is None:
+            value = self._solve_unit_potentials(d)
+            if path is not None:
+                with contextlib.suppress(OSError):
+                    path.parent.mkdir(parents=True, exist_ok=True)
+                    tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp.npz")
+                    np.savez(tmp, value=value)
+                    tmp.replace(path)
+        self._cache[key] = value
+        return value
+
+    def _solve_unit_potentials(self, d: Discretization) -> np.ndarray:
+        problem = space_problem(d, self.mesh, self.survey, self.wavenumbers.double().numpy(),
+                                self.weights.double().numpy())
+        plan, info, order = self._create_plan(problem)
+        lib, N, E, W = self._lib, d.dof_count, self.E, self.W
+        try:
+            with torch.cuda.device(self.device):
+                stream = self._stream()
+                ones = torch.ones((1, self.C), dtype=torch.float32, device=self.device)
+                free, _ = torch.cuda.mem_get_info(self.device)
+                per_system = 8.0 * (info["factor_doubles_per_system"] + info["nnz"] + N * E)
+                chunk = int(max(1, min(W, 0.4 * free // max(per_system, 1.0))))
+                rows = torch.as_tensor(np.ascontiguousarray(d.electrode_matrix.T[order]), device=self.device)
+                out = np.empty((W, E, N))
+                for w0 in range(0, W, chunk):
+                    count = min(chunk, W - w0)
+                    _native.check(lib.adt_factorize_wavenumbers(plan, 0, _native.ptr(ones), w0, count, stream), plan,
+                                  "adt_factorize_wavenumbers")
+                    rhs = rows[None].repeat(count, 1, 1).contiguous()
+                    _native.check(lib.adt_solve(plan, 0, count, E, _native.ptr(rhs), stream), plan, "adt_solve")
+                    solved = rhs.cpu().numpy()  # (count, N solver order, E)
+                    out[w0:w0 + count][:, :, order] = solved.transpose(0, 2, 1)
+                if not np.all(np.isfinite(out)):
+                    raise FloatingPointError("unit potentials: non-finite values")
+                return out
+        finally:
+            torch.cuda.synchronize(self.device)
+            lib.adt_plan_destroy(plan)
+
+    def _numerical_geometric_factors(self) -> Tensor:
+        """1 / (normal transfer of the unit-conductivity potentials on the geometric
+        discretization) (ert2p5d.py:697-706)."""
+
+        d = self.geometric_discretization
+        potential = self.primary_potential_discretization
+        same = (d.dof_count == potential.dof_count and np.array_equal(d.cell_dofs, potential.cell_dofs)
+                and np.array_equal(d.dof_nodes, potential.dof_nodes))
+        units = self._unit_potentials(potential if same else d)
+        integrated = np.tensordot(self.weights.double().numpy(), units, axes=([0], [0]))  # (E, dofs)
+        table = np.zeros((self.E + 1, self.E + 1))
+        table[:self.E, :self.E] = integrated @ d.electrode_matrix.T
+        a, b, m, n = self.survey.measurement_slots().T
+        sources = table[a] - table[b]
+        rows = np.arange(self.D)
+        return torch.as_tensor(1.0 / (sources[rows, m] - sources[rows, n]), dtype=torch.float64)
 
     # ------------------------------------------------------------------ helpers
     def _stream(self):
@@ -329,15 +496,17 @@ class ERTForward2p5D:
 
     @property
     def dtype(self) -> torch.dtype:
-        return FLOAT_DTYPE
+        """Result precision: float64 on terrain (as the reference), ``FLOAT_DTYPE`` otherwise."""
+
+        return torch.float64 if self._terrain else FLOAT_DTYPE
 
     @property
     def use_numerical_primary(self) -> bool:
-        return False
+        return self.primary_potential_discretization is not None
 
     @property
     def use_numerical_geometric_factors(self) -> bool:
-        return False
+        return self.geometric_discretization is not None
 
     def kernel_launches(self) -> int:
         return int(self._lib.adt_kernel_launches(self._plan))
@@ -349,6 +518,12 @@ class ERTForward2p5D:
         return conductivity_series(conductivities, self.C)
 
     def _geometric_factors(self) -> Tensor:
+        if self._geometric is None:
+            if self.use_numerical_geometric_factors:
+                self._geometric = self._numerical_geometric_factors()
+            else:
+                self._geometric = torch.as_tensor(
+                    geometric_factors(self.survey.electrode_positions, self.survey.measurements), dtype=FLOAT_DTYPE)
         return self._geometric
 
     def _call(self, name: str, *args) -> None:
@@ -422,52 +597,62 @@ class ERTForward2p5D:
         integrated = torch.empty((self.E, self.N), dtype=torch.float32, device=self.device)
         self._call("adt_integrated_potentials", _native.ptr(fields.total), _native.ptr(integrated), self._stream())
         check_finite(integrated, "integrated potentials")
-        resistance = self._combine(normal.cpu(), reciprocal.cpu()).to(FLOAT_DTYPE)
+        resistance = self._combine(normal.cpu(), reciprocal.cpu()).to(self.dtype)
         current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
         if potentials is None:
             _, _, pot = self._transfers(fields.total[None], potentials=True)
             potentials = pot[0]
         return ForwardResponse(
-            apparent_resistivity=self._geometric * resistance / current,
+            apparent_resistivity=self._geometric_factors() * resistance / current,
             resistance=resistance,
-            electrode_potentials=potentials.cpu().to(FLOAT_DTYPE),
-            integrated_potentials=integrated.cpu(),
+            electrode_potentials=potentials.cpu().to(self.dtype),
+            integrated_potentials=integrated.cpu().to(self.dtype),
             wavenumbers=self.wavenumbers,
             weights=self.weights,
         )
 
     def resistance(self, conductivity) -> Tensor:
         _, normal, reciprocal = self._measure(conductivity)
-        return self._combine(normal.cpu(), reciprocal.cpu()).to(FLOAT_DTYPE)
+        return self._combine(normal.cpu(), reciprocal.cpu()).to(self.dtype)
 
     def apparent_resistivity_values(self, conductivity, currents=1.0) -> Tensor:
         current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
-        return self._geometric * self.resistance(conductivity) / current
+        return self._geometric_factors() * self.resistance(conductivity) / current
 
     def resistance_series(self, conductivities) -> Tensor:
         fields, _ = self._fields_series(self._series(conductivities))
         normal, reciprocal, _ = self._transfers(self._stack(fields))
-        return self._combine(normal.cpu(), reciprocal.cpu()).to(FLOAT_DTYPE)
+        return self._combine(normal.cpu(), reciprocal.cpu()).to(self.dtype)
 
     def apparent_resistivity_series(self, conductivities, currents=1.0) -> Tensor:
         current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
-        return self._geometric * self.resistance_series(conductivities) / current
+        resistance = self.resistance_series(conductivities)
+        if current.ndim == 1 and current.shape[0] == resistance.shape[0] and current.shape[0] != resistance.shape[1]:
+            current = current[:, None]
+        return self._geometric_factors() * resistance / current
 
     def prepare(self, conductivity=None, *, include_solver_state: bool = True) -> None:
-        """Populate solver and field caches before timed solves (the set-up is done at construction)."""
+        """Populate the geometric factors and, optionally, the solver and field caches before
+        timed solves (the rest of the set-up is done at construction)."""
 
+        self._geometric_factors()
         if include_solver_state:
             self._fields(torch.ones(self.C) if conductivity is None else conductivity)
 
     # ------------------------------------------------------------------ derivatives
-    def _columns(self, cell_parameter_ids=None, parameter_count=None):
-        """(key, columns, ptr, cells) of the aggregation into parameters, or None for identity."""
+    def _columns(self, cell_parameter_ids=None, parameter_count=None, discretization: bool = False):
+        """(key, columns, ptr, cells) of the aggregation of model cells (or, with
+        ``discretization``, of the discretization's cells through their parents) into parameters,
+        or None for the identity (ert2p5d.py:751-763)."""
 
         ids, count = parameter_targets(cell_parameter_ids, parameter_count, self.C)
-        if cell_parameter_ids is None:
+        refined = discretization and self.Cd != self.C
+        if cell_parameter_ids is None and not refined:
             return None
-        digest = hashlib.blake2b(ids.tobytes(), digest_size=16).digest()
-        key = ("columns", digest, count)
+        if refined:
+            ids = ids[self.discretization.parent_cell_ids]
+        digest = hashlib.blake2b(np.ascontiguousarray(ids).tobytes(), digest_size=16).digest()
+        key = ("columns", digest, count, len(ids))
         if key not in self._cache:
             active = np.flatnonzero(ids >= 0)
             order = active[np.argsort(ids[active], kind="stable")]
@@ -495,9 +680,10 @@ class ERTForward2p5D:
         return int(batch_size)
 
     def _jacobian_device(self, fields: _Fields, columns=None) -> Tensor:
-        """Normal-quadrupole Jacobian (D, C or P) on the device; every row in one launch."""
+        """Normal-quadrupole Jacobian (D, C or P) on the device; every row in one launch over the
+        discretization's cells, then summed into model cells or parameters."""
 
-        J = torch.empty((self.D, self.C), dtype=torch.float32, device=self.device)
+        J = torch.empty((self.D, self.Cd), dtype=torch.float32, device=self.device)
         self._call("adt_normal_jacobian", _native.ptr(fields.total), 0, self.D, _native.ptr(J), self._stream())
         return self._aggregate(J, columns)
 
@@ -508,7 +694,7 @@ class ERTForward2p5D:
         direct = normal_sensitivity and not include_robin_boundary_derivative
         batch = self._batch_size(batch_size, direct)
         if direct:
-            columns = self._columns(jacobian_cell_parameter_ids, jacobian_parameter_count)
+            columns = self._columns(jacobian_cell_parameter_ids, jacobian_parameter_count, discretization=True)
             jacobian = _to_host(self._jacobian_device(fields, columns))
         else:
             key = self._field_cache.key(self._sigma(conductivity))
@@ -521,7 +707,7 @@ class ERTForward2p5D:
                            start, count, int(include_robin_boundary_derivative), int(normal_sensitivity), _native.ptr(out), self._stream())
                 rows.append(out)
             jacobian = _to_host(torch.cat(rows))
-        return self._response(fields, normal, reciprocal, None, currents), jacobian
+        return self._response(fields, normal, reciprocal, None, currents), jacobian.to(self.dtype)
 
     def jacobian(self, conductivity, *, batch_size=None, include_robin_boundary_derivative: bool = False,
                  normal_sensitivity: bool = True) -> Tensor:
@@ -530,7 +716,7 @@ class ERTForward2p5D:
                                         normal_sensitivity=normal_sensitivity)[1]
 
     def jacobian_columnwise(self, conductivity) -> Tensor:
-        basis = torch.eye(self.C, dtype=FLOAT_DTYPE)
+        basis = torch.eye(self.C, dtype=self.dtype)
         return torch.stack([self.jvp(conductivity, column) for column in basis], dim=1)
 
     def vjp(self, conductivity, cotangent) -> Tensor:
@@ -553,7 +739,7 @@ class ERTForward2p5D:
                        _native.ptr(cot), len(batch), _native.ptr(grad), self._stream())
             for i, step in enumerate(batch):
                 gradients[step] = grad[i]
-        gradient = torch.stack([gradients[step] for step in range(len(fields))]).cpu()
+        gradient = torch.stack([gradients[step] for step in range(len(fields))]).cpu().to(self.dtype)
         check_finite(gradient, "conductivity gradient")
         return gradient
 
@@ -566,7 +752,7 @@ class ERTForward2p5D:
         self._call("adt_jvp", slot, _native.ptr(fields.total), _native.ptr(normal), _native.ptr(reciprocal),
                    _native.ptr(direction), _native.ptr(out), self._stream())
         check_finite(out, "tangent fields")
-        return out.cpu().to(FLOAT_DTYPE)
+        return out.cpu().to(self.dtype)
 
     def normal_vjp(self, conductivity, cotangent, *, cell_parameter_ids=None, parameter_count=None) -> Tensor:
         columns = self._columns(cell_parameter_ids, parameter_count)
@@ -574,7 +760,7 @@ class ERTForward2p5D:
         weights = measurement_vector(cotangent, self.D, torch.float64).to(self.device).contiguous()
         grad = torch.empty((1, self.C), dtype=torch.float32, device=self.device)
         self._call("adt_normal_vjp", _native.ptr(fields.total), _native.ptr(weights), 0, _native.ptr(grad), self._stream())
-        gradient = self._aggregate(grad, columns)[0].cpu()
+        gradient = self._aggregate(grad, columns)[0].cpu().to(self.dtype)
         check_finite(gradient, "normal sensitivity vjp")
         return gradient
 
@@ -591,7 +777,7 @@ class ERTForward2p5D:
         direction = cell_vector(delta_conductivity, self.C).to(self.device, torch.float32).contiguous()
         out = torch.empty(self.D, dtype=torch.float64, device=self.device)
         self._call("adt_normal_jvp", _native.ptr(fields.total), _native.ptr(direction), 0, _native.ptr(out), self._stream())
-        result = out.cpu().to(FLOAT_DTYPE)
+        result = out.cpu().to(self.dtype)
         check_finite(result, "normal sensitivity jvp")
         return result
 

@@ -19,7 +19,7 @@ __global__ void assemble_kernel(AssembleArgs a) {
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int t = (int)(idx / a.nnz), slot = (int)(idx - (int64_t)t * a.nnz);
-    const int w = t % a.W, s = t / a.W;
+    const int w = a.w0 + t % a.W, s = t / a.W;
     const float* sig = a.sigma + (int64_t)s * a.Cm;
     const double k2 = a.k2[w];
     const int volume = a.C * a.K2;

@@ -21,6 +21,7 @@ struct AssembleArgs {
   double* values;  // [systems][nnz]
   int systems, nnz, W, C, Cm, K2, BL2, Nb, robin;
   int identity;    // add the unit diagonal of fixed dofs (system matrices, not derivatives)
+  int w0;          // wavenumber of system 0 (systems cover wavenumbers w0 .. w0 + W - 1)
 };
 
 struct SpmmArgs {

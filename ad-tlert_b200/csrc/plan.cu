@@ -125,6 +125,7 @@ AssembleArgs assemble_args(adt_plan* p, const float* sigma, int systems, double*
   a.Nb = p->Nb;
   a.robin = robin ? 1 : 0;
   a.identity = identity ? 1 : 0;
+  a.w0 = 0;
   return a;
 }
 
@@ -552,6 +553,34 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
                                                                          p->N, p->E, systems, fields);
   p->launches++;
   return check_launch(p, "field solve");
+}
+
+adt_status adt_factorize_wavenumbers(adt_plan* p, int32_t slot, const float* sigma, int32_t w_begin,
+                                     int32_t w_count, adt_stream stream) {
+  if (!p || !sigma || w_begin < 0 || w_count <= 0 || w_begin + w_count > p->W)
+    return fail(p, ADT_INVALID_ARG, "invalid wavenumber range");
+  cudaStream_t s = (cudaStream_t)stream;
+  adt_status st = ensure_slot(p, slot, w_count);
+  if (st != ADT_OK) return st;
+  Slot& sl = p->slots[slot];
+  AssembleArgs a = assemble_args(p, sigma, w_count, sl.values, true, true);
+  a.W = w_count;
+  a.w0 = w_begin;
+  assemble_kernel<<<grid_for((int64_t)w_count * p->nnz), 256, 0, s>>>(a);
+  p->launches++;
+  st = factorize_systems(p, w_count, sl.values, sl.factors, s);
+  sl.systems = w_count;
+  return st;
+}
+
+adt_status adt_solve(adt_plan* p, int32_t slot, int32_t systems, int32_t nrhs, double* rhs,
+                     adt_stream stream) {
+  if (!p || !rhs || systems <= 0 || nrhs <= 0) return fail(p, ADT_INVALID_ARG, "invalid solve arguments");
+  if (slot < 0 || slot >= (int)p->slots.size() || p->slots[slot].systems < systems)
+    return fail(p, ADT_INVALID_ARG, "slot does not hold that many factorized systems");
+  const adt_status st = solve_systems(p, systems, nrhs, p->slots[slot].factors, rhs, (cudaStream_t)stream);
+  if (st != ADT_OK) return st;
+  return check_launch(p, "solve");
 }
 
 adt_status adt_measure(adt_plan* p, const float* fields, int32_t models, double* normal,

@@ -128,6 +128,21 @@ adt_status adt_factorize(adt_plan* plan, int32_t slot, const float* sigma, int32
 adt_status adt_solve_fields(adt_plan* plan, int32_t slot, const float* sigma, int32_t models,
                             float* fields, adt_stream stream);
 
+/* Assembles and factorizes the operators of wavenumbers [w_begin, w_begin + w_count) of one
+ * model into `slot` (system i is wavenumber w_begin + i), so that large discretizations can be
+ * factorized a few wavenumbers at a time. Replaces the per-batch assembly and factorization of
+ * _unit_potentials (adtlert/forward/ert2p5d.py:404-416). */
+adt_status adt_factorize_wavenumbers(adt_plan* plan, int32_t slot, const float* sigma,
+                                     int32_t w_begin, int32_t w_count, adt_stream stream);
+
+/* Solves A_s X = B in place with the factorization held in `slot` for its first `systems`
+ * systems (system s = model * W + w): rhs [systems][N][nrhs] float64 in solver dof order.
+ * Replaces the solve phase of BatchedSolver.solve (adtlert/forward/cudss.py:63-122), e.g. for
+ * the unit potentials of a terrain operator's auxiliary discretizations
+ * (adtlert/forward/ert2p5d.py:404-416). */
+adt_status adt_solve(adt_plan* plan, int32_t slot, int32_t systems, int32_t nrhs, double* rhs,
+                     adt_stream stream);
+
 /* Normal and reciprocal transfer resistances of S models (and, if not NULL, the E*E electrode
  * potentials per model). Replaces: _integrate + _normal_reciprocal (ert2p5d.py:560-589). */
 adt_status adt_measure(adt_plan* plan, const float* fields, int32_t models, double* normal,
