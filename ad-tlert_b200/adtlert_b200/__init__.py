@@ -17,6 +17,7 @@ from .fem import inverse_cosine_weights, wavenumber_bounds
 from .geometry import Mesh, Survey
 from .geometry3d import Mesh3D
 from .inputs import FLOAT_DTYPE
+from .modeling import log_response_and_jacobian
 
 __all__ = [
     "Discretization",
@@ -33,5 +34,6 @@ __all__ = [
     "Survey",
     "apparent_resistivity_autograd",
     "inverse_cosine_weights",
+    "log_response_and_jacobian",
     "wavenumber_bounds",
 ]

@@ -39,6 +39,7 @@ SYMBOLS = (
     "adt_normal_jvp",
     "adt_boundary_jacobian",
     "adt_measure_static",
+    "adt_scale_rows_columns",
     "adt_kernel_launches",
 )
 
@@ -135,6 +136,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_normal_jvp": (status, [_p, _p, _p, _i32, _p, _p]),
         "adt_boundary_jacobian": (status, [_p, _p, _i32, _i32, _p, _p]),
         "adt_measure_static": (status, [_p, _p, _i32, _p, _p, _p]),
+        "adt_scale_rows_columns": (status, [_p, _i32, _i32, _p, _p, _p]),
         "adt_kernel_launches": (_i64, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():

@@ -690,12 +690,24 @@ class ERTForward2p5D:
     def solve_with_jacobian(self, conductivity, currents=1.0, *, batch_size=None,
                             include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
                             jacobian_cell_parameter_ids=None, jacobian_parameter_count=None):
+        response, jacobian = self._solve_with_jacobian_device(
+            conductivity, currents, batch_size=batch_size,
+            include_robin_boundary_derivative=include_robin_boundary_derivative,
+            normal_sensitivity=normal_sensitivity, jacobian_cell_parameter_ids=jacobian_cell_parameter_ids,
+            jacobian_parameter_count=jacobian_parameter_count)
+        return response, _to_host(jacobian).to(self.dtype)
+
+    def _solve_with_jacobian_device(self, conductivity, currents=1.0, *, batch_size=None,
+                                    include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
+                                    jacobian_cell_parameter_ids=None, jacobian_parameter_count=None):
+        """The response (CPU) and the Jacobian still on the device (float32)."""
+
         fields, normal, reciprocal = self._measure(conductivity)
         direct = normal_sensitivity and not include_robin_boundary_derivative
         batch = self._batch_size(batch_size, direct)
         if direct:
             columns = self._columns(jacobian_cell_parameter_ids, jacobian_parameter_count, discretization=True)
-            jacobian = _to_host(self._jacobian_device(fields, columns))
+            jacobian = self._jacobian_device(fields, columns)
         else:
             key = self._field_cache.key(self._sigma(conductivity))
             slot = self._factorize(self._sigma(conductivity).to(self.device)[None].contiguous(), factorization_name([key]))
@@ -706,8 +718,8 @@ class ERTForward2p5D:
                 self._call("adt_adjoint_jacobian", slot, _native.ptr(fields.total), _native.ptr(normal), _native.ptr(reciprocal),
                            start, count, int(include_robin_boundary_derivative), int(normal_sensitivity), _native.ptr(out), self._stream())
                 rows.append(out)
-            jacobian = _to_host(torch.cat(rows))
-        return self._response(fields, normal, reciprocal, None, currents), jacobian.to(self.dtype)
+            jacobian = torch.cat(rows) if len(rows) > 1 else rows[0]
+        return self._response(fields, normal, reciprocal, None, currents), jacobian
 
     def jacobian(self, conductivity, *, batch_size=None, include_robin_boundary_derivative: bool = False,
                  normal_sensitivity: bool = True) -> Tensor:

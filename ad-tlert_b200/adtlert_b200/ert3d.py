@@ -530,14 +530,30 @@ class ERTForward3D:
                             include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
                             include_fields: bool = False, jacobian_cell_parameter_ids=None,
                             jacobian_parameter_count=None):
+        response, jacobian = self._solve_with_jacobian_device(
+            conductivity, currents, batch_size=batch_size,
+            include_robin_boundary_derivative=include_robin_boundary_derivative,
+            normal_sensitivity=normal_sensitivity, include_fields=include_fields,
+            jacobian_cell_parameter_ids=jacobian_cell_parameter_ids,
+            jacobian_parameter_count=jacobian_parameter_count)
+        result = _to_host(jacobian)
+        check_finite(result, "jacobian")
+        return response, result
+
+    def _solve_with_jacobian_device(self, conductivity, currents=1.0, *, batch_size=None,
+                                    include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
+                                    include_fields: bool = False, jacobian_cell_parameter_ids=None,
+                                    jacobian_parameter_count=None):
+        """The response (CPU) and the Jacobian still on the device (float32)."""
+
+        del normal_sensitivity
+        if batch_size is not None and int(batch_size) < 1:
+            raise ValueError("batch_size must be >= 1")
         sigma = self._sigma(conductivity)
-        response = self._response(self._fields(sigma), currents, include_fields=include_fields)
-        jacobian = self.jacobian(sigma, batch_size=batch_size,
-                                 include_robin_boundary_derivative=include_robin_boundary_derivative,
-                                 normal_sensitivity=normal_sensitivity,
-                                 jacobian_cell_parameter_ids=jacobian_cell_parameter_ids,
-                                 jacobian_parameter_count=jacobian_parameter_count)
-        return response, jacobian
+        fields = self._fields(sigma)
+        response = self._response(fields, currents, include_fields=include_fields)
+        columns = self._columns(jacobian_cell_parameter_ids, jacobian_parameter_count)
+        return response, self._jacobian_device(fields, include_robin_boundary_derivative, columns)
 
     def prepare(self, conductivity=None, *, include_solver_state: bool = True) -> None:
         self._geometric_factors()

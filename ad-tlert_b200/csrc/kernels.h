@@ -135,6 +135,8 @@ cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s);
 __global__ void cell_gradient_kernel(CellGradientArgs a);
 __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a);
 __global__ void add_kernel(double* y, const double* x, int64_t count);
+__global__ void scale_rows_columns_kernel(float* values, int rows, int columns, const double* row_scale,
+                                          const double* column_scale);
 __global__ void zero_rows_kernel(double* x, const int* rows, int count, int W, int N, int E);
 __global__ void aggregate_kernel(const double* in, int rows, int C, int columns, const int* ptr,
                                  const int* cells, float* out, int64_t in_stride);

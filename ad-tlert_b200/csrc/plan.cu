@@ -833,6 +833,19 @@ adt_status adt_boundary_jacobian(adt_plan* p, const float* fields, int32_t row_b
   return check_launch(p, "boundary jacobian");
 }
 
+adt_status adt_scale_rows_columns(float* values, int32_t rows, int32_t columns,
+                                  const double* row_scale, const double* column_scale,
+                                  adt_stream stream) {
+  if (!values || rows < 0 || columns < 0) return fail(nullptr, ADT_INVALID_ARG, "invalid scaling arguments");
+  if ((int64_t)rows * columns == 0) return ADT_OK;
+  scale_rows_columns_kernel<<<grid_for((int64_t)rows * columns), 256, 0, (cudaStream_t)stream>>>(
+      values, rows, columns, row_scale, column_scale);
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess)
+    return fail(nullptr, ADT_CUDA_ERROR, std::string("scaling: ") + cudaGetErrorString(err));
+  return ADT_OK;
+}
+
 int64_t adt_kernel_launches(const adt_plan* p) { return p ? p->launches : 0; }
 
 }  // extern "C"

@@ -308,6 +308,20 @@ __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a) {
   }
 }
 
+// values[r][c] *= row_scale[r] * column_scale[c] (null scales are ones).
+__global__ void scale_rows_columns_kernel(float* values, int rows, int columns, const double* row_scale,
+                                          const double* column_scale) {
+  const int64_t total = (int64_t)rows * columns;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / columns), c = (int)(idx - (int64_t)r * columns);
+    double v = values[idx];
+    if (row_scale) v *= row_scale[r];
+    if (column_scale) v *= column_scale[c];
+    values[idx] = (float)v;
+  }
+}
+
 // y += x elementwise.
 __global__ void add_kernel(double* y, const double* x, int64_t count) {
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;

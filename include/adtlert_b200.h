@@ -222,6 +222,15 @@ adt_status adt_boundary_jacobian(adt_plan* plan, const float* fields, int32_t ro
 adt_status adt_measure_static(adt_plan* plan, const float* fields, int32_t models, double* normal,
                               double* reciprocal, adt_stream stream);
 
+/* values[r][c] *= row_scale[r] * column_scale[c] for a rows x columns float32 device array
+ * (row_scale, column_scale: float64 device arrays; either may be NULL for ones). Used for the
+ * log-space Jacobian d log(rhoa) / d log(rho) = k J_R (-sigma) / rhoa without moving J off the
+ * device. Replaces the chain rule of log_response_and_jacobian
+ * (adtlert/forward/modeling.py:137-162). */
+adt_status adt_scale_rows_columns(float* values, int32_t rows, int32_t columns,
+                                  const double* row_scale, const double* column_scale,
+                                  adt_stream stream);
+
 /* Number of kernels this library has launched since the plan was created. */
 int64_t adt_kernel_launches(const adt_plan* plan);
 
