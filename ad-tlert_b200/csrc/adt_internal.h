@@ -81,6 +81,8 @@ struct adt_plan {
   int nfixed = 0;
   int* owners = nullptr;        // cells owning boundary elements
   int nowners = 0;
+  int* update_items = nullptr;  // eager Schur update items (task, pull begin, pull end)
+  std::vector<int> update_begin;
   // tiled solver (blocks wider than kMaxBlock): device work items, host ranges
   bool tiled = false;
   int* titems = nullptr;

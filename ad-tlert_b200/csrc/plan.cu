@@ -353,6 +353,8 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   ADT_UP(&p->rdof_dof, hp.rdof_dof);
   ADT_UP(&p->fixed, hp.fixed);
   ADT_UP(&p->titems, hp.titems);
+  ADT_UP(&p->update_items, hp.update_items);
+  p->update_begin = hp.update_begin;
   p->tiled = hp.tiled;
   p->tranges = hp.tranges;
   p->panel_ptr = hp.panel_ptr;
@@ -372,7 +374,7 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
                   p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
-                  p->fixed, p->owners, p->titems};
+                  p->fixed, p->owners, p->titems, p->update_items};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& s : p->slots) {

@@ -331,7 +331,7 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
   std::vector<int64_t> loff(hp.nb);
   int64_t cursor = 0;
   for (int b = 0; b < hp.nb; ++b) { loff[b] = cursor; cursor += (int64_t)bm[b] * bm[b]; }
-  struct Elim { int j, p, q; int64_t u, v; };
+  struct Elim { int j, p, q; int64_t u, v, ru = -1, rv = -1; };
   std::vector<Elim> elims;
   std::vector<int64_t> task_rows;
   std::vector<int> elim_level;
@@ -354,6 +354,10 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
       e.u = cursor; cursor += (int64_t)bm[e.j] * bm[e.p];
       e.v = -1;
       if (e.q >= 0) { e.v = cursor; cursor += (int64_t)bm[e.q] * bm[e.j]; }
+      if (!hp.tiled) {  // the inverse-based kernels keep the couplings for the Schur updates
+        e.ru = cursor; cursor += (int64_t)bm[e.j] * bm[e.p];
+        if (e.q >= 0) { e.rv = cursor; cursor += (int64_t)bm[e.q] * bm[e.j]; }
+      }
       task_elim.push_back(e);
       level_of_task.push_back(level);
     }
@@ -383,6 +387,8 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
         row[T_Q] = -1; row[T_MQ] = 0; row[T_OFFQ] = 0;
       }
       row[T_FILL] = fills[k];
+      row[T_RUOFF] = e.ru;
+      row[T_RVOFF] = e.rv;
       task_rows.insert(task_rows.end(), row.begin(), row.end());
     }
     link = next_link;
@@ -405,6 +411,7 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
   hp.factor_stride = cursor;
   // pulls: for task j, every earlier elimination next to j (left one first, per level)
   std::vector<int64_t> pulls;
+  std::vector<int> pull_level;
   std::vector<std::vector<int>> by_block_q(hp.nb), by_block_p(hp.nb);
   for (size_t t = 0; t + 1 < task_elim.size(); ++t) {
     if (task_elim[t].q >= 0) by_block_q[task_elim[t].q].push_back((int)t);
@@ -427,8 +434,25 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
       pulls.push_back(type == 0 ? el.u : el.v);
       pulls.push_back(bm[el.j]);
       pulls.push_back(boff[el.j]);
+      pulls.push_back(type == 0 ? el.ru : el.rv);
+      pull_level.push_back(level_of_task[e]);
     }
     task_rows[t * T_FIELDS + T_PULL1] = (int64_t)pulls.size() / P_FIELDS;
+  }
+  // eager updates: after level l, every block next to an elimination of level l applies the
+  // pulls of that level (a contiguous run of its pull list, which is sorted by level)
+  hp.update_begin.assign(1, 0);
+  hp.update_items.clear();
+  for (int l = 0; l < hp.levels; ++l) {
+    for (size_t t = 0; t < task_elim.size(); ++t) {
+      const int64_t u0 = task_rows[t * T_FIELDS + T_PULL0], u1 = task_rows[t * T_FIELDS + T_PULL1];
+      int64_t b = u0;
+      while (b < u1 && pull_level[b] < l) ++b;
+      int64_t e = b;
+      while (e < u1 && pull_level[e] == l) ++e;
+      if (e > b) hp.update_items.insert(hp.update_items.end(), {(int)t, (int)b, (int)e});
+    }
+    hp.update_begin.push_back((int)(hp.update_items.size() / 3));
   }
 
   if (hp.tiled) build_tile_items(hp, task_rows);

@@ -23,13 +23,14 @@ enum TaskField : int {
   T_P, T_MP, T_OFFP, T_UOFF, T_LINKP,
   T_Q, T_MQ, T_OFFQ, T_VOFF, T_LINKQ,
   T_FILL, T_PULL0, T_PULL1,
+  T_RUOFF, T_RVOFF,  // shared-memory solver: copies of the couplings A[j,p] and A[q,j]
   T_FIELDS
 };
 // Row segments of a tiled elimination: the eliminated block j and its chain neighbours p, q.
 enum TileSegment : int { SEG_J = 0, SEG_P = 1, SEG_Q = 2 };
 
 // Fields of one pull (a Schur-complement contribution of an earlier elimination).
-enum PullField : int { P_TYPE = 0, P_OFF, P_ME, P_EOFF, P_FIELDS };
+enum PullField : int { P_TYPE = 0, P_OFF, P_ME, P_EOFF, P_AOFF, P_FIELDS };
 
 struct HostPlan {
   int N = 0, dim = 2, C = 0, K = 0, Cm = 0, Nb = 0, BL = 0, W = 0, E = 0, D = 0, RW = 0;
@@ -51,6 +52,9 @@ struct HostPlan {
   // Range r: scatter items of level r (task, row0, rows, -); r = L + l: fill tiles of level l
   // (task, qi, pi, -); r = 2L + l: row tiles of the eliminated blocks of level l (task, i, -, -);
   // r = 3L + panel_ptr[l] + k: panel k of level l (task, segment, tile row, -).
+  // eager Schur updates of the shared-memory solver: items (task, pull begin, pull end) of
+  // the blocks that apply level l's pulls right after level l, range update_begin[l] ..
+  std::vector<int> update_items, update_begin;
   bool tiled = false;
   std::vector<int> titems, tranges, panel_ptr;
 };

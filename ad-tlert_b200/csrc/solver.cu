@@ -167,10 +167,6 @@ __device__ void tile_gemm(double* C, int ldc, const double* A, int lda, const do
   }
 }
 
-__device__ __forceinline__ void zero_rows(double* a, int ld, int rows) {
-  for (int i = threadIdx.x; i < rows * ld; i += blockDim.x) a[i] = 0.0;
-}
-
 // In-place lower Cholesky of the m x m tile `a` (leading dimension LD); rinv[i] = 1 / L[i][i].
 // A non-positive pivot becomes NaN, which propagates to every result of the system. Only the
 // lower triangle is read; the strict upper triangle is zeroed on exit.
@@ -293,24 +289,91 @@ __device__ void upper_solve(const double* l, int ldl, const double* rinv, double
 }
 
 template <int MAXM>
-constexpr size_t factor_smem() { return sizeof(double) * ((size_t)MAXM * (MAXM + 1) + (size_t)MAXM * (2 * MAXM + 2) + MAXM); }
+__host__ __device__ constexpr int aug_ld() { return 3 * MAXM + 1; }
 template <int MAXM>
-constexpr size_t forward_smem() { return sizeof(double) * (4 * (size_t)MAXM * (MAXM + 1) + MAXM); }
+constexpr size_t invert_smem() {
+  return sizeof(double) * ((size_t)MAXM * aug_ld<MAXM>() + 2 * 8 * 3 * (size_t)MAXM + (size_t)MAXM * 9 + 8 * 9);
+}
 template <int MAXM>
-constexpr size_t backward_smem() { return sizeof(double) * (6 * (size_t)MAXM * (MAXM + 1) + MAXM); }
+constexpr size_t update_smem() { return sizeof(double) * (5 * (size_t)MAXM * (MAXM + 1)); }
+template <int MAXM>
+constexpr size_t forward_update_smem() { return sizeof(double) * (5 * (size_t)MAXM * (MAXM + 1)); }
+template <int MAXM>
+constexpr size_t backward_smem() { return sizeof(double) * (6 * (size_t)MAXM * (MAXM + 1)); }
 
+// D_j of every block from the assembled CSR values, into the block's G_j storage (the eager
+// Schur updates then subtract from it level by level).
+__global__ void __launch_bounds__(kSolverThreads)
+scatter_diagonal_kernel(const int64_t* __restrict__ tasks, const int* __restrict__ csr_ptr,
+                        const int* __restrict__ csr_row, const int* __restrict__ csr_col, int nnz,
+                        const double* __restrict__ values, double* __restrict__ factors, int64_t stride) {
+  const int64_t* t = tasks + (int64_t)blockIdx.x * T_FIELDS;
+  const double* val = values + (int64_t)blockIdx.y * nnz;
+  double* d = factors + (int64_t)blockIdx.y * stride + t[T_LOFF];
+  const int mj = (int)t[T_MJ], offj = (int)t[T_OFFJ];
+  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) d[i] = 0.0;
+  __syncthreads();
+  for (int s = csr_ptr[offj] + threadIdx.x; s < csr_ptr[offj + mj]; s += blockDim.x) {
+    const int c = csr_col[s];
+    if (c >= offj && c < offj + mj) d[(csr_row[s] - offj) * mj + (c - offj)] = val[s];
+  }
+}
+
+// C (m x n, leading dimension ldc, may be global memory) = acc, combining split halves through
+// `scratch` (>= 128 x 16 doubles). Entered by all threads; ends with a barrier.
+__device__ void store_tile(double (&acc)[4][4], const Micro& u, double* C, int64_t ldc, int m, int n,
+                           double* scratch) {
+  if (u.nsplit == 2) {
+    if (u.part == 1 && u.active)
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) scratch[u.tile * 16 + r * 4 + s] = acc[r][s];
+    __syncthreads();
+  }
+  if (u.part == 0 && u.active) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = u.ti + r * u.mt;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int j = u.tj + s * u.nt;
+        double v = acc[r][s];
+        if (u.nsplit == 2) v += scratch[u.tile * 16 + r * 4 + s];
+        if (i < m && j < n) C[i * ldc + j] = v;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// One BCR level, inverse form. For the eliminated block j with chain neighbours p and q, the
+// augmented matrix [D_j | A[j,p] | A[q,j]^T] (D_j with every earlier Schur update applied) is
+// reduced by block Gauss-Jordan elimination without pivoting (D_j is SPD) to
+// [G_j | Z_p | Z_q], G_j = D_j^-1, Z_p = G_j A[j,p], Z_q = G_j A[q,j]^T. Pivots go in panels of
+// 8: with the panel P (8 x 8), its rows R, its columns L and the rest S, one step is
+// P <- P^-1, R <- P^-1 R, L <- -L P^-1, S <- S - L P^-1 R. Every thread holds a fixed set of
+// augmented entries in registers (rows tr + 8 r, columns tc + 32 c; a panel's rows are pass
+// r = k0 / 8 of the 8 row groups), panel rows and columns go through shared memory, and warp 0
+// inverts the 8 x 8 pivot block with shuffles; four barriers per panel. Stored: G_j, Z_p,
+// V_q = Z_q^T, copies of the couplings (for the Schur updates) and the fill A[q,p] = -A[q,j] Z_p.
+// A non-positive pivot becomes NaN, which reaches every result of the system.
 template <int MAXM>
-__global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 3 : 1)
-factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict__ pulls,
-                    int task_begin, const int* __restrict__ csr_ptr,
+__global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
+invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int* __restrict__ csr_ptr,
                     const int* __restrict__ csr_row, const int* __restrict__ csr_col, int nnz,
-                    const double* __restrict__ values, double* __restrict__ factors,
-                    int64_t stride) {
-  constexpr int LD = MAXM + 1, LDB = 2 * MAXM + 2;
+                    const double* __restrict__ values, double* __restrict__ factors, int64_t stride) {
+  constexpr int LDA = aug_ld<MAXM>();
+  constexpr int W3 = 3 * MAXM;
+  constexpr int RP = MAXM / 8;                  // rows per thread
+  constexpr int CP = (W3 + 31) / 32;            // columns per thread
+  constexpr int PB = 8;                         // pivot panel
   extern __shared__ double sm[];
-  double* dm = sm;                // D_j -> L_j -> fill                        (MAXM x LD)
-  double* bt = dm + MAXM * LD;    // pull buffers, then [A[j,p] | A[q,j]^T] -> [U_p | V_q^T]
-  double* rinv = bt + MAXM * LDB;
+  double* aug = sm;                             // [MAXM][LDA]
+  double* rbuf = aug + MAXM * LDA;              // panel rows      [PB][W3]
+  double* rnew = rbuf + PB * W3;                // P^-1 R          [PB][W3]
+  double* lbuf = rnew + PB * W3;                // panel columns   [MAXM][PB + 1]
+  double* pinv = lbuf + MAXM * (PB + 1);        // P^-1            [PB][PB + 1]
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* val = values + (int64_t)blockIdx.y * nnz;
   double* f = factors + (int64_t)blockIdx.y * stride;
@@ -318,26 +381,212 @@ factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict
   const int p = (int)t[T_P], mp = p >= 0 ? (int)t[T_MP] : 0, offp = (int)t[T_OFFP];
   const int q = (int)t[T_Q], mq = q >= 0 ? (int)t[T_MQ] : 0, offq = (int)t[T_OFFQ];
   const bool p_csr = p >= 0 && t[T_LINKP] < 0, q_csr = q >= 0 && t[T_LINKQ] < 0;
+  const int width = mj + mp + mq;
   const int s0 = csr_ptr[offj], s1 = csr_ptr[offj + mj];
-  const int64_t u0 = t[T_PULL0], u1 = t[T_PULL1];
-  auto issue = [&](int64_t u, double* dst) {
-    const int64_t* pl = pulls + u * P_FIELDS;
-    const int me = (int)pl[P_ME];
-    if (pl[P_TYPE] == 0) async_tile(dst, LD, f + pl[P_OFF], me, mj);  // U (me x mj)
-    else async_tile(dst, LD, f + pl[P_OFF], mj, me);                  // V (mj x me)
-    async_commit();
-  };
-  if (u0 < u1) issue(u0, bt);
 
-  // 1. the original diagonal block D_j from the assembled CSR values
-  zero_rows(dm, LD, mj);
+  // 1. [D_j | A[j,p] | A[q,j]^T] in shared memory
+  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
+    const int r = i / mj, c = i - r * mj;
+    async_copy8(aug + r * LDA + c, f + t[T_LOFF] + i);
+  }
+  if (p >= 0 && !p_csr)  // A[j,p] (mj x mp): the previous level's fill
+    for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
+      const int r = i / mp, c = i - r * mp;
+      async_copy8(aug + r * LDA + mj + c, f + t[T_LINKP] + i);
+    }
+  async_commit();
+  for (int i = threadIdx.x; i < mj * (mp + mq); i += blockDim.x) {
+    const int r = i / (mp + mq), c = i - r * (mp + mq);
+    if (p_csr || c >= mp) aug[r * LDA + mj + c] = 0.0;
+  }
   __syncthreads();
   for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-    const int c = csr_col[s];
-    if (c >= offj && c < offj + mj) dm[(csr_row[s] - offj) * LD + (c - offj)] = val[s];
+    const int r = csr_row[s] - offj, c = csr_col[s];
+    if (p_csr && c >= offp && c < offp + mp) aug[r * LDA + mj + (c - offp)] = val[s];
+    else if (q_csr && c >= offq && c < offq + mq) aug[r * LDA + mj + mp + (c - offq)] = val[s];
   }
-  // 2. Schur-complement updates of blocks eliminated next to j at earlier levels:
-  //    D -= sum U^T U (left-eliminated) / V V^T (right-eliminated), accumulated in registers
+  if (q >= 0 && !q_csr) {  // A[q,j] (mq x mj), stored transposed after A[j,p]
+    const double* src = f + t[T_LINKQ];
+    for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
+      const int r = i / mj, k = i - r * mj;
+      aug[k * LDA + mj + mp + r] = src[i];
+    }
+  }
+  async_wait_all();
+  __syncthreads();
+
+  // 2. copies of the couplings (read by the Schur updates and the fill)
+  if (p >= 0)
+    for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
+      const int r = i / mp, c = i - r * mp;
+      f[t[T_RUOFF] + i] = aug[r * LDA + mj + c];
+    }
+  if (q >= 0)
+    for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
+      const int r = i / mj, k = i - r * mj;
+      f[t[T_RVOFF] + i] = aug[k * LDA + mj + mp + r];
+    }
+
+  // 3. block Gauss-Jordan in registers
+  const int tc = threadIdx.x & 31, tr = threadIdx.x >> 5;
+  double a[RP][CP];
+#pragma unroll
+  for (int r = 0; r < RP; ++r)
+#pragma unroll
+    for (int c = 0; c < CP; ++c) {
+      const int i = tr + 8 * r, j = tc + 32 * c;
+      a[r][c] = (i < mj && j < width) ? aug[i * LDA + j] : 0.0;
+    }
+  for (int k0 = 0; k0 < mj; k0 += PB) {
+    const int nb = min(PB, mj - k0), rb = k0 / PB;
+    // (a) publish the panel rows (row k0 + tr: pass rb) and the panel columns
+#pragma unroll
+    for (int r = 0; r < RP; ++r) {
+      const int i = tr + 8 * r;
+#pragma unroll
+      for (int c = 0; c < CP; ++c) {
+        const int j = tc + 32 * c;
+        if (r == rb && j < W3) rbuf[tr * W3 + j] = (tr < nb && j < width) ? a[r][c] : 0.0;
+        const unsigned s = (unsigned)(j - k0);
+        if (s < (unsigned)PB && i < MAXM) lbuf[i * (PB + 1) + s] = (s < (unsigned)nb && i < mj) ? a[r][c] : 0.0;
+      }
+    }
+    __syncthreads();
+    // (b) P^-1 by warp 0: lane s holds row s (the padding beyond nb is the identity)
+    if (tr == 0) {
+      double row[PB];
+#pragma unroll
+      for (int c = 0; c < PB; ++c) row[c] = (tc < nb && c < nb) ? rbuf[tc * W3 + k0 + c] : (tc == c ? 1.0 : 0.0);
+#pragma unroll
+      for (int k = 0; k < PB; ++k) {
+        const double pivot = __shfl_sync(0xffffffffu, row[k], k);
+        const double inv = pivot > 0.0 ? 1.0 / pivot : quiet_nan();
+        double rk[PB];
+#pragma unroll
+        for (int c = 0; c < PB; ++c) rk[c] = __shfl_sync(0xffffffffu, row[c], k);
+        const double lik = row[k] * inv;
+#pragma unroll
+        for (int c = 0; c < PB; ++c) {
+          if (tc == k) row[c] = (c == k) ? inv : row[c] * inv;
+          else row[c] = (c == k) ? -lik : fma(-lik, rk[c], row[c]);
+        }
+      }
+      if (tc < PB)
+#pragma unroll
+        for (int c = 0; c < PB; ++c) pinv[tc * (PB + 1) + c] = row[c];
+    }
+    __syncthreads();
+    // (c) R' = P^-1 R (rows s < nb; zero beyond), with P^-1 itself in the panel columns, so that
+    //     one rank-8 update below gives S - L P^-1 R and (from zero) -L P^-1
+    for (int idx = threadIdx.x; idx < PB * W3; idx += blockDim.x) {
+      const int s = idx / W3, j = idx - s * W3;
+      const unsigned sj = (unsigned)(j - k0);
+      double v = 0.0;
+      if (s < nb) {
+        if (sj < (unsigned)nb) {
+          v = pinv[s * (PB + 1) + sj];
+        } else {
+#pragma unroll
+          for (int u = 0; u < PB; ++u) v = fma(pinv[s * (PB + 1) + u], rbuf[u * W3 + j], v);
+        }
+      }
+      rnew[idx] = v;
+    }
+    __syncthreads();
+    // (d) rank-8 update of every held entry (outer products), then the panel rows take R'
+#pragma unroll
+    for (int c = 0; c < CP; ++c) {
+      const unsigned sj = (unsigned)(tc + 32 * c - k0);
+      if (sj < (unsigned)nb)
+#pragma unroll
+        for (int r = 0; r < RP; ++r) a[r][c] = 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < PB; ++u) {
+      double lu[RP], ru[CP];
+#pragma unroll
+      for (int r = 0; r < RP; ++r) lu[r] = lbuf[(tr + 8 * r) * (PB + 1) + u];
+#pragma unroll
+      for (int c = 0; c < CP; ++c) {
+        const int j = tc + 32 * c;
+        ru[c] = j < W3 ? rnew[u * W3 + j] : 0.0;
+      }
+#pragma unroll
+      for (int r = 0; r < RP; ++r)
+#pragma unroll
+        for (int c = 0; c < CP; ++c) a[r][c] = fma(-lu[r], ru[c], a[r][c]);
+    }
+    if (tr < nb)
+#pragma unroll
+      for (int r = 0; r < RP; ++r)
+        if (r == rb)
+#pragma unroll
+          for (int c = 0; c < CP; ++c) {
+            const int j = tc + 32 * c;
+            a[r][c] = j < W3 ? rnew[tr * W3 + j] : 0.0;
+          }
+    __syncthreads();
+  }
+
+  // 4. G_j, Z_p, V_q to the factor storage; Z_p back to shared memory for the fill
+#pragma unroll
+  for (int r = 0; r < RP; ++r)
+#pragma unroll
+    for (int c = 0; c < CP; ++c) {
+      const int i = tr + 8 * r, j = tc + 32 * c;
+      if (i >= mj || j >= width) continue;
+      const double v = a[r][c];
+      aug[i * LDA + j] = v;
+      if (j < mj) f[t[T_LOFF] + i * mj + j] = v;
+      else if (j < mj + mp) f[t[T_UOFF] + i * mp + (j - mj)] = v;
+      else f[t[T_VOFF] + (j - mj - mp) * mj + i] = v;
+    }
+  if (p < 0 || q < 0) return;
+  __syncthreads();
+  // 5. fill A[q,p] = -A[q,j] Z_p: the coupling copy (written by this block above) replaces G_j
+  //    in shared memory
+  for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
+    const int r = i / mj, k = i - r * mj;
+    aug[r * LDA + k] = f[t[T_RVOFF] + i];
+  }
+  double* fill = f + t[T_FILL];
+  for (int i = threadIdx.x; i < mq * mp; i += blockDim.x) fill[i] = 0.0;
+  __syncthreads();
+  tile_gemm<false, false>(fill, mp, aug, LDA, aug + mj, LDA, mq, mp, mj, -1.0);
+}
+
+// Eager Schur updates after a level: block j of every item subtracts the pulls [u0, u1) of that
+// level from D_j, in place in its G_j storage: A[e,j]^T Z_j for the elimination e on its right,
+// V_j A[j,e]^T for the one on its left (operands stream in with cp.async, products accumulate in
+// registers).
+template <int MAXM>
+__global__ void __launch_bounds__(kSolverThreads, 2)
+update_level_kernel(const int* __restrict__ items, int item_begin, const int64_t* __restrict__ tasks,
+                    const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride) {
+  constexpr int LD = MAXM + 1;
+  extern __shared__ double sm[];
+  auto tile = [&](int i) { return sm + i * MAXM * LD; };
+  double* dm = tile(4);
+  const int* it = items + 3 * (item_begin + blockIdx.x);
+  const int64_t* t = tasks + (int64_t)it[0] * T_FIELDS;
+  const int64_t u0 = it[1], u1 = it[2];
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  const int mj = (int)t[T_MJ];
+  double* d = f + t[T_LOFF];
+  auto issue = [&](int64_t u, int pair) {
+    const int64_t* pl = pulls + u * P_FIELDS;
+    const int me = (int)pl[P_ME];
+    if (pl[P_TYPE] == 0) {  // coupling A[e,j] and Z_j, both me x mj
+      async_tile(tile(2 * pair), LD, f + pl[P_AOFF], me, mj);
+      async_tile(tile(2 * pair + 1), LD, f + pl[P_OFF], me, mj);
+    } else {                // V_j and coupling A[j,e], both mj x me
+      async_tile(tile(2 * pair), LD, f + pl[P_OFF], mj, me);
+      async_tile(tile(2 * pair + 1), LD, f + pl[P_AOFF], mj, me);
+    }
+  };
+  async_tile(dm, LD, d, mj, mj);
+  issue(u0, 0);
+  async_commit();
   const Micro mu(mj, mj);
   double acc[4][4];
 #pragma unroll
@@ -347,108 +596,54 @@ factor_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict
   for (int64_t u = u0; u < u1; ++u) {
     async_wait_all();
     __syncthreads();
-    if (u + 1 < u1) issue(u + 1, bt + ((u + 1 - u0) & 1) * MAXM * LD);
-    const double* cur = bt + ((u - u0) & 1) * MAXM * LD;
+    const int cur = (int)((u - u0) & 1);
+    if (u + 1 < u1) {
+      issue(u + 1, cur ^ 1);
+      async_commit();
+    }
+    const double* X = tile(2 * cur);
+    const double* Y = tile(2 * cur + 1);
     const int me = (int)pulls[u * P_FIELDS + P_ME];
-    if (pulls[u * P_FIELDS + P_TYPE] == 0) accumulate<true, false>(acc, mu, cur, LD, cur, LD, me);
-    else accumulate<false, true>(acc, mu, cur, LD, cur, LD, me);
+    if (pulls[u * P_FIELDS + P_TYPE] == 0) accumulate<true, false>(acc, mu, X, LD, Y, LD, me);
+    else accumulate<false, true>(acc, mu, X, LD, Y, LD, me);
   }
   __syncthreads();
-  if (u0 < u1) subtract_tile(acc, mu, dm, LD, mj, mj, bt);
-
-  // 3. couplings to the chain neighbours: [A[j,p] | A[q,j]^T]
-  zero_rows(bt, LDB, mj);
-  __syncthreads();
-  for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-    const int r = csr_row[s] - offj, c = csr_col[s];
-    if (p_csr && c >= offp && c < offp + mp) bt[r * LDB + (c - offp)] = val[s];
-    else if (q_csr && c >= offq && c < offq + mq) bt[r * LDB + mp + (c - offq)] = val[s];
-  }
-  if (p >= 0 && !p_csr) {  // A[j,p] (mj x mp): the previous level's fill
-    async_tile(bt, LDB, f + t[T_LINKP], mj, mp);
-    async_commit();
-  }
-  if (q >= 0 && !q_csr) {  // A[q,j] (mq x mj), stored transposed next to A[j,p]
-    const double* src = f + t[T_LINKQ];
-    for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
-      const int r = i / mj, k = i - r * mj;
-      bt[k * LDB + mp + r] = src[i];
-    }
-  }
-  async_wait_all();
-  __syncthreads();
-
-  // 4. L_j, then [U_p | V_q^T] = L_j^-1 [A[j,p] | A[q,j]^T]
-  cholesky<LD>(dm, mj, rinv);
-  {
-    double* out = f + t[T_LOFF];
-    for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
-      const int r = i / mj, c = i - r * mj;
-      out[i] = dm[r * LD + c];
-    }
-  }
-  if (mp + mq == 0) return;
-  lower_solve(dm, LD, rinv, bt, LDB, mj, mp + mq);
-  double* up = f + t[T_UOFF];
-  for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
-    const int r = i / mp, c = i - r * mp;
-    up[i] = bt[r * LDB + c];
-  }
-  if (q < 0) return;
-  double* vq = f + t[T_VOFF];
-  for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
-    const int r = i / mj, k = i - r * mj;
-    vq[i] = bt[k * LDB + mp + r];
-  }
-  if (p < 0) return;
-  // 5. fill A[q,p] = -V_q U_p, built in the L_j tile (already stored)
-  __syncthreads();
-  zero_rows(dm, LD, mq);
-  __syncthreads();
-  tile_gemm<true, false>(dm, LD, bt + mp, LDB, bt, LDB, mq, mp, mj, -1.0);
-  __syncthreads();
-  double* out = f + t[T_FILL];
-  for (int i = threadIdx.x; i < mq * mp; i += blockDim.x) {
-    const int r = i / mp, c = i - r * mp;
-    out[i] = dm[r * LD + c];
+  subtract_tile(acc, mu, dm, LD, mj, mj, tile(0));
+  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
+    const int r = i / mj, c = i - r * mj;
+    d[i] = dm[r * LD + c];
   }
 }
 
-// Forward level: y_j = L_j^-1 (b_j - pulls); the root also back-substitutes.
+// Eager forward updates after a level: b_j -= Z_j^T b_e / V_j b_e for the pulls [u0, u1) of the
+// item, right-hand-side columns [c0, c0 + strip).
 template <int MAXM>
-__global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 3 : 1)
-forward_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restrict__ pulls,
-                     int task_begin, const double* __restrict__ factors, int64_t stride,
-                     double* __restrict__ rhs, int64_t rhs_stride, int nrhs, int root) {
+__global__ void __launch_bounds__(kSolverThreads, 2)
+forward_update_kernel(const int* __restrict__ items, int item_begin, const int64_t* __restrict__ tasks,
+                      const int64_t* __restrict__ pulls, const double* __restrict__ factors,
+                      int64_t stride, double* __restrict__ rhs, int64_t rhs_stride, int nrhs, int strip) {
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
   auto tile = [&](int i) { return sm + i * MAXM * LD; };
-  double* rinv = sm + 4 * MAXM * LD;
-  const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
+  double* bt = tile(4);
+  const int* it = items + 3 * (item_begin + blockIdx.x);
+  const int64_t* t = tasks + (int64_t)it[0] * T_FIELDS;
+  const int64_t u0 = it[1], u1 = it[2];
   const double* f = factors + (int64_t)blockIdx.y * stride;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
-  const int c0 = blockIdx.z * MAXM;
-  const int nc = min(MAXM, nrhs - c0);
+  const int c0 = blockIdx.z * strip;
+  const int nc = min(strip, nrhs - c0);
   const int mj = (int)t[T_MJ], offj = (int)t[T_OFFJ];
-  const int64_t u0 = t[T_PULL0], u1 = t[T_PULL1];
-  // pairs (tile[0], tile[1]) and (tile[2], tile[3]) alternate between pulls; the pair free
-  // during the last pull receives b_j and L_j
-  auto issue_pull = [&](int64_t u, int pair) {
+  auto issue = [&](int64_t u, int pair) {
     const int64_t* pl = pulls + u * P_FIELDS;
     const int me = (int)pl[P_ME];
     if (pl[P_TYPE] == 0) async_tile(tile(2 * pair), LD, f + pl[P_OFF], me, mj);
     else async_tile(tile(2 * pair), LD, f + pl[P_OFF], mj, me);
     async_rows(tile(2 * pair + 1), LD, x + (int64_t)pl[P_EOFF] * nrhs + c0, nrhs, me, nc);
-    async_commit();
   };
-  auto issue_final = [&](int pair) {
-    async_rows(tile(2 * pair), LD, x + (int64_t)offj * nrhs + c0, nrhs, mj, nc);
-    async_tile(tile(2 * pair + 1), LD, f + t[T_LOFF], mj, mj);
-    async_commit();
-  };
-  int final_pair = 0;
-  if (u0 == u1) issue_final(0);
-  else issue_pull(u0, 0);
+  async_rows(bt, LD, x + (int64_t)offj * nrhs + c0, nrhs, mj, nc);
+  issue(u0, 0);
+  async_commit();
   const Micro mu(mj, nc);
   double acc[4][4];
 #pragma unroll
@@ -458,49 +653,45 @@ forward_level_kernel(const int64_t* __restrict__ tasks, const int64_t* __restric
   for (int64_t u = u0; u < u1; ++u) {
     async_wait_all();
     __syncthreads();
-    const int cur = (int)((u - u0) & 1), nxt = cur ^ 1;
-    if (u + 1 < u1) issue_pull(u + 1, nxt);
-    else { issue_final(nxt); final_pair = nxt; }
+    const int cur = (int)((u - u0) & 1);
+    if (u + 1 < u1) {
+      issue(u + 1, cur ^ 1);
+      async_commit();
+    }
     const double* M = tile(2 * cur);
     const double* Y = tile(2 * cur + 1);
     const int me = (int)pulls[u * P_FIELDS + P_ME];
-    if (pulls[u * P_FIELDS + P_TYPE] == 0) accumulate<true, false>(acc, mu, M, LD, Y, LD, me);   // U^T y
-    else accumulate<false, false>(acc, mu, M, LD, Y, LD, me);                                     // V y
+    if (pulls[u * P_FIELDS + P_TYPE] == 0) accumulate<true, false>(acc, mu, M, LD, Y, LD, me);   // Z^T b
+    else accumulate<false, false>(acc, mu, M, LD, Y, LD, me);                                     // V b
   }
-  async_wait_all();
   __syncthreads();
-  double* bt = tile(2 * final_pair);
-  double* lt = tile(2 * final_pair + 1);
-  if (u0 < u1) subtract_tile(acc, mu, bt, LD, mj, nc, tile(2 * (final_pair ^ 1)));
-  reciprocal_diagonal(lt, LD, mj, rinv);
-  lower_solve(lt, LD, rinv, bt, LD, mj, nc);
-  if (root) upper_solve(lt, LD, rinv, bt, LD, mj, nc);
+  subtract_tile(acc, mu, bt, LD, mj, nc, tile(0));
   for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
     const int r = i / nc, c = i - r * nc;
     x[(int64_t)(offj + r) * nrhs + c0 + c] = bt[r * LD + c];
   }
 }
 
-// Backward level: x_j = L_j^-T (y_j - U_p x_p - V_q^T x_q), every operand prefetched at once.
+// Backward level: x_j = G_j b_j - Z_p x_p - V_q^T x_q (the root: x = G b), every operand
+// prefetched at once; columns [c0, c0 + strip).
 template <int MAXM>
-__global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
+__global__ void __launch_bounds__(kSolverThreads, 2)
 backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
                       const double* __restrict__ factors, int64_t stride,
-                      double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
+                      double* __restrict__ rhs, int64_t rhs_stride, int nrhs, int strip) {
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
-  double* ut = sm;                 // U_p (mj x mp)
-  double* xp = ut + MAXM * LD;     // x_p (mp x nc)
+  double* ut = sm;                 // Z_p (mj x mp)
+  double* xp = ut + MAXM * LD;     // -x_p (mp x nc)
   double* vt = xp + MAXM * LD;     // V_q (mq x mj)
-  double* xq = vt + MAXM * LD;     // x_q (mq x nc)
-  double* bt = xq + MAXM * LD;     // y_j -> x_j
-  double* lt = bt + MAXM * LD;     // L_j
-  double* rinv = lt + MAXM * LD;
+  double* xq = vt + MAXM * LD;     // -x_q (mq x nc)
+  double* bt = xq + MAXM * LD;     // b_j
+  double* gt = bt + MAXM * LD;     // G_j
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* f = factors + (int64_t)blockIdx.y * stride;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
-  const int c0 = blockIdx.z * MAXM;
-  const int nc = min(MAXM, nrhs - c0);
+  const int c0 = blockIdx.z * strip;
+  const int nc = min(strip, nrhs - c0);
   const int mj = (int)t[T_MJ], offj = (int)t[T_OFFJ];
   const int p = (int)t[T_P], q = (int)t[T_Q];
   const int mp = p >= 0 ? (int)t[T_MP] : 0, mq = q >= 0 ? (int)t[T_MQ] : 0;
@@ -513,9 +704,12 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
     async_rows(xq, LD, x + t[T_OFFQ] * nrhs + c0, nrhs, mq, nc);
   }
   async_rows(bt, LD, x + (int64_t)offj * nrhs + c0, nrhs, mj, nc);
-  async_tile(lt, LD, f + t[T_LOFF], mj, mj);
+  async_tile(gt, LD, f + t[T_LOFF], mj, mj);
   async_commit();
   async_wait_all();
+  __syncthreads();
+  for (int i = threadIdx.x; i < mp * nc; i += blockDim.x) xp[(i / nc) * LD + i % nc] *= -1.0;
+  for (int i = threadIdx.x; i < mq * nc; i += blockDim.x) xq[(i / nc) * LD + i % nc] *= -1.0;
   __syncthreads();
   const Micro mu(mj, nc);
   double acc[4][4];
@@ -523,16 +717,11 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int s = 0; s < 4; ++s) acc[r][s] = 0.0;
+  accumulate<false, false>(acc, mu, gt, LD, bt, LD, mj);
   if (p >= 0) accumulate<false, false>(acc, mu, ut, LD, xp, LD, mp);
   if (q >= 0) accumulate<true, false>(acc, mu, vt, LD, xq, LD, mq);
   __syncthreads();
-  if (p >= 0 || q >= 0) subtract_tile(acc, mu, bt, LD, mj, nc, ut);
-  reciprocal_diagonal(lt, LD, mj, rinv);
-  upper_solve(lt, LD, rinv, bt, LD, mj, nc);
-  for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
-    const int r = i / nc, c = i - r * nc;
-    x[(int64_t)(offj + r) * nrhs + c0 + c] = bt[r * LD + c];
-  }
+  store_tile(acc, mu, x + (int64_t)offj * nrhs + c0, nrhs, mj, nc, ut);
 }
 
 // ============================================================================================
@@ -1003,39 +1192,59 @@ void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, doub
 
 template <int MAXM>
 void configure() {
-  cudaFuncSetAttribute(factor_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)factor_smem<MAXM>());
-  cudaFuncSetAttribute(forward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)forward_smem<MAXM>());
+  cudaFuncSetAttribute(invert_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)invert_smem<MAXM>());
+  cudaFuncSetAttribute(update_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)update_smem<MAXM>());
+  cudaFuncSetAttribute(forward_update_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)forward_update_smem<MAXM>());
   cudaFuncSetAttribute(backward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)backward_smem<MAXM>());
 }
 
 template <int MAXM>
 void factor_levels(adt_plan* p, int systems, const double* values, double* factors, cudaStream_t s) {
+  const int tasks = p->level_begin[p->levels];
+  scatter_diagonal_kernel<<<dim3(tasks, systems), kSolverThreads, 0, s>>>(
+      p->tasks, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
+  p->launches++;
   for (int level = 0; level < p->levels; ++level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    dim3 grid(t1 - t0, systems);
-    factor_level_kernel<MAXM><<<grid, kSolverThreads, factor_smem<MAXM>(), s>>>(
-        p->tasks, p->pulls, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors,
-        p->factor_stride);
+    invert_level_kernel<MAXM><<<dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s>>>(
+        p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
     p->launches++;
+    const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
+    if (i1 > i0) {
+      update_level_kernel<MAXM><<<dim3(i1 - i0, systems), kSolverThreads, update_smem<MAXM>(), s>>>(
+          p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride);
+      p->launches++;
+    }
   }
+}
+
+// Column strip of the substitution kernels: the full tile unless that leaves most SMs idle.
+template <int MAXM>
+int strip_for(int blocks, int nrhs) {
+  int strip = MAXM;
+  while (strip > 16 && (int64_t)blocks * ((nrhs + strip - 1) / strip) < 2 * 148) strip /= 2;
+  return strip;
 }
 
 template <int MAXM>
 void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s) {
   const int64_t rhs_stride = (int64_t)p->N * nrhs;
-  const int tiles = (nrhs + MAXM - 1) / MAXM;
-  for (int level = 0; level < p->levels; ++level) {
-    const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    dim3 grid(t1 - t0, systems, tiles);
-    forward_level_kernel<MAXM><<<grid, kSolverThreads, forward_smem<MAXM>(), s>>>(
-        p->tasks, p->pulls, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs, level == p->levels - 1);
+  for (int level = 0; level < p->levels; ++level) {  // forward: eager updates only
+    const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
+    if (i1 <= i0) continue;
+    const int strip = strip_for<MAXM>((i1 - i0) * systems, nrhs);
+    forward_update_kernel<MAXM><<<dim3(i1 - i0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
+                                  forward_update_smem<MAXM>(), s>>>(
+        p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
   }
-  for (int level = p->levels - 2; level >= 0; --level) {
+  for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    dim3 grid(t1 - t0, systems, tiles);
-    backward_level_kernel<MAXM><<<grid, kSolverThreads, backward_smem<MAXM>(), s>>>(
-        p->tasks, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs);
+    backward_level_kernel<MAXM><<<dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
+                                  backward_smem<MAXM>(), s>>>(p->tasks, t0, factors, p->factor_stride, rhs,
+                                                              rhs_stride, nrhs, strip);
     p->launches++;
   }
 }

@@ -19,9 +19,10 @@ ROOT = Path(__file__).resolve().parents[1]
 CSRC = ROOT / "ad-tlert_b200" / "csrc"
 BUILD = ROOT / "tests" / "_build"
 
-T_J, T_MJ, T_OFFJ, T_LOFF, T_P, T_MP, T_OFFP, T_UOFF, T_LINKP, T_Q, T_MQ, T_OFFQ, T_VOFF, T_LINKQ, T_FILL, T_PULL0, T_PULL1 = range(17)
-T_FIELDS = 17
-P_TYPE, P_OFF, P_ME, P_EOFF = range(4)
+(T_J, T_MJ, T_OFFJ, T_LOFF, T_P, T_MP, T_OFFP, T_UOFF, T_LINKP, T_Q, T_MQ, T_OFFQ, T_VOFF, T_LINKQ, T_FILL, T_PULL0,
+ T_PULL1, T_RUOFF, T_RVOFF) = range(19)
+T_FIELDS = 19
+P_TYPE, P_OFF, P_ME, P_EOFF, P_AOFF = range(5)
 
 _TYPES = {
     "task_rows": np.int64, "pulls": np.int64, "features": np.float32, "fscale": np.float32,
@@ -66,13 +67,14 @@ class HostPlan:
             for name in ("perm", "iperm", "level_begin", "csr_ptr", "csr_col", "csr_row", "contrib_ptr", "contrib",
                          "task_rows", "pulls", "features", "fscale", "pair_ptr", "pair_list", "rcv_dofs", "rcv_w",
                          "rdof_ptr", "rdof_rcv", "rdof_dof", "rdof_w", "cdofs", "bd", "cell_bptr", "cell_blist",
-                         "model_ptr", "model_list", "k2", "bowners", "fixed", "titems", "tranges", "panel_ptr"):
+                         "model_ptr", "model_list", "k2", "bowners", "fixed", "titems", "tranges", "panel_ptr",
+                         "update_items", "update_begin"):
                 size = lib.shim_table(handle, name.encode(), None)
                 out = np.empty(size, dtype=_TYPES.get(name, np.int32))
                 lib.shim_table(handle, name.encode(), out.ctypes.data_as(ctypes.c_void_p))
                 setattr(self, name, out)
             self.tasks = self.task_rows.reshape(-1, T_FIELDS)
-            self.pull_table = self.pulls.reshape(-1, 4)
+            self.pull_table = self.pulls.reshape(-1, 5)
 
     def __del__(self):
         try:
@@ -108,26 +110,42 @@ def _check(offset, size, stride, what):
     assert 0 <= offset and offset + size <= stride, f"{what}: [{offset}, {offset + size}) outside [0, {stride})"
 
 
+def _update_items(hp: HostPlan, level: int):
+    items = hp.update_items.reshape(-1, 3)
+    return items[hp.update_begin[level]:hp.update_begin[level + 1]]
+
+
 def replay_factor(hp: HostPlan, values: np.ndarray) -> np.ndarray:
-    """Factor storage of one system, written as factor_level_kernel writes it."""
+    """Factor storage of one system as the shared-memory kernels write it: D of every block
+    scattered into its G storage; per level the eliminations (inverse launch: G_j = D_j^-1,
+    Z_p = G_j A[j,p], V_q = A[q,j] G_j, coupling copies, fill -A[q,j] Z_p) and the eager Schur
+    updates of the neighbouring blocks (A[e,j]^T Z_j, V_j A[j,e]^T). Every access is
+    bounds-checked, every read must follow a write, and no item of a launch may write what another
+    item of that launch reads or writes."""
 
     stride = hp.factor_stride
     f = np.full(stride, np.nan)
-    written = np.zeros(stride, dtype=bool)
 
-    def store(offset, block, what):
-        _check(offset, block.size, stride, what)
-        assert not written[offset:offset + block.size].any(), f"{what}: storage written twice"
-        f[offset:offset + block.size] = block.reshape(-1)
-        written[offset:offset + block.size] = True
+    def idx(offset, rows, cols, what):
+        _check(offset, rows * cols, stride, what)
+        return np.arange(offset, offset + rows * cols)
 
     def load(offset, rows, cols, what):
-        _check(offset, rows * cols, stride, what)
-        block = f[offset:offset + rows * cols].reshape(rows, cols)
+        block = f[idx(offset, rows, cols, what)].reshape(rows, cols)
         assert np.all(np.isfinite(block)), f"{what}: read before written"
-        return block
+        return block.copy()
 
+    for t in range(len(hp.tasks)):  # scatter launch
+        row = hp.tasks[t]
+        mj, offj = int(row[T_MJ]), int(row[T_OFFJ])
+        dm = np.zeros((mj, mj))
+        for s in range(hp.csr_ptr[offj], hp.csr_ptr[offj + mj]):
+            c = hp.csr_col[s]
+            if offj <= c < offj + mj:
+                dm[hp.csr_row[s] - offj, c - offj] = values[s]
+        f[idx(int(row[T_LOFF]), mj, mj, "D")] = dm.reshape(-1)
     for level in range(hp.levels):
+        launch, results = _Launch("invert"), []
         for t in range(hp.level_begin[level], hp.level_begin[level + 1]):
             row = hp.tasks[t]
             mj, offj = int(row[T_MJ]), int(row[T_OFFJ])
@@ -135,43 +153,66 @@ def replay_factor(hp: HostPlan, values: np.ndarray) -> np.ndarray:
             q, mq, offq = int(row[T_Q]), int(row[T_MQ]), int(row[T_OFFQ])
             assert 0 < mj <= 64 and (p < 0 or 0 < mp <= 64) and (q < 0 or 0 < mq <= 64)
             p_csr, q_csr = p >= 0 and row[T_LINKP] < 0, q >= 0 and row[T_LINKQ] < 0
-            dm, ap, aq = np.zeros((mj, mj)), np.zeros((mj, max(mp, 0))), np.zeros((max(mq, 0), mj))
+            reads = [idx(int(row[T_LOFF]), mj, mj, "D")]
+            dm = load(int(row[T_LOFF]), mj, mj, "D")
+            ap, aq = np.zeros((mj, max(mp, 0))), np.zeros((max(mq, 0), mj))
             for s in range(hp.csr_ptr[offj], hp.csr_ptr[offj + mj]):
                 r, c = hp.csr_row[s] - offj, hp.csr_col[s]
                 assert 0 <= r < mj
-                if offj <= c < offj + mj:
-                    dm[r, c - offj] = values[s]
-                elif p_csr and offp <= c < offp + mp:
+                if p_csr and offp <= c < offp + mp:
                     ap[r, c - offp] = values[s]
                 elif q_csr and offq <= c < offq + mq:
                     aq[c - offq, r] = values[s]
             if p >= 0 and not p_csr:
-                ap = load(int(row[T_LINKP]), mj, mp, "link p").copy()
+                ap = load(int(row[T_LINKP]), mj, mp, "link p")
+                reads.append(idx(int(row[T_LINKP]), mj, mp, "link p"))
             if q >= 0 and not q_csr:
-                aq = load(int(row[T_LINKQ]), mq, mj, "link q").copy()
-            for u in range(row[T_PULL0], row[T_PULL1]):
-                kind, off, me = (int(v) for v in hp.pull_table[u, :3])
-                if kind == 0:
-                    U = load(off, me, mj, "pull U")
-                    dm -= U.T @ U
-                else:
-                    V = load(off, mj, me, "pull V")
-                    dm -= V @ V.T
-            L = np.linalg.cholesky(np.tril(dm) + np.tril(dm, -1).T)
-            store(int(row[T_LOFF]), L, "L")
+                aq = load(int(row[T_LINKQ]), mq, mj, "link q")
+                reads.append(idx(int(row[T_LINKQ]), mq, mj, "link q"))
+            G = np.linalg.inv(dm)
+            out = [(int(row[T_LOFF]), G, "G")]
             if p >= 0:
-                U = sla.solve_triangular(L, ap, lower=True)
-                store(int(row[T_UOFF]), U, "U")
+                Z = G @ ap
+                out += [(int(row[T_UOFF]), Z, "Z"), (int(row[T_RUOFF]), ap, "coupling p")]
             if q >= 0:
-                V = sla.solve_triangular(L, aq.T, lower=True).T
-                store(int(row[T_VOFF]), V, "V")
+                V = aq @ G
+                out += [(int(row[T_VOFF]), V, "V"), (int(row[T_RVOFF]), aq, "coupling q")]
             if p >= 0 and q >= 0:
-                store(int(row[T_FILL]), -V @ U, "fill")
+                out.append((int(row[T_FILL]), -aq @ Z, "fill"))
+            launch.item(reads, [idx(off, *block.shape, what) for off, block, what in out])
+            results += out
+        launch.check()
+        for off, block, what in results:
+            f[idx(off, *block.shape, what)] = block.reshape(-1)
+        launch, results = _Launch("update"), []
+        for t, u0, u1 in _update_items(hp, level):
+            row = hp.tasks[t]
+            mj, loff = int(row[T_MJ]), int(row[T_LOFF])
+            dm = load(loff, mj, mj, "D (update)")
+            reads = [idx(loff, mj, mj, "D")]
+            for u in range(u0, u1):
+                assert row[T_PULL0] <= u < row[T_PULL1]
+                kind, off, me, _, aoff = (int(v) for v in hp.pull_table[u])
+                if kind == 0:
+                    A, Z = load(aoff, me, mj, "coupling"), load(off, me, mj, "Z")
+                    dm -= A.T @ Z
+                    reads += [idx(aoff, me, mj, "coupling"), idx(off, me, mj, "Z")]
+                else:
+                    V, A = load(off, mj, me, "V"), load(aoff, mj, me, "coupling")
+                    dm -= V @ A.T
+                    reads += [idx(off, mj, me, "V"), idx(aoff, mj, me, "coupling")]
+            launch.item(reads, [idx(loff, mj, mj, "D")])
+            results.append((loff, dm))
+        launch.check()
+        for loff, dm in results:
+            f[loff:loff + dm.size] = dm.reshape(-1)
     return f
 
 
 def replay_solve(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarray:
-    """Solution of one system for rhs (N, nrhs) in solver order, as the level kernels compute it."""
+    """Solution of one system for rhs (N, nrhs) in solver order, as the shared-memory kernels
+    compute it: forward = the eager updates b_j -= Z_j^T b_e / V_j b_e level by level; backward
+    = x_j = G_j b_j - Z_p x_p - V_q^T x_q from the root down."""
 
     x = rhs.astype(float).copy()
 
@@ -179,32 +220,25 @@ def replay_solve(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarray:
         return f[off:off + rows * cols].reshape(rows, cols)
 
     for level in range(hp.levels):
-        root = level == hp.levels - 1
-        for t in range(hp.level_begin[level], hp.level_begin[level + 1]):
+        for t, u0, u1 in _update_items(hp, level):
             row = hp.tasks[t]
             mj, offj = int(row[T_MJ]), int(row[T_OFFJ])
-            b = x[offj:offj + mj].copy()
-            for u in range(row[T_PULL0], row[T_PULL1]):
-                kind, off, me, eoff = (int(v) for v in hp.pull_table[u])
+            for u in range(u0, u1):
+                kind, off, me, eoff, _ = (int(v) for v in hp.pull_table[u])
                 y = x[eoff:eoff + me]
-                b -= (block(off, me, mj).T @ y) if kind == 0 else (block(off, mj, me) @ y)
-            L = block(int(row[T_LOFF]), mj, mj)
-            b = sla.solve_triangular(L, b, lower=True)
-            if root:
-                b = sla.solve_triangular(L.T, b, lower=False)
-            x[offj:offj + mj] = b
-    for level in range(hp.levels - 2, -1, -1):
+                x[offj:offj + mj] -= (block(off, me, mj).T @ y) if kind == 0 else (block(off, mj, me) @ y)
+    for level in range(hp.levels - 1, -1, -1):
         for t in range(hp.level_begin[level], hp.level_begin[level + 1]):
             row = hp.tasks[t]
             mj, offj = int(row[T_MJ]), int(row[T_OFFJ])
-            y = x[offj:offj + mj].copy()
+            y = block(int(row[T_LOFF]), mj, mj) @ x[offj:offj + mj]
             if row[T_P] >= 0:
                 mp, offp = int(row[T_MP]), int(row[T_OFFP])
                 y -= block(int(row[T_UOFF]), mj, mp) @ x[offp:offp + mp]
             if row[T_Q] >= 0:
                 mq, offq = int(row[T_MQ]), int(row[T_OFFQ])
                 y -= block(int(row[T_VOFF]), mq, mj).T @ x[offq:offq + mq]
-            x[offj:offj + mj] = sla.solve_triangular(block(int(row[T_LOFF]), mj, mj).T, y, lower=False)
+            x[offj:offj + mj] = y
     return x
 
 
@@ -330,7 +364,7 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray) -> np.ndarray:
                     reads += [ia, ib]
                 if seg == SEG_J:
                     for u in range(v.pull0, v.pull1):
-                        typ, off, me, _ = hp.pull_table[u]
+                        typ, off, me = hp.pull_table[u][:3]
                         if typ == 0:
                             ia = _strided(f, off + TILE * i, 1, v.mj, ni, me, "pull U")
                             ib = _strided(f, off + TILE * k, 1, v.mj, mk, me, "pull U")
@@ -397,7 +431,7 @@ def replay_solve_tiled(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarr
             ni = min(TILE, v.mj - TILE * i)
             rows = slice(v.offj + TILE * i, v.offj + TILE * i + ni)
             for u in range(v.pull0, v.pull1):
-                typ, off, me, eoff = hp.pull_table[u]
+                typ, off, me, eoff = hp.pull_table[u][:4]
                 if typ == 0:
                     a = f[_strided(f, off + TILE * i, 1, v.mj, ni, me, "pull U")]
                 else:

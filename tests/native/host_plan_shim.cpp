@@ -60,7 +60,7 @@ long long shim_table(void* h, const char* name, void* dst) {
   T(perm) T(iperm) T(level_begin) T(csr_ptr) T(csr_col) T(csr_row) T(contrib_ptr) T(contrib)
   T(task_rows) T(pulls) T(features) T(fscale) T(pair_ptr) T(pair_list) T(rcv_dofs) T(rcv_w)
   T(rdof_ptr) T(rdof_rcv) T(rdof_dof) T(rdof_w) T(cdofs) T(bd) T(cell_bptr) T(cell_blist)
-  T(model_ptr) T(model_list) T(k2) T(bowners) T(fixed) T(titems) T(tranges) T(panel_ptr)
+  T(model_ptr) T(model_list) T(k2) T(bowners) T(fixed) T(titems) T(tranges) T(panel_ptr) T(update_items) T(update_begin)
 #undef T
   return size;
 }
