@@ -102,6 +102,10 @@ struct adt_plan {
   std::string error;
   int64_t launches = 0;
   int device = 0;
+  int sms = 148;                // multiprocessors of the device
+  bool jacobian_tc = true;      // tensor-core Jacobian where it applies
+  int* tc_error = nullptr;      // device flag raised by a tensor-core block that timed out
+  int* tc_error_host = nullptr; // pinned copy, refreshed after each tensor-core launch
 };
 
 namespace adt {

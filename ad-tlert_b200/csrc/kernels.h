@@ -132,6 +132,8 @@ __global__ void integrated_kernel(const float* fields, const double* weights, co
 __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, int E,
                            double* current);
 cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s);
+bool jacobian_tc_supported(int E, int W, int R, int K, int rows);
+cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaStream_t s);
 __global__ void cell_gradient_kernel(CellGradientArgs a);
 __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a);
 __global__ void add_kernel(double* y, const double* x, int64_t count);

@@ -9,6 +9,9 @@
 #include <string>
 #include <vector>
 
+#include <cstdlib>
+#include <cstring>
+
 #include "adt_internal.h"
 #include "kernels.h"
 #include "plan_host.h"
@@ -299,6 +302,8 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   if (built != ADT_OK) return fail(nullptr, built, err);
   adt_plan* p = new adt_plan();
   cudaGetDevice(&p->device);
+  cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device);
+  if (const char* choice = std::getenv("ADTLERT_B200_JACOBIAN")) p->jacobian_tc = std::strcmp(choice, "fma") != 0;
   configure_solver_kernels();
   auto bail = [&](adt_status st) {
     g_create_error = p->error;
@@ -360,6 +365,10 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   p->panel_ptr = hp.panel_ptr;
   ADT_UP(&p->owners, hp.bowners);
   p->nfixed = (int)hp.fixed.size();
+  if (cudaMalloc(&p->tc_error, sizeof(int)) != cudaSuccess || cudaMemset(p->tc_error, 0, sizeof(int)) != cudaSuccess ||
+      cudaHostAlloc(&p->tc_error_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+    return bail(fail(p, ADT_OOM, "error flag allocation failed"));
+  *p->tc_error_host = 0;
   p->nowners = (int)hp.bowners.size();
 #undef ADT_UP
   *out = p;
@@ -374,9 +383,10 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
                   p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
-                  p->fixed, p->owners, p->titems, p->update_items};
+                  p->fixed, p->owners, p->titems, p->update_items, p->tc_error};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  if (p->tc_error_host) cudaFreeHost(p->tc_error_host);
   for (auto& s : p->slots) {
     if (s.values) cudaFree(s.values);
     if (s.factors) cudaFree(s.factors);
@@ -617,6 +627,33 @@ adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_beg
   if (!p || !fields || !jacobian || row_begin < 0 || row_count < 0 || row_begin + row_count > p->D)
     return fail(p, ADT_INVALID_ARG, "invalid jacobian arguments");
   if (row_count == 0) return ADT_OK;
+  if (p->tc_error_host && *p->tc_error_host != 0)
+    return fail(p, ADT_TIMEOUT, "a tensor-core Jacobian launch of this plan timed out waiting for its MMAs");
+  if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count)) {
+    JacobianArgs a;
+    a.fields = fields;
+    a.features = p->features;
+    a.cell_dofs = p->cell_dofs;
+    a.fscale = p->fscale;
+    a.abmn = p->abmn;
+    a.out = jacobian;
+    a.W = p->W;
+    a.N = p->N;
+    a.E = p->E;
+    a.C = p->C;
+    a.K = p->K;
+    a.R = p->R;
+    a.row_begin = row_begin;
+    a.rows = row_count;
+    a.cells_per_block = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    const cudaError_t err = launch_jacobian_tc(a, p->tc_error, p->sms, s);
+    p->launches++;
+    if (err != cudaSuccess)
+      return fail(p, ADT_CUDA_ERROR, std::string("tensor-core jacobian: ") + cudaGetErrorString(err));
+    cudaMemcpyAsync(p->tc_error_host, p->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s);
+    return check_launch(p, "normal jacobian");
+  }
   const int E4 = (p->E + 3) & ~3;
   const int nt4 = E4 / 4, NT = nt4 * (nt4 + 1) / 2;
   // cells per block: a power of two (threads split evenly over cells), at most 5 Gram tiles and

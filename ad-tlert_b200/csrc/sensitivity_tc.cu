@@ -1,0 +1,367 @@
+// Normal-quadrupole Jacobian on the 5th-generation tensor cores (tcgen05, TMEM accumulators).
+//
+// Same contraction as jacobian_kernel: for every cell c the electrode Gram
+//   G_c = F_c^T F_c,   F_c[w R + f][e] = sqrt(w_w) (k_w) L_c[f] . x_we   (R features per wavenumber),
+// and each ABMN row takes four Gram entries, J[d][c] = -(G[M][A] - G[M][B] - G[N][A] + G[N][B]).
+// Here the Gram is one tcgen05.mma chain per cell: A = B = F_c^T (electrodes x features,
+// K-major) in shared memory, D = G_c (64 x N, fp32) in tensor memory, M = 64 rows (rows >= E read
+// whatever follows in shared memory and only feed rows of D that are never read), N = E rounded
+// up to 8, K = 8 features per instruction. Float32 accuracy comes from a hi/lo split of every
+// feature (hi = TF32 rounding, lo = the remainder): G = hi.hi + hi.lo + lo.hi, three MMAs per
+// K-step accumulating in fp32.
+//
+// Persistent blocks (two per SM; 256 threads each) loop over groups of kCells consecutive cells:
+// (1) all threads compute the features of the group into shared memory (generic proxy, then
+// fence.proxy.async); (2) one thread issues the MMAs (each cell into its own TMEM columns) and
+// commits them to an mbarrier; (3) all threads wait on it (bounded: on timeout the block raises
+// the error flag, writes NaN for its rows and stops); (4) warps read their TMEM lanes back
+// (tcgen05.ld), stage the Grams in shared memory and gather the rows, kCells consecutive floats
+// per row. Shared-memory operand layout (no swizzle, K-major canonical layout): feature chunk kc
+// (4 features, 16 bytes) of electrode row e at ((part*kCells + cell)*KC + kc)*E*16 + e*16, so one
+// 8-row core matrix is 128 contiguous bytes (stride byte offset 128) and the two 16-byte K halves
+// of one MMA are E*16 bytes apart (leading byte offset).
+#include "adt_internal.h"
+#include "kernels.h"
+
+namespace adt {
+namespace {
+
+constexpr int kTcThreads = 256;
+constexpr int kTcCells = 2;      // cells per group (two blocks share an SM)
+constexpr int kTcM = 64;         // MMA M (electrode rows, padded)
+constexpr uint32_t kTcWaitLimit = 1u << 20;  // mbarrier polls before the block gives up
+constexpr int kTcRowTable = 4096;            // rows whose Gram offsets stay in shared memory
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor (sm_100 format: version 1 at bits 46-47).
+__device__ __forceinline__ uint64_t operand_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;  // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: fp32 accumulate, TF32 A and B, both K-major, M x N.
+__host__ __device__ constexpr uint32_t tf32_idesc(int m, int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ float tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ void tmem_load16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+}
+
+}  // namespace
+
+// Shared memory of jacobian_tc_kernel for E electrodes, W wavenumbers, R features, K dofs.
+size_t jacobian_tc_smem(int E, int W, int R, int K, int rows) {
+  const int KC = (W * R + 7) / 8 * 2;  // 16-byte feature chunks per electrode row (K padded to 8)
+  const size_t feat = (size_t)2 * kTcCells * KC * E * 16 + (size_t)(kTcM + 8) * 16;
+  const size_t gram = (size_t)kTcCells * (E * (E + 1) + 1) * 4;
+  const size_t tables = (size_t)kTcCells * (R * K + K) * 4 + (size_t)W * R * 4;
+  // per row: Gram offsets of (M,A) (M,B) (N,A) (N,B); at most kTcRowTable rows resident
+  const size_t offsets = (size_t)(rows < kTcRowTable ? rows : kTcRowTable) * 8;
+  return (feat + gram + tables + offsets + 64 + 31) / 16 * 16;
+}
+
+// KT dofs and RT features per cell are compile-time.
+template <int KT, int RT>
+__global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs a, int* error) {
+  extern __shared__ __align__(128) unsigned char tc_sm[];
+  constexpr int K = KT, R = RT;
+  const int E = a.E, W = a.W;
+  const int N = (E + 7) & ~7;
+  const int KF = W * R, KC = (KF + 7) / 8 * 2, KS = KC / 2;  // features, 16B chunks, MMA K-steps
+  const size_t part_bytes = (size_t)kTcCells * KC * E * 16;
+  unsigned char* feat = tc_sm;                                         // [2][kTcCells][KC][E][4] fp32
+  float* gram = reinterpret_cast<float*>(feat + 2 * part_bytes + (kTcM + 8) * 16);  // [kTcCells][E(E+1)+1]
+  const int GLD = E + 1, GS = E * GLD + 1;                            // entry GS-1 is the remote zero
+  float* coef = gram + (size_t)kTcCells * GS;                          // [kTcCells][R][K]
+  float* scale = coef + kTcCells * R * K;                              // [W][R]
+  int* dofs = reinterpret_cast<int*>(scale + W * R);                   // [kTcCells][K]
+  const int table_rows = min(a.rows, kTcRowTable);
+  short4* offs = reinterpret_cast<short4*>(
+      (reinterpret_cast<uintptr_t>(dofs + kTcCells * K) + 7) & ~uintptr_t(7));  // [table_rows]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(offs + table_rows) + 15) & ~uintptr_t(15));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int groups = (a.C + kTcCells - 1) / kTcCells;
+  const uint32_t columns_needed = (uint32_t)(kTcCells * N);
+  uint32_t tmem_cols = 32;
+  while (tmem_cols < columns_needed) tmem_cols <<= 1;
+
+  // set-up: mbarrier (one arrival per group) and the tensor-memory columns of the block
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 ::"r"(smem_addr(tmem_slot)), "r"(tmem_cols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = tf32_idesc(kTcM, N);
+  bool failed = false;
+  uint32_t phase = 0;
+  // per-block tables: feature scales, Gram offsets of every row (remote slot: the zero entry)
+  for (int i = tid; i < W * R; i += kTcThreads) scale[i] = a.fscale[i];
+  auto fill_offsets = [&](int r0, int n) {
+    for (int d = tid; d < n; d += kTcThreads) {
+      const int4 q = *reinterpret_cast<const int4*>(a.abmn + 4 * (a.row_begin + r0 + d));
+      auto at = [&](int i, int k) -> short {
+        return (short)(((unsigned)i < (unsigned)E && (unsigned)k < (unsigned)E) ? i * GLD + k : GS - 1);
+      };
+      offs[d] = make_short4(at(q.z, q.x), at(q.z, q.y), at(q.w, q.x), at(q.w, q.y));
+    }
+  };
+  const bool resident = a.rows <= kTcRowTable;
+  if (resident) fill_offsets(0, a.rows);
+  for (int ci = tid; ci < kTcCells; ci += kTcThreads) gram[(size_t)ci * GS + GS - 1] = 0.f;
+  // padded features (KF .. 8 KS) are zero for every group: written once
+  for (int item = tid; item < kTcCells * (KC * 4 - KF) * E; item += kTcThreads) {
+    const int e = item % E, rest = item / E;
+    const int kf = KF + rest % (KC * 4 - KF), ci = rest / (KC * 4 - KF);
+    const size_t off = (((size_t)ci * KC + (kf >> 2)) * E + e) * 16 + (kf & 3) * 4;
+    *reinterpret_cast<float*>(feat + off) = 0.f;
+    *reinterpret_cast<float*>(feat + part_bytes + off) = 0.f;
+  }
+
+  for (int group = blockIdx.x; group < groups && !failed; group += gridDim.x) {
+    const int c0 = group * kTcCells;
+    // (1) cell tables, then features (hi part 0, lo part 1); padded features are zero
+    for (int i = tid; i < kTcCells * R * K; i += kTcThreads) {
+      const int c = min(c0 + i / (R * K), a.C - 1);
+      coef[i] = a.features[(int64_t)c * R * K + i % (R * K)];
+    }
+    for (int i = tid; i < kTcCells * K; i += kTcThreads) {
+      const int c = c0 + i / K;
+      dofs[i] = c < a.C ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
+    }
+    __syncthreads();
+    {
+      // 4 lane groups of 64 threads; thread e of a group handles electrode e of wavenumbers
+      // lg, lg + 4, ... of every cell of the group; all its field loads are issued first
+      constexpr int kMaxWPer = 8;
+      const int lg = tid >> 6, e = tid & 63;
+      if (e < E) {
+        for (int ci = 0; ci < kTcCells; ++ci) {
+          int dof[K];
+#pragma unroll
+          for (int k = 0; k < K; ++k) dof[k] = dofs[ci * K + k];
+          float x[kMaxWPer][K];
+#pragma unroll
+          for (int j = 0; j < kMaxWPer; ++j) {
+            const int w = lg + 4 * j;
+            const float* fw = a.fields + (int64_t)w * a.N * E + e;
+#pragma unroll
+            for (int k = 0; k < K; ++k) x[j][k] = (w < W && dof[k] >= 0) ? __ldg(fw + (int64_t)dof[k] * E) : 0.f;
+          }
+          float cf[R][K];
+#pragma unroll
+          for (int f = 0; f < R; ++f)
+#pragma unroll
+            for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
+          unsigned char* cell_feat = feat + (size_t)ci * KC * E * 16 + (size_t)e * 16;
+#pragma unroll
+          for (int j = 0; j < kMaxWPer; ++j) {
+            const int w = lg + 4 * j;
+            if (w >= W) break;
+#pragma unroll
+            for (int f = 0; f < R; ++f) {
+              float v = 0.f;
+#pragma unroll
+              for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[j][k], v);
+              v *= scale[w * R + f];
+              const float hi = tf32_round(v);
+              const int kf = w * R + f;
+              float* dst = reinterpret_cast<float*>(cell_feat + (size_t)(kf >> 2) * E * 16) + (kf & 3);
+              dst[0] = hi;
+              dst[part_bytes / 4] = v - hi;
+            }
+          }
+        }
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+    // (2) one thread issues every MMA of the group and commits them to the mbarrier
+    if (tid == 0) {
+      const uint32_t base = smem_addr(feat);
+      for (int ci = 0; ci < kTcCells; ++ci) {
+        const uint32_t d = tmem + (uint32_t)(ci * N);
+        for (int s = 0; s < KS; ++s) {
+          const uint32_t hi = base + (uint32_t)(((size_t)ci * KC + 2 * s) * E * 16);
+          const uint32_t lo = hi + (uint32_t)part_bytes;
+          const uint64_t dh = operand_desc(hi, (uint32_t)E * 16, 128);
+          const uint64_t dl = operand_desc(lo, (uint32_t)E * 16, 128);
+          mma_tf32(d, dh, dh, idesc, s > 0 ? 1u : 0u);
+          mma_tf32(d, dh, dl, idesc, 1u);
+          mma_tf32(d, dl, dh, idesc, 1u);
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                   ::"r"(smem_addr(bar)) : "memory");
+    }
+
+    // (3) bounded wait for the MMAs
+    uint32_t polls = 0;
+    while (!mbar_try_wait(smem_addr(bar), phase)) {
+      if (++polls >= kTcWaitLimit) { failed = true; break; }
+    }
+    phase ^= 1u;
+    failed = __syncthreads_or(failed);
+    if (failed) break;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+    // (4) tensor memory -> staged Grams: warp q (and q + 4) owns TMEM lanes 32q..32q+31, which
+    //     hold rows 16q..16q+15 of every M = 64 accumulator in lanes 0..15
+    {
+      const int q = warp & 3;
+      const int row = 16 * q + lane;
+      for (int ci = warp >> 2; ci < kTcCells; ci += 2) {
+        for (int cc = 0; cc < N; cc += 16) {
+          uint32_t v[16];
+          tmem_load16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(ci * N + cc), v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+          if (lane < 16 && row < E) {
+            float* g = gram + (size_t)ci * GS + (size_t)row * GLD;
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if (cc + j < E) g[cc + j] = __uint_as_float(v[j]);
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    // (5) rows: one thread per row, both cells of the group (adjacent floats of J); with more
+    //     rows than the table holds, the table is refilled chunk by chunk
+    const int ncells = min(kTcCells, a.C - c0);
+    for (int r0 = 0; r0 < a.rows; r0 += kTcRowTable) {
+      const int n = min(kTcRowTable, a.rows - r0);
+      if (!resident) {
+        if (r0 > 0) __syncthreads();
+        fill_offsets(r0, n);
+        __syncthreads();
+      }
+      for (int d = tid; d < n; d += kTcThreads) {
+        const int dl = r0 + d;
+        const short4 o = offs[d];
+        float v[kTcCells];
+#pragma unroll
+        for (int ci = 0; ci < kTcCells; ++ci) {
+          const float* g = gram + (size_t)ci * GS;
+          v[ci] = -((g[o.x] - g[o.y]) - (g[o.z] - g[o.w]));
+        }
+        float* out = a.out + (int64_t)dl * a.C + c0;
+        if (ncells == kTcCells && (((uintptr_t)out & 7) == 0)) {
+          *reinterpret_cast<float2*>(out) = make_float2(v[0], v[1]);
+        } else {
+          for (int ci = 0; ci < ncells; ++ci) out[ci] = v[ci];
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  if (failed) {
+    if (tid == 0) atomicOr(error, 1);
+    // NaN in every row of this block's remaining cells
+    for (int group = blockIdx.x; group < groups; group += gridDim.x)
+      for (int idx = tid; idx < a.rows * kTcCells; idx += kTcThreads) {
+        const int c = group * kTcCells + idx % kTcCells;
+        if (c < a.C) a.out[(int64_t)(idx / kTcCells) * a.C + c] = __int_as_float(0x7fc00000);
+      }
+    // the last commit may still be pending: give it a bounded second chance before freeing
+    uint32_t polls = 0;
+    while (!mbar_try_wait(smem_addr(bar), phase ^ 1u) && ++polls < kTcWaitLimit) {
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmem_cols) : "memory");
+}
+
+template __global__ void jacobian_tc_kernel<3, 5>(JacobianArgs, int*);
+template __global__ void jacobian_tc_kernel<3, 6>(JacobianArgs, int*);
+template __global__ void jacobian_tc_kernel<4, 3>(JacobianArgs, int*);
+template __global__ void jacobian_tc_kernel<4, 7>(JacobianArgs, int*);
+template __global__ void jacobian_tc_kernel<4, 8>(JacobianArgs, int*);
+
+namespace {
+bool tc_shape(int K, int R) {
+  return (K == 3 && (R == 5 || R == 6)) || (K == 4 && (R == 3 || R == 7 || R == 8));
+}
+}  // namespace
+
+// Whether the tensor-core kernel applies: E <= 64 electrode slots, an instantiated (K, R), and
+// two blocks' shared memory per SM.
+bool jacobian_tc_supported(int E, int W, int R, int K, int rows) {
+  return E <= kTcM && tc_shape(K, R) && W <= 32 && jacobian_tc_smem(E, W, R, K, rows) <= 110 * 1024;
+}
+
+cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaStream_t s) {
+  const size_t smem = jacobian_tc_smem(a.E, a.W, a.R, a.K, a.rows);
+  const int groups = (a.C + kTcCells - 1) / kTcCells;
+  const int blocks = groups < 2 * sms ? groups : 2 * sms;
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<blocks, kTcThreads, smem, s>>>(a, error);
+    return cudaGetLastError();
+  };
+  if (a.K == 3 && a.R == 5) return go(jacobian_tc_kernel<3, 5>);
+  if (a.K == 3 && a.R == 6) return go(jacobian_tc_kernel<3, 6>);
+  if (a.K == 4 && a.R == 3) return go(jacobian_tc_kernel<4, 3>);
+  if (a.K == 4 && a.R == 7) return go(jacobian_tc_kernel<4, 7>);
+  return go(jacobian_tc_kernel<4, 8>);
+}
+
+}  // namespace adt

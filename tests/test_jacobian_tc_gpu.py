@@ -1,0 +1,73 @@
+"""The tensor-core (tcgen05) Jacobian against the CUDA-core Jacobian kernel and the FP64 oracle.
+
+``ADTLERT_B200_JACOBIAN=fma`` at plan creation selects the CUDA-core kernel; both must agree to
+float32 accuracy on 2.5D sections (12 and 48 electrodes) and a 3D box."""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from adtlert_b200 import ERTForward2p5D, ERTForward3D, Mesh, Mesh3D, Survey, synthetic
+from cases import case3d_inputs, case_inputs
+from conftest import assert_close
+from oracle.ert2p5d import Oracle2p5D
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(make):
+    tc = make()
+    os.environ["ADTLERT_B200_JACOBIAN"] = "fma"
+    try:
+        fma = make()
+    finally:
+        del os.environ["ADTLERT_B200_JACOBIAN"]
+    return tc, fma
+
+
+def test_tensor_core_jacobian_matches_the_cuda_core_kernel_2p5d():
+    inputs = case_inputs("tri_flat")
+    mesh = Mesh.from_arrays(inputs["nodes"], inputs["cells"])
+    survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
+    tc, fma = _pair(lambda: ERTForward2p5D(mesh, survey))
+    sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float32)
+    a, b = tc.jacobian(sigma), fma.jacobian(sigma)
+    assert_close(a, b, 2e-6, "tcgen05 vs FMA jacobian")
+    oracle = Oracle2p5D(inputs["nodes"], inputs["cells"], inputs["electrodes"], inputs["measurements"])
+    assert_close(a, oracle.normal_jacobian(inputs["sigma"]), 1e-4, "tcgen05 jacobian vs oracle")
+
+
+def test_tensor_core_jacobian_on_the_benchmark_section():
+    nodes, cells, electrodes, abmn = synthetic.flat_section()
+    mesh, survey = Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, abmn)
+    tc, fma = _pair(lambda: ERTForward2p5D(mesh, survey))
+    sigma = torch.as_tensor(synthetic.layered_model(nodes, cells, 1), dtype=torch.float32)
+    a, b = tc.jacobian(sigma), fma.jacobian(sigma)
+    assert torch.isfinite(a).all()
+    assert_close(a, b, 2e-6, "tcgen05 vs FMA jacobian (48 electrodes)")
+    assert torch.equal(a, tc.jacobian(sigma)), "bitwise repeatable"
+
+
+def test_tensor_core_jacobian_3d():
+    inputs = case3d_inputs("tet_mixed")
+    mesh = Mesh3D.from_arrays(inputs["nodes"], inputs["cells"])
+    survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
+    tc, fma = _pair(lambda: ERTForward3D(mesh, survey))
+    sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float32)
+    assert_close(tc.jacobian(sigma), fma.jacobian(sigma), 2e-6, "tcgen05 vs FMA jacobian (3D)")
+
+
+def test_tensor_core_jacobian_with_more_rows_than_the_offset_table():
+    # 4 x 1232 = 4928 rows: more than the 4096 rows whose Gram offsets stay in shared memory
+    nodes, cells, electrodes, abmn = synthetic.flat_section()
+    abmn = np.concatenate([abmn, abmn[::-1], abmn, abmn[::-1]])
+    mesh, survey = Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, abmn)
+    tc, fma = _pair(lambda: ERTForward2p5D(mesh, survey))
+    sigma = torch.as_tensor(synthetic.layered_model(nodes, cells, 2), dtype=torch.float32)
+    a, b = tc.jacobian(sigma), fma.jacobian(sigma)
+    assert a.shape[0] == 4928 and torch.isfinite(a).all()
+    assert_close(a, b, 2e-6, "tcgen05 vs FMA jacobian (4928 rows)")
+    n = len(abmn) // 4
+    assert torch.equal(a[:n], a[2 * n:3 * n]) and torch.equal(a[n:2 * n], a[3 * n:])
