@@ -290,9 +290,24 @@ __device__ void upper_solve(const double* l, int ldl, const double* rinv, double
 
 template <int MAXM>
 __host__ __device__ constexpr int aug_ld() { return 3 * MAXM + 1; }
+// Augmented matrix, two buffers of panel rows (8 x 3 MAXM) and panel columns (MAXM x 9), and per
+// warp the pivot-block inverse (8 x 8) and its own rows of L P^-1 (MAXM / 8 x 8).
 template <int MAXM>
 constexpr size_t invert_smem() {
-  return sizeof(double) * ((size_t)MAXM * aug_ld<MAXM>() + 2 * 8 * 3 * (size_t)MAXM + (size_t)MAXM * 9 + 8 * 9);
+  return sizeof(double) * ((size_t)MAXM * aug_ld<MAXM>() + 2 * 8 * 3 * (size_t)MAXM + 2 * (size_t)MAXM * 9 +
+                           8 * 64 + 8 * (size_t)MAXM);
+}
+
+// 1 / x for x > 0 (NaN otherwise): the hardware approximation refined by two Newton-Raphson steps
+// y <- y + y (1 - x y), each of which squares the relative error.
+__device__ __forceinline__ double positive_reciprocal(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  return x > 0.0 ? y : quiet_nan();
 }
 template <int MAXM>
 constexpr size_t update_smem() { return sizeof(double) * (5 * (size_t)MAXM * (MAXM + 1)); }
@@ -354,10 +369,12 @@ __device__ void store_tile(double (&acc)[4][4], const Micro& u, double* C, int64
 // 8: with the panel P (8 x 8), its rows R, its columns L and the rest S, one step is
 // P <- P^-1, R <- P^-1 R, L <- -L P^-1, S <- S - L P^-1 R. Every thread holds a fixed set of
 // augmented entries in registers (rows tr + 8 r, columns tc + 32 c; a panel's rows are pass
-// r = k0 / 8 of the 8 row groups), panel rows and columns go through shared memory, and warp 0
-// inverts the 8 x 8 pivot block with shuffles; four barriers per panel. Stored: G_j, Z_p,
-// V_q = Z_q^T, copies of the couplings (for the Schur updates) and the fill A[q,p] = -A[q,j] Z_p.
-// A non-positive pivot becomes NaN, which reaches every result of the system.
+// r = k0 / 8 of the 8 row groups). A step publishes the panel rows (with the identity in the
+// panel columns) and columns to one of two buffers, then one barrier; every warp inverts P
+// itself, forms C = L P^-1 for its own rows (C = -P^-1 on the panel rows, which start from
+// zero), and updates its entries by a <- a - C R. Stored: G_j, Z_p, V_q = Z_q^T, copies of the
+// couplings (for the Schur updates) and the fill A[q,p] = -A[q,j] Z_p. A non-positive pivot
+// becomes NaN, which reaches every result of the system.
 template <int MAXM>
 __global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
 invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int* __restrict__ csr_ptr,
@@ -370,10 +387,10 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
   constexpr int PB = 8;                         // pivot panel
   extern __shared__ double sm[];
   double* aug = sm;                             // [MAXM][LDA]
-  double* rbuf = aug + MAXM * LDA;              // panel rows      [PB][W3]
-  double* rnew = rbuf + PB * W3;                // P^-1 R          [PB][W3]
-  double* lbuf = rnew + PB * W3;                // panel columns   [MAXM][PB + 1]
-  double* pinv = lbuf + MAXM * (PB + 1);        // P^-1            [PB][PB + 1]
+  double* rbuf = aug + MAXM * LDA;              // panel rows      [2][PB][W3]
+  double* lbuf = rbuf + 2 * PB * W3;            // panel columns   [2][MAXM][PB + 1]
+  double* pinv_all = lbuf + 2 * MAXM * (PB + 1);  // per warp P^-1 [8][PB][PB]
+  double* c_all = pinv_all + 8 * PB * PB;       // per warp C      [8][RP][PB]
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* val = values + (int64_t)blockIdx.y * nnz;
   double* f = factors + (int64_t)blockIdx.y * stride;
@@ -429,6 +446,8 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
 
   // 3. block Gauss-Jordan in registers
   const int tc = threadIdx.x & 31, tr = threadIdx.x >> 5;
+  double* pinv = pinv_all + tr * PB * PB;
+  double* cw = c_all + tr * RP * PB;
   double a[RP][CP];
 #pragma unroll
   for (int r = 0; r < RP; ++r)
@@ -437,95 +456,88 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
       const int i = tr + 8 * r, j = tc + 32 * c;
       a[r][c] = (i < mj && j < width) ? aug[i * LDA + j] : 0.0;
     }
-  for (int k0 = 0; k0 < mj; k0 += PB) {
+  for (int k0 = 0, buf = 0; k0 < mj; k0 += PB, buf ^= 1) {
     const int nb = min(PB, mj - k0), rb = k0 / PB;
-    // (a) publish the panel rows (row k0 + tr: pass rb) and the panel columns
+    double* rows = rbuf + buf * PB * W3;
+    double* cols = lbuf + buf * MAXM * (PB + 1);
+    // (a) publish the panel rows (row k0 + tr: pass rb; identity in the panel columns) and the
+    //     panel columns (P itself in rows k0 .. k0 + 7); no warp still reads this buffer, since
+    //     every warp has passed the previous step's barrier
 #pragma unroll
     for (int r = 0; r < RP; ++r) {
       const int i = tr + 8 * r;
 #pragma unroll
       for (int c = 0; c < CP; ++c) {
         const int j = tc + 32 * c;
-        if (r == rb && j < W3) rbuf[tr * W3 + j] = (tr < nb && j < width) ? a[r][c] : 0.0;
         const unsigned s = (unsigned)(j - k0);
-        if (s < (unsigned)PB && i < MAXM) lbuf[i * (PB + 1) + s] = (s < (unsigned)nb && i < mj) ? a[r][c] : 0.0;
+        if (r == rb && j < W3)
+          rows[tr * W3 + j] = tr >= nb ? 0.0 : s < (unsigned)nb ? (s == (unsigned)tr ? 1.0 : 0.0)
+                                                                  : (j < width ? a[r][c] : 0.0);
+        if (s < (unsigned)PB) cols[i * (PB + 1) + s] = (s < (unsigned)nb && i < mj) ? a[r][c] : 0.0;
       }
     }
     __syncthreads();
-    // (b) P^-1 by warp 0: lane s holds row s (the padding beyond nb is the identity)
-    if (tr == 0) {
+    // (b) P^-1 by every warp (lane s < 8 holds row s; the padding beyond nb is the identity)
+    {
       double row[PB];
+      const int ls = tc & (PB - 1);
 #pragma unroll
-      for (int c = 0; c < PB; ++c) row[c] = (tc < nb && c < nb) ? rbuf[tc * W3 + k0 + c] : (tc == c ? 1.0 : 0.0);
+      for (int c = 0; c < PB; ++c)
+        row[c] = (ls < nb && c < nb) ? cols[(k0 + ls) * (PB + 1) + c] : (ls == c ? 1.0 : 0.0);
 #pragma unroll
       for (int k = 0; k < PB; ++k) {
-        const double pivot = __shfl_sync(0xffffffffu, row[k], k);
-        const double inv = pivot > 0.0 ? 1.0 / pivot : quiet_nan();
         double rk[PB];
 #pragma unroll
         for (int c = 0; c < PB; ++c) rk[c] = __shfl_sync(0xffffffffu, row[c], k);
+        const double inv = positive_reciprocal(rk[k]);
         const double lik = row[k] * inv;
 #pragma unroll
         for (int c = 0; c < PB; ++c) {
-          if (tc == k) row[c] = (c == k) ? inv : row[c] * inv;
+          if (ls == k) row[c] = (c == k) ? inv : row[c] * inv;
           else row[c] = (c == k) ? -lik : fma(-lik, rk[c], row[c]);
         }
       }
       if (tc < PB)
 #pragma unroll
-        for (int c = 0; c < PB; ++c) pinv[tc * (PB + 1) + c] = row[c];
+        for (int c = 0; c < PB; ++c) pinv[tc * PB + c] = row[c];
     }
-    __syncthreads();
-    // (c) R' = P^-1 R (rows s < nb; zero beyond), with P^-1 itself in the panel columns, so that
-    //     one rank-8 update below gives S - L P^-1 R and (from zero) -L P^-1
-    for (int idx = threadIdx.x; idx < PB * W3; idx += blockDim.x) {
-      const int s = idx / W3, j = idx - s * W3;
-      const unsigned sj = (unsigned)(j - k0);
+    __syncwarp();
+    // (c) C for this warp's rows: L P^-1, or -P^-1 on a panel row
+    for (int e = tc; e < RP * PB; e += 32) {
+      const int r = e / PB, u = e - r * PB, i = tr + 8 * r;
       double v = 0.0;
-      if (s < nb) {
-        if (sj < (unsigned)nb) {
-          v = pinv[s * (PB + 1) + sj];
-        } else {
+      if (r == rb && tr < nb) {
+        v = -pinv[tr * PB + u];
+      } else {
 #pragma unroll
-          for (int u = 0; u < PB; ++u) v = fma(pinv[s * (PB + 1) + u], rbuf[u * W3 + j], v);
-        }
+        for (int w = 0; w < PB; ++w) v = fma(cols[i * (PB + 1) + w], pinv[w * PB + u], v);
       }
-      rnew[idx] = v;
+      cw[e] = v;
     }
-    __syncthreads();
-    // (d) rank-8 update of every held entry (outer products), then the panel rows take R'
+    __syncwarp();
+    // (d) a <- keep a - C R: the panel columns and the panel rows start from zero
 #pragma unroll
     for (int c = 0; c < CP; ++c) {
       const unsigned sj = (unsigned)(tc + 32 * c - k0);
-      if (sj < (unsigned)nb)
 #pragma unroll
-        for (int r = 0; r < RP; ++r) a[r][c] = 0.0;
+      for (int r = 0; r < RP; ++r)
+        if (sj < (unsigned)nb || (r == rb && tr < nb)) a[r][c] = 0.0;
     }
 #pragma unroll
     for (int u = 0; u < PB; ++u) {
       double lu[RP], ru[CP];
 #pragma unroll
-      for (int r = 0; r < RP; ++r) lu[r] = lbuf[(tr + 8 * r) * (PB + 1) + u];
+      for (int r = 0; r < RP; ++r) lu[r] = cw[r * PB + u];
 #pragma unroll
       for (int c = 0; c < CP; ++c) {
         const int j = tc + 32 * c;
-        ru[c] = j < W3 ? rnew[u * W3 + j] : 0.0;
+        ru[c] = j < W3 ? rows[u * W3 + j] : 0.0;
       }
 #pragma unroll
       for (int r = 0; r < RP; ++r)
 #pragma unroll
         for (int c = 0; c < CP; ++c) a[r][c] = fma(-lu[r], ru[c], a[r][c]);
     }
-    if (tr < nb)
-#pragma unroll
-      for (int r = 0; r < RP; ++r)
-        if (r == rb)
-#pragma unroll
-          for (int c = 0; c < CP; ++c) {
-            const int j = tc + 32 * c;
-            a[r][c] = j < W3 ? rnew[tr * W3 + j] : 0.0;
-          }
-    __syncthreads();
   }
 
   // 4. G_j, Z_p, V_q to the factor storage; Z_p back to shared memory for the fill
