@@ -314,6 +314,7 @@ class ERTForward2p5D:
         self._lib = _native.load_library()
         self._cache: dict = {}
         self._field_cache = FieldCache(self.normal_field_cache_max_entries)
+        self._pending_checks = None  # (device flag, context) pairs read back with a host result
         self._solver = _Slots()
         self._plan = None
         self._build(int(quadrature_order))
@@ -551,8 +552,28 @@ class ERTForward2p5D:
         self._solver.factorizations += 1
         total = torch.empty((batch, self.W, self.N, self.E), dtype=torch.float32, device=self.device)
         self._call("adt_solve_fields", entry["slot"], _native.ptr(sig), batch, _native.ptr(total), self._stream())
-        check_finite(total, "total fields")
+        if self._pending_checks is not None:
+            self._pending_checks.append((torch.isfinite(total).all(), "total fields"))
+        else:
+            check_finite(total, "total fields")
         return [_Fields(total[i]) for i in range(batch)]
+
+    @contextlib.contextmanager
+    def _deferred_checks(self):
+        """Finiteness checks of solved fields queued on the device and read after the block, whose
+        result copy synchronizes anyway; on a failure the field cache is cleared (so non-finite
+        fields are never served later) and the same FloatingPointError is raised."""
+
+        self._pending_checks = []
+        try:
+            yield
+            pending = self._pending_checks
+        finally:
+            self._pending_checks = None
+        if pending and not bool(torch.stack([flag for flag, _ in pending]).all()):
+            self._field_cache.clear()
+            context = next(what for flag, what in pending if not bool(flag))
+            raise FloatingPointError(f"{context} produced non-finite values")
 
     def _fields_series(self, models: Tensor):
         return self._field_cache.solve_series(models, self.series_batch_steps, self._solve_fields)
@@ -723,9 +744,20 @@ class ERTForward2p5D:
 
     def jacobian(self, conductivity, *, batch_size=None, include_robin_boundary_derivative: bool = False,
                  normal_sensitivity: bool = True) -> Tensor:
-        return self.solve_with_jacobian(conductivity, batch_size=batch_size,
-                                        include_robin_boundary_derivative=include_robin_boundary_derivative,
-                                        normal_sensitivity=normal_sensitivity)[1]
+        """The Jacobian of ``solve_with_jacobian`` without the response: on the direct path only the
+        fields and J are computed, and J's copy to the host is the call's one synchronization."""
+
+        direct = normal_sensitivity and not include_robin_boundary_derivative
+        if not direct:
+            return self.solve_with_jacobian(conductivity, batch_size=batch_size,
+                                            include_robin_boundary_derivative=include_robin_boundary_derivative,
+                                            normal_sensitivity=normal_sensitivity)[1]
+        self._batch_size(batch_size, direct)
+        with self._deferred_checks():
+            J = self._jacobian_device(self._fields(conductivity),
+                                      self._columns(None, None, discretization=True))
+            host = _to_host(J)
+        return host.to(self.dtype)
 
     def jacobian_columnwise(self, conductivity) -> Tensor:
         basis = torch.eye(self.C, dtype=self.dtype)

@@ -243,3 +243,19 @@ def test_flat_benchmark_section_matches_the_oracle():
     sub = Oracle2p5D(nodes, cells, electrodes, rows[picks])
     assert_close(J[picks], sub.normal_jacobian(sigma.astype(float)), TOL, "flat section jacobian rows")
     assert forward.kernel_launches() > 0
+
+
+def test_non_finite_fields_raise_and_are_not_cached():
+    # a subnormal conductivity puts the float32 fields beyond the float32 range
+    inputs = case_inputs("tri_flat")
+    forward = ERTForward2p5D(Mesh.from_arrays(inputs["nodes"], inputs["cells"]),
+                             Survey.from_arrays(inputs["electrodes"], inputs["measurements"]))
+    tiny = torch.full((forward.C,), 1e-40)
+    for _ in range(2):  # the second call solves again instead of serving cached fields
+        with pytest.raises(FloatingPointError, match="total fields"):
+            forward.jacobian(tiny)
+    assert forward.normal_field_cache_info()["entries"] == 0
+    with pytest.raises(FloatingPointError, match="total fields"):
+        forward.solve(tiny)
+    sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float32)
+    assert torch.isfinite(forward.jacobian(sigma)).all()
