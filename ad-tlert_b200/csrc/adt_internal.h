@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "adtlert_b200.h"
@@ -14,6 +15,32 @@ namespace adt {
 
 // Threads of the solver kernels.
 constexpr int kSolverThreads = 256;
+
+// The library's kernels run as one dependent chain per stream. Each kernel's first statement
+// waits for the grid before it in the stream (griddepcontrol.wait: that grid has completed and
+// its memory is visible) and then lets the next grid be scheduled; every launch allows
+// programmatic stream serialization, so a grid's launch overlaps the drain of the one before.
+// A kernel launched without the attribute, or after a foreign kernel, waits as usual.
+__device__ __forceinline__ void chain_wait() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
+template <typename... P, typename... A>
+inline cudaError_t launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  A&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 struct Slot {
   int systems = 0;          // systems currently factorized (models * W)

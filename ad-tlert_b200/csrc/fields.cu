@@ -15,6 +15,7 @@ namespace adt {
 // for systems t = model * W + w. Replaces _assemble + GroupSum (adtlert/forward/ert2p5d.py:275-314,
 // adtlert/forward/kernels.py:30-85).
 __global__ void assemble_kernel(AssembleArgs a) {
+  chain_wait();
   const int64_t total = (int64_t)a.systems * a.nnz;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -47,6 +48,7 @@ __global__ void assemble_kernel(AssembleArgs a) {
 // cell (a list of one). Replaces _source_resistivities (ert2p5d.py:480-511).
 __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
                                   const int* ptr, const int* cells, double* rho) {
+  chain_wait();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= models * E) return;
   const int s = idx / E, e = idx % E;
@@ -60,6 +62,7 @@ __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
 // where coef(t,e) = scale * (rho ? rho[model(t)][e] : 1). `x_per_model` selects whether x is indexed
 // by system (fields of each system) or by wavenumber (the primary field shared by all models).
 __global__ void spmm_kernel(SpmmArgs a) {
+  chain_wait();
   const int64_t total = (int64_t)a.systems * a.N * a.E;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -90,6 +93,7 @@ __global__ void spmm_kernel(SpmmArgs a) {
 // fields[t][n][e] = x[t][n][e] + rho[s][e] * primary[w][n][e]
 __global__ void total_kernel(const double* x, const double* primary, const double* rho, int W,
                              int N, int E, int systems, float* fields) {
+  chain_wait();
   const int64_t total = (int64_t)systems * N * E;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -106,6 +110,7 @@ __global__ void total_kernel(const double* x, const double* primary, const doubl
 // a padded (E+1) x (E+1) table (slot E: the zero remote row and column), one thread per entry.
 // Replaces _integrate + the electrode product of _normal_reciprocal (ert2p5d.py:560-582).
 __global__ void potentials_kernel(MeasureArgs a, int models, double* pot) {
+  chain_wait();
   const int E1 = a.E + 1;
   const int64_t total = (int64_t)models * E1 * E1;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
@@ -135,6 +140,7 @@ __global__ void potentials_kernel(MeasureArgs a, int models, double* pot) {
 // Normal and reciprocal transfers of every (model, row) from the potential table; in combine
 // mode the tangent of sign(n) sqrt|n r| instead (ert2p5d.py:584-589, 647-655, 886-890).
 __global__ void transfers_kernel(MeasureArgs a, int models, const double* pot) {
+  chain_wait();
   const int E1 = a.E + 1;
   const int64_t total = (int64_t)models * a.D;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
@@ -161,6 +167,7 @@ __global__ void transfers_kernel(MeasureArgs a, int models, const double* pot) {
 // names a row d and whether it carries the normal or the reciprocal cotangent.
 // Replaces _pair_cotangent (ert2p5d.py:591-629).
 __global__ void pair_kernel(PairArgs a) {
+  chain_wait();
   const int64_t total = (int64_t)a.count * a.E * a.E;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -198,6 +205,7 @@ __global__ void pair_kernel(PairArgs a) {
 // weight_w * sum_r pairs[q][e][r] Pel[r][n], nonzero only at receiver dofs (routed list).
 // Replaces _adjoint_rhs (ert2p5d.py:631-639).
 __global__ void adjoint_rhs_kernel(AdjointRhsArgs a) {
+  chain_wait();
   const int ncol = a.q_per_model * a.E;
   const int64_t total = (int64_t)a.systems * a.rdofs * ncol;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
@@ -219,6 +227,7 @@ __global__ void adjoint_rhs_kernel(AdjointRhsArgs a) {
 // weight_w * phi[w][n][e] * y[w][n][f]; a second pass sums the partials in block order.
 __global__ void gram_partial_kernel(const float* phi, const double* y, const double* weights,
                                     int W, int N, int E, int chunk, double* partial) {
+  chain_wait();
   extern __shared__ double rows[];
   const int64_t total = (int64_t)W * N;
   const int64_t begin = (int64_t)blockIdx.x * chunk;
@@ -237,6 +246,7 @@ __global__ void gram_partial_kernel(const float* phi, const double* y, const dou
 
 __global__ void gram_gather_kernel(const double* partial, int blocks, int E, int D,
                                    const int* abmn, double* out) {
+  chain_wait();
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= D) return;
   const int A = abmn[4 * d], B = abmn[4 * d + 1], M = abmn[4 * d + 2], N = abmn[4 * d + 3];
@@ -252,6 +262,7 @@ __global__ void gram_gather_kernel(const double* partial, int blocks, int E, int
 // integrated[e][orig] = sum_w weight_w fields[w][pos(orig)][e]
 __global__ void integrated_kernel(const float* fields, const double* weights, const int* iperm,
                                   int W, int N, int E, float* integrated) {
+  chain_wait();
   const int64_t total = (int64_t)N * E;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {

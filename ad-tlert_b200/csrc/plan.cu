@@ -136,7 +136,7 @@ AssembleArgs assemble_args(adt_plan* p, const float* sigma, int systems, double*
 void launch_assemble(adt_plan* p, const float* sigma, int systems, double* values, bool robin,
                      bool identity, cudaStream_t s) {
   AssembleArgs a = assemble_args(p, sigma, systems, values, robin, identity);
-  assemble_kernel<<<grid_for((int64_t)systems * p->nnz), 256, 0, s>>>(a);
+  launch_chained(assemble_kernel, grid_for((int64_t)systems * p->nnz), 256, 0, s, a);
   p->launches++;
 }
 
@@ -161,7 +161,7 @@ void launch_spmm(adt_plan* p, const double* values, bool values_per_wavenumber, 
   a.nnz = p->nnz;
   a.x_per_system = x_per_system ? 1 : 0;
   a.values_per_wavenumber = values_per_wavenumber ? 1 : 0;
-  spmm_kernel<<<grid_for((int64_t)systems * p->N * p->E), 256, 0, s>>>(a);
+  launch_chained(spmm_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, a);
   p->launches++;
 }
 
@@ -195,8 +195,8 @@ void launch_measure(adt_plan* p, const TF* fields, int models, double* normal, d
     if (cudaMalloc(&p->pot, need * sizeof(double)) != cudaSuccess) return;
     p->pot_count = need;
   }
-  potentials_kernel<<<grid_for((int64_t)need), 256, 0, s>>>(a, models, p->pot);
-  transfers_kernel<<<grid_for((int64_t)models * p->D), 256, 0, s>>>(a, models, p->pot);
+  launch_chained(potentials_kernel, grid_for((int64_t)need), 256, 0, s, a, models, p->pot);
+  launch_chained(transfers_kernel, grid_for((int64_t)models * p->D), 256, 0, s, a, models, p->pot);
   p->launches += 2;
 }
 
@@ -217,7 +217,7 @@ void launch_pairs(adt_plan* p, const double* cot, const double* normal, const do
   a.unit = unit ? 1 : 0;
   a.row_begin = row_begin;
   a.model_of_count = model_of_count ? 1 : 0;
-  pair_kernel<<<grid_for((int64_t)count * p->E * p->E), 256, 0, s>>>(a);
+  launch_chained(pair_kernel, grid_for((int64_t)count * p->E * p->E), 256, 0, s, a);
   p->launches++;
 }
 
@@ -238,7 +238,7 @@ void launch_adjoint_rhs(adt_plan* p, const double* pairs, int systems, int q_per
   a.E = p->E;
   a.W = p->W;
   a.N = p->N;
-  adjoint_rhs_kernel<<<grid_for((int64_t)systems * p->rdofs * q_per_model * p->E), 256, 0, s>>>(a);
+  launch_chained(adjoint_rhs_kernel, grid_for((int64_t)systems * p->rdofs * q_per_model * p->E), 256, 0, s, a);
   p->launches++;
 }
 
@@ -275,13 +275,13 @@ void launch_cell_gradient(adt_plan* p, const void* x, bool x_double, int x_cols,
   a.x_cols = x_cols;
   a.q_per_model = q_per_model;
   const int64_t warps = (int64_t)models * q_per_model * p->C;
-  cell_gradient_kernel<<<(int)((warps + 7) / 8), 256, 0, s>>>(a);
+  launch_chained(cell_gradient_kernel, (int)((warps + 7) / 8), 256, 0, s, a);
   p->launches++;
 }
 
 // Sum discretization-cell values [rows][C] (double) into model cells [rows][Cm] (float).
 void launch_to_model_cells(adt_plan* p, const double* in, int rows, float* out, cudaStream_t s) {
-  aggregate_kernel<<<grid_for((int64_t)rows * p->Cm), 256, 0, s>>>(
+  launch_chained(aggregate_kernel, grid_for((int64_t)rows * p->Cm), 256, 0, s, 
       in, rows, p->C, p->Cm, p->model_ptr, p->model_list, out, p->C);
   p->launches++;
 }
@@ -496,12 +496,12 @@ adt_status adt_set_static_rhs(adt_plan* p, const double* unit_primary, const dou
   if (direct) {
     const std::vector<double> host = permuted(direct);
     cudaMemcpyAsync(x, host.data(), count * sizeof(double), cudaMemcpyHostToDevice, s);
-    add_kernel<<<grid_for((int64_t)count), 256, 0, s>>>(p->refrhs, x, (int64_t)count);
+    launch_chained(add_kernel, grid_for((int64_t)count), 256, 0, s, p->refrhs, x, (int64_t)count);
     p->launches++;
     cudaStreamSynchronize(s);
   }
   if (p->nfixed > 0) {
-    zero_rows_kernel<<<grid_for((int64_t)p->W * p->nfixed * p->E), 256, 0, s>>>(
+    launch_chained(zero_rows_kernel, grid_for((int64_t)p->W * p->nfixed * p->E), 256, 0, s, 
         p->refrhs, p->fixed, p->nfixed, p->W, p->N, p->E);
     p->launches++;
   }
@@ -548,12 +548,12 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
                       cudaMemcpyDeviceToDevice, s);
     adt_status st = solve_systems(p, systems, p->E, p->slots[slot].factors, x, s);
     if (st != ADT_OK) return st;
-    total_kernel<<<grid_for((int64_t)systems * p->N * p->E), 256, 0, s>>>(x, nullptr, nullptr, p->W,
+    launch_chained(total_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, x, nullptr, nullptr, p->W,
                                                                            p->N, p->E, systems, fields);
     p->launches++;
     return check_launch(p, "field solve");
   }
-  source_rho_kernel<<<grid_for((int64_t)models * p->E), 256, 0, s>>>(sigma, p->Cm, p->E, models,
+  launch_chained(source_rho_kernel, grid_for((int64_t)models * p->E), 256, 0, s, sigma, p->Cm, p->E, models,
                                                                       p->src_ptr, p->src_cells, rho);
   p->launches++;
   const Slot& sl = p->slots[slot];
@@ -561,7 +561,7 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
   launch_spmm<double>(p, sl.values, false, p->primary, false, rho, p->refrhs, -1.0, systems, x, s);
   adt_status st = solve_systems(p, systems, p->E, sl.factors, x, s);
   if (st != ADT_OK) return st;
-  total_kernel<<<grid_for((int64_t)systems * p->N * p->E), 256, 0, s>>>(x, p->primary, rho, p->W,
+  launch_chained(total_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, x, p->primary, rho, p->W,
                                                                          p->N, p->E, systems, fields);
   p->launches++;
   return check_launch(p, "field solve");
@@ -578,7 +578,7 @@ adt_status adt_factorize_wavenumbers(adt_plan* p, int32_t slot, const float* sig
   AssembleArgs a = assemble_args(p, sigma, w_count, sl.values, true, true);
   a.W = w_count;
   a.w0 = w_begin;
-  assemble_kernel<<<grid_for((int64_t)w_count * p->nnz), 256, 0, s>>>(a);
+  launch_chained(assemble_kernel, grid_for((int64_t)w_count * p->nnz), 256, 0, s, a);
   p->launches++;
   st = factorize_systems(p, w_count, sl.values, sl.factors, s);
   sl.systems = w_count;
@@ -615,7 +615,7 @@ adt_status adt_integrated_potentials(adt_plan* p, const float* fields, float* in
   iperm = (int*)(base + cv.offsets[ii]);
   cudaStream_t s = (cudaStream_t)stream;
   cudaMemcpyAsync(iperm, p->iperm.data(), p->N * sizeof(int), cudaMemcpyHostToDevice, s);
-  integrated_kernel<<<grid_for((int64_t)p->N * p->E), 256, 0, s>>>(fields, p->weights, iperm, p->W,
+  launch_chained(integrated_kernel, grid_for((int64_t)p->N * p->E), 256, 0, s, fields, p->weights, iperm, p->W,
                                                                     p->N, p->E, integrated);
   p->launches++;
   cudaStreamSynchronize(s);
@@ -711,7 +711,7 @@ adt_status adt_aggregate_columns(adt_plan* p, int32_t key, int32_t columns,
     agg = &p->aggregations.back();
   }
   if (rows == 0) return ADT_OK;
-  aggregate_float_kernel<<<grid_for((int64_t)rows * columns), 256, 0, (cudaStream_t)stream>>>(
+  launch_chained(aggregate_float_kernel, grid_for((int64_t)rows * columns), 256, 0, (cudaStream_t)stream, 
       values, rows, in_columns, columns, agg->ptr, agg->cells, out);
   p->launches++;
   return check_launch(p, "aggregation");
@@ -810,7 +810,7 @@ adt_status adt_normal_vjp(adt_plan* p, const float* fields, const double* cotang
   double* current = (double*)(base + cv.offsets[ix]);
   double* g = (double*)(base + cv.offsets[ig]);
   launch_pairs(p, cotangent, nullptr, nullptr, 1, true, false, 0, false, pairs, s);
-  mix_kernel<<<grid_for((int64_t)p->W * p->N * p->E), 256, 0, s>>>(pairs, fields, p->W, p->N, p->E, current);
+  launch_chained(mix_kernel, grid_for((int64_t)p->W * p->N * p->E), 256, 0, s, pairs, fields, p->W, p->N, p->E, current);
   p->launches++;
   launch_cell_gradient(p, current, true, p->E, nullptr, fields, false, p->weights, 1, 1, robin != 0, g, s);
   launch_to_model_cells(p, g, 1, gradient, s);
@@ -835,9 +835,9 @@ adt_status adt_normal_jvp(adt_plan* p, const float* fields, const float* directi
   double* partial = (double*)(base + cv.offsets[ip]);
   launch_assemble(p, direction, p->W, values, robin != 0, false, s);
   launch_spmm<float>(p, values, false, fields, true, nullptr, nullptr, 1.0, p->W, y, s);
-  gram_partial_kernel<<<blocks, 256, 0, s>>>(fields, y, p->weights, p->W, p->N, p->E, chunk, partial);
+  launch_chained(gram_partial_kernel, blocks, 256, 0, s, fields, y, p->weights, p->W, p->N, p->E, chunk, partial);
   p->launches++;
-  gram_gather_kernel<<<(p->D + 255) / 256, 256, 0, s>>>(partial, blocks, p->E, p->D, p->abmn, out);
+  launch_chained(gram_gather_kernel, (p->D + 255) / 256, 256, 0, s, partial, blocks, p->E, p->D, p->abmn, out);
   p->launches++;
   return check_launch(p, "normal jvp");
 }
@@ -867,7 +867,7 @@ adt_status adt_boundary_jacobian(adt_plan* p, const float* fields, int32_t row_b
   a.owner_count = p->nowners;
   a.row_begin = row_begin;
   a.rows = row_count;
-  boundary_jacobian_kernel<<<grid_for((int64_t)row_count * p->nowners), 256, 0, (cudaStream_t)stream>>>(a);
+  launch_chained(boundary_jacobian_kernel, grid_for((int64_t)row_count * p->nowners), 256, 0, (cudaStream_t)stream, a);
   p->launches++;
   return check_launch(p, "boundary jacobian");
 }
@@ -877,7 +877,7 @@ adt_status adt_scale_rows_columns(float* values, int32_t rows, int32_t columns,
                                   adt_stream stream) {
   if (!values || rows < 0 || columns < 0) return fail(nullptr, ADT_INVALID_ARG, "invalid scaling arguments");
   if ((int64_t)rows * columns == 0) return ADT_OK;
-  scale_rows_columns_kernel<<<grid_for((int64_t)rows * columns), 256, 0, (cudaStream_t)stream>>>(
+  launch_chained(scale_rows_columns_kernel, grid_for((int64_t)rows * columns), 256, 0, (cudaStream_t)stream, 
       values, rows, columns, row_scale, column_scale);
   const cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess)

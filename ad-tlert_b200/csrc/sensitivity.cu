@@ -37,6 +37,7 @@ __device__ __forceinline__ int packed_index(int i, int j, int E) {
 // K local dofs and R features per cell and wavenumber are compile-time (K = R = 0: runtime).
 template <int KC, int RC>
 __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a) {
+  chain_wait();
   extern __shared__ float jsm[];
   const int K = KC > 0 ? KC : a.K;
   const int R = RC > 0 ? RC : a.R;
@@ -198,7 +199,7 @@ cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s) 
   const int blocks = (a.C + a.cells_per_block - 1) / a.cells_per_block;
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kernel<<<blocks, kJacThreads, smem, s>>>(a);
+    launch_chained(kernel, blocks, kJacThreads, smem, s, a);
     return cudaGetLastError();
   };
   if (a.K == 3 && a.R == 5) return go(jacobian_kernel<3, 5>);
@@ -215,6 +216,7 @@ cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s) 
 // Lanes own electrodes; the lane sums are combined by a fixed shuffle tree.
 // Replaces _cell_gradient (adtlert/forward/ert2p5d.py:765-825).
 __global__ void cell_gradient_kernel(CellGradientArgs a) {
+  chain_wait();
   const int warps = blockDim.x / 32;
   const int64_t warp_id = (int64_t)blockIdx.x * warps + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
@@ -279,6 +281,7 @@ __global__ void cell_gradient_kernel(CellGradientArgs a) {
 // and subtracts it from out[row][cell]. This is the Robin template of the reference's cell
 // templates (adtlert/forward/ert3d.py:224-256, used by jacobian at 867-927).
 __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a) {
+  chain_wait();
   const int64_t total = (int64_t)a.rows * a.owner_count;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -311,6 +314,7 @@ __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a) {
 // values[r][c] *= row_scale[r] * column_scale[c] (null scales are ones).
 __global__ void scale_rows_columns_kernel(float* values, int rows, int columns, const double* row_scale,
                                           const double* column_scale) {
+  chain_wait();
   const int64_t total = (int64_t)rows * columns;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -324,6 +328,7 @@ __global__ void scale_rows_columns_kernel(float* values, int rows, int columns, 
 
 // y += x elementwise.
 __global__ void add_kernel(double* y, const double* x, int64_t count) {
+  chain_wait();
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
        idx += (int64_t)gridDim.x * blockDim.x)
     y[idx] += x[idx];
@@ -331,6 +336,7 @@ __global__ void add_kernel(double* y, const double* x, int64_t count) {
 
 // x[w][row][e] = 0 for the listed rows (the fixed dofs of a Dirichlet boundary).
 __global__ void zero_rows_kernel(double* x, const int* rows, int count, int W, int N, int E) {
+  chain_wait();
   const int64_t total = (int64_t)W * count * E;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -345,6 +351,7 @@ __global__ void zero_rows_kernel(double* x, const int* rows, int count, int W, i
 // adtlert/forward/ert2p5d.py:907-908).
 __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, int E,
                            double* current) {
+  chain_wait();
   const int64_t total = (int64_t)W * N * E;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -360,6 +367,7 @@ __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, 
 // out[r][col] = sum over the column's cells (fixed order) of in[r][cell].
 __global__ void aggregate_kernel(const double* in, int rows, int C, int columns, const int* ptr,
                                  const int* cells, float* out, int64_t in_stride) {
+  chain_wait();
   const int64_t total = (int64_t)rows * columns;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -372,6 +380,7 @@ __global__ void aggregate_kernel(const double* in, int rows, int C, int columns,
 
 __global__ void aggregate_float_kernel(const float* in, int rows, int C, int columns,
                                        const int* ptr, const int* cells, float* out) {
+  chain_wait();
   const int64_t total = (int64_t)rows * columns;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {

@@ -105,6 +105,7 @@ size_t jacobian_tc_smem(int E, int W, int R, int K, int rows) {
 // KT dofs and RT features per cell are compile-time.
 template <int KT, int RT>
 __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs a, int* error) {
+  chain_wait();
   extern __shared__ __align__(128) unsigned char tc_sm[];
   constexpr int K = KT, R = RT;
   const int E = a.E, W = a.W;
@@ -354,7 +355,7 @@ cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaS
   const int blocks = groups < 2 * sms ? groups : 2 * sms;
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kernel<<<blocks, kTcThreads, smem, s>>>(a, error);
+    launch_chained(kernel, blocks, kTcThreads, smem, s, a, error);
     return cudaGetLastError();
   };
   if (a.K == 3 && a.R == 5) return go(jacobian_tc_kernel<3, 5>);

@@ -322,6 +322,7 @@ __global__ void __launch_bounds__(kSolverThreads)
 scatter_diagonal_kernel(const int64_t* __restrict__ tasks, const int* __restrict__ csr_ptr,
                         const int* __restrict__ csr_row, const int* __restrict__ csr_col, int nnz,
                         const double* __restrict__ values, double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   const int64_t* t = tasks + (int64_t)blockIdx.x * T_FIELDS;
   const double* val = values + (int64_t)blockIdx.y * nnz;
   double* d = factors + (int64_t)blockIdx.y * stride + t[T_LOFF];
@@ -380,6 +381,7 @@ __global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
 invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int* __restrict__ csr_ptr,
                     const int* __restrict__ csr_row, const int* __restrict__ csr_col, int nnz,
                     const double* __restrict__ values, double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   constexpr int LDA = aug_ld<MAXM>();
   constexpr int W3 = 3 * MAXM;
   constexpr int RP = MAXM / 8;                  // rows per thread
@@ -575,6 +577,7 @@ template <int MAXM>
 __global__ void __launch_bounds__(kSolverThreads, 2)
 update_level_kernel(const int* __restrict__ items, int item_begin, const int64_t* __restrict__ tasks,
                     const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
   auto tile = [&](int i) { return sm + i * MAXM * LD; };
@@ -634,6 +637,7 @@ __global__ void __launch_bounds__(kSolverThreads, 2)
 forward_update_kernel(const int* __restrict__ items, int item_begin, const int64_t* __restrict__ tasks,
                       const int64_t* __restrict__ pulls, const double* __restrict__ factors,
                       int64_t stride, double* __restrict__ rhs, int64_t rhs_stride, int nrhs, int strip) {
+  chain_wait();
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
   auto tile = [&](int i) { return sm + i * MAXM * LD; };
@@ -691,6 +695,7 @@ __global__ void __launch_bounds__(kSolverThreads, 2)
 backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
                       const double* __restrict__ factors, int64_t stride,
                       double* __restrict__ rhs, int64_t rhs_stride, int nrhs, int strip) {
+  chain_wait();
   constexpr int LD = MAXM + 1;
   extern __shared__ double sm[];
   double* ut = sm;                 // Z_p (mj x mp)
@@ -885,6 +890,7 @@ tiled_scatter_kernel(const int* __restrict__ items, int begin, const int64_t* __
                      const int* __restrict__ csr_ptr, const int* __restrict__ csr_row,
                      const int* __restrict__ csr_col, int nnz, const double* __restrict__ values,
                      double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
   const int r0 = it[1], rows = it[2];
@@ -916,6 +922,7 @@ tiled_scatter_kernel(const int* __restrict__ items, int begin, const int64_t* __
 __global__ void __launch_bounds__(kTT)
 tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                     const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
@@ -962,6 +969,7 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
 __global__ void __launch_bounds__(kTT)
 tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                     double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   extern __shared__ double sm[];
   double* dm = sm;                // diagonal tile -> L_kk
   double* tt = dm + kTile * kTLD; // transposed tile below
@@ -997,6 +1005,7 @@ tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64
 __global__ void __launch_bounds__(kTT)
 tiled_fill_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                   double* __restrict__ factors, int64_t stride) {
+  chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
@@ -1016,6 +1025,7 @@ __global__ void __launch_bounds__(kTT)
 tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                             const int64_t* __restrict__ pulls, const double* __restrict__ factors,
                             int64_t stride, double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
+  chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
@@ -1043,6 +1053,7 @@ __global__ void __launch_bounds__(kTT)
 tiled_backward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                              const double* __restrict__ factors, int64_t stride,
                              double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
+  chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
@@ -1069,6 +1080,7 @@ __global__ void __launch_bounds__(kTT)
 tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
                         const double* __restrict__ factors, int64_t stride, double* __restrict__ rhs,
                         int64_t rhs_stride, int nrhs, int forward, int backward) {
+  chain_wait();
   extern __shared__ double sm[];
   double* dm = sm;                 // L_rr
   double* bt = dm + kTile * kTLD;  // right-hand-side rows of tile r
@@ -1156,21 +1168,21 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
   auto range = [&](int r) { return std::make_pair(p->tranges[2 * r], p->tranges[2 * r + 1]); };
   for (int level = 0; level < L; ++level) {
     auto [b, e] = range(level);
-    tiled_scatter_kernel<<<dim3(e - b, systems), kTT, 0, s>>>(p->titems, b, p->tasks, p->csr_ptr, p->csr_row,
+    launch_chained(tiled_scatter_kernel, dim3(e - b, systems), kTT, 0, s, p->titems, b, p->tasks, p->csr_ptr, p->csr_row,
                                                              p->csr_col, p->nnz, values, factors, p->factor_stride);
     p->launches++;
     for (int k = 0; k < p->panel_ptr[level + 1] - p->panel_ptr[level]; ++k) {
       auto [pb, pe] = range(3 * L + p->panel_ptr[level] + k);
       if (pe == pb) continue;
-      tiled_update_kernel<<<dim3(pe - pb, systems), kTT, kUpdateSmem, s>>>(p->titems, pb, k, p->tasks, p->pulls,
+      launch_chained(tiled_update_kernel, dim3(pe - pb, systems), kTT, kUpdateSmem, s, p->titems, pb, k, p->tasks, p->pulls,
                                                                          factors, p->factor_stride);
-      tiled_factor_kernel<<<dim3(pe - pb, systems), kTT, kFactorSmem, s>>>(p->titems, pb, k, p->tasks, factors,
+      launch_chained(tiled_factor_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks, factors,
                                                                            p->factor_stride);
       p->launches += 2;
     }
     auto [fb, fe] = range(L + level);
     if (fe > fb) {
-      tiled_fill_kernel<<<dim3(fe - fb, systems), kTT, kGemmSmem, s>>>(p->titems, fb, p->tasks, factors,
+      launch_chained(tiled_fill_kernel, dim3(fe - fb, systems), kTT, kGemmSmem, s, p->titems, fb, p->tasks, factors,
                                                                        p->factor_stride);
       p->launches++;
     }
@@ -1184,19 +1196,19 @@ void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, doub
   auto range = [&](int r) { return std::make_pair(p->tranges[2 * r], p->tranges[2 * r + 1]); };
   for (int level = 0; level < L; ++level) {
     auto [b, e] = range(2 * L + level);
-    tiled_forward_update_kernel<<<dim3(e - b, systems, strips), kTT, kGemmSmem, s>>>(
+    launch_chained(tiled_forward_update_kernel, dim3(e - b, systems, strips), kTT, kGemmSmem, s, 
         p->titems, b, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs);
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    tiled_substitute_kernel<<<dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s>>>(
+    launch_chained(tiled_substitute_kernel, dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s, 
         t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 1, level == L - 1);
     p->launches += 2;
   }
   for (int level = L - 2; level >= 0; --level) {
     auto [b, e] = range(2 * L + level);
-    tiled_backward_update_kernel<<<dim3(e - b, systems, strips), kTT, kGemmSmem, s>>>(
+    launch_chained(tiled_backward_update_kernel, dim3(e - b, systems, strips), kTT, kGemmSmem, s, 
         p->titems, b, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs);
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    tiled_substitute_kernel<<<dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s>>>(
+    launch_chained(tiled_substitute_kernel, dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s, 
         t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 0, 1);
     p->launches += 2;
   }
@@ -1214,17 +1226,17 @@ void configure() {
 template <int MAXM>
 void factor_levels(adt_plan* p, int systems, const double* values, double* factors, cudaStream_t s) {
   const int tasks = p->level_begin[p->levels];
-  scatter_diagonal_kernel<<<dim3(tasks, systems), kSolverThreads, 0, s>>>(
+  launch_chained(scatter_diagonal_kernel, dim3(tasks, systems), kSolverThreads, 0, s, 
       p->tasks, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
   p->launches++;
   for (int level = 0; level < p->levels; ++level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    invert_level_kernel<MAXM><<<dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s>>>(
+    launch_chained(invert_level_kernel<MAXM>, dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s, 
         p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
     p->launches++;
     const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
     if (i1 > i0) {
-      update_level_kernel<MAXM><<<dim3(i1 - i0, systems), kSolverThreads, update_smem<MAXM>(), s>>>(
+      launch_chained(update_level_kernel<MAXM>, dim3(i1 - i0, systems), kSolverThreads, update_smem<MAXM>(), s, 
           p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride);
       p->launches++;
     }
@@ -1246,16 +1258,14 @@ void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, dou
     const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
     if (i1 <= i0) continue;
     const int strip = strip_for<MAXM>((i1 - i0) * systems, nrhs);
-    forward_update_kernel<MAXM><<<dim3(i1 - i0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
-                                  forward_update_smem<MAXM>(), s>>>(
+    launch_chained(forward_update_kernel<MAXM>, dim3(i1 - i0, systems, (nrhs + strip - 1) / strip), kSolverThreads, forward_update_smem<MAXM>(), s, 
         p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
   }
   for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
     const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs);
-    backward_level_kernel<MAXM><<<dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
-                                  backward_smem<MAXM>(), s>>>(p->tasks, t0, factors, p->factor_stride, rhs,
+    launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads, backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs,
                                                               rhs_stride, nrhs, strip);
     p->launches++;
   }
