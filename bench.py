@@ -275,7 +275,7 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     clock = clocks.summary()
 
     # per-stage breakdown (same workload, L2 flushed, after the timed region)
-    stage_ms = {}
+    stage_ms, stage_launches = {}, {}
     reps = max(3, min(args.steps, 10))
     for name, fn in stages:
         total = 0.0
@@ -288,7 +288,9 @@ def run_b200(args, rank: int, world: int) -> dict | None:
             flush.fill_(1.0)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
+            before = forward.kernel_launches()
             fn(i)
+            stage_launches[name] = forward.kernel_launches() - before
             b.record(stream)
             torch.cuda.synchronize(device)
             total += a.elapsed_time(b)
@@ -306,13 +308,13 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     }
     dominant = max(stage_ms, key=stage_ms.get)
     peaks = measured_peaks()
-    launches_per_stage = {"normal_jacobian": 1, "measure": 1, "factorize": info["levels"] + 1,
-                          "solve_fields": 2 * info["levels"] + 1}
     def roofline(name):
-        per_launch_bytes = algorithmic[name] / launches_per_stage[name]
-        per_launch_s = stage_ms[name] / 1e3 / launches_per_stage[name]
+        launches = max(1, stage_launches[name])
+        per_launch_bytes = algorithmic[name] / launches
+        per_launch_s = stage_ms[name] / 1e3 / launches
         achieved = per_launch_bytes / per_launch_s / 1e9
-        traffic = ncu_traffic().get(name)
+        measured = ncu_traffic().get(name)
+        traffic = measured["dram_bytes_per_step"] / launches if measured else None
         return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": name,
                 "algorithmic_bytes_per_launch": per_launch_bytes, "launch_ms": per_launch_s * 1e3,
