@@ -458,53 +458,65 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
       const int i = tr + 8 * r, j = tc + 32 * c;
       a[r][c] = (i < mj && j < width) ? aug[i * LDA + j] : 0.0;
     }
-  for (int k0 = 0, buf = 0; k0 < mj; k0 += PB, buf ^= 1) {
-    const int nb = min(PB, mj - k0), rb = k0 / PB;
-    double* rows = rbuf + buf * PB * W3;
-    double* cols = lbuf + buf * MAXM * (PB + 1);
-    // (a) publish the panel rows (row k0 + tr: pass rb; identity in the panel columns) and the
-    //     panel columns (P itself in rows k0 .. k0 + 7); no warp still reads this buffer, since
-    //     every warp has passed the previous step's barrier
+  // the panel loop is unrolled over the register row rb that holds the panel's rows, so the
+  // panel's row, column group and buffer are compile-time in each copy
 #pragma unroll
-    for (int r = 0; r < RP; ++r) {
-      const int i = tr + 8 * r;
+  for (int rb = 0; rb < RP; ++rb) {
+    const int k0 = rb * PB;
+    if (k0 >= mj) break;
+    const int nb = min(PB, mj - k0);
+    double* rows = rbuf + (rb & 1) * PB * W3;
+    double* cols = lbuf + (rb & 1) * MAXM * (PB + 1);
+    const int cg = k0 >> 5;                                  // column group of the panel columns
+    const unsigned s = (unsigned)(tc - (k0 & 31));           // this lane's panel column, if < PB
+    // (a) publish the panel rows (row k0 + tr from register row rb; identity in the panel
+    //     columns) and the panel columns (P itself in rows k0 .. k0 + 7); no warp still reads
+    //     this buffer, since every warp has passed the previous step's barrier
 #pragma unroll
-      for (int c = 0; c < CP; ++c) {
-        const int j = tc + 32 * c;
-        const unsigned s = (unsigned)(j - k0);
-        if (r == rb && j < W3)
-          rows[tr * W3 + j] = tr >= nb ? 0.0 : s < (unsigned)nb ? (s == (unsigned)tr ? 1.0 : 0.0)
-                                                                  : (j < width ? a[r][c] : 0.0);
-        if (s < (unsigned)PB) cols[i * (PB + 1) + s] = (s < (unsigned)nb && i < mj) ? a[r][c] : 0.0;
-      }
+    for (int c = 0; c < CP; ++c) {
+      const int j = tc + 32 * c;
+      const unsigned sj = (unsigned)(j - k0);
+      if (j < W3)
+        rows[tr * W3 + j] = tr >= nb ? 0.0 : sj < (unsigned)nb ? (sj == (unsigned)tr ? 1.0 : 0.0)
+                                                                : (j < width ? a[rb][c] : 0.0);
     }
-    __syncthreads();
-    // (b) P^-1 by every warp (lane s < 8 holds row s; the padding beyond nb is the identity)
-    {
-      double row[PB];
-      const int ls = tc & (PB - 1);
+    if (s < (unsigned)PB)
 #pragma unroll
-      for (int c = 0; c < PB; ++c)
-        row[c] = (ls < nb && c < nb) ? cols[(k0 + ls) * (PB + 1) + c] : (ls == c ? 1.0 : 0.0);
+      for (int c = 0; c < CP; ++c)
+        if (c == cg)
+#pragma unroll
+          for (int r = 0; r < RP; ++r) {
+            const int i = tr + 8 * r;
+            cols[i * (PB + 1) + s] = (s < (unsigned)nb && i < mj) ? a[r][c] : 0.0;
+          }
+    __syncthreads();
+    // (b) P^-1 by every warp: lane 4 v + h holds row v, columns 2 h and 2 h + 1 (the padding
+    //     beyond nb is the identity)
+    {
+      const int v = tc >> 2, h = tc & 3;
+      double x0 = (v < nb && 2 * h < nb) ? cols[(k0 + v) * (PB + 1) + 2 * h] : (v == 2 * h ? 1.0 : 0.0);
+      double x1 = (v < nb && 2 * h + 1 < nb) ? cols[(k0 + v) * (PB + 1) + 2 * h + 1] : (v == 2 * h + 1 ? 1.0 : 0.0);
 #pragma unroll
       for (int k = 0; k < PB; ++k) {
-        double rk[PB];
-#pragma unroll
-        for (int c = 0; c < PB; ++c) rk[c] = __shfl_sync(0xffffffffu, row[c], k);
-        const double inv = positive_reciprocal(rk[k]);
-        const double lik = row[k] * inv;
-#pragma unroll
-        for (int c = 0; c < PB; ++c) {
-          if (ls == k) row[c] = (c == k) ? inv : row[c] * inv;
-          else row[c] = (c == k) ? -lik : fma(-lik, rk[c], row[c]);
+        const double r0 = __shfl_sync(0xffffffffu, x0, 4 * k + h);   // row k, columns 2h, 2h + 1
+        const double r1 = __shfl_sync(0xffffffffu, x1, 4 * k + h);
+        const double pivot = __shfl_sync(0xffffffffu, (k & 1) ? x1 : x0, 4 * k + (k >> 1));
+        const double mk = __shfl_sync(0xffffffffu, (k & 1) ? x1 : x0, 4 * v + (k >> 1));  // row v, column k
+        const double inv = positive_reciprocal(pivot);
+        const double lik = mk * inv;
+        const bool c0k = 2 * h == k, c1k = 2 * h + 1 == k;
+        if (v == k) {
+          x0 = c0k ? inv : x0 * inv;
+          x1 = c1k ? inv : x1 * inv;
+        } else {
+          x0 = c0k ? -lik : fma(-lik, r0, x0);
+          x1 = c1k ? -lik : fma(-lik, r1, x1);
         }
       }
-      if (tc < PB)
-#pragma unroll
-        for (int c = 0; c < PB; ++c) pinv[tc * PB + c] = row[c];
+      *reinterpret_cast<double2*>(pinv + v * PB + 2 * h) = make_double2(x0, x1);
     }
     __syncwarp();
-    // (c) C for this warp's rows: L P^-1, or -P^-1 on a panel row
+    // (c) C for this warp's rows: L P^-1, or -P^-1 on the panel row
     for (int e = tc; e < RP * PB; e += 32) {
       const int r = e / PB, u = e - r * PB, i = tr + 8 * r;
       double v = 0.0;
@@ -517,28 +529,32 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
       cw[e] = v;
     }
     __syncwarp();
-    // (d) a <- keep a - C R: the panel columns and the panel rows start from zero
+    // (d) a <- keep a - C R: the panel columns and the panel row start from zero
+    if (s < (unsigned)nb)
 #pragma unroll
-    for (int c = 0; c < CP; ++c) {
-      const unsigned sj = (unsigned)(tc + 32 * c - k0);
+      for (int c = 0; c < CP; ++c)
+        if (c == cg)
 #pragma unroll
-      for (int r = 0; r < RP; ++r)
-        if (sj < (unsigned)nb || (r == rb && tr < nb)) a[r][c] = 0.0;
-    }
+          for (int r = 0; r < RP; ++r) a[r][c] = 0.0;
+    if (tr < nb)
 #pragma unroll
-    for (int u = 0; u < PB; ++u) {
-      double lu[RP], ru[CP];
+      for (int c = 0; c < CP; ++c) a[rb][c] = 0.0;
 #pragma unroll
-      for (int r = 0; r < RP; ++r) lu[r] = cw[r * PB + u];
+    for (int u = 0; u < PB; u += 2) {
+      double2 lu[RP];
+      double ru0[CP], ru1[CP];
+#pragma unroll
+      for (int r = 0; r < RP; ++r) lu[r] = *reinterpret_cast<const double2*>(cw + r * PB + u);
 #pragma unroll
       for (int c = 0; c < CP; ++c) {
         const int j = tc + 32 * c;
-        ru[c] = j < W3 ? rows[u * W3 + j] : 0.0;
+        ru0[c] = j < W3 ? rows[u * W3 + j] : 0.0;
+        ru1[c] = j < W3 ? rows[(u + 1) * W3 + j] : 0.0;
       }
 #pragma unroll
       for (int r = 0; r < RP; ++r)
 #pragma unroll
-        for (int c = 0; c < CP; ++c) a[r][c] = fma(-lu[r], ru[c], a[r][c]);
+        for (int c = 0; c < CP; ++c) a[r][c] = fma(-lu[r].y, ru1[c], fma(-lu[r].x, ru0[c], a[r][c]));
     }
   }
 
