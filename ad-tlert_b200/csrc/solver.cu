@@ -167,6 +167,80 @@ __device__ void tile_gemm(double* C, int ldc, const double* A, int lda, const do
   }
 }
 
+// ---- FP64 tensor-core tiles (mma.sync m8n8k4 f64) for the fill GEMM of the level kernel.
+// An m x n output is a grid of 8 x 8 tiles; warp w of the block owns tiles w, w + 8, w + 16, ...
+// (row-major over the grid), at most MAXT of them, and lane (g, t) = (lane / 4, lane % 4) holds
+// entries (8 ti + g, 8 tj + 2 t + {0, 1}) of each. Operands are read from shared memory straight
+// into fragments: A's (row g, column p + t) and B's (row p + t, column g) of each k-step of 4.
+// Rows and columns past m / n read whatever the operand tiles hold there and only feed entries
+// that are never stored; the reduction index is exact (the last partial k-step is masked).
+constexpr int kSolverWarps = kSolverThreads / 32;
+
+template <int MAXM>
+constexpr int mma_tiles() { return ((MAXM / 8) * (MAXM / 8) + kSolverWarps - 1) / kSolverWarps; }
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// acc = -A B (A: m x k row-major, lda; B: k x n row-major, ldb) for the warp's tiles.
+template <int MAXT>
+__device__ __forceinline__ void mma_negated_product(double (&acc)[MAXT][2], int m, int n, const double* A,
+                                                    int lda, const double* B, int ldb, int k) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int tn = (n + 7) >> 3, tiles = ((m + 7) >> 3) * tn;
+  const double* ap[MAXT];
+  const double* bp[MAXT];
+#pragma unroll
+  for (int x = 0; x < MAXT; ++x) {
+    acc[x][0] = acc[x][1] = 0.0;
+    const int tile = min(warp + kSolverWarps * x, tiles - 1);
+    const int ti = tile / tn, tj = tile - ti * tn;
+    ap[x] = A + (8 * ti + g) * lda + t;
+    bp[x] = B + t * ldb + 8 * tj + g;
+  }
+  int p0 = 0;
+  for (; p0 + 4 <= k; p0 += 4) {
+#pragma unroll
+    for (int x = 0; x < MAXT; ++x) {
+      if (warp + kSolverWarps * x >= tiles) break;
+      dmma(acc[x], -*ap[x], *bp[x]);
+      ap[x] += 4;
+      bp[x] += 4 * ldb;
+    }
+  }
+  if (p0 < k) {
+    const bool ok = p0 + t < k;
+#pragma unroll
+    for (int x = 0; x < MAXT; ++x) {
+      if (warp + kSolverWarps * x >= tiles) break;
+      dmma(acc[x], ok ? -*ap[x] : 0.0, ok ? *bp[x] : 0.0);
+    }
+  }
+}
+
+// For each held entry (i, j) of an m x n output with i < m, j < n: f(i, j, value).
+template <int MAXT, typename F>
+__device__ __forceinline__ void mma_for_each(const double (&acc)[MAXT][2], int m, int n, F&& f) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int tn = (n + 7) >> 3, tiles = ((m + 7) >> 3) * tn;
+#pragma unroll
+  for (int x = 0; x < MAXT; ++x) {
+    const int tile = warp + kSolverWarps * x;
+    if (tile >= tiles) break;
+    const int ti = tile / tn, tj = tile - ti * tn;
+    const int i = 8 * ti + g, j = 8 * tj + 2 * t;
+    if (i < m) {
+      if (j < n) f(i, j, acc[x][0]);
+      if (j + 1 < n) f(i, j + 1, acc[x][1]);
+    }
+  }
+}
+
 // In-place lower Cholesky of the m x m tile `a` (leading dimension LD); rinv[i] = 1 / L[i][i].
 // A non-positive pivot becomes NaN, which propagates to every result of the system. Only the
 // lower triangle is read; the strict upper triangle is zeroed on exit.
@@ -580,9 +654,10 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
     aug[r * LDA + k] = f[t[T_RVOFF] + i];
   }
   double* fill = f + t[T_FILL];
-  for (int i = threadIdx.x; i < mq * mp; i += blockDim.x) fill[i] = 0.0;
   __syncthreads();
-  tile_gemm<false, false>(fill, mp, aug, LDA, aug + mj, LDA, mq, mp, mj, -1.0);
+  double acc[mma_tiles<MAXM>()][2];
+  mma_negated_product(acc, mq, mp, aug, LDA, aug + mj, LDA, mj);
+  mma_for_each(acc, mq, mp, [&](int i, int j, double v) { fill[i * mp + j] = v; });
 }
 
 // Eager Schur updates after a level: block j of every item subtracts the pulls [u0, u1) of that
