@@ -31,6 +31,7 @@ SYMBOLS = (
     "adt_measure",
     "adt_integrated_potentials",
     "adt_normal_jacobian",
+    "adt_normal_jacobian_to_host",
     "adt_aggregate_columns",
     "adt_vjp",
     "adt_adjoint_jacobian",
@@ -128,6 +129,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_measure": (status, [_p, _p, _i32, _p, _p, _p, _p]),
         "adt_integrated_potentials": (status, [_p, _p, _p, _p]),
         "adt_normal_jacobian": (status, [_p, _p, _i32, _i32, _p, _p]),
+        "adt_normal_jacobian_to_host": (status, [_p, _p, _p, _p, _i32, _p]),
         "adt_aggregate_columns": (status, [_p, _i32, _i32, _p, _p, _p, _i32, _i32, _p, _p]),
         "adt_vjp": (status, [_p, _i32, _p, _p, _p, _p, _i32, _p, _p]),
         "adt_adjoint_jacobian": (status, [_p, _i32, _p, _p, _p, _i32, _i32, _i32, _i32, _p, _p]),

@@ -251,6 +251,11 @@ def _terrain_cache_dir(value) -> Path | None:
     return Path(env).expanduser() if env else None
 
 
+JACOBIAN_CHUNKS = 8
+"""Column chunks of a Jacobian computed straight into host memory (copy of chunk k overlaps
+the computation of chunk k + 1)."""
+
+
 def _to_host(tensor: Tensor) -> Tensor:
     """Device tensor -> CPU tensor in page-locked memory (torch's caching host allocator), so the
     copy runs at full link bandwidth."""
@@ -754,10 +759,21 @@ class ERTForward2p5D:
                                             normal_sensitivity=normal_sensitivity)[1]
         self._batch_size(batch_size, direct)
         with self._deferred_checks():
-            J = self._jacobian_device(self._fields(conductivity),
-                                      self._columns(None, None, discretization=True))
-            host = _to_host(J)
+            fields = self._fields(conductivity)
+            columns = self._columns(None, None, discretization=True)
+            host = self._jacobian_to_host(fields) if columns is None else _to_host(self._jacobian_device(fields, columns))
         return host.to(self.dtype)
+
+    def _jacobian_to_host(self, fields: _Fields) -> Tensor:
+        """J (D, C) in page-locked host memory: computed in column chunks whose copies to the host
+        overlap the computation of the next chunk (adt_normal_jacobian_to_host)."""
+
+        J = torch.empty((self.D, self.Cd), dtype=torch.float32, device=self.device)
+        host = torch.empty((self.D, self.Cd), dtype=torch.float32, pin_memory=True)
+        self._call("adt_normal_jacobian_to_host", _native.ptr(fields.total), _native.ptr(J), _native.ptr(host),
+                   JACOBIAN_CHUNKS, self._stream())
+        torch.cuda.current_stream(self.device).synchronize()
+        return host
 
     def jacobian_columnwise(self, conductivity) -> Tensor:
         basis = torch.eye(self.C, dtype=self.dtype)

@@ -133,6 +133,8 @@ struct adt_plan {
   bool jacobian_tc = true;      // tensor-core Jacobian where it applies
   int* tc_error = nullptr;      // device flag raised by a tensor-core block that timed out
   int* tc_error_host = nullptr; // pinned copy, refreshed after each tensor-core launch
+  cudaStream_t copy_stream = nullptr;        // device-to-host copies of Jacobian column chunks
+  std::vector<cudaEvent_t> chunk_events;     // chunk done (compute stream), copies done (copy stream)
 };
 
 namespace adt {

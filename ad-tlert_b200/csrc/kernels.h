@@ -79,8 +79,10 @@ struct JacobianArgs {
   const int* cell_dofs;   // [C][K]
   const float* fscale;    // [W][R] per-wavenumber feature scales
   const int* abmn;        // [D][4]
-  float* out;             // [rows][C]
+  float* out;             // row d, cell c at out[d * ldo + c]
   int W, N, E, C, K, R, row_begin, rows, cells_per_block;
+  int c_begin, c_end;     // cells computed: [c_begin, c_end)
+  int64_t ldo;            // row stride of out
 };
 
 struct CellGradientArgs {

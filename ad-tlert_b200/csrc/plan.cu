@@ -387,6 +387,8 @@ adt_status adt_plan_destroy(adt_plan* p) {
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->tc_error_host) cudaFreeHost(p->tc_error_host);
+  for (cudaEvent_t e : p->chunk_events) cudaEventDestroy(e);
+  if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   for (auto& s : p->slots) {
     if (s.values) cudaFree(s.values);
     if (s.factors) cudaFree(s.factors);
@@ -622,57 +624,19 @@ adt_status adt_integrated_potentials(adt_plan* p, const float* fields, float* in
   return check_launch(p, "integrated potentials");
 }
 
-adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_begin,
-                               int32_t row_count, float* jacobian, adt_stream stream) {
-  if (!p || !fields || !jacobian || row_begin < 0 || row_count < 0 || row_begin + row_count > p->D)
-    return fail(p, ADT_INVALID_ARG, "invalid jacobian arguments");
-  if (row_count == 0) return ADT_OK;
-  if (p->tc_error_host && *p->tc_error_host != 0)
-    return fail(p, ADT_TIMEOUT, "a tensor-core Jacobian launch of this plan timed out waiting for its MMAs");
-  if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count)) {
-    JacobianArgs a;
-    a.fields = fields;
-    a.features = p->features;
-    a.cell_dofs = p->cell_dofs;
-    a.fscale = p->fscale;
-    a.abmn = p->abmn;
-    a.out = jacobian;
-    a.W = p->W;
-    a.N = p->N;
-    a.E = p->E;
-    a.C = p->C;
-    a.K = p->K;
-    a.R = p->R;
-    a.row_begin = row_begin;
-    a.rows = row_count;
-    a.cells_per_block = 0;
-    cudaStream_t s = (cudaStream_t)stream;
-    const cudaError_t err = launch_jacobian_tc(a, p->tc_error, p->sms, s);
-    p->launches++;
-    if (err != cudaSuccess)
-      return fail(p, ADT_CUDA_ERROR, std::string("tensor-core jacobian: ") + cudaGetErrorString(err));
-    cudaMemcpyAsync(p->tc_error_host, p->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s);
-    return check_launch(p, "normal jacobian");
-  }
-  const int E4 = (p->E + 3) & ~3;
-  const int nt4 = E4 / 4, NT = nt4 * (nt4 + 1) / 2;
-  // cells per block: a power of two (threads split evenly over cells), at most 5 Gram tiles and
-  // 4 feature items per thread, and shared memory for two blocks per SM
-  const int E4c = (p->E + 3) & ~3;
-  int cells = 32;
-  while (cells > 1 && (cells * NT > 256 * 5 || cells * E4c > 256 * 4 ||
-                       jacobian_smem(cells, p->R, p->E, p->K) > 110 * 1024))
-    cells /= 2;
-  const size_t smem = jacobian_smem(cells, p->R, p->E, p->K);
-  if (smem > 220 * 1024 || cells * NT > 256 * 5 || cells * E4c > 256 * 4)
-    return fail(p, ADT_INVALID_ARG, "too many electrodes for the sensitivity kernel");
+namespace {
+
+// Jacobian rows [row_begin, row_begin + row_count) for cells [c_begin, c_end) into
+// out[d * ldo + c] (d relative to row_begin); the tensor-core kernel when it applies.
+adt_status launch_normal_jacobian(adt_plan* p, const float* fields, int row_begin, int row_count, int c_begin,
+                                  int c_end, float* out, int64_t ldo, cudaStream_t s) {
   JacobianArgs a;
   a.fields = fields;
   a.features = p->features;
   a.cell_dofs = p->cell_dofs;
   a.fscale = p->fscale;
   a.abmn = p->abmn;
-  a.out = jacobian;
+  a.out = out;
   a.W = p->W;
   a.N = p->N;
   a.E = p->E;
@@ -681,10 +645,95 @@ adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_beg
   a.R = p->R;
   a.row_begin = row_begin;
   a.rows = row_count;
+  a.c_begin = c_begin;
+  a.c_end = c_end;
+  a.ldo = ldo;
+  if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count)) {
+    a.cells_per_block = 0;
+    const cudaError_t err = launch_jacobian_tc(a, p->tc_error, p->sms, s);
+    p->launches++;
+    if (err != cudaSuccess)
+      return fail(p, ADT_CUDA_ERROR, std::string("tensor-core jacobian: ") + cudaGetErrorString(err));
+    return ADT_OK;
+  }
+  const int E4 = (p->E + 3) & ~3;
+  const int nt4 = E4 / 4, NT = nt4 * (nt4 + 1) / 2;
+  // cells per block: a power of two (threads split evenly over cells), at most 5 Gram tiles and
+  // 4 feature items per thread, and shared memory for two blocks per SM
+  int cells = 32;
+  while (cells > 1 && (cells * NT > 256 * 5 || cells * E4 > 256 * 4 ||
+                       jacobian_smem(cells, p->R, p->E, p->K) > 110 * 1024))
+    cells /= 2;
+  const size_t smem = jacobian_smem(cells, p->R, p->E, p->K);
+  if (smem > 220 * 1024 || cells * NT > 256 * 5 || cells * E4 > 256 * 4)
+    return fail(p, ADT_INVALID_ARG, "too many electrodes for the sensitivity kernel");
   a.cells_per_block = cells;
-  launch_jacobian(a, smem, (cudaStream_t)stream);
+  launch_jacobian(a, smem, s);
   p->launches++;
+  return ADT_OK;
+}
+
+adt_status jacobian_timeout_status(adt_plan* p) {
+  if (p->tc_error_host && *p->tc_error_host != 0)
+    return fail(p, ADT_TIMEOUT, "a tensor-core Jacobian launch of this plan timed out waiting for its MMAs");
+  return ADT_OK;
+}
+
+// After tensor-core launches: the error flag to the pinned host word read by the next call.
+void fetch_jacobian_error(adt_plan* p, cudaStream_t s) {
+  if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, p->D))
+    cudaMemcpyAsync(p->tc_error_host, p->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s);
+}
+
+}  // namespace
+
+adt_status adt_normal_jacobian(adt_plan* p, const float* fields, int32_t row_begin,
+                               int32_t row_count, float* jacobian, adt_stream stream) {
+  if (!p || !fields || !jacobian || row_begin < 0 || row_count < 0 || row_begin + row_count > p->D)
+    return fail(p, ADT_INVALID_ARG, "invalid jacobian arguments");
+  if (row_count == 0) return ADT_OK;
+  if (adt_status st = jacobian_timeout_status(p)) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (adt_status st = launch_normal_jacobian(p, fields, row_begin, row_count, 0, p->C, jacobian, p->C, s)) return st;
+  if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count))
+    cudaMemcpyAsync(p->tc_error_host, p->tc_error, sizeof(int), cudaMemcpyDeviceToHost, s);
   return check_launch(p, "normal jacobian");
+}
+
+adt_status adt_normal_jacobian_to_host(adt_plan* p, const float* fields, float* device_jacobian,
+                                       float* host_jacobian, int32_t chunks, adt_stream stream) {
+  if (!p || !fields || !device_jacobian || !host_jacobian || chunks < 1)
+    return fail(p, ADT_INVALID_ARG, "invalid jacobian arguments");
+  if (p->D == 0) return ADT_OK;
+  if (adt_status st = jacobian_timeout_status(p)) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  chunks = std::min<int32_t>(chunks, std::max(1, p->C / 64));
+  if (!p->copy_stream) {
+    if (cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(p, ADT_CUDA_ERROR, "could not create the copy stream");
+  }
+  while ((int)p->chunk_events.size() < chunks + 1) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+      return fail(p, ADT_CUDA_ERROR, "could not create a chunk event");
+    p->chunk_events.push_back(e);
+  }
+  const size_t pitch = (size_t)p->C * sizeof(float);
+  for (int k = 0; k < chunks; ++k) {
+    // even cell boundaries keep the paired stores of a row aligned
+    const int c0 = k == 0 ? 0 : (int)(((int64_t)p->C * k / chunks) & ~int64_t(1));
+    const int c1 = k == chunks - 1 ? p->C : (int)(((int64_t)p->C * (k + 1) / chunks) & ~int64_t(1));
+    if (c1 <= c0) continue;
+    if (adt_status st = launch_normal_jacobian(p, fields, 0, p->D, c0, c1, device_jacobian, p->C, s)) return st;
+    cudaEventRecord(p->chunk_events[k], s);
+    cudaStreamWaitEvent(p->copy_stream, p->chunk_events[k], 0);
+    cudaMemcpy2DAsync(host_jacobian + c0, pitch, device_jacobian + c0, pitch, (size_t)(c1 - c0) * sizeof(float),
+                      p->D, cudaMemcpyDeviceToHost, p->copy_stream);
+  }
+  cudaEventRecord(p->chunk_events[chunks], p->copy_stream);
+  cudaStreamWaitEvent(s, p->chunk_events[chunks], 0);
+  fetch_jacobian_error(p, s);
+  return check_launch(p, "normal jacobian to host");
 }
 
 adt_status adt_aggregate_columns(adt_plan* p, int32_t key, int32_t columns,

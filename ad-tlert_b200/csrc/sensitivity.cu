@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
   const int P = (E * (E + 1) / 2) | 1;  // packed Gram stride (odd: cells hit distinct banks)
   const int fsize = CT * R * E4;
   float* gram = jsm + 2 * fsize;  // [CT][P]
-  const int c0 = blockIdx.x * CT;
+  const int c0 = a.c_begin + blockIdx.x * CT;
   const int tid = threadIdx.x;
 
   // this thread's Gram tiles: smem offsets of the two 4-electrode strips they multiply (-1: none)
@@ -71,12 +71,12 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
   float* coef = gram + CT * P;                           // [CT][R][K]
   int* dofs = reinterpret_cast<int*>(coef + CT * R * K);  // [CT][K]
   for (int i = tid; i < CT * R * K; i += kJacThreads) {
-    const int c = min(c0 + i / (R * K), a.C - 1);
+    const int c = min(c0 + i / (R * K), a.c_end - 1);
     coef[i] = a.features[(int64_t)c * R * K + i % (R * K)];
   }
   for (int i = tid; i < CT * K; i += kJacThreads) {
     const int c = c0 + i / K;
-    dofs[i] = c < a.C ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
+    dofs[i] = c < a.c_end ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
   }
   const int TPC = kJacThreads / CT;
   const int my_cell = tid / TPC, my_eg = tid - my_cell * TPC;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
   __syncthreads();
   // rows go to groups of CT threads (CT is a power of two <= 32); thread ci of a group reads cell
   // ci's four Gram entries, so a group stores CT contiguous floats of one row
-  const int ncells = min(CT, a.C - c0);
+  const int ncells = min(CT, a.c_end - c0);
   const int ci = tid % CT;
   for (int dl = tid / CT; dl < a.rows; dl += kJacThreads / CT) {
     const int4 q = *reinterpret_cast<const int4*>(a.abmn + 4 * (a.row_begin + dl));
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kJacThreads, 2) jacobian_kernel(JacobianArgs a
       const float* g = gram + ci * P;
       const float ma = ima >= 0 ? g[ima] : 0.f, mb = imb >= 0 ? g[imb] : 0.f;
       const float na = ina >= 0 ? g[ina] : 0.f, nb = inb >= 0 ? g[inb] : 0.f;
-      a.out[(int64_t)dl * a.C + c0 + ci] = -((ma - mb) - (na - nb));
+      a.out[(int64_t)dl * a.ldo + c0 + ci] = -((ma - mb) - (na - nb));
     }
   }
 }
@@ -196,7 +196,7 @@ template __global__ void jacobian_kernel<0, 0>(JacobianArgs);
 
 // Launch the instantiation matching the plan's (K, R).
 cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s) {
-  const int blocks = (a.C + a.cells_per_block - 1) / a.cells_per_block;
+  const int blocks = (a.c_end - a.c_begin + a.cells_per_block - 1) / a.cells_per_block;
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     launch_chained(kernel, blocks, kJacThreads, smem, s, a);

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
       (reinterpret_cast<uintptr_t>(offs + table_rows) + 15) & ~uintptr_t(15));
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int groups = (a.C + kTcCells - 1) / kTcCells;
+  const int groups = (a.c_end - a.c_begin + kTcCells - 1) / kTcCells;
   const uint32_t columns_needed = (uint32_t)(kTcCells * N);
   uint32_t tmem_cols = 32;
   while (tmem_cols < columns_needed) tmem_cols <<= 1;
@@ -171,15 +171,15 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   }
 
   for (int group = blockIdx.x; group < groups && !failed; group += gridDim.x) {
-    const int c0 = group * kTcCells;
+    const int c0 = a.c_begin + group * kTcCells;
     // (1) cell tables, then features (hi part 0, lo part 1); padded features are zero
     for (int i = tid; i < kTcCells * R * K; i += kTcThreads) {
-      const int c = min(c0 + i / (R * K), a.C - 1);
+      const int c = min(c0 + i / (R * K), a.c_end - 1);
       coef[i] = a.features[(int64_t)c * R * K + i % (R * K)];
     }
     for (int i = tid; i < kTcCells * K; i += kTcThreads) {
       const int c = c0 + i / K;
-      dofs[i] = c < a.C ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
+      dofs[i] = c < a.c_end ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
     }
     __syncthreads();
     {
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
     __syncthreads();
     // (5) rows: one thread per row, both cells of the group (adjacent floats of J); with more
     //     rows than the table holds, the table is refilled chunk by chunk
-    const int ncells = min(kTcCells, a.C - c0);
+    const int ncells = min(kTcCells, a.c_end - c0);
     for (int r0 = 0; r0 < a.rows; r0 += kTcRowTable) {
       const int n = min(kTcRowTable, a.rows - r0);
       if (!resident) {
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
           const float* g = gram + (size_t)ci * GS;
           v[ci] = -((g[o.x] - g[o.y]) - (g[o.z] - g[o.w]));
         }
-        float* out = a.out + (int64_t)dl * a.C + c0;
+        float* out = a.out + (int64_t)dl * a.ldo + c0;
         if (ncells == kTcCells && (((uintptr_t)out & 7) == 0)) {
           *reinterpret_cast<float2*>(out) = make_float2(v[0], v[1]);
         } else {
@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
     // NaN in every row of this block's remaining cells
     for (int group = blockIdx.x; group < groups; group += gridDim.x)
       for (int idx = tid; idx < a.rows * kTcCells; idx += kTcThreads) {
-        const int c = group * kTcCells + idx % kTcCells;
-        if (c < a.C) a.out[(int64_t)(idx / kTcCells) * a.C + c] = __int_as_float(0x7fc00000);
+        const int c = a.c_begin + group * kTcCells + idx % kTcCells;
+        if (c < a.c_end) a.out[(int64_t)(idx / kTcCells) * a.ldo + c] = __int_as_float(0x7fc00000);
       }
     // the last commit may still be pending: give it a bounded second chance before freeing
     uint32_t polls = 0;
@@ -351,7 +351,7 @@ bool jacobian_tc_supported(int E, int W, int R, int K, int rows) {
 
 cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaStream_t s) {
   const size_t smem = jacobian_tc_smem(a.E, a.W, a.R, a.K, a.rows);
-  const int groups = (a.C + kTcCells - 1) / kTcCells;
+  const int groups = (a.c_end - a.c_begin + kTcCells - 1) / kTcCells;
   const int blocks = groups < 2 * sms ? groups : 2 * sms;
   auto go = [&](auto kernel) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -163,6 +163,16 @@ adt_status adt_integrated_potentials(adt_plan* plan, const float* fields, float*
 adt_status adt_normal_jacobian(adt_plan* plan, const float* fields, int32_t row_begin,
                                int32_t row_count, float* jacobian, adt_stream stream);
 
+/* The whole normal Jacobian of one model (the adt_normal_jacobian product for rows 0 .. D-1)
+ * into host_jacobian [D][C] float32, which must be page-locked (cudaHostAlloc / pinned), through
+ * device_jacobian (same layout, on the device). J is computed on `stream` in `chunks` column
+ * ranges (at most C/64), and each finished range is copied to the host on a stream of the plan
+ * while the next range is computed; `stream` then waits for the last copy, so synchronizing
+ * `stream` makes host_jacobian complete. Replaces: the device Jacobian and its copy to the host
+ * in jacobian() (adtlert/forward/ert2p5d.py:984-1010 and its torch .cpu()). */
+adt_status adt_normal_jacobian_to_host(adt_plan* plan, const float* fields, float* device_jacobian,
+                                       float* host_jacobian, int32_t chunks, adt_stream stream);
+
 /* Sums the `in_columns` columns of values [rows][in_columns] into `columns` outputs:
  * column_ptr[columns+1] / column_cells[] list the input columns of every output column in
  * summation order (host arrays, cached in the plan under `key`; inputs listed nowhere are

@@ -71,3 +71,21 @@ def test_tensor_core_jacobian_with_more_rows_than_the_offset_table():
     assert_close(a, b, 2e-6, "tcgen05 vs FMA jacobian (4928 rows)")
     n = len(abmn) // 4
     assert torch.equal(a[:n], a[2 * n:3 * n]) and torch.equal(a[n:2 * n], a[3 * n:])
+
+
+def test_jacobian_to_host_in_column_chunks_is_the_device_jacobian():
+    from adtlert_b200 import _native
+    nodes, cells, electrodes, abmn = synthetic.flat_section()
+    mesh, survey = Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, abmn)
+    sigma = torch.as_tensor(synthetic.layered_model(nodes, cells, 3), dtype=torch.float32)
+    for forward in _pair(lambda: ERTForward2p5D(mesh, survey)):
+        fields = forward._fields(sigma)
+        expected = forward._jacobian_device(fields).cpu()
+        for chunks in (1, 3, 8, 1000):  # 1000 is capped at C / 64
+            device = torch.full_like(expected, float("nan"), device="cuda")
+            host = torch.full(tuple(expected.shape), float("nan"), pin_memory=True)
+            forward._call("adt_normal_jacobian_to_host", _native.ptr(fields.total), _native.ptr(device),
+                          _native.ptr(host), chunks, forward._stream())
+            torch.cuda.current_stream().synchronize()
+            assert torch.equal(host, expected), f"{chunks} chunks"
+        assert torch.equal(forward.jacobian(sigma), expected)
