@@ -3,23 +3,25 @@
 // Same contraction as jacobian_kernel: for every cell c the electrode Gram
 //   G_c = F_c^T F_c,   F_c[w R + f][e] = sqrt(w_w) (k_w) L_c[f] . x_we   (R features per wavenumber),
 // and each ABMN row takes four Gram entries, J[d][c] = -(G[M][A] - G[M][B] - G[N][A] + G[N][B]).
-// Here the Gram is one tcgen05.mma chain per cell: A = B = F_c^T (electrodes x features,
-// K-major) in shared memory, D = G_c (64 x N, fp32) in tensor memory, M = 64 rows (rows >= E read
-// whatever follows in shared memory and only feed rows of D that are never read), N = E rounded
-// up to 8, K = 8 features per instruction. Float32 accuracy comes from a hi/lo split of every
-// feature (hi = TF32 rounding, lo = the remainder): G = hi.hi + hi.lo + lo.hi, three MMAs per
-// K-step accumulating in fp32.
+// Here the Grams of a pair of cells are one tcgen05.mma chain: the two cells' feature matrices
+// are stacked as rows (electrode e of cell i at row i Ep + e, Ep = E rounded up to 8) of one
+// K-major operand S in shared memory, and A = S (M = 128 rows; rows past 2 Ep read whatever
+// follows and only feed rows of D that are never read), B = S (N = 2 Ep), so D = S S^T (fp32, in
+// tensor memory) holds both Grams as its diagonal blocks. K = 8 features per instruction.
+// Float32 accuracy comes from a hi/lo split of every feature (hi = TF32 rounding, lo = the
+// remainder): G = hi.hi + hi.lo + lo.hi, three MMAs per K-step accumulating in fp32.
 //
-// Persistent blocks (two per SM; 256 threads each) loop over groups of kCells consecutive cells:
-// (1) all threads compute the features of the group into shared memory (generic proxy, then
-// fence.proxy.async); (2) one thread issues the MMAs (each cell into its own TMEM columns) and
-// commits them to an mbarrier; (3) all threads wait on it (bounded: on timeout the block raises
-// the error flag, writes NaN for its rows and stops); (4) warps read their TMEM lanes back
-// (tcgen05.ld), stage the Grams in shared memory and gather the rows, kCells consecutive floats
-// per row. Shared-memory operand layout (no swizzle, K-major canonical layout): feature chunk kc
-// (4 features, 16 bytes) of electrode row e at ((part*kCells + cell)*KC + kc)*E*16 + e*16, so one
-// 8-row core matrix is 128 contiguous bytes (stride byte offset 128) and the two 16-byte K halves
-// of one MMA are E*16 bytes apart (leading byte offset).
+// Persistent blocks (two per SM; 256 threads each) loop over the cell pairs: (1) all threads
+// compute the features of the pair into shared memory (thread e of each 64-thread lane group
+// handles electrode e for every fourth wavenumber; generic proxy, then fence.proxy.async); (2) one
+// thread issues the MMAs and commits them to an mbarrier; (3) all threads wait on it (bounded: on
+// timeout the block raises the error flag, writes NaN for its rows and stops); (4) warps read
+// their TMEM lanes back (tcgen05.ld; warps 0-3 the first cell's columns, 4-7 the second's),
+// stage the Grams in shared memory and write two consecutive floats per row. Shared-memory
+// operand layout (no swizzle, K-major canonical layout): chunk q of row r at
+// (part*KC + q)*2Ep*16 + r*16, so one 8-row core matrix is 128 contiguous bytes (stride byte
+// offset 128) and the two 16-byte K halves of one MMA are 2Ep*16 bytes apart (leading byte
+// offset).
 #include "adt_internal.h"
 #include "kernels.h"
 
@@ -27,8 +29,8 @@ namespace adt {
 namespace {
 
 constexpr int kTcThreads = 256;
-constexpr int kTcCells = 2;      // cells per group (two blocks share an SM)
-constexpr int kTcM = 64;         // MMA M (electrode rows, padded)
+constexpr int kTcCells = 2;      // cells per group (stacked in one MMA operand)
+constexpr int kTcM = 128;        // MMA M (rows of the stacked operand)
 constexpr uint32_t kTcWaitLimit = 1u << 20;  // mbarrier polls before the block gives up
 constexpr int kTcRowTable = 4096;            // rows whose Gram offsets stay in shared memory
 
@@ -80,21 +82,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
-__device__ __forceinline__ void tmem_load16(uint32_t addr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(addr));
+__device__ __forceinline__ void tmem_load8(uint32_t addr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(addr));
 }
 
 }  // namespace
 
 // Shared memory of jacobian_tc_kernel for E electrodes, W wavenumbers, R features, K dofs.
 size_t jacobian_tc_smem(int E, int W, int R, int K, int rows) {
-  const int KC = (W * R + 7) / 8 * 2;  // 16-byte feature chunks per electrode row (K padded to 8)
-  const size_t feat = (size_t)2 * kTcCells * KC * E * 16 + (size_t)(kTcM + 8) * 16;
+  const int Ep = (E + 7) & ~7, RW = kTcCells * Ep;
+  const int KC = (W * R + 7) / 8 * 2;  // 16-byte feature chunks per row and part (K padded to 8)
+  const size_t feat = (size_t)2 * KC * RW * 16 + (size_t)kTcM * 16;  // + rows read past the end
   const size_t gram = (size_t)kTcCells * (E * (E + 1) + 1) * 4;
   const size_t tables = (size_t)kTcCells * (R * K + K) * 4 + (size_t)W * R * 4;
   // per row: Gram offsets of (M,A) (M,B) (N,A) (N,B); at most kTcRowTable rows resident
@@ -109,11 +109,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   extern __shared__ __align__(128) unsigned char tc_sm[];
   constexpr int K = KT, R = RT;
   const int E = a.E, W = a.W;
-  const int N = (E + 7) & ~7;
+  const int Ep = (E + 7) & ~7, RW = kTcCells * Ep;           // rows of the stacked operand
   const int KF = W * R, KC = (KF + 7) / 8 * 2, KS = KC / 2;  // features, 16B chunks, MMA K-steps
-  const size_t part_bytes = (size_t)kTcCells * KC * E * 16;
-  unsigned char* feat = tc_sm;                                         // [2][kTcCells][KC][E][4] fp32
-  float* gram = reinterpret_cast<float*>(feat + 2 * part_bytes + (kTcM + 8) * 16);  // [kTcCells][E(E+1)+1]
+  const size_t part_bytes = (size_t)KC * RW * 16;
+  unsigned char* feat = tc_sm;                                         // [2][KC][RW][4] fp32
+  float* gram = reinterpret_cast<float*>(feat + 2 * part_bytes + kTcM * 16);  // [kTcCells][E(E+1)+1]
   const int GLD = E + 1, GS = E * GLD + 1;                            // entry GS-1 is the remote zero
   float* coef = gram + (size_t)kTcCells * GS;                          // [kTcCells][R][K]
   float* scale = coef + kTcCells * R * K;                              // [W][R]
@@ -126,9 +126,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int groups = (a.c_end - a.c_begin + kTcCells - 1) / kTcCells;
-  const uint32_t columns_needed = (uint32_t)(kTcCells * N);
   uint32_t tmem_cols = 32;
-  while (tmem_cols < columns_needed) tmem_cols <<= 1;
+  while (tmem_cols < (uint32_t)RW) tmem_cols <<= 1;
 
   // set-up: mbarrier (one arrival per group) and the tensor-memory columns of the block
   if (tid == 0) {
@@ -144,7 +143,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = tf32_idesc(kTcM, N);
+  const uint32_t idesc = tf32_idesc(kTcM, RW);
   bool failed = false;
   uint32_t phase = 0;
   // per-block tables: feature scales, Gram offsets of every row (remote slot: the zero entry)
@@ -161,18 +160,17 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   const bool resident = a.rows <= kTcRowTable;
   if (resident) fill_offsets(0, a.rows);
   for (int ci = tid; ci < kTcCells; ci += kTcThreads) gram[(size_t)ci * GS + GS - 1] = 0.f;
-  // padded features (KF .. 8 KS) are zero for every group: written once
-  for (int item = tid; item < kTcCells * (KC * 4 - KF) * E; item += kTcThreads) {
-    const int e = item % E, rest = item / E;
-    const int kf = KF + rest % (KC * 4 - KF), ci = rest / (KC * 4 - KF);
-    const size_t off = (((size_t)ci * KC + (kf >> 2)) * E + e) * 16 + (kf & 3) * 4;
+  // features KF .. 4 KC - 1 are zero for every group: written once
+  for (int item = tid; item < RW * (KC * 4 - KF); item += kTcThreads) {
+    const int r = item % RW, kf = KF + item / RW;
+    const size_t off = ((size_t)(kf >> 2) * RW + r) * 16 + (kf & 3) * 4;
     *reinterpret_cast<float*>(feat + off) = 0.f;
     *reinterpret_cast<float*>(feat + part_bytes + off) = 0.f;
   }
 
   for (int group = blockIdx.x; group < groups && !failed; group += gridDim.x) {
     const int c0 = a.c_begin + group * kTcCells;
-    // (1) cell tables, then features (hi part 0, lo part 1); padded features are zero
+    // (1) cell tables, then features (hi part 0, lo part 1)
     for (int i = tid; i < kTcCells * R * K; i += kTcThreads) {
       const int c = min(c0 + i / (R * K), a.c_end - 1);
       coef[i] = a.features[(int64_t)c * R * K + i % (R * K)];
@@ -182,9 +180,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
       dofs[i] = c < a.c_end ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
     }
     __syncthreads();
+    // 4 lane groups of 64 threads; thread e of a group handles electrode e of wavenumbers
+    // lg, lg + 4, ... of both cells, all its field loads issued first; features past KF stay
+    // zero (written once before the loop)
     {
-      // 4 lane groups of 64 threads; thread e of a group handles electrode e of wavenumbers
-      // lg, lg + 4, ... of every cell of the group; all its field loads are issued first
       constexpr int kMaxWPer = 8;
       const int lg = tid >> 6, e = tid & 63;
       if (e < E) {
@@ -205,7 +204,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
           for (int f = 0; f < R; ++f)
 #pragma unroll
             for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
-          unsigned char* cell_feat = feat + (size_t)ci * KC * E * 16 + (size_t)e * 16;
+          unsigned char* row_feat = feat + (size_t)(ci * Ep + e) * 16;
 #pragma unroll
           for (int j = 0; j < kMaxWPer; ++j) {
             const int w = lg + 4 * j;
@@ -218,7 +217,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
               v *= scale[w * R + f];
               const float hi = tf32_round(v);
               const int kf = w * R + f;
-              float* dst = reinterpret_cast<float*>(cell_feat + (size_t)(kf >> 2) * E * 16) + (kf & 3);
+              float* dst = reinterpret_cast<float*>(row_feat + (size_t)(kf >> 2) * RW * 16) + (kf & 3);
               dst[0] = hi;
               dst[part_bytes / 4] = v - hi;
             }
@@ -231,20 +230,19 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
-    // (2) one thread issues every MMA of the group and commits them to the mbarrier
+    // (2) one thread issues every MMA of the pair and commits them to the mbarrier; a K-step
+    //     advances both descriptors by two chunks
     if (tid == 0) {
       const uint32_t base = smem_addr(feat);
-      for (int ci = 0; ci < kTcCells; ++ci) {
-        const uint32_t d = tmem + (uint32_t)(ci * N);
-        for (int s = 0; s < KS; ++s) {
-          const uint32_t hi = base + (uint32_t)(((size_t)ci * KC + 2 * s) * E * 16);
-          const uint32_t lo = hi + (uint32_t)part_bytes;
-          const uint64_t dh = operand_desc(hi, (uint32_t)E * 16, 128);
-          const uint64_t dl = operand_desc(lo, (uint32_t)E * 16, 128);
-          mma_tf32(d, dh, dh, idesc, s > 0 ? 1u : 0u);
-          mma_tf32(d, dh, dl, idesc, 1u);
-          mma_tf32(d, dl, dh, idesc, 1u);
-        }
+      uint64_t dh = operand_desc(base, (uint32_t)RW * 16, 128);
+      uint64_t dl = operand_desc(base + (uint32_t)part_bytes, (uint32_t)RW * 16, 128);
+      const uint64_t step = (uint64_t)(2 * RW * 16) >> 4;
+      for (int s = 0; s < KS; ++s) {
+        mma_tf32(tmem, dh, dh, idesc, s > 0 ? 1u : 0u);
+        mma_tf32(tmem, dh, dl, idesc, 1u);
+        mma_tf32(tmem, dl, dh, idesc, 1u);
+        dh += step;
+        dl += step;
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                    ::"r"(smem_addr(bar)) : "memory");
@@ -260,22 +258,22 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
     if (failed) break;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
-    // (4) tensor memory -> staged Grams: warp q (and q + 4) owns TMEM lanes 32q..32q+31, which
-    //     hold rows 16q..16q+15 of every M = 64 accumulator in lanes 0..15
+    // (4) tensor memory -> staged Grams: warp w reads TMEM lanes 32 (w % 4) .. + 31 (= rows of D)
+    //     in the columns of cell h = w / 4; a lane keeps the entries of its row when the row
+    //     belongs to cell h
     {
-      const int q = warp & 3;
-      const int row = 16 * q + lane;
-      for (int ci = warp >> 2; ci < kTcCells; ci += 2) {
-        for (int cc = 0; cc < N; cc += 16) {
-          uint32_t v[16];
-          tmem_load16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(ci * N + cc), v);
-          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-          if (lane < 16 && row < E) {
-            float* g = gram + (size_t)ci * GS + (size_t)row * GLD;
+      const int h = warp >> 2, row = 32 * (warp & 3) + lane;
+      const int lr = row - h * Ep;
+      const bool mine = lr >= 0 && lr < E;
+      float* g = gram + (size_t)h * GS + (size_t)(mine ? lr : 0) * GLD;
+      for (int cc = 0; cc < Ep; cc += 8) {
+        uint32_t v[8];
+        tmem_load8(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(h * Ep + cc), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (mine) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j)
-              if (cc + j < E) g[cc + j] = __uint_as_float(v[j]);
-          }
+          for (int j = 0; j < 8; ++j)
+            if (cc + j < E) g[cc + j] = __uint_as_float(v[j]);
         }
       }
     }
@@ -297,8 +295,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
         float v[kTcCells];
 #pragma unroll
         for (int ci = 0; ci < kTcCells; ++ci) {
-          const float* g = gram + (size_t)ci * GS;
-          v[ci] = -((g[o.x] - g[o.y]) - (g[o.z] - g[o.w]));
+          const float* gc = gram + (size_t)ci * GS;
+          v[ci] = -((gc[o.x] - gc[o.y]) - (gc[o.z] - gc[o.w]));
         }
         float* out = a.out + (int64_t)dl * a.ldo + c0;
         if (ncells == kTcCells && (((uintptr_t)out & 7) == 0)) {
@@ -343,10 +341,10 @@ bool tc_shape(int K, int R) {
 }
 }  // namespace
 
-// Whether the tensor-core kernel applies: E <= 64 electrode slots, an instantiated (K, R), and
-// two blocks' shared memory per SM.
+// Whether the tensor-core kernel applies: E <= 64 electrode slots (two cells stack into the
+// 128 rows of one MMA), an instantiated (K, R), and two blocks' shared memory per SM.
 bool jacobian_tc_supported(int E, int W, int R, int K, int rows) {
-  return E <= kTcM && tc_shape(K, R) && W <= 32 && jacobian_tc_smem(E, W, R, K, rows) <= 110 * 1024;
+  return E <= kTcM / kTcCells && tc_shape(K, R) && jacobian_tc_smem(E, W, R, K, rows) <= 110 * 1024;
 }
 
 cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaStream_t s) {
