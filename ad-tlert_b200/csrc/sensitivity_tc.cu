@@ -12,8 +12,9 @@
 // remainder): G = hi.hi + hi.lo + lo.hi, three MMAs per K-step accumulating in fp32.
 //
 // Persistent blocks (two per SM; 256 threads each) loop over the cell pairs: (1) all threads
-// compute the features of the pair into shared memory (thread e of each 64-thread lane group
-// handles electrode e for every fourth wavenumber; generic proxy, then fence.proxy.async); (2) one
+// compute the features of the pair into shared memory (thread e of a 64-thread lane group
+// handles electrode e of (cell, four consecutive wavenumbers) work pairs and stores whole 16-byte
+// chunks; generic proxy, then fence.proxy.async); (2) one
 // thread issues the MMAs and commits them to an mbarrier; (3) all threads wait on it (bounded: on
 // timeout the block raises the error flag, writes NaN for its rows and stops); (4) warps read
 // their TMEM lanes back (tcgen05.ld; warps 0-3 the first cell's columns, 4-7 the second's),
@@ -160,10 +161,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   const bool resident = a.rows <= kTcRowTable;
   if (resident) fill_offsets(0, a.rows);
   for (int ci = tid; ci < kTcCells; ci += kTcThreads) gram[(size_t)ci * GS + GS - 1] = 0.f;
-  // features KF .. 4 KC - 1 are zero for every group: written once
-  for (int item = tid; item < RW * (KC * 4 - KF); item += kTcThreads) {
-    const int r = item % RW, kf = KF + item / RW;
-    const size_t off = ((size_t)(kf >> 2) * RW + r) * 16 + (kf & 3) * 4;
+  // chunks past the ones the wavenumber quads write (R ceil(W / 4) .. KC - 1) are K padding:
+  // zero for every group, written once
+  for (int item = tid, q0 = min(R * ((W + 3) >> 2), KC); item < (KC - q0) * RW * 4; item += kTcThreads) {
+    const size_t off = ((size_t)q0 * RW) * 16 + (size_t)item * 4;
     *reinterpret_cast<float*>(feat + off) = 0.f;
     *reinterpret_cast<float*>(feat + part_bytes + off) = 0.f;
   }
@@ -180,46 +181,60 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
       dofs[i] = c < a.c_end ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
     }
     __syncthreads();
-    // 4 lane groups of 64 threads; thread e of a group handles electrode e of wavenumbers
-    // lg, lg + 4, ... of both cells, all its field loads issued first; features past KF stay
-    // zero (written once before the loop)
+    // work pairs (cell ci, wavenumber quad m): features of wavenumbers 4m .. 4m + 3 are the R
+    // whole chunks R m .. R m + R - 1. Thread e of lane group lg takes electrode e of pairs
+    // lg, lg + 4, ..., two at a time with all their field loads issued first, and stores whole
+    // 16-byte chunks (consecutive lanes: consecutive rows); chunks past KC hold only padding
     {
-      constexpr int kMaxWPer = 8;
       const int lg = tid >> 6, e = tid & 63;
+      const int NQ = (W + 3) >> 2, pairs = kTcCells * NQ;
       if (e < E) {
-        for (int ci = 0; ci < kTcCells; ++ci) {
-          int dof[K];
+        for (int p0 = lg; p0 < pairs; p0 += 8) {
+          float x[2][4][K];
 #pragma unroll
-          for (int k = 0; k < K; ++k) dof[k] = dofs[ci * K + k];
-          float x[kMaxWPer][K];
+          for (int pp = 0; pp < 2; ++pp) {
+            const int p = p0 + 4 * pp;
+            const int ci = p / NQ, m = p - ci * NQ;
 #pragma unroll
-          for (int j = 0; j < kMaxWPer; ++j) {
-            const int w = lg + 4 * j;
-            const float* fw = a.fields + (int64_t)w * a.N * E + e;
+            for (int k = 0; k < K; ++k) {
+              const int dof = p < pairs ? dofs[ci * K + k] : -1;
 #pragma unroll
-            for (int k = 0; k < K; ++k) x[j][k] = (w < W && dof[k] >= 0) ? __ldg(fw + (int64_t)dof[k] * E) : 0.f;
+              for (int wq = 0; wq < 4; ++wq) {
+                const int w = 4 * m + wq;
+                x[pp][wq][k] = (dof >= 0 && w < W) ? __ldg(a.fields + ((int64_t)w * a.N + dof) * E + e) : 0.f;
+              }
+            }
           }
-          float cf[R][K];
 #pragma unroll
-          for (int f = 0; f < R; ++f)
+          for (int pp = 0; pp < 2; ++pp) {
+            const int p = p0 + 4 * pp;
+            if (p >= pairs) break;
+            const int ci = p / NQ, m = p - ci * NQ;
+            float cf[R][K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
-          unsigned char* row_feat = feat + (size_t)(ci * Ep + e) * 16;
+            for (int f = 0; f < R; ++f)
 #pragma unroll
-          for (int j = 0; j < kMaxWPer; ++j) {
-            const int w = lg + 4 * j;
-            if (w >= W) break;
+              for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
+            unsigned char* row_feat = feat + ((size_t)R * m * RW + ci * Ep + e) * 16;
+            float hi[4], lo[4];
 #pragma unroll
-            for (int f = 0; f < R; ++f) {
-              float v = 0.f;
+            for (int wq = 0; wq < 4; ++wq) {
+              const int w = min(4 * m + wq, W - 1);
 #pragma unroll
-              for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[j][k], v);
-              v *= scale[w * R + f];
-              const float hi = tf32_round(v);
-              const int kf = w * R + f;
-              float* dst = reinterpret_cast<float*>(row_feat + (size_t)(kf >> 2) * RW * 16) + (kf & 3);
-              dst[0] = hi;
-              dst[part_bytes / 4] = v - hi;
+              for (int f = 0; f < R; ++f) {
+                float v = 0.f;
+#pragma unroll
+                for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[pp][wq][k], v);
+                v *= scale[w * R + f];
+                const int kl = wq * R + f;  // compile-time: chunk kl / 4, lane kl % 4
+                hi[kl & 3] = tf32_round(v);
+                lo[kl & 3] = v - hi[kl & 3];
+                if ((kl & 3) == 3 && R * m + (kl >> 2) < KC) {
+                  const size_t off = (size_t)(kl >> 2) * RW * 16;
+                  *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+                  *reinterpret_cast<float4*>(row_feat + part_bytes + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+                }
+              }
             }
           }
         }
