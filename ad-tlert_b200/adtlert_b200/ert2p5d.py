@@ -550,7 +550,7 @@ class ERTForward2p5D:
     # ------------------------------------------------------------------ fields
     def _solve_fields(self, sigmas: Tensor, name) -> list[_Fields]:
         batch = int(sigmas.shape[0])
-        sig = sigmas.to(self.device, torch.float32).contiguous()
+        sig = sigmas.to(self.device, torch.float32, non_blocking=True).contiguous()
         entry = self._solver.lookup(batch)
         self._call("adt_factorize", entry["slot"], _native.ptr(sig), batch, self._stream())
         entry["name"] = name

@@ -17,6 +17,8 @@ def step_batches(steps: Sequence[int], batch_steps: int) -> list[list[int]]:
     steps = list(steps)
     if not steps:
         return []
+    if len(steps) <= batch_steps:
+        return [[int(step) for step in steps]]
     count = -(-len(steps) // batch_steps)
     return [list(map(int, batch)) for batch in np.array_split(np.asarray(steps), count)]
 
@@ -35,7 +37,8 @@ def factorization_name(keys) -> tuple | None:
 
 
 class FieldCache:
-    """Fields of recently solved models keyed by a blake2b digest of the model bytes."""
+    """Fields of recently solved models keyed by a digest of the model bytes (SHA-256, the
+    fastest of hashlib's digests on the host here, truncated to 16 bytes) and their dtype."""
 
     def __init__(self, max_entries: int) -> None:
         if int(max_entries) < 0:
@@ -48,7 +51,7 @@ class FieldCache:
         if self.max_entries < 1:
             return None
         host = np.ascontiguousarray(model.detach().cpu().numpy())
-        return hashlib.blake2b(host.view(np.uint8), digest_size=16).digest() + host.dtype.str.encode()
+        return hashlib.sha256(host.view(np.uint8)).digest()[:16] + host.dtype.str.encode()
 
     def _lookup(self, key):
         if key is None:
@@ -79,7 +82,8 @@ class FieldCache:
         missing = [step for step in range(len(keys)) if step not in fields]
         for batch in step_batches(missing, batch_steps):
             name = factorization_name([keys[step] for step in batch])
-            for step, solved in zip(batch, solve(models[batch], name), strict=True):
+            chosen = models if batch == list(range(len(models))) else models[batch]
+            for step, solved in zip(batch, solve(chosen, name), strict=True):
                 fields[step] = solved
                 self._store(keys[step], solved)
         return [fields[step] for step in range(len(keys))], keys

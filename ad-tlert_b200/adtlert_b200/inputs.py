@@ -13,6 +13,22 @@ factorizes in float64); the reference's optional float64 mode is not provided.""
 Tensor = torch.Tensor
 
 
+def _host(values: Tensor):
+    """NumPy view of a CPU float tensor (checks on it avoid torch's per-op overhead), else None."""
+
+    return values.detach().numpy() if values.device.type == "cpu" else None
+
+
+def _all_finite(values: Tensor) -> bool:
+    host = _host(values)
+    return bool(np.isfinite(host).all()) if host is not None else bool(torch.isfinite(values).all())
+
+
+def _any_nonpositive(values: Tensor) -> bool:
+    host = _host(values)
+    return bool((host <= 0.0).any()) if host is not None else bool(torch.any(values <= 0.0))
+
+
 def check_finite(values: Tensor, context: str) -> None:
     if not bool(torch.isfinite(values).all()):
         raise FloatingPointError(f"{context} produced non-finite values")
@@ -24,14 +40,14 @@ def cell_vector(values, count: int, dtype: torch.dtype = FLOAT_DTYPE) -> Tensor:
         vector = vector.expand(count)
     elif vector.shape != (count,):
         raise ValueError(f"conductivity must be scalar or shape ({count},)")
-    if not bool(torch.isfinite(vector).all()):
+    if not _all_finite(vector):
         raise ValueError("conductivity must contain finite values")
     return vector
 
 
 def conductivity_model(values, count: int, dtype: torch.dtype = FLOAT_DTYPE) -> Tensor:
     model = cell_vector(values, count, dtype)
-    if bool(torch.any(model <= 0.0)):
+    if _any_nonpositive(model):
         raise ValueError("conductivity must contain positive finite values")
     return model
 
@@ -40,7 +56,7 @@ def conductivity_series(values, count: int, dtype: torch.dtype = FLOAT_DTYPE) ->
     models = torch.as_tensor(values, dtype=dtype)
     if models.ndim != 2 or models.shape[1] != count:
         raise ValueError(f"conductivities must have shape (n_steps, {count})")
-    if not bool(torch.isfinite(models).all()) or bool(torch.any(models <= 0.0)):
+    if not _all_finite(models) or _any_nonpositive(models):
         raise ValueError("conductivity must contain positive finite values")
     return models
 
