@@ -25,6 +25,7 @@ SYMBOLS = (
     "adt_set_primary",
     "adt_set_static_rhs",
     "adt_factorize",
+    "adt_factorize_fields",
     "adt_solve_fields",
     "adt_solve",
     "adt_factorize_wavenumbers",
@@ -123,6 +124,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_set_primary": (status, [_p, _p, _p]),
         "adt_set_static_rhs": (status, [_p, _p, _p, _p]),
         "adt_factorize": (status, [_p, _i32, _p, _i32, _p]),
+        "adt_factorize_fields": (status, [_p, _i32, _p, _i32, _p]),
         "adt_solve_fields": (status, [_p, _i32, _p, _i32, _p, _p]),
         "adt_solve": (status, [_p, _i32, _i32, _i32, _p, _p]),
         "adt_factorize_wavenumbers": (status, [_p, _i32, _p, _i32, _i32, _p]),

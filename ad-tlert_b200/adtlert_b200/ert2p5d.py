@@ -552,7 +552,8 @@ class ERTForward2p5D:
         batch = int(sigmas.shape[0])
         sig = sigmas.to(self.device, torch.float32, non_blocking=True).contiguous()
         entry = self._solver.lookup(batch)
-        self._call("adt_factorize", entry["slot"], _native.ptr(sig), batch, self._stream())
+        # the factorization also forward-reduces the field right-hand sides solved just below
+        self._call("adt_factorize_fields", entry["slot"], _native.ptr(sig), batch, self._stream())
         entry["name"] = name
         self._solver.factorizations += 1
         total = torch.empty((batch, self.W, self.N, self.E), dtype=torch.float32, device=self.device)

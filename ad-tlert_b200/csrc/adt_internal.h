@@ -47,6 +47,14 @@ struct Slot {
   size_t capacity = 0;      // systems allocated
   double* values = nullptr; // [systems][nnz]
   double* factors = nullptr;// [systems][factor_stride]
+  // field right-hand sides forward-reduced by adt_factorize_fields, consumed by the next
+  // adt_solve_fields of the same sigma and model count
+  double* rhs = nullptr;    // [systems][N][E]
+  double* rho = nullptr;    // [models][E] source resistivities
+  size_t rhs_capacity = 0;  // systems allocated for rhs
+  bool rhs_ready = false;
+  const float* rhs_sigma = nullptr;
+  int rhs_models = 0;
 };
 
 struct Aggregation {

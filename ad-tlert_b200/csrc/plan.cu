@@ -22,6 +22,10 @@ adt_status factorize_systems(adt_plan* p, int systems, const double* values, dou
                              cudaStream_t s);
 adt_status solve_systems(adt_plan* p, int systems, int nrhs, const double* factors,
                          double* rhs, cudaStream_t s);
+bool fused_rhs_supported(const adt_plan* p, int nrhs);
+adt_status factorize_systems_rhs(adt_plan* p, int systems, const double* values, double* factors, double* rhs,
+                                 int nrhs, cudaStream_t s);
+adt_status backward_systems(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s);
 void configure_solver_kernels();
 size_t jacobian_smem(int cells, int R, int E, int K);
 
@@ -392,6 +396,8 @@ adt_status adt_plan_destroy(adt_plan* p) {
   for (auto& s : p->slots) {
     if (s.values) cudaFree(s.values);
     if (s.factors) cudaFree(s.factors);
+    if (s.rhs) cudaFree(s.rhs);
+    if (s.rho) cudaFree(s.rho);
   }
   for (auto& a : p->aggregations) {
     if (a.ptr) cudaFree(a.ptr);
@@ -521,10 +527,47 @@ adt_status adt_factorize(adt_plan* p, int32_t slot, const float* sigma, int32_t 
   adt_status st = ensure_slot(p, slot, systems);
   if (st != ADT_OK) return st;
   Slot& sl = p->slots[slot];
+  sl.rhs_ready = false;
   launch_assemble(p, sigma, systems, sl.values, true, true, s);
   st = factorize_systems(p, systems, sl.values, sl.factors, s);
   sl.systems = systems;
   return st;
+}
+
+adt_status adt_factorize_fields(adt_plan* p, int32_t slot, const float* sigma, int32_t models,
+                                adt_stream stream) {
+  if (!p || !sigma || models <= 0) return fail(p, ADT_INVALID_ARG, "invalid factorize arguments");
+  if (!p->has_primary || p->static_rhs || !fused_rhs_supported(p, p->E))
+    return adt_factorize(p, slot, sigma, models, stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int systems = models * p->W;
+  adt_status st = ensure_slot(p, slot, systems);
+  if (st != ADT_OK) return st;
+  Slot& sl = p->slots[slot];
+  sl.rhs_ready = false;
+  if (sl.rhs_capacity < (size_t)systems) {
+    if (sl.rhs) cudaFree(sl.rhs);
+    if (sl.rho) cudaFree(sl.rho);
+    sl.rhs = sl.rho = nullptr;
+    sl.rhs_capacity = 0;
+    if (cudaMalloc(&sl.rhs, (size_t)systems * p->N * p->E * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&sl.rho, (size_t)systems * p->E * sizeof(double)) != cudaSuccess)
+      return fail(p, ADT_OOM, "field right-hand side allocation failed");
+    sl.rhs_capacity = systems;
+  }
+  launch_assemble(p, sigma, systems, sl.values, true, true, s);
+  launch_chained(source_rho_kernel, grid_for((int64_t)models * p->E), 256, 0, s, sigma, p->Cm, p->E, models,
+                 p->src_ptr, p->src_cells, sl.rho);
+  p->launches++;
+  // rhs = A(1) u_p - rho A(sigma) u_p, forward-reduced level by level with the factorization
+  launch_spmm<double>(p, sl.values, false, p->primary, false, sl.rho, p->refrhs, -1.0, systems, sl.rhs, s);
+  st = factorize_systems_rhs(p, systems, sl.values, sl.factors, sl.rhs, p->E, s);
+  sl.systems = systems;
+  if (st != ADT_OK) return st;
+  sl.rhs_ready = true;
+  sl.rhs_sigma = sigma;
+  sl.rhs_models = models;
+  return ADT_OK;
 }
 
 adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32_t models,
@@ -536,6 +579,17 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
     return fail(p, ADT_INVALID_ARG, "slot does not hold a factorization of these models");
   cudaStream_t s = (cudaStream_t)stream;
   const int systems = models * p->W;
+  Slot& fs = p->slots[slot];
+  if (fs.rhs_ready && fs.rhs_sigma == sigma && fs.rhs_models == models && fs.systems == systems) {
+    // right-hand sides formed and forward-reduced by adt_factorize_fields: backward levels only
+    fs.rhs_ready = false;  // solved in place
+    adt_status st = backward_systems(p, systems, p->E, fs.factors, fs.rhs, s);
+    if (st != ADT_OK) return st;
+    launch_chained(total_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, fs.rhs, p->primary, fs.rho,
+                   p->W, p->N, p->E, systems, fields);
+    p->launches++;
+    return check_launch(p, "field solve");
+  }
   Carve cv;
   const size_t ir = cv.add((size_t)models * p->E * sizeof(double));
   const size_t ix = cv.add((size_t)systems * p->N * p->E * sizeof(double));
@@ -577,6 +631,7 @@ adt_status adt_factorize_wavenumbers(adt_plan* p, int32_t slot, const float* sig
   adt_status st = ensure_slot(p, slot, w_count);
   if (st != ADT_OK) return st;
   Slot& sl = p->slots[slot];
+  sl.rhs_ready = false;
   AssembleArgs a = assemble_args(p, sigma, w_count, sl.values, true, true);
   a.W = w_count;
   a.w0 = w_begin;

@@ -721,6 +721,77 @@ update_level_kernel(const int* __restrict__ items, int item_begin, const int64_t
   }
 }
 
+// The Schur updates of one level with the forward substitution of the same level fused in: block
+// j of every item subtracts, for each of its pulls, A[e,j]^T Z_j (or V_j A[j,e]^T) from D_j and
+// Z_j^T b_e (or V_j b_e) from b_j, all nrhs (<= MAXM) columns of the right-hand side. Operands
+// of one pull at a time (coupling, Z_j or V_j, b_e) plus D_j and b_j in shared memory; products
+// accumulate in registers; D_j and b_j are written back once.
+template <int MAXM>
+__global__ void __launch_bounds__(kSolverThreads, 2)
+update_rhs_level_kernel(const int* __restrict__ items, int item_begin, const int64_t* __restrict__ tasks,
+                        const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride,
+                        double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
+  chain_wait();
+  constexpr int LD = MAXM + 1;
+  extern __shared__ double sm[];
+  auto tile = [&](int i) { return sm + i * MAXM * LD; };
+  double* X = tile(0);   // A[e,j] (type 0) or V_j (type 1)
+  double* Y = tile(1);   // Z_j (type 0) or A[j,e] (type 1)
+  double* be = tile(2);  // b_e (me x nrhs)
+  double* dm = tile(3);  // D_j
+  double* bt = tile(4);  // b_j
+  const int* it = items + 3 * (item_begin + blockIdx.x);
+  const int64_t* t = tasks + (int64_t)it[0] * T_FIELDS;
+  const int64_t u0 = it[1], u1 = it[2];
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
+  const int mj = (int)t[T_MJ], offj = (int)t[T_OFFJ];
+  double* d = f + t[T_LOFF];
+  async_tile(dm, LD, d, mj, mj);
+  async_rows(bt, LD, x + (int64_t)offj * nrhs, nrhs, mj, nrhs);
+  const Micro md(mj, mj), mb(mj, nrhs);
+  double accd[4][4], accb[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) accd[r][c] = accb[r][c] = 0.0;
+  for (int64_t u = u0; u < u1; ++u) {
+    if (u > u0) __syncthreads();  // the previous pull's operands have been read
+    const int64_t* pl = pulls + u * P_FIELDS;
+    const int me = (int)pl[P_ME];
+    const bool right = pl[P_TYPE] == 0;
+    if (right) {
+      async_tile(X, LD, f + pl[P_AOFF], me, mj);
+      async_tile(Y, LD, f + pl[P_OFF], me, mj);
+    } else {
+      async_tile(X, LD, f + pl[P_OFF], mj, me);
+      async_tile(Y, LD, f + pl[P_AOFF], mj, me);
+    }
+    async_rows(be, LD, x + (int64_t)pl[P_EOFF] * nrhs, nrhs, me, nrhs);
+    async_commit();
+    async_wait_all();
+    __syncthreads();
+    if (right) {
+      accumulate<true, false>(accd, md, X, LD, Y, LD, me);   // A[e,j]^T Z_j
+      accumulate<true, false>(accb, mb, Y, LD, be, LD, me);  // Z_j^T b_e
+    } else {
+      accumulate<false, true>(accd, md, X, LD, Y, LD, me);   // V_j A[j,e]^T
+      accumulate<false, false>(accb, mb, X, LD, be, LD, me); // V_j b_e
+    }
+  }
+  __syncthreads();
+  subtract_tile(accd, md, dm, LD, mj, mj, tile(0));
+  subtract_tile(accb, mb, bt, LD, mj, nrhs, tile(0));
+  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
+    const int r = i / mj, c = i - r * mj;
+    d[i] = dm[r * LD + c];
+  }
+  for (int i = threadIdx.x; i < mj * nrhs; i += blockDim.x) {
+    const int r = i / nrhs, c = i - r * nrhs;
+    x[(int64_t)(offj + r) * nrhs + c] = bt[r * LD + c];
+  }
+}
+
 // Eager forward updates after a level: b_j -= Z_j^T b_e / V_j b_e for the pulls [u0, u1) of the
 // item, right-hand-side columns [c0, c0 + strip).
 template <int MAXM>
@@ -1312,6 +1383,8 @@ void configure() {
   cudaFuncSetAttribute(forward_update_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)forward_update_smem<MAXM>());
   cudaFuncSetAttribute(backward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)backward_smem<MAXM>());
+  cudaFuncSetAttribute(update_rhs_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)update_smem<MAXM>());
 }
 
 template <int MAXM>
@@ -1334,12 +1407,49 @@ void factor_levels(adt_plan* p, int systems, const double* values, double* facto
   }
 }
 
+// factor_levels with the forward substitution of `rhs` (nrhs <= MAXM columns per system) fused
+// into the Schur-update launches.
+template <int MAXM>
+void factor_levels_rhs(adt_plan* p, int systems, const double* values, double* factors, double* rhs, int nrhs,
+                       cudaStream_t s) {
+  const int tasks = p->level_begin[p->levels];
+  const int64_t rhs_stride = (int64_t)p->N * nrhs;
+  launch_chained(scatter_diagonal_kernel, dim3(tasks, systems), kSolverThreads, 0, s,
+      p->tasks, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
+  p->launches++;
+  for (int level = 0; level < p->levels; ++level) {
+    const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
+    launch_chained(invert_level_kernel<MAXM>, dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s,
+        p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
+    p->launches++;
+    const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
+    if (i1 > i0) {
+      launch_chained(update_rhs_level_kernel<MAXM>, dim3(i1 - i0, systems), kSolverThreads, update_smem<MAXM>(), s,
+          p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+      p->launches++;
+    }
+  }
+}
+
 // Column strip of the substitution kernels: the full tile unless that leaves most SMs idle.
 template <int MAXM>
 int strip_for(int blocks, int nrhs) {
   int strip = MAXM;
   while (strip > 16 && (int64_t)blocks * ((nrhs + strip - 1) / strip) < 2 * 148) strip /= 2;
   return strip;
+}
+
+// The backward levels alone (the right-hand side already forward-reduced).
+template <int MAXM>
+void backward_levels(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s) {
+  const int64_t rhs_stride = (int64_t)p->N * nrhs;
+  for (int level = p->levels - 1; level >= 0; --level) {
+    const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
+    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs);
+    launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
+                   backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
+    p->launches++;
+  }
 }
 
 template <int MAXM>
@@ -1388,6 +1498,30 @@ adt_status solve_systems(adt_plan* p, int systems, int nrhs, const double* facto
   else if (p->max_m <= 48) solve_levels<48>(p, systems, nrhs, factors, rhs, s);
   else solve_levels<64>(p, systems, nrhs, factors, rhs, s);
   return check_launch(p, "solve");
+}
+
+// Whether the field right-hand side can be forward-reduced during the factorization: the
+// shared-memory solver, and nrhs within its block width.
+bool fused_rhs_supported(const adt_plan* p, int nrhs) {
+  const int width = p->max_m <= 32 ? 32 : p->max_m <= 48 ? 48 : 64;
+  return !p->tiled && nrhs <= width;
+}
+
+adt_status factorize_systems_rhs(adt_plan* p, int systems, const double* values, double* factors, double* rhs,
+                                 int nrhs, cudaStream_t s) {
+  if (!fused_rhs_supported(p, nrhs)) return fail(p, ADT_INVALID_ARG, "fused right-hand side not supported");
+  if (p->max_m <= 32) factor_levels_rhs<32>(p, systems, values, factors, rhs, nrhs, s);
+  else if (p->max_m <= 48) factor_levels_rhs<48>(p, systems, values, factors, rhs, nrhs, s);
+  else factor_levels_rhs<64>(p, systems, values, factors, rhs, nrhs, s);
+  return check_launch(p, "factorization with right-hand side");
+}
+
+adt_status backward_systems(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s) {
+  if (!fused_rhs_supported(p, nrhs)) return fail(p, ADT_INVALID_ARG, "fused right-hand side not supported");
+  if (p->max_m <= 32) backward_levels<32>(p, systems, nrhs, factors, rhs, s);
+  else if (p->max_m <= 48) backward_levels<48>(p, systems, nrhs, factors, rhs, s);
+  else backward_levels<64>(p, systems, nrhs, factors, rhs, s);
+  return check_launch(p, "backward substitution");
 }
 
 }  // namespace adt

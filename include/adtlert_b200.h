@@ -123,6 +123,18 @@ adt_status adt_set_static_rhs(adt_plan* plan, const double* unit_primary, const 
 adt_status adt_factorize(adt_plan* plan, int32_t slot, const float* sigma, int32_t models,
                          adt_stream stream);
 
+/* adt_factorize plus the field right-hand sides of the same models: forms
+ * A(1) u_p - rho A(sigma) u_p and forward-reduces it during the factorization (each level's
+ * forward updates run in that level's Schur-update launch), keeping it in the slot. The next
+ * adt_solve_fields on this slot with the same sigma pointer and model count then runs only the
+ * backward substitution and the total field; any other call factorizing into the slot drops the
+ * reduced right-hand sides. Plans where this does not apply (3D static right-hand sides, the
+ * tiled solver, more electrodes than the solver's block width) factorize as adt_factorize.
+ * Replaces: the factorization + solve phases of _solve_fields (adtlert/forward/ert2p5d.py:532-553,
+ * cudss.py:63-122) when called back to back. */
+adt_status adt_factorize_fields(adt_plan* plan, int32_t slot, const float* sigma, int32_t models,
+                                adt_stream stream);
+
 /* Secondary-field solve with the slot's factorization of the same models, writing total
  * fields u = u_s + rho_src u_p. Replaces: _solve_fields (ert2p5d.py:532-553). */
 adt_status adt_solve_fields(adt_plan* plan, int32_t slot, const float* sigma, int32_t models,

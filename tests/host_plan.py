@@ -115,15 +115,23 @@ def _update_items(hp: HostPlan, level: int):
     return items[hp.update_begin[level]:hp.update_begin[level + 1]]
 
 
-def replay_factor(hp: HostPlan, values: np.ndarray) -> np.ndarray:
+def replay_factor(hp: HostPlan, values: np.ndarray, rhs: np.ndarray | None = None):
     """Factor storage of one system as the shared-memory kernels write it: D of every block
     scattered into its G storage; per level the eliminations (inverse launch: G_j = D_j^-1,
     Z_p = G_j A[j,p], V_q = A[q,j] G_j, coupling copies, fill -A[q,j] Z_p) and the eager Schur
     updates of the neighbouring blocks (A[e,j]^T Z_j, V_j A[j,e]^T). Every access is
     bounds-checked, every read must follow a write, and no item of a launch may write what another
-    item of that launch reads or writes."""
+    item of that launch reads or writes. With ``rhs`` (N, nrhs) the update launches also apply the
+    forward substitution (b_j -= Z_j^T b_e / V_j b_e, update_rhs_level_kernel) and the forward-
+    reduced right-hand side is returned with the factors; its rows join the race checks (indices
+    offset past the factor storage)."""
 
     stride = hp.factor_stride
+    x = None if rhs is None else rhs.astype(float).copy()
+
+    def rows(off, count):
+        assert 0 <= off and off + count <= x.shape[0], "rhs rows out of range"
+        return stride + (np.arange(off, off + count)[:, None] * x.shape[1] + np.arange(x.shape[1])[None, :])
     f = np.full(stride, np.nan)
 
     def idx(offset, rows, cols, what):
@@ -187,26 +195,39 @@ def replay_factor(hp: HostPlan, values: np.ndarray) -> np.ndarray:
         launch, results = _Launch("update"), []
         for t, u0, u1 in _update_items(hp, level):
             row = hp.tasks[t]
-            mj, loff = int(row[T_MJ]), int(row[T_LOFF])
+            mj, loff, offj = int(row[T_MJ]), int(row[T_LOFF]), int(row[T_OFFJ])
             dm = load(loff, mj, mj, "D (update)")
-            reads = [idx(loff, mj, mj, "D")]
+            reads, writes = [idx(loff, mj, mj, "D")], [idx(loff, mj, mj, "D")]
+            bj = None
+            if x is not None:
+                bj = x[offj:offj + mj].copy()
+                reads.append(rows(offj, mj))
+                writes.append(rows(offj, mj))
             for u in range(u0, u1):
                 assert row[T_PULL0] <= u < row[T_PULL1]
-                kind, off, me, _, aoff = (int(v) for v in hp.pull_table[u])
+                kind, off, me, eoff, aoff = (int(v) for v in hp.pull_table[u])
                 if kind == 0:
                     A, Z = load(aoff, me, mj, "coupling"), load(off, me, mj, "Z")
                     dm -= A.T @ Z
                     reads += [idx(aoff, me, mj, "coupling"), idx(off, me, mj, "Z")]
+                    if x is not None:
+                        bj -= Z.T @ x[eoff:eoff + me]
                 else:
                     V, A = load(off, mj, me, "V"), load(aoff, mj, me, "coupling")
                     dm -= V @ A.T
                     reads += [idx(off, mj, me, "V"), idx(aoff, mj, me, "coupling")]
-            launch.item(reads, [idx(loff, mj, mj, "D")])
-            results.append((loff, dm))
+                    if x is not None:
+                        bj -= V @ x[eoff:eoff + me]
+                if x is not None:
+                    reads.append(rows(eoff, me))
+            launch.item(reads, writes)
+            results.append((loff, dm, offj, bj))
         launch.check()
-        for loff, dm in results:
+        for loff, dm, offj, bj in results:
             f[loff:loff + dm.size] = dm.reshape(-1)
-    return f
+            if bj is not None:
+                x[offj:offj + bj.shape[0]] = bj
+    return f if x is None else (f, x)
 
 
 def replay_solve(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarray:
@@ -227,6 +248,17 @@ def replay_solve(hp: HostPlan, f: np.ndarray, rhs: np.ndarray) -> np.ndarray:
                 kind, off, me, eoff, _ = (int(v) for v in hp.pull_table[u])
                 y = x[eoff:eoff + me]
                 x[offj:offj + mj] -= (block(off, me, mj).T @ y) if kind == 0 else (block(off, mj, me) @ y)
+    return replay_backward(hp, f, x)
+
+
+def replay_backward(hp: HostPlan, f: np.ndarray, reduced: np.ndarray) -> np.ndarray:
+    """The backward levels alone on a forward-reduced right-hand side (backward_level_kernel)."""
+
+    x = reduced.astype(float).copy()
+
+    def block(off, rows, cols):
+        return f[off:off + rows * cols].reshape(rows, cols)
+
     for level in range(hp.levels - 1, -1, -1):
         for t in range(hp.level_begin[level], hp.level_begin[level + 1]):
             row = hp.tasks[t]

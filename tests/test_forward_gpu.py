@@ -259,3 +259,28 @@ def test_non_finite_fields_raise_and_are_not_cached():
         forward.solve(tiny)
     sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float32)
     assert torch.isfinite(forward.jacobian(sigma)).all()
+
+
+def test_fused_forward_substitution_gives_the_two_phase_fields():
+    from adtlert_b200 import _native
+    nodes, cells, electrodes, abmn = synthetic.flat_section()
+    forward = ERTForward2p5D(Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, abmn))
+    sigma = torch.as_tensor(synthetic.layered_model(nodes, cells, 4), dtype=torch.float32).cuda()[None].contiguous()
+    other = sigma.clone()
+    slot, stream = forward._solver.lookup(1)["slot"], forward._stream()
+
+    def fields(factorize, solve_sigma):
+        out = torch.full((1, forward.W, forward.N, forward.E), float("nan"), device="cuda")
+        if factorize:
+            forward._call(factorize, slot, _native.ptr(sigma), 1, stream)
+        forward._call("adt_solve_fields", slot, _native.ptr(solve_sigma), 1, _native.ptr(out), stream)
+        return out.cpu().double()
+
+    two_phase = fields("adt_factorize", sigma)
+    fused = fields("adt_factorize_fields", sigma)
+    again = fields(None, sigma)            # reduced right-hand sides consumed: the full solve
+    forward._call("adt_factorize_fields", slot, _native.ptr(sigma), 1, stream)
+    elsewhere = fields(None, other)        # another sigma buffer: the full solve
+    for name, value in (("fused", fused), ("again", again), ("elsewhere", elsewhere)):
+        assert torch.isfinite(value).all()
+        assert_close(value, two_phase, 1e-6, f"{name} fields vs factorize + solve_fields")

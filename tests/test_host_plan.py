@@ -13,7 +13,7 @@ from adtlert_b200 import Mesh, Survey, synthetic
 from adtlert_b200.ert2p5d import build_problem
 from cases import FLAT_CASES, case_inputs
 from conftest import assert_close
-from host_plan import HostPlan, replay_assembly, replay_factor, replay_solve
+from host_plan import HostPlan, replay_assembly, replay_backward, replay_factor, replay_solve
 from oracle.ert2p5d import Oracle2p5D
 
 
@@ -68,6 +68,10 @@ def test_replayed_block_cyclic_reduction_solves_the_system(case):
     rhs = np.random.default_rng(0).standard_normal((hp.N, 7))
     expected = spl.splu(A).solve(rhs)
     assert_close(replay_solve(hp, factors, rhs), expected, 1e-10, "solve")
+    # forward substitution fused into the Schur-update launches, then the backward levels alone
+    fused, reduced = replay_factor(hp, values, rhs)
+    assert np.array_equal(fused, factors, equal_nan=True)
+    assert_close(replay_backward(hp, fused, reduced), expected, 1e-10, "fused forward + backward")
 
 
 def test_template_factors_reproduce_the_templates(case):
