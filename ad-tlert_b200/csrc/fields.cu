@@ -63,30 +63,33 @@ __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
 // by system (fields of each system) or by wavenumber (the primary field shared by all models).
 __global__ void spmm_kernel(SpmmArgs a) {
   chain_wait();
-  const int64_t total = (int64_t)a.systems * a.N * a.E;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int e = (int)(idx % a.E);
-    const int64_t rest = idx / a.E;
-    const int n = (int)(rest % a.N), t = (int)(rest / a.N);
+  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x
+  const int NE = a.N * a.E;
+  for (int t = blockIdx.y; t < a.systems; t += gridDim.y) {
     const int w = t % a.W, s = t / a.W;
     const double* v = a.values + (int64_t)(a.values_per_wavenumber ? w : t) * a.nnz;
-    const int64_t xo = (int64_t)(a.x_per_system ? t : w) * a.N * a.E;
-    double acc = 0.0;
-    if (a.x_double) {
-      const double* x = (const double*)a.x + xo;
-      for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
-        acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E + e];
-    } else {
-      const float* x = (const float*)a.x + xo;
-      for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
-        acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E + e];
+    const int64_t xo = (int64_t)(a.x_per_system ? t : w) * NE;
+    const double* rho = a.rho ? a.rho + (int64_t)s * a.E : nullptr;
+    const double* base = a.base ? a.base + (int64_t)w * NE : nullptr;
+    double* out = a.out + (int64_t)t * NE;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NE; i += gridDim.x * blockDim.x) {
+      const int n = i / a.E, e = i - n * a.E;
+      double acc = 0.0;
+      if (a.x_double) {
+        const double* x = (const double*)a.x + xo;
+        for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
+          acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E + e];
+      } else {
+        const float* x = (const float*)a.x + xo;
+        for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
+          acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E + e];
+      }
+      double coef = a.scale;
+      if (rho) coef *= rho[e];
+      double o = coef * acc;
+      if (base) o += base[i];
+      out[i] = o;
     }
-    double coef = a.scale;
-    if (a.rho) coef *= a.rho[s * a.E + e];
-    double out = coef * acc;
-    if (a.base) out += a.base[((int64_t)w * a.N + n) * a.E + e];
-    a.out[idx] = out;
   }
 }
 
@@ -94,15 +97,20 @@ __global__ void spmm_kernel(SpmmArgs a) {
 __global__ void total_kernel(const double* x, const double* primary, const double* rho, int W,
                              int N, int E, int systems, float* fields) {
   chain_wait();
-  const int64_t total = (int64_t)systems * N * E;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int e = (int)(idx % E);
-    const int64_t rest = idx / E;
-    const int n = (int)(rest % N), t = (int)(rest / N);
+  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x
+  const int NE = N * E;
+  for (int t = blockIdx.y; t < systems; t += gridDim.y) {
     const int w = t % W, s = t / W;
-    fields[idx] = primary ? (float)(x[idx] + rho[s * E + e] * primary[((int64_t)w * N + n) * E + e])
-                          : (float)x[idx];
+    const double* xs = x + (int64_t)t * NE;
+    float* out = fields + (int64_t)t * NE;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NE; i += gridDim.x * blockDim.x) {
+      if (primary) {
+        const int e = i % E;
+        out[i] = (float)(xs[i] + rho[s * E + e] * primary[(int64_t)w * NE + i]);
+      } else {
+        out[i] = (float)xs[i];
+      }
+    }
   }
 }
 

@@ -90,6 +90,11 @@ inline int grid_for(int64_t work, int threads = 256) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(blocks, 148 * 32));
 }
 
+// Systems over y (grid-stride beyond 65535), a system's `per_system` entries over x.
+inline dim3 system_grid(int systems, int64_t per_system) {
+  return dim3(grid_for(per_system), (unsigned)std::max(1, std::min(systems, 65535)));
+}
+
 adt_status ensure_slot(adt_plan* p, int slot, int systems) {
   if (slot < 0) return fail(p, ADT_INVALID_ARG, "slot must be non-negative");
   if ((int)p->slots.size() <= slot) p->slots.resize(slot + 1);
@@ -165,7 +170,7 @@ void launch_spmm(adt_plan* p, const double* values, bool values_per_wavenumber, 
   a.nnz = p->nnz;
   a.x_per_system = x_per_system ? 1 : 0;
   a.values_per_wavenumber = values_per_wavenumber ? 1 : 0;
-  launch_chained(spmm_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, a);
+  launch_chained(spmm_kernel, system_grid(systems, (int64_t)p->N * p->E), 256, 0, s, a);
   p->launches++;
 }
 
@@ -585,7 +590,7 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
     fs.rhs_ready = false;  // solved in place
     adt_status st = backward_systems(p, systems, p->E, fs.factors, fs.rhs, s);
     if (st != ADT_OK) return st;
-    launch_chained(total_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, fs.rhs, p->primary, fs.rho,
+    launch_chained(total_kernel, system_grid(systems, (int64_t)p->N * p->E), 256, 0, s, fs.rhs, p->primary, fs.rho,
                    p->W, p->N, p->E, systems, fields);
     p->launches++;
     return check_launch(p, "field solve");
@@ -604,7 +609,7 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
                       cudaMemcpyDeviceToDevice, s);
     adt_status st = solve_systems(p, systems, p->E, p->slots[slot].factors, x, s);
     if (st != ADT_OK) return st;
-    launch_chained(total_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, x, nullptr, nullptr, p->W,
+    launch_chained(total_kernel, system_grid(systems, (int64_t)p->N * p->E), 256, 0, s, x, nullptr, nullptr, p->W,
                                                                            p->N, p->E, systems, fields);
     p->launches++;
     return check_launch(p, "field solve");
@@ -617,7 +622,7 @@ adt_status adt_solve_fields(adt_plan* p, int32_t slot, const float* sigma, int32
   launch_spmm<double>(p, sl.values, false, p->primary, false, rho, p->refrhs, -1.0, systems, x, s);
   adt_status st = solve_systems(p, systems, p->E, sl.factors, x, s);
   if (st != ADT_OK) return st;
-  launch_chained(total_kernel, grid_for((int64_t)systems * p->N * p->E), 256, 0, s, x, p->primary, rho, p->W,
+  launch_chained(total_kernel, system_grid(systems, (int64_t)p->N * p->E), 256, 0, s, x, p->primary, rho, p->W,
                                                                          p->N, p->E, systems, fields);
   p->launches++;
   return check_launch(p, "field solve");
