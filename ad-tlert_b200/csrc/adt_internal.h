@@ -69,6 +69,7 @@ struct adt_plan {
   // sizes
   int N = 0, dim = 2, C = 0, K = 0, Cm = 0, Nb = 0, BL = 0, W = 0, E = 0, D = 0, RW = 0;
   int nnz = 0, nb = 0, max_m = 0, levels = 0;
+  int max_width = 0;  // widest augmented row [D_j | A_jp | A_qj^T] of the level blocks
   int64_t contributions = 0;
   int64_t factor_stride = 0;
   int RS = 0;  // stiffness features per wavenumber

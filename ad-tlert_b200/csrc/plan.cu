@@ -322,6 +322,11 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   p->N = hp.N; p->dim = hp.dim; p->C = hp.C; p->K = hp.K; p->Cm = hp.Cm; p->Nb = hp.Nb;
   p->BL = hp.BL; p->W = hp.W; p->E = hp.E; p->D = hp.D; p->RW = hp.RW;
   p->nnz = hp.nnz; p->nb = hp.nb; p->max_m = hp.max_m; p->levels = hp.levels;
+  for (size_t t = 0; t + T_FIELDS <= hp.task_rows.size(); t += T_FIELDS) {
+    const int64_t* row = hp.task_rows.data() + t;
+    const int width = (int)(row[T_MJ] + (row[T_P] >= 0 ? row[T_MP] : 0) + (row[T_Q] >= 0 ? row[T_MQ] : 0));
+    p->max_width = std::max(p->max_width, width);
+  }
   p->RS = hp.RS; p->R = hp.R; p->rdofs = hp.rdofs;
   p->contributions = hp.contributions; p->factor_stride = hp.factor_stride;
   p->perm = hp.perm; p->iperm = hp.iperm; p->level_begin = hp.level_begin;

@@ -362,13 +362,13 @@ __device__ void upper_solve(const double* l, int ldl, const double* rinv, double
   }
 }
 
-template <int MAXM>
-__host__ __device__ constexpr int aug_ld() { return 3 * MAXM + 1; }
-// Augmented matrix, two buffers of panel rows (8 x 3 MAXM) and panel columns (MAXM x 9), and per
-// warp the pivot-block inverse (8 x 8) and its own rows of L P^-1 (MAXM / 8 x 8).
-template <int MAXM>
+// Column capacity of the level kernel: 3 MAXM, or 128 when every augmented row fits in it.
+constexpr int kNarrowColumns = 128;
+// Augmented matrix (MAXM x WCOL + 1), two buffers of panel rows (8 x WCOL) and panel columns
+// (MAXM x 9), and per warp the pivot-block inverse (8 x 8) and its own rows of L P^-1 (MAXM / 8 x 8).
+template <int MAXM, int WCOL = 3 * MAXM>
 constexpr size_t invert_smem() {
-  return sizeof(double) * ((size_t)MAXM * aug_ld<MAXM>() + 2 * 8 * 3 * (size_t)MAXM + 2 * (size_t)MAXM * 9 +
+  return sizeof(double) * ((size_t)MAXM * (WCOL + 1) + 2 * 8 * (size_t)WCOL + 2 * (size_t)MAXM * 9 +
                            8 * 64 + 8 * (size_t)MAXM);
 }
 
@@ -450,14 +450,14 @@ __device__ void store_tile(double (&acc)[4][4], const Micro& u, double* C, int64
 // zero), and updates its entries by a <- a - C R. Stored: G_j, Z_p, V_q = Z_q^T, copies of the
 // couplings (for the Schur updates) and the fill A[q,p] = -A[q,j] Z_p. A non-positive pivot
 // becomes NaN, which reaches every result of the system.
-template <int MAXM>
+template <int MAXM, int WCOL = 3 * MAXM>
 __global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
 invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int* __restrict__ csr_ptr,
                     const int* __restrict__ csr_row, const int* __restrict__ csr_col, int nnz,
                     const double* __restrict__ values, double* __restrict__ factors, int64_t stride) {
   chain_wait();
-  constexpr int LDA = aug_ld<MAXM>();
-  constexpr int W3 = 3 * MAXM;
+  constexpr int LDA = WCOL + 1;
+  constexpr int W3 = WCOL;                      // column capacity (>= every mj + mp + mq)
   constexpr int RP = MAXM / 8;                  // rows per thread
   constexpr int CP = (W3 + 31) / 32;            // columns per thread
   constexpr int PB = 8;                         // pivot panel
@@ -1379,12 +1379,30 @@ void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, doub
 template <int MAXM>
 void configure() {
   cudaFuncSetAttribute(invert_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)invert_smem<MAXM>());
+  if constexpr (3 * MAXM > kNarrowColumns)
+    cudaFuncSetAttribute(invert_level_kernel<MAXM, kNarrowColumns>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)invert_smem<MAXM, kNarrowColumns>());
   cudaFuncSetAttribute(update_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)update_smem<MAXM>());
   cudaFuncSetAttribute(forward_update_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)forward_update_smem<MAXM>());
   cudaFuncSetAttribute(backward_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)backward_smem<MAXM>());
   cudaFuncSetAttribute(update_rhs_level_kernel<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)update_smem<MAXM>());
+}
+
+// One level of inversions: the narrow column capacity when every augmented row fits in it.
+template <int MAXM>
+void launch_invert(adt_plan* p, int t0, int t1, int systems, const double* values, double* factors, cudaStream_t s) {
+  if constexpr (3 * MAXM > kNarrowColumns) {
+    if (p->max_width <= kNarrowColumns) {
+      launch_chained(invert_level_kernel<MAXM, kNarrowColumns>, dim3(t1 - t0, systems), kSolverThreads,
+                     invert_smem<MAXM, kNarrowColumns>(), s, p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col,
+                     p->nnz, values, factors, p->factor_stride);
+      return;
+    }
+  }
+  launch_chained(invert_level_kernel<MAXM>, dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s,
+                 p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
 }
 
 template <int MAXM>
@@ -1395,8 +1413,7 @@ void factor_levels(adt_plan* p, int systems, const double* values, double* facto
   p->launches++;
   for (int level = 0; level < p->levels; ++level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    launch_chained(invert_level_kernel<MAXM>, dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s, 
-        p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
+    launch_invert<MAXM>(p, t0, t1, systems, values, factors, s);
     p->launches++;
     const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
     if (i1 > i0) {
@@ -1419,8 +1436,7 @@ void factor_levels_rhs(adt_plan* p, int systems, const double* values, double* f
   p->launches++;
   for (int level = 0; level < p->levels; ++level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    launch_chained(invert_level_kernel<MAXM>, dim3(t1 - t0, systems), kSolverThreads, invert_smem<MAXM>(), s,
-        p->tasks, t0, p->csr_ptr, p->csr_row, p->csr_col, p->nnz, values, factors, p->factor_stride);
+    launch_invert<MAXM>(p, t0, t1, systems, values, factors, s);
     p->launches++;
     const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
     if (i1 > i0) {
