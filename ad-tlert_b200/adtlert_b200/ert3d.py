@@ -1,4 +1,4 @@
-"""3D P1 tetrahedral DC operator on the B200 kernels of ``libadtlert_b200``.
+"""3D P1/P2 tetrahedral DC operator on the B200 kernels of ``libadtlert_b200``.
 
 Drop-in for ``adtlert.forward.ERTForward3D`` (adtlert/forward/ert3d.py:114-983): same
 constructor options, methods, keyword arguments, exceptions and CPU results. One model is one
@@ -30,7 +30,14 @@ import torch
 from . import _native
 from .ert2p5d import _Slots, _survey_arrays, _to_host
 from .field_cache import FieldCache
-from .geometry3d import Mesh3D, tetrahedron_stiffness
+from .geometry3d import (
+    Mesh3D,
+    p2_shape_values,
+    p2_triangle_mass,
+    quadratic_topology,
+    tetrahedron_p2_stiffness,
+    tetrahedron_stiffness,
+)
 from .inputs import (
     FLOAT_DTYPE,
     cell_vector,
@@ -78,13 +85,14 @@ class Problem3D:
     def struct(self) -> _native.Problem:
         a, c = self.arrays, self.counts
         h = _native.host_ptr
+        K, BL = a["cell_dofs"].shape[1], a["bdofs"].shape[1]
         return _native.Problem(
-            dof_count=c["N"], dim=3, dof_coordinates=h(a["coords"]), cell_count=c["C"], local_dofs=4,
+            dof_count=c["N"], dim=3, dof_coordinates=h(a["coords"]), cell_count=c["C"], local_dofs=K,
             cell_dofs=h(a["cell_dofs"]), stiffness=h(a["stiffness"]), mass=h(a["mass"]), parent_cells=None,
-            model_cell_count=c["C"], boundary_count=c["Nb"], boundary_local=3, boundary_dofs=h(a["bdofs"]),
+            model_cell_count=c["C"], boundary_count=c["Nb"], boundary_local=BL, boundary_dofs=h(a["bdofs"]),
             boundary_cells=h(a["bcells"]), boundary_mass=h(a["bmass"]), boundary_coefficients=h(a["bcoef"]),
             wavenumber_count=1, wavenumbers=h(a["k"]), weights=h(a["w"]), electrode_count=c["E"],
-            receiver_width=4, receiver_dofs=h(a["rdofs"]), receiver_weights=h(a["rw"]),
+            receiver_width=K, receiver_dofs=h(a["rdofs"]), receiver_weights=h(a["rw"]),
             measurement_count=c["D"], abmn=h(a["abmn"]), source_cell_ptr=h(a["sptr"]), source_cells=h(a["scells"]),
             fixed_count=len(self.fixed), fixed_dofs=h(a["fixed"]) if len(self.fixed) else None,
         )
@@ -112,11 +120,13 @@ def primary_potential(nodes: np.ndarray, source: np.ndarray, surface_z: float) -
     return (1.0 / direct + 1.0 / image) / (4.0 * np.pi)
 
 
-def robin_faces(mesh: Mesh3D, center: np.ndarray):
-    """Far-field faces with their Robin boundary mass alpha * area * M_face, alpha =
-    max(r.n / |r|^2, 0) for r from the electrode centroid to the face center; surface faces and
-    faces with alpha = 0 carry none (ert3d.py:224-256)."""
+def robin_faces(mesh: Mesh3D, center: np.ndarray, face_dofs: np.ndarray, element_order: int = 1):
+    """Far-field faces (their dofs: 3 for P1, 6 for P2) with their Robin boundary mass alpha *
+    M_face (area * the linear face mass, or the quadratic one), alpha = max(r.n / |r|^2, 0) for r
+    from the electrode centroid to the face center; surface faces and faces with alpha = 0 carry
+    none (ert3d.py:224-256)."""
 
+    width = face_dofs.shape[1]
     faces, cells, masses = [], [], []
     for f in np.flatnonzero(~mesh.surface_face_mask):
         radial = mesh.boundary_face_centers[f] - center
@@ -126,21 +136,30 @@ def robin_faces(mesh: Mesh3D, center: np.ndarray):
         alpha = max(float(radial @ mesh.boundary_face_normals[f]) / r2, 0.0)
         if alpha == 0.0:
             continue
-        faces.append(mesh.boundary_faces[f])
+        faces.append(face_dofs[f])
         cells.append(mesh.boundary_face_cells[f])
-        masses.append(alpha * mesh.boundary_face_areas[f] * FACE_MASS)
+        area = mesh.boundary_face_areas[f]
+        masses.append(alpha * (p2_triangle_mass(area) if element_order == 2 else area * FACE_MASS))
     if not faces:
-        return np.zeros((0, 3), np.int32), np.zeros(0, np.int32), np.zeros((0, 3, 3))
+        return np.zeros((0, width), np.int32), np.zeros(0, np.int32), np.zeros((0, width, width))
     return np.asarray(faces, np.int32), np.asarray(cells, np.int32), np.asarray(masses)
 
 
 def build_problem_3d(mesh: Mesh3D, survey, boundary_mode: str = "mixed",
-                     singularity_removal: bool = True) -> Problem3D:
-    """Templates, Robin faces, Dirichlet dofs, field columns and right-hand sides of a P1
-    operator (ert3d.py:140-413), built on the host without a GPU."""
+                     singularity_removal: bool = True, element_order: int = 1) -> Problem3D:
+    """Templates, Robin faces, Dirichlet dofs, field columns and right-hand sides of a P1 or
+    ten-node P2 operator (ert3d.py:140-413), built on the host without a GPU. P2 dofs are the
+    vertices and the edge midpoints (quadratic_topology); electrodes interpolate with the P2
+    shape functions at their barycentric coordinates (ert3d.py:71-90)."""
 
-    nodes, cells = mesh.nodes, mesh.cells
-    N, C, E = mesh.node_count, mesh.cell_count, survey.electrode_count
+    if element_order == 2:
+        nodes, cells, face_dofs = quadratic_topology(mesh.nodes, mesh.cells, mesh.boundary_faces)
+        stiffness = tetrahedron_p2_stiffness(mesh.nodes, mesh.cells)
+    else:
+        nodes, cells, face_dofs = mesh.nodes, mesh.cells, mesh.boundary_faces
+        stiffness = tetrahedron_stiffness(mesh.nodes, mesh.cells)
+    K = cells.shape[1]
+    N, C, E = len(nodes), mesh.cell_count, survey.electrode_count
     positions = np.asarray(survey.electrode_positions, dtype=float)
     slots = survey.measurement_slots()
     current_ids = electrode_rows(slots[:, :2], E)
@@ -158,8 +177,9 @@ def build_problem_3d(mesh: Mesh3D, survey, boundary_mode: str = "mixed",
     if Ec > 160:
         raise ValueError(f"{Ec} field columns exceed the 160 supported by the sensitivity kernels")
     cell_ids, bary = mesh.locate_points(positions)
+    weights = p2_shape_values(bary) if element_order == 2 else bary
     electrode_matrix = np.zeros((E, N))
-    np.add.at(electrode_matrix, (np.repeat(np.arange(E), 4), cells[cell_ids].reshape(-1)), bary.reshape(-1))
+    np.add.at(electrode_matrix, (np.repeat(np.arange(E), K), cells[cell_ids].reshape(-1)), weights.reshape(-1))
 
     def mapped(role: dict, values: np.ndarray) -> np.ndarray:
         return np.asarray([Ec if v == E else role[int(v)] for v in values], dtype=np.int32)
@@ -177,18 +197,18 @@ def build_problem_3d(mesh: Mesh3D, survey, boundary_mode: str = "mixed",
     if points:
         direct = np.zeros((1, Ec, N))
         direct[0, points] = electrode_matrix[electrodes[points]]
+    BL = face_dofs.shape[1]
     if boundary_mode == "mixed":
-        bdofs, bcells, bmass = robin_faces(mesh, positions.mean(axis=0))
+        bdofs, bcells, bmass = robin_faces(mesh, positions.mean(axis=0), face_dofs, element_order)
         fixed = np.zeros(0, dtype=np.int32)
     else:
-        bdofs, bcells, bmass = np.zeros((0, 3), np.int32), np.zeros(0, np.int32), np.zeros((0, 3, 3))
-        fixed = np.unique(mesh.boundary_faces[~mesh.surface_face_mask].reshape(-1)).astype(np.int32)
-    stiffness = tetrahedron_stiffness(nodes, cells)
+        bdofs, bcells, bmass = np.zeros((0, BL), np.int32), np.zeros(0, np.int32), np.zeros((0, BL, BL))
+        fixed = np.unique(face_dofs[~mesh.surface_face_mask].reshape(-1)).astype(np.int32)
     arrays = {
         "coords": np.ascontiguousarray(nodes, dtype=np.float64),
         "cell_dofs": np.ascontiguousarray(cells, dtype=np.int32),
         "stiffness": np.ascontiguousarray(stiffness, dtype=np.float64),
-        "mass": np.zeros((C, 4, 4)),
+        "mass": np.zeros((C, K, K)),
         "bdofs": np.ascontiguousarray(bdofs, dtype=np.int32),
         "bcells": np.ascontiguousarray(bcells, dtype=np.int32),
         "bmass": np.ascontiguousarray(bmass, dtype=np.float64),
@@ -196,7 +216,7 @@ def build_problem_3d(mesh: Mesh3D, survey, boundary_mode: str = "mixed",
         "k": np.zeros(1),
         "w": np.ones(1),
         "rdofs": np.ascontiguousarray(cells[cell_ids[electrodes]], dtype=np.int32),
-        "rw": np.ascontiguousarray(bary[electrodes], dtype=np.float64),
+        "rw": np.ascontiguousarray(weights[electrodes], dtype=np.float64),
         "abmn": np.ascontiguousarray(abmn, dtype=np.int32),
         "sptr": np.zeros(Ec + 1, dtype=np.int32),
         "scells": np.zeros(1, dtype=np.int32),
@@ -230,7 +250,7 @@ def _mesh3d(mesh) -> Mesh3D:
 
 
 class ERTForward3D:
-    """3D tetrahedral DC operator (P1, mixed or Dirichlet far field) on B200 kernels."""
+    """3D tetrahedral DC operator (P1 or ten-node P2, mixed or Dirichlet far field) on B200 kernels."""
 
     def __init__(self, mesh, survey, boundary_mode: str = "mixed", singularity_removal: bool = True,
                  element_order: int = 1, geometric_factor_mode: str = "auto",
@@ -242,8 +262,6 @@ class ERTForward3D:
             raise RuntimeError("ADTLERT requires an NVIDIA GPU with CUDA (B200 kernels)")
         if element_order not in (1, 2):
             raise ValueError("element_order must be 1 or 2")
-        if element_order == 2:
-            raise NotImplementedError("P2 tetrahedra are not supported by this build")
         self.source_mesh, self.source_survey = mesh, survey
         self.mesh = _mesh3d(mesh)
         self.survey = _survey_arrays(survey)
@@ -269,7 +287,8 @@ class ERTForward3D:
 
     # ------------------------------------------------------------------ set-up
     def _build(self) -> None:
-        problem = build_problem_3d(self.mesh, self.survey, self.boundary_mode, self.singularity_removal)
+        problem = build_problem_3d(self.mesh, self.survey, self.boundary_mode, self.singularity_removal,
+                                   self.element_order)
         self._problem = problem
         struct = problem.struct()
         plan = ctypes.c_void_p()
@@ -284,7 +303,7 @@ class ERTForward3D:
                 self._lib.adt_set_static_rhs(plan, _native.host_ptr(problem.unit_primary),
                                              _native.host_ptr(problem.direct), self._stream()),
                 plan, "adt_set_static_rhs")
-        self.C, self.N = self.mesh.cell_count, self.mesh.node_count
+        self.C, self.N = self.mesh.cell_count, problem.counts["N"]  # dofs (vertices + P2 midpoints)
         self.E, self.D = self.survey.electrode_count, self.survey.measurement_count
         self.columns = problem.counts["E"]
         self._current_electrode_ids = problem.current_ids

@@ -1,7 +1,8 @@
-"""Tetrahedral meshes: boundary faces, ground surface, point location and P1 templates.
+"""Tetrahedral meshes: boundary faces, ground surface, point location, P1 and P2 templates.
 
-Restates adtlert/mesh/core3d.py:16-230 (``Mesh3D``) and adtlert/fem/tetrahedron.py:37-56
-(``build_tetrahedron_p1_data``) in float64 NumPy. This is host set-up, run once per operator.
+Restates adtlert/mesh/core3d.py:16-234 (``Mesh3D``, ``build_quadratic_topology``) and
+adtlert/fem/tetrahedron.py:37-127 (P1 and ten-node P2 tetrahedron data) in float64 NumPy. This
+is host set-up, run once per operator.
 """
 
 from __future__ import annotations
@@ -14,6 +15,10 @@ from .geometry import _as_numpy
 
 # local vertex triples of the four faces of a tetrahedron (core3d.py:16)
 TETRA_FACES = ((1, 2, 3), (0, 3, 2), (0, 1, 3), (0, 2, 1))
+# edges of the ten-node tetrahedron after its four vertices, and of the six-node face after its
+# three (the dof order of tetrahedron.py:13 and core3d.py:211-234)
+P2_CELL_EDGES = ((0, 1), (1, 2), (2, 0), (0, 3), (1, 3), (2, 3))
+P2_FACE_EDGES = ((0, 1), (1, 2), (2, 0))
 
 
 def _edge_matrices(cell_nodes: np.ndarray) -> np.ndarray:
@@ -84,6 +89,84 @@ def tetrahedron_stiffness(nodes: np.ndarray, cells: np.ndarray) -> np.ndarray:
     gradients = np.einsum("ij,ejk->eik", reference, np.linalg.inv(jac))
     volumes = np.abs(np.linalg.det(jac)) / 6.0
     return volumes[:, None, None] * np.einsum("eid,ejd->eij", gradients, gradients)
+
+
+def quadratic_topology(nodes: np.ndarray, cells: np.ndarray, faces: np.ndarray):
+    """P2 dofs shared between cells: the vertices keep their numbers and every edge midpoint is
+    numbered once, in the order the cells first use it (cell by cell, edges 01, 12, 20, 03, 13,
+    23), as core3d.py:211-234 numbers them. Returns the dof coordinates, the cell dofs (C x 10:
+    vertices, then edge midpoints) and the face dofs (F x 6: vertices, then edges 01, 12, 20)."""
+
+    nodes = np.asarray(nodes, dtype=float)
+    cells = np.asarray(cells, dtype=np.int64)
+    faces = np.asarray(faces, dtype=np.int64)
+    n = len(nodes)
+    pairs = np.stack([cells[:, [i, j]] for i, j in P2_CELL_EDGES], axis=1).reshape(-1, 2)
+    lo, hi = pairs.min(axis=1), pairs.max(axis=1)
+    keys = lo * n + hi
+    unique, first, inverse = np.unique(keys, return_index=True, return_inverse=True)
+    rank = np.empty(len(unique), dtype=np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(len(unique))
+    cell_mid = (n + rank[inverse]).reshape(-1, 6)
+    order = np.argsort(rank)
+    ua, ub = unique[order] // n, unique[order] % n
+    dof_nodes = np.vstack((nodes, 0.5 * (nodes[ua] + nodes[ub])))
+    face_pairs = np.stack([faces[:, [i, j]] for i, j in P2_FACE_EDGES], axis=1).reshape(-1, 2)
+    face_keys = face_pairs.min(axis=1) * n + face_pairs.max(axis=1)
+    position = np.searchsorted(unique, face_keys)
+    if np.any(position >= len(unique)) or np.any(unique[np.minimum(position, len(unique) - 1)] != face_keys):
+        raise ValueError("a boundary face edge is not an edge of any cell")
+    face_mid = (n + rank[position]).reshape(-1, 3)
+    return dof_nodes, np.hstack((cells, cell_mid)), np.hstack((faces, face_mid))
+
+
+def p2_shape_values(barycentric: np.ndarray) -> np.ndarray:
+    """Ten-node tetrahedron shape functions at barycentric points: l_i (2 l_i - 1) at the
+    vertices, 4 l_i l_j at the edges (tetrahedron.py:59-66)."""
+
+    b = np.asarray(barycentric, dtype=float)
+    edges = np.stack([4.0 * b[..., i] * b[..., j] for i, j in P2_CELL_EDGES], axis=-1)
+    return np.concatenate((b * (2.0 * b - 1.0), edges), axis=-1)
+
+
+def tetrahedron_p2_stiffness(nodes: np.ndarray, cells: np.ndarray) -> np.ndarray:
+    """Unit-conductivity ten-node stiffness templates (tetrahedron.py:92-127). The shape-function
+    gradients are linear, so the 4-point symmetric rule (barycentric points with one coordinate
+    (5 + 3 sqrt 5) / 20 and three (5 - sqrt 5) / 20, weights |T| / 4) integrates G G^T exactly;
+    gradients: (4 l_i - 1) grad l_i at vertex i, 4 (l_i grad l_j + l_j grad l_i) at edge ij."""
+
+    jac = _edge_matrices(nodes[cells])
+    reference = np.asarray(((-1.0, -1.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)))
+    grad = np.einsum("ij,ejk->eik", reference, np.linalg.inv(jac))  # (C, 4, 3) of the l_i
+    volumes = np.abs(np.linalg.det(jac)) / 6.0
+    major, minor = (5.0 + 3.0 * np.sqrt(5.0)) / 20.0, (5.0 - np.sqrt(5.0)) / 20.0
+    stiffness = np.zeros((len(cells), 10, 10))
+    for q in range(4):
+        lam = np.full(4, minor)
+        lam[q] = major
+        g = np.concatenate((
+            (4.0 * lam - 1.0)[None, :, None] * grad,
+            np.stack([4.0 * (lam[i] * grad[:, j] + lam[j] * grad[:, i]) for i, j in P2_CELL_EDGES], axis=1),
+        ), axis=1)
+        stiffness += np.einsum("eid,ejd->eij", g, g)
+    return stiffness * (volumes / 4.0)[:, None, None]
+
+
+def p2_triangle_mass(area: float) -> np.ndarray:
+    """Six-node triangle mass matrix (vertices, then edges 01, 12, 20), exact: area / 180 times
+    6 / -1 between vertices, 32 / 16 between edge midpoints, -4 between a vertex and the midpoint
+    of the opposite edge, 0 otherwise (the matrix tetrahedron.py:69-89 integrates with a
+    degree-4 rule)."""
+
+    m = np.asarray((
+        (6, -1, -1, 0, -4, 0),
+        (-1, 6, -1, 0, 0, -4),
+        (-1, -1, 6, -4, 0, 0),
+        (0, 0, -4, 32, 16, 16),
+        (-4, 0, 0, 16, 32, 16),
+        (0, -4, 0, 16, 16, 32),
+    ), dtype=float)
+    return float(area) / 180.0 * m
 
 
 @dataclass(frozen=True)

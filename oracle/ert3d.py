@@ -1,7 +1,7 @@
-"""FP64 NumPy/SciPy restatement of AD-TLERT's 3D P1 tetrahedral operator (adtlert/forward/ert3d.py).
+"""FP64 NumPy/SciPy restatement of AD-TLERT's 3D tetrahedral operator (adtlert/forward/ert3d.py).
 
 TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``): the product never imports this.
-Covers element order 1, mixed and Dirichlet far-field boundaries, singularity removal on flat
+Covers element orders 1 and 2, mixed and Dirichlet far-field boundaries, singularity removal on flat
 surfaces (point sources otherwise) and analytic or numerical geometric factors. The sparse solve
 uses SciPy SuperLU where the reference calls cuDSS.
 """
@@ -16,6 +16,68 @@ import scipy.sparse.linalg as spl
 
 ELECTRODE_RADIUS_FRACTION_3D = 0.5  # adtlert/forward/ert3d.py:47-49
 _TETRA_FACES = ((1, 2, 3), (0, 3, 2), (0, 1, 3), (0, 2, 1))  # adtlert/mesh/core3d.py:16
+_P2_EDGES = ((0, 1), (1, 2), (2, 0), (0, 3), (1, 3), (2, 3))  # adtlert/fem/tetrahedron.py:13
+
+
+def quadratic_dofs(nodes, cells, faces):
+    """Edge-midpoint dofs numbered on first use, cell by cell (adtlert/mesh/core.py:27-44,
+    core3d.py:211-234): dof coordinates, cell dofs (C x 10), face dofs (F x 6)."""
+
+    points, index = [np.asarray(p, dtype=float) for p in nodes], {}
+
+    def midpoint(a, b):
+        key = (min(a, b), max(a, b))
+        if key not in index:
+            index[key] = len(points)
+            points.append(0.5 * (points[key[0]] + points[key[1]]))
+        return index[key]
+
+    cell_dofs = [[*c] + [midpoint(c[i], c[j]) for i, j in _P2_EDGES] for c in cells.tolist()]
+    face_dofs = [[*f] + [midpoint(f[i], f[j]) for i, j in ((0, 1), (1, 2), (2, 0))] for f in faces.tolist()]
+    return np.asarray(points), np.asarray(cell_dofs, dtype=np.int64), np.asarray(face_dofs, dtype=np.int64)
+
+
+def p2_values(bary):
+    """Ten-node shape functions (tetrahedron.py:59-66)."""
+
+    edges = np.stack([4.0 * bary[..., i] * bary[..., j] for i, j in _P2_EDGES], axis=-1)
+    return np.concatenate((bary * (2.0 * bary - 1.0), edges), axis=-1)
+
+
+def p2_stiffness(grads, vol):
+    """Ten-node stiffness with the 4-point rule (tetrahedron.py:92-127), grads (C, 4, 3)."""
+
+    a, b = (5.0 + 3.0 * math.sqrt(5.0)) / 20.0, (5.0 - math.sqrt(5.0)) / 20.0
+    out = np.zeros((len(vol), 10, 10))
+    for q in range(4):
+        lam = np.full(4, b)
+        lam[q] = a
+        vertex = (4.0 * lam - 1.0)[None, :, None] * grads
+        edge = np.stack([4.0 * (lam[i] * grads[:, j] + lam[j] * grads[:, i]) for i, j in _P2_EDGES], axis=1)
+        g = np.concatenate((vertex, edge), axis=1)
+        out += np.einsum("eid,ejd->eij", g, g)
+    return out * (vol / 4.0)[:, None, None]
+
+
+def p2_face_mass(area):
+    """Six-node triangle mass matrix by a 7-point degree-5 rule (tetrahedron.py:69-89 uses a
+    degree-4 rule; both are exact for the degree-4 products)."""
+
+    s15 = math.sqrt(15.0)
+    a1, a2 = (6.0 - s15) / 21.0, (6.0 + s15) / 21.0
+    w1, w2 = (155.0 - s15) / 1200.0, (155.0 + s15) / 1200.0
+    pts = [(1 / 3, 1 / 3, 1 / 3)]
+    wts = [9.0 / 40.0]
+    for a, w in ((a1, w1), (a2, w2)):
+        for k in range(3):
+            p = [a, a, a]
+            p[k] = 1.0 - 2.0 * a
+            pts.append(tuple(p))
+            wts.append(w)
+    bary = np.asarray(pts)
+    shape = np.concatenate((bary * (2.0 * bary - 1.0),
+                            np.stack([4.0 * bary[:, i] * bary[:, j] for i, j in ((0, 1), (1, 2), (2, 0))], 1)), 1)
+    return area * np.einsum("q,qi,qj->ij", np.asarray(wts), shape, shape)
 
 
 def boundary_faces(nodes, cells):
@@ -60,29 +122,39 @@ def locate(nodes, cells, points, tol=1e-8):
 
 
 class Oracle3D:
-    """P1 tetrahedral DC operator (adtlert/forward/ert3d.py:114-983, element_order=1)."""
+    """P1 or ten-node P2 tetrahedral DC operator (adtlert/forward/ert3d.py:114-983)."""
 
     def __init__(self, nodes, cells, electrodes, measurements, boundary_mode="mixed",
-                 singularity_removal=True, geometric_factor_mode="auto"):
-        self.nodes = np.asarray(nodes, dtype=float)
+                 singularity_removal=True, geometric_factor_mode="auto", element_order=1):
+        self.vertices = np.asarray(nodes, dtype=float)
         self.cells = np.asarray(cells, dtype=np.int64)
+        self.nodes = self.vertices
         self.electrodes = np.asarray(electrodes, dtype=float)
         self.measurements = np.asarray(measurements, dtype=np.int64)
+        self.faces, self.face_cells, centers, areas, normals = boundary_faces(self.vertices, self.cells)
+        if element_order == 2:  # ert3d.py:179-193
+            self.nodes, self.dofs, face_dofs = quadratic_dofs(self.vertices, self.cells, self.faces)
+        else:
+            self.dofs, face_dofs = self.cells, self.faces
+        K = self.dofs.shape[1]
+        self.K = K
         N, C, E = len(self.nodes), len(self.cells), len(self.electrodes)
         self.N, self.C, self.E = N, C, E
-        self.faces, self.face_cells, centers, areas, normals = boundary_faces(self.nodes, self.cells)
         self.surface_mask = normals[:, 2] > 1e-8
         surface_nodes = np.unique(self.faces[self.surface_mask])
         self.surface_level = float(self.nodes[:, 2].max())
         tol = max(1e-8, max(float(np.ptp(self.nodes[:, 2])), 1.0) * 1e-8)
         self.flat = bool(np.ptp(self.nodes[surface_nodes, 2]) <= tol)
         # P1 stiffness templates (fem/tetrahedron.py:37-56)
-        cn = self.nodes[self.cells]
+        cn = self.vertices[self.cells]
         jac = np.stack([cn[:, i] - cn[:, 0] for i in (1, 2, 3)], axis=-1)
         ref = np.asarray(((-1.0, -1.0, -1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0), (0.0, 0.0, 1.0)))
         grads = np.einsum("ij,ejk->eik", ref, np.linalg.inv(jac))
         vol = np.abs(np.linalg.det(jac)) / 6.0
-        self.volume_templates = vol[:, None, None] * np.einsum("eid,ejd->eij", grads, grads)
+        if element_order == 2:
+            self.volume_templates = p2_stiffness(grads, vol)
+        else:
+            self.volume_templates = vol[:, None, None] * np.einsum("eid,ejd->eij", grads, grads)
         self.cell_templates = self.volume_templates.copy()
         self.boundary_mode = boundary_mode
         if boundary_mode == "mixed":  # ert3d.py:235-266
@@ -97,12 +169,13 @@ class Oracle3D:
                 if alpha == 0.0:
                     continue
                 c = self.face_cells[f]
-                local = [int(np.flatnonzero(self.cells[c] == n)[0]) for n in self.faces[f]]
-                self.cell_templates[c][np.ix_(local, local)] += alpha * areas[f] * mass
+                local = [int(np.flatnonzero(self.dofs[c] == n)[0]) for n in face_dofs[f]]
+                face_mass = p2_face_mass(areas[f]) if element_order == 2 else areas[f] * mass
+                self.cell_templates[c][np.ix_(local, local)] += alpha * face_mass
         # assembly routing (ert3d.py:292-351)
-        rows = np.repeat(self.cells, 4, axis=1).reshape(-1)
-        cols = np.tile(self.cells, (1, 4)).reshape(-1)
-        self.fixed = np.unique(self.faces[~self.surface_mask].reshape(-1)) if boundary_mode == "dirichlet" else np.zeros(0, int)
+        rows = np.repeat(self.dofs, K, axis=1).reshape(-1)
+        cols = np.tile(self.dofs, (1, K)).reshape(-1)
+        self.fixed = np.unique(face_dofs[~self.surface_mask].reshape(-1)) if boundary_mode == "dirichlet" else np.zeros(0, int)
         fixed_mask = np.zeros(N, dtype=bool)
         fixed_mask[self.fixed] = True
         self.pair_keep = ~fixed_mask[rows] & ~fixed_mask[cols]
@@ -118,9 +191,11 @@ class Oracle3D:
         rmap[self.rcv_ids] = np.arange(len(self.rcv_ids))
         rmap[E] = len(self.rcv_ids)
         self.abmn = np.stack((cmap[slots[:, 0]], cmap[slots[:, 1]], rmap[slots[:, 2]], rmap[slots[:, 3]]), 1)
-        ids, w = locate(self.nodes, self.cells, self.electrodes)
+        ids, w = locate(self.vertices, self.cells, self.electrodes)
+        if element_order == 2:  # ert3d.py:71-90
+            w = p2_values(w)
         self.electrode_matrix = sp.coo_matrix(
-            (w.reshape(-1), (np.repeat(np.arange(E), 4), self.cells[ids].reshape(-1))), shape=(E, N)
+            (w.reshape(-1), (np.repeat(np.arange(E), K), self.dofs[ids].reshape(-1))), shape=(E, N)
         ).tocsr()
         self.singularity = singularity_removal and self.flat
         self.use_numerical_gf = geometric_factor_mode == "numerical" or (geometric_factor_mode == "auto" and not self.flat)
@@ -198,8 +273,8 @@ class Oracle3D:
 
     def _cell_gradient(self, phi, lam, robin):
         T = self.cell_templates if robin else self.volume_templates
-        T = np.where(self.pair_keep.reshape(-1, 4, 4), T, 0.0)
-        return -np.einsum("sci,cij,scj->c", lam[:, self.cells], T, phi[:, self.cells])
+        T = np.where(self.pair_keep.reshape(-1, self.K, self.K), T, 0.0)
+        return -np.einsum("sci,cij,scj->c", lam[:, self.dofs], T, phi[:, self.dofs])
 
     def vjp(self, sigma, cotangent):
         current, receiver, lu = self.fields(sigma)
@@ -227,10 +302,10 @@ class Oracle3D:
     def jacobian(self, sigma, include_robin_boundary_derivative=False):
         current, receiver, _ = self.fields(sigma)
         T = self.cell_templates if include_robin_boundary_derivative else self.volume_templates
-        T = np.where(self.pair_keep.reshape(-1, 4, 4), T, 0.0)
+        T = np.where(self.pair_keep.reshape(-1, self.K, self.K), T, 0.0)
         cur = np.vstack((current, np.zeros((1, self.N))))
         rcv = np.vstack((receiver, np.zeros((1, self.N))))
         a, b, m, n = self.abmn.T
-        u = (cur[a] - cur[b])[:, self.cells]
-        v = (rcv[m] - rcv[n])[:, self.cells]
+        u = (cur[a] - cur[b])[:, self.dofs]
+        v = (rcv[m] - rcv[n])[:, self.dofs]
         return -np.einsum("dci,cij,dcj->dc", v, T, u)  # ert3d.py:867-927

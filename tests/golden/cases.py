@@ -217,6 +217,10 @@ CASES3D = {
     "tet_dirichlet": {"relief": 0.0, "boundary": "dirichlet", "seed": 12},
     # bent top surface: point sources and numerical geometric factors
     "tet_relief": {"relief": 1.0, "boundary": "mixed", "seed": 13},
+    # the same three set-ups with ten-node P2 tetrahedra (element_order=2)
+    "tet_p2_mixed": {"relief": 0.0, "boundary": "mixed", "seed": 14, "order": 2},
+    "tet_p2_dirichlet": {"relief": 0.0, "boundary": "dirichlet", "seed": 15, "order": 2},
+    "tet_p2_relief": {"relief": 1.0, "boundary": "mixed", "seed": 16, "order": 2},
 }
 
 
@@ -249,4 +253,5 @@ def case3d_inputs(name: str) -> dict:
         "cotangent": rng.standard_normal(len(measurements)),
         "direction": rng.standard_normal(len(cells)) * sigma * 1e-2,
         "boundary": spec["boundary"],
+        "order": spec.get("order", 1),
     }

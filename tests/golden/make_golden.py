@@ -156,7 +156,8 @@ def _run_3d(name: str, precision: str) -> dict:
     inputs = case3d_inputs(name)
     mesh = Mesh3D.from_arrays(inputs["nodes"], inputs["cells"])
     survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
-    forward = e3.ERTForward3D.from_mesh_survey(mesh, survey, boundary_mode=inputs["boundary"])
+    forward = e3.ERTForward3D.from_mesh_survey(mesh, survey, boundary_mode=inputs["boundary"],
+                                               element_order=inputs["order"])
     sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float64)
     cotangent = torch.as_tensor(inputs["cotangent"], dtype=torch.float64)
     direction = torch.as_tensor(inputs["direction"], dtype=torch.float64)

@@ -25,7 +25,8 @@ def case(request):
     inputs = case3d_inputs(name)
     mesh = Mesh3D.from_arrays(inputs["nodes"], inputs["cells"])
     survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
-    forward = ERTForward3D.from_mesh_survey(mesh, survey, boundary_mode=inputs["boundary"])
+    forward = ERTForward3D.from_mesh_survey(mesh, survey, boundary_mode=inputs["boundary"],
+                                            element_order=inputs["order"])
     golden32 = np.load(ROOT / "tests" / "golden" / f"{name}_float32.npz")
     golden64 = np.load(ROOT / "tests" / "golden" / f"{name}_float64.npz")
     return name, inputs, forward, golden32, golden64
@@ -43,7 +44,7 @@ def test_forward_matches_the_reference(case):
     response = forward.solve(sigma)
     assert response.apparent_resistivity.device.type == "cpu"
     assert response.apparent_resistivity.dtype == torch.float32
-    both(forward._geometric_factors(), "geometric_factors", g32, g64, 1e-5 if name != "tet_relief" else TOL)
+    both(forward._geometric_factors(), "geometric_factors", g32, g64, 1e-5 if "relief" not in name else TOL)
     both(response.apparent_resistivity, "apparent_resistivity", g32, g64)
     both(response.resistance, "resistance", g32, g64)
     used = forward._current_electrode_ids
@@ -93,7 +94,7 @@ def test_jvp_matches_finite_differences(case):
     sigma = inputs["sigma"]
     direction = inputs["direction"] / np.abs(inputs["direction"]).max() * sigma.min() * 1e-1
     oracle = Oracle3D(inputs["nodes"], inputs["cells"], inputs["electrodes"], inputs["measurements"],
-                      boundary_mode=inputs["boundary"])
+                      boundary_mode=inputs["boundary"], element_order=inputs["order"])
     h = 1e-3
     fd = (oracle.resistance(sigma + h * direction) - oracle.resistance(sigma - h * direction)) / (2 * h)
     ours = forward.jvp(torch.as_tensor(sigma, dtype=torch.float32), torch.as_tensor(direction, dtype=torch.float32))

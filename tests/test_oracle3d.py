@@ -13,7 +13,7 @@ def pinned(request):
     inputs = case3d_inputs(request.param)
     golden = np.load(ROOT / "tests" / "golden" / f"{request.param}_float64.npz")
     oracle = Oracle3D(inputs["nodes"], inputs["cells"], inputs["electrodes"], inputs["measurements"],
-                      boundary_mode=inputs["boundary"])
+                      boundary_mode=inputs["boundary"], element_order=inputs["order"])
     return request.param, inputs, golden, oracle
 
 
