@@ -395,14 +395,17 @@ def cpu_baseline(args, nodes, cells, electrodes, rows) -> dict:
 
 def main():
     args = parse_args()
-    rank, world = dist_setup(args)
     if args.impl == "reference":
+        # the reference's CPU path on rank 0 only; the other ranks exit at once (no process group,
+        # so no collective waits on rank 0's minutes of host work)
+        rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
         if rank == 0:
             print(json.dumps(run_reference(args, rank, world)), flush=True)
-    else:
-        result = run_b200(args, rank, world)
-        if result is not None:
-            print(json.dumps(result), flush=True)
+        return
+    rank, world = dist_setup(args)
+    result = run_b200(args, rank, world)
+    if result is not None:
+        print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist
 
