@@ -53,6 +53,7 @@ from .inputs import (
 Tensor = torch.Tensor
 
 ELECTRODE_RADIUS_FRACTION = 0.5  # fallback radius of a source on a node (ert3d.py:47)
+MAX_COLUMNS = 200  # field columns per model (kMaxColumns of the library)
 FACE_MASS = np.asarray(((2.0, 1.0, 1.0), (1.0, 2.0, 1.0), (1.0, 1.0, 2.0))) / 12.0
 
 
@@ -174,8 +175,8 @@ def build_problem_3d(mesh: Mesh3D, survey, boundary_mode: str = "mixed",
         columns = [("point", int(e)) for e in union]
         current_col = receiver_col = {int(e): i for i, e in enumerate(union)}
     Ec = len(columns)
-    if Ec > 160:
-        raise ValueError(f"{Ec} field columns exceed the 160 supported by the sensitivity kernels")
+    if Ec > MAX_COLUMNS:
+        raise ValueError(f"{Ec} field columns exceed the {MAX_COLUMNS} supported by the sensitivity kernels")
     cell_ids, bary = mesh.locate_points(positions)
     weights = p2_shape_values(bary) if element_order == 2 else bary
     electrode_matrix = np.zeros((E, N))

@@ -150,7 +150,7 @@ adt_status build_host_plan(const adt_problem* pr, HostPlan& hp, std::string& err
   const int N = pr->dof_count, C = pr->cell_count, K = pr->local_dofs;
   const int Nb = pr->boundary_count, BL = pr->boundary_local, W = pr->wavenumber_count;
   const int E = pr->electrode_count, D = pr->measurement_count, RW = pr->receiver_width;
-  if (N <= 0 || C <= 0 || K <= 0 || K > 16 || W <= 0 || E <= 0 || E > 160 || D < 0 || RW <= 0 ||
+  if (N <= 0 || C <= 0 || K <= 0 || K > 16 || W <= 0 || E <= 0 || E > kMaxColumns || D < 0 || RW <= 0 ||
       (Nb > 0 && (BL <= 0 || BL > 16)) || pr->model_cell_count <= 0 || !pr->cell_dofs ||
       !pr->stiffness || !pr->mass || !pr->dof_coordinates || pr->dim < 1 || pr->dim > 3)
     { err = "invalid problem sizes or missing arrays"; return ADT_INVALID_ARG; }

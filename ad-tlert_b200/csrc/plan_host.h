@@ -13,6 +13,9 @@ namespace adt {
 
 constexpr int kMaxBlock = 64;  // largest block of the shared-memory solver kernels
 constexpr int kMaxTiledBlock = 4096;  // largest block of the tiled (global-memory) solver
+// Most field columns (electrodes in 2.5D; current + receiver columns in 3D): the FP32 Gram kernel
+// holds one cell's packed E x E Gram as at most 1280 4 x 4 tiles of a 256-thread block.
+constexpr int kMaxColumns = 200;
 constexpr int kTile = 64;       // tile edge of the tiled solver
 constexpr int kScatterRows = 32;  // block rows per scatter item of the tiled solver
 constexpr int kUnitCode = -1;  // assembly contribution of constant 1 (a fixed dof's diagonal)

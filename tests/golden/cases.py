@@ -192,11 +192,11 @@ def case_inputs(name: str) -> dict:
     return out
 
 
-def box_tetrahedra(nx: int = 6, ny: int = 6, nz: int = 4, relief: float = 0.0):
-    """Box 12 m x 12 m x 8 m of hexahedra split into six tetrahedra around the main diagonal;
-    ``relief`` bends the top surface (z' = z + relief * depth fraction * sin(x / 4))."""
+def box_tetrahedra(nx: int = 6, ny: int = 6, nz: int = 4, relief: float = 0.0, size=(12.0, 12.0, 8.0)):
+    """Box (default 12 m x 12 m x 8 m) of hexahedra split into six tetrahedra around the main
+    diagonal; ``relief`` bends the top surface (z' = z + relief * depth fraction * sin(x / 4))."""
 
-    xs, ys, zs = np.linspace(0, 12, nx + 1), np.linspace(0, 12, ny + 1), np.linspace(-8, 0, nz + 1)
+    xs, ys, zs = np.linspace(0, size[0], nx + 1), np.linspace(0, size[1], ny + 1), np.linspace(-size[2], 0, nz + 1)
     gx, gy, gz = np.meshgrid(xs, ys, zs, indexing="ij")
     gz = gz + relief * (gz - gz.min()) / (gz.max() - gz.min()) * np.sin(gx / 4.0)
     nodes = np.column_stack((gx.ravel(), gy.ravel(), gz.ravel()))
@@ -255,3 +255,35 @@ def case3d_inputs(name: str) -> dict:
         "boundary": spec["boundary"],
         "order": spec.get("order", 1),
     }
+
+
+def grid_survey_3d():
+    """The shape of the 3D benchmark survey at a test-sized mesh: a 12 x 8 surface grid of
+    electrodes at 4 m spacing (96) on a 52 m x 36 m x 16 m box of 13.8k tetrahedra, dipole-dipole
+    lines in x and y (a <= 3, n <= 6) plus cross-line quadrupoles, every electrode both a current
+    and a receiver electrode: 192 field columns with singularity removal."""
+
+    nodes, cells = box_tetrahedra(nx=26, ny=18, nz=6, size=(52.0, 36.0, 16.0))
+    grid = np.stack(np.meshgrid(4.0 + 4.0 * np.arange(12), 4.0 + 4.0 * np.arange(8), indexing="ij"), -1)
+    electrodes = np.concatenate((grid.reshape(-1, 2), np.zeros((96, 1))), axis=1)
+    index = np.arange(96).reshape(12, 8)
+    lines = [index[:, j] for j in range(8)] + [index[i, :] for i in range(12)]
+    rows = []
+    for line in lines:
+        count = len(line)
+        for a in (1, 2, 3):
+            for n in range(1, 7):
+                for i in range(count - a * (n + 2)):
+                    rows.append((line[i], line[i + a], line[i + a * (n + 1)], line[i + a * (n + 2)]))
+    for i in range(11):
+        for j in range(7):
+            rows.append((index[i, j], index[i, j + 1], index[i + 1, j], index[i + 1, j + 1]))
+    measurements = np.asarray(rows, dtype=np.int64)
+    rng = np.random.default_rng(21)
+    centers = nodes[cells].mean(axis=1)
+    sigma = np.full(len(cells), 0.01)
+    for cx, cy, cz, r, factor in ((16.0, 12.0, -4.0, 5.0, 10.0), (34.0, 22.0, -6.0, 6.0, 0.1)):
+        inside = np.sum((centers - (cx, cy, cz)) ** 2, axis=1) < r * r
+        sigma[inside] *= factor
+    return {"nodes": nodes, "cells": cells, "electrodes": electrodes, "measurements": measurements,
+            "sigma": sigma * np.exp(0.05 * rng.standard_normal(len(cells)))}
