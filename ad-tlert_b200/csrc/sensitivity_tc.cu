@@ -34,6 +34,7 @@ constexpr int kTcCells = 2;      // cells per group (stacked in one MMA operand)
 constexpr int kTcM = 128;        // MMA M (rows of the stacked operand)
 constexpr uint32_t kTcWaitLimit = 1u << 20;  // mbarrier polls before the block gives up
 constexpr int kTcRowTable = 4096;            // rows whose Gram offsets stay in shared memory
+constexpr int kTcStaticW = 17;  // the 2.5D quadrature's wavenumber count: a compile-time variant
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -103,8 +104,9 @@ size_t jacobian_tc_smem(int E, int W, int R, int K, int rows) {
   return (feat + gram + tables + offsets + 64 + 31) / 16 * 16;
 }
 
-// KT dofs and RT features per cell are compile-time.
-template <int KT, int RT>
+// KT dofs and RT features per cell are compile-time; WT > 0 makes the wavenumber count
+// compile-time too (the feature stage then indexes registers and chunks statically).
+template <int KT, int RT, int WT = 0>
 __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs a, int* error) {
   chain_wait();
   extern __shared__ __align__(128) unsigned char tc_sm[];
@@ -161,9 +163,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
   const bool resident = a.rows <= kTcRowTable;
   if (resident) fill_offsets(0, a.rows);
   for (int ci = tid; ci < kTcCells; ci += kTcThreads) gram[(size_t)ci * GS + GS - 1] = 0.f;
-  // chunks past the ones the wavenumber quads write (R ceil(W / 4) .. KC - 1) are K padding:
-  // zero for every group, written once
-  for (int item = tid, q0 = min(R * ((W + 3) >> 2), KC); item < (KC - q0) * RW * 4; item += kTcThreads) {
+  // chunks past the ones the feature stage writes (R ceil(W / 4), or the two halves' 2R +
+  // ceil((WT - 8) R / 4), .. KC - 1) are K padding: zero for every group, written once
+  constexpr int WT_CHUNKS = WT > 0 ? 2 * R + ((WT - 8) * R + 3) / 4 : 0;
+  const int written = WT > 0 ? WT_CHUNKS : R * ((W + 3) >> 2);
+  for (int item = tid, q0 = min(written, KC); item < (KC - q0) * RW * 4; item += kTcThreads) {
     const size_t off = ((size_t)q0 * RW) * 16 + (size_t)item * 4;
     *reinterpret_cast<float*>(feat + off) = 0.f;
     *reinterpret_cast<float*>(feat + part_bytes + off) = 0.f;
@@ -181,58 +185,117 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
       dofs[i] = c < a.c_end ? a.cell_dofs[(int64_t)c * K + i % K] : -1;
     }
     __syncthreads();
-    // work pairs (cell ci, wavenumber quad m): features of wavenumbers 4m .. 4m + 3 are the R
-    // whole chunks R m .. R m + R - 1. Thread e of lane group lg takes electrode e of pairs
-    // lg, lg + 4, ..., two at a time with all their field loads issued first, and stores whole
-    // 16-byte chunks (consecutive lanes: consecutive rows); chunks past KC hold only padding
-    {
-      const int lg = tid >> 6, e = tid & 63;
-      const int NQ = (W + 3) >> 2, pairs = kTcCells * NQ;
+    if constexpr (WT > 0) {
+      // thread (cell ci, half h, electrode e): wavenumbers 0 .. 7 (h = 0: chunks 0 .. 2R - 1) or
+      // 8 .. WT - 1 (h = 1: chunks 2R .. KC - 1, the tail padded with zeros); its field loads
+      // are issued first, then whole 16-byte chunks are stored
+      constexpr int WH = 8, WB = WT - WH, CH0 = WH * R / 4;
+      static_assert(WB >= WH && WB <= 16, "two halves of at most 16 wavenumbers");
+      const int e = tid & 63, h = (tid >> 6) & 1, ci = tid >> 7;
       if (e < E) {
-        for (int p0 = lg; p0 < pairs; p0 += 8) {
-          float x[2][4][K];
+        int dof[K];
 #pragma unroll
-          for (int pp = 0; pp < 2; ++pp) {
-            const int p = p0 + 4 * pp;
-            const int ci = p / NQ, m = p - ci * NQ;
+        for (int k = 0; k < K; ++k) dof[k] = dofs[ci * K + k];
+        const int w0 = h * WH, wn = h ? WB : WH;
+        float x[WB][K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-              const int dof = p < pairs ? dofs[ci * K + k] : -1;
+        for (int j = 0; j < WB; ++j)
 #pragma unroll
-              for (int wq = 0; wq < 4; ++wq) {
-                const int w = 4 * m + wq;
-                x[pp][wq][k] = (dof >= 0 && w < W) ? __ldg(a.fields + ((int64_t)w * a.N + dof) * E + e) : 0.f;
-              }
+          for (int k = 0; k < K; ++k)
+            x[j][k] = (j < wn && dof[k] >= 0) ? __ldg(a.fields + ((int64_t)(w0 + j) * a.N + dof[k]) * E + e) : 0.f;
+        float cf[R][K];
+#pragma unroll
+        for (int f = 0; f < R; ++f)
+#pragma unroll
+          for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
+        const int nch = h ? KC - CH0 : CH0;
+        unsigned char* row_feat = feat + ((size_t)(h * CH0) * RW + ci * Ep + e) * 16;
+        float hi[4] = {0.f, 0.f, 0.f, 0.f}, lo[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int j = 0; j < WB; ++j) {
+#pragma unroll
+          for (int f = 0; f < R; ++f) {
+            const int kl = j * R + f;  // compile-time: chunk kl / 4, lane kl % 4
+            float v = 0.f;
+            if (j < wn) {
+#pragma unroll
+              for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[j][k], v);
+              v *= scale[(w0 + j) * R + f];
+            }
+            hi[kl & 3] = tf32_round(v);
+            lo[kl & 3] = v - hi[kl & 3];
+            if ((kl & 3) == 3 && (kl >> 2) < nch) {
+              const size_t off = (size_t)(kl >> 2) * RW * 16;
+              *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+              *reinterpret_cast<float4*>(row_feat + part_bytes + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
             }
           }
+        }
+        constexpr int last = WB * R;  // a partial last chunk: its remaining lanes are padding
+        if constexpr (last % 4 != 0) {
 #pragma unroll
-          for (int pp = 0; pp < 2; ++pp) {
-            const int p = p0 + 4 * pp;
-            if (p >= pairs) break;
-            const int ci = p / NQ, m = p - ci * NQ;
-            float cf[R][K];
-#pragma unroll
-            for (int f = 0; f < R; ++f)
-#pragma unroll
-              for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
-            unsigned char* row_feat = feat + ((size_t)R * m * RW + ci * Ep + e) * 16;
-            float hi[4], lo[4];
-#pragma unroll
-            for (int wq = 0; wq < 4; ++wq) {
-              const int w = min(4 * m + wq, W - 1);
-#pragma unroll
-              for (int f = 0; f < R; ++f) {
-                float v = 0.f;
-#pragma unroll
-                for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[pp][wq][k], v);
-                v *= scale[w * R + f];
-                const int kl = wq * R + f;  // compile-time: chunk kl / 4, lane kl % 4
-                hi[kl & 3] = tf32_round(v);
-                lo[kl & 3] = v - hi[kl & 3];
-                if ((kl & 3) == 3 && R * m + (kl >> 2) < KC) {
-                  const size_t off = (size_t)(kl >> 2) * RW * 16;
-                  *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-                  *reinterpret_cast<float4*>(row_feat + part_bytes + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+          for (int i = last % 4; i < 4; ++i) hi[i] = lo[i] = 0.f;
+          if ((last >> 2) < nch) {
+            const size_t off = (size_t)(last >> 2) * RW * 16;
+            *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<float4*>(row_feat + part_bytes + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+          }
+        }
+      }
+    } else {
+      // work pairs (cell ci, wavenumber quad m): features of wavenumbers 4m .. 4m + 3 are the R
+      // whole chunks R m .. R m + R - 1. Thread e of lane group lg takes electrode e of pairs
+      // lg, lg + 4, ..., two at a time with all their field loads issued first, and stores whole
+      // 16-byte chunks (consecutive lanes: consecutive rows); chunks past KC hold only padding
+      {
+        const int lg = tid >> 6, e = tid & 63;
+        const int NQ = (W + 3) >> 2, pairs = kTcCells * NQ;
+        if (e < E) {
+          for (int p0 = lg; p0 < pairs; p0 += 8) {
+            float x[2][4][K];
+  #pragma unroll
+            for (int pp = 0; pp < 2; ++pp) {
+              const int p = p0 + 4 * pp;
+              const int ci = p / NQ, m = p - ci * NQ;
+  #pragma unroll
+              for (int k = 0; k < K; ++k) {
+                const int dof = p < pairs ? dofs[ci * K + k] : -1;
+  #pragma unroll
+                for (int wq = 0; wq < 4; ++wq) {
+                  const int w = 4 * m + wq;
+                  x[pp][wq][k] = (dof >= 0 && w < W) ? __ldg(a.fields + ((int64_t)w * a.N + dof) * E + e) : 0.f;
+                }
+              }
+            }
+  #pragma unroll
+            for (int pp = 0; pp < 2; ++pp) {
+              const int p = p0 + 4 * pp;
+              if (p >= pairs) break;
+              const int ci = p / NQ, m = p - ci * NQ;
+              float cf[R][K];
+  #pragma unroll
+              for (int f = 0; f < R; ++f)
+  #pragma unroll
+                for (int k = 0; k < K; ++k) cf[f][k] = coef[(ci * R + f) * K + k];
+              unsigned char* row_feat = feat + ((size_t)R * m * RW + ci * Ep + e) * 16;
+              float hi[4], lo[4];
+  #pragma unroll
+              for (int wq = 0; wq < 4; ++wq) {
+                const int w = min(4 * m + wq, W - 1);
+  #pragma unroll
+                for (int f = 0; f < R; ++f) {
+                  float v = 0.f;
+  #pragma unroll
+                  for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[pp][wq][k], v);
+                  v *= scale[w * R + f];
+                  const int kl = wq * R + f;  // compile-time: chunk kl / 4, lane kl % 4
+                  hi[kl & 3] = tf32_round(v);
+                  lo[kl & 3] = v - hi[kl & 3];
+                  if ((kl & 3) == 3 && R * m + (kl >> 2) < KC) {
+                    const size_t off = (size_t)(kl >> 2) * RW * 16;
+                    *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+                    *reinterpret_cast<float4*>(row_feat + part_bytes + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+                  }
                 }
               }
             }
@@ -371,6 +434,13 @@ cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaS
     launch_chained(kernel, blocks, kTcThreads, smem, s, a, error);
     return cudaGetLastError();
   };
+  if (a.W == kTcStaticW) {
+    if (a.K == 3 && a.R == 5) return go(jacobian_tc_kernel<3, 5, kTcStaticW>);
+    if (a.K == 3 && a.R == 6) return go(jacobian_tc_kernel<3, 6, kTcStaticW>);
+    if (a.K == 4 && a.R == 3) return go(jacobian_tc_kernel<4, 3, kTcStaticW>);
+    if (a.K == 4 && a.R == 7) return go(jacobian_tc_kernel<4, 7, kTcStaticW>);
+    return go(jacobian_tc_kernel<4, 8, kTcStaticW>);
+  }
   if (a.K == 3 && a.R == 5) return go(jacobian_tc_kernel<3, 5>);
   if (a.K == 3 && a.R == 6) return go(jacobian_tc_kernel<3, 6>);
   if (a.K == 4 && a.R == 3) return go(jacobian_tc_kernel<4, 3>);
