@@ -344,7 +344,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
       const int lr = row - h * Ep;
       const bool mine = lr >= 0 && lr < E;
       float* g = gram + (size_t)h * GS + (size_t)(mine ? lr : 0) * GLD;
-      for (int cc = 0; cc < Ep; cc += 8) {
+      // warp-uniform: whether any row of this warp's lane quarter belongs to cell h
+      const int first = 32 * (warp & 3) - h * Ep;
+      const bool any = first < E && first + 32 > 0;
+      for (int cc = 0; any && cc < Ep; cc += 8) {
         uint32_t v[8];
         tmem_load8(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(h * Ep + cc), v);
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
