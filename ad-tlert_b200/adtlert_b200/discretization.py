@@ -20,7 +20,7 @@ from .fem import (
     serendipity_templates,
     triangle_templates,
 )
-from .geometry import Mesh, edge_midpoint_builder
+from .geometry import Mesh, first_use_numbers, midpoint_nodes
 
 
 @dataclass(frozen=True)
@@ -85,31 +85,42 @@ def structured_quads(mesh: Mesh) -> Mesh | None:
 def refine_quads(mesh: Mesh) -> tuple[Mesh, np.ndarray]:
     """Split every quad into four through its edge midpoints and center (discretization.py:314-341)."""
 
-    points, midpoint, _ = edge_midpoint_builder(mesh.nodes)
-    cells, parents = [], []
-    for parent, (bl, br, tr, tl) in enumerate(mesh.cells.tolist()):
-        b, r, t, left = midpoint(bl, br), midpoint(br, tr), midpoint(tr, tl), midpoint(tl, bl)
-        center = len(points)
-        points.append(0.25 * (points[bl] + points[br] + points[tr] + points[tl]))
-        cells += [[bl, b, center, left], [b, br, r, center], [center, r, tr, t], [left, center, t, tl]]
-        parents += [parent] * 4
-    surface = mesh.surface_node_ids.tolist()
-    refined_surface = [surface[0]]
-    for start, stop in zip(surface[:-1], surface[1:]):
-        refined_surface += [midpoint(start, stop), stop]
-    refined = Mesh.from_arrays(np.asarray(points), np.asarray(cells), surface_node_ids=np.asarray(refined_surface))
-    return refined, np.asarray(parents, dtype=np.int64)
+    nodes = np.asarray(mesh.nodes, dtype=float)
+    q, surface, n = mesh.cells, mesh.surface_node_ids, len(mesh.nodes)
+    count = len(q)
+    # per quad the events of the incremental builder: midpoints of edges b, r, t, l (new on first
+    # use), then the center (always new); surface midpoints follow
+    edges = q[:, [0, 1, 1, 2, 2, 3, 3, 0]].reshape(count, 4, 2)
+    lo, hi = edges.min(axis=2), edges.max(axis=2)
+    keys = np.concatenate((np.column_stack((lo * n + hi, -1 - np.arange(count))).reshape(-1),
+                           np.minimum(surface[:-1], surface[1:]) * n + np.maximum(surface[:-1], surface[1:])))
+    ids, first = first_use_numbers(keys, n)
+    mids = 0.5 * (nodes[lo] + nodes[hi])
+    centers = 0.25 * (nodes[q[:, 0]] + nodes[q[:, 1]] + nodes[q[:, 2]] + nodes[q[:, 3]])
+    sp_lo, sp_hi = np.minimum(surface[:-1], surface[1:]), np.maximum(surface[:-1], surface[1:])
+    events = np.concatenate((np.concatenate((mids, centers[:, None]), axis=1).reshape(-1, 2),
+                             0.5 * (nodes[sp_lo] + nodes[sp_hi])))
+    points = np.vstack((nodes, events[first]))
+    cell_ids = ids[:5 * count].reshape(count, 5)
+    b, r, t, left, center = cell_ids.T
+    bl, br, tr, tl = q.T
+    cells = np.stack((np.stack((bl, b, center, left), 1), np.stack((b, br, r, center), 1),
+                      np.stack((center, r, tr, t), 1), np.stack((left, center, t, tl), 1)), axis=1).reshape(-1, 4)
+    refined_surface = np.empty(max(2 * len(surface) - 1, 0), dtype=np.int64)
+    refined_surface[0::2], refined_surface[1::2] = surface, ids[5 * count:]
+    refined = Mesh.from_arrays(points, cells, surface_node_ids=refined_surface)
+    return refined, np.repeat(np.arange(count, dtype=np.int64), 4)
 
 
 def serendipity_topology(mesh: Mesh) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Corner + edge-midpoint dofs of 8-node quads and (end, midpoint, end) boundary dofs
     (discretization.py:344-363)."""
 
-    points, midpoint, _ = edge_midpoint_builder(mesh.nodes)
-    cells = [[bl, br, tr, tl, midpoint(bl, br), midpoint(br, tr), midpoint(tr, tl), midpoint(tl, bl)]
-             for bl, br, tr, tl in mesh.cells.tolist()]
-    boundary = [[a, midpoint(a, b), b] for a, b in mesh.boundary_edges.tolist()]
-    return np.asarray(points), np.asarray(cells, dtype=np.int64), np.asarray(boundary, dtype=np.int64)
+    q, boundary = mesh.cells, mesh.boundary_edges
+    pairs = np.concatenate((q[:, [0, 1, 1, 2, 2, 3, 3, 0]].reshape(-1, 2), boundary))
+    points, ids = midpoint_nodes(mesh.nodes, pairs)
+    cells = np.hstack((q, ids[:4 * len(q)].reshape(-1, 4)))
+    return points, cells, np.column_stack((boundary[:, 0], ids[4 * len(q):], boundary[:, 1]))
 
 
 def _points_on_segments(points: np.ndarray, segments: np.ndarray, tol: float) -> np.ndarray:

@@ -44,6 +44,7 @@ from .inputs import (
     cell_vector,
     check_finite,
     conductivity_model,
+    finite_flag,
     conductivity_series,
     cotangent_series,
     measurement_vector,
@@ -266,6 +267,17 @@ def _to_host(tensor: Tensor) -> Tensor:
     return out
 
 
+def _checked_to_host(tensor: Tensor, context: str) -> Tensor:
+    """``_to_host`` with the finiteness check done on the device, queued before the copy, so a
+    large result is never scanned on the host."""
+
+    finite = finite_flag(tensor)
+    out = _to_host(tensor)
+    if not bool(finite):
+        raise FloatingPointError(f"{context} produced non-finite values")
+    return out
+
+
 def _mesh_arrays(mesh) -> Mesh:
     """Our Mesh for the reference's or our own mesh object."""
 
@@ -460,21 +472,26 @@ class ERTForward2p5D:
                 stream = self._stream()
                 ones = torch.ones((1, self.C), dtype=torch.float32, device=self.device)
                 free, _ = torch.cuda.mem_get_info(self.device)
-                per_system = 8.0 * (info["factor_doubles_per_system"] + info["nnz"] + N * E)
+                per_system = 8.0 * (info["factor_doubles_per_system"] + info["nnz"] + 2 * N * E)
                 chunk = int(max(1, min(W, 0.4 * free // max(per_system, 1.0))))
                 rows = torch.as_tensor(np.ascontiguousarray(d.electrode_matrix.T[order]), device=self.device)
-                out = np.empty((W, E, N))
+                solver_position = torch.as_tensor(np.argsort(order), device=self.device)  # dof -> solver row
+                out = torch.empty((W, E, N), dtype=torch.float64)
+                finite = torch.ones((), dtype=torch.bool, device=self.device)
                 for w0 in range(0, W, chunk):
                     count = min(chunk, W - w0)
                     _native.check(lib.adt_factorize_wavenumbers(plan, 0, _native.ptr(ones), w0, count, stream), plan,
                                   "adt_factorize_wavenumbers")
                     rhs = rows[None].repeat(count, 1, 1).contiguous()
                     _native.check(lib.adt_solve(plan, 0, count, E, _native.ptr(rhs), stream), plan, "adt_solve")
-                    solved = rhs.cpu().numpy()  # (count, N solver order, E)
-                    out[w0:w0 + count][:, :, order] = solved.transpose(0, 2, 1)
-                if not np.all(np.isfinite(out)):
+                    # (count, N solver order, E) -> (count, E, N dof order) on the device
+                    solved = rhs.index_select(1, solver_position).transpose(1, 2).contiguous()
+                    del rhs
+                    finite &= finite_flag(solved)
+                    out[w0:w0 + count].copy_(solved)
+                if not bool(finite):
                     raise FloatingPointError("unit potentials: non-finite values")
-                return out
+                return out.numpy()
         finally:
             torch.cuda.synchronize(self.device)
             lib.adt_plan_destroy(plan)

@@ -28,7 +28,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .ert2p5d import _Slots, _survey_arrays, _to_host
+from .ert2p5d import _checked_to_host, _Slots, _survey_arrays
 from .field_cache import FieldCache
 from .geometry3d import (
     Mesh3D,
@@ -538,9 +538,7 @@ class ERTForward3D:
             raise ValueError("batch_size must be >= 1")
         columns = self._columns(jacobian_cell_parameter_ids, jacobian_parameter_count)
         fields = self._fields(conductivity)
-        result = _to_host(self._jacobian_device(fields, include_robin_boundary_derivative, columns))
-        check_finite(result, "jacobian")
-        return result
+        return _checked_to_host(self._jacobian_device(fields, include_robin_boundary_derivative, columns), "jacobian")
 
     def jacobian_columnwise(self, conductivity) -> Tensor:
         basis = torch.eye(self.C, dtype=FLOAT_DTYPE)
@@ -556,9 +554,7 @@ class ERTForward3D:
             normal_sensitivity=normal_sensitivity, include_fields=include_fields,
             jacobian_cell_parameter_ids=jacobian_cell_parameter_ids,
             jacobian_parameter_count=jacobian_parameter_count)
-        result = _to_host(jacobian)
-        check_finite(result, "jacobian")
-        return response, result
+        return response, _checked_to_host(jacobian, "jacobian")
 
     def _solve_with_jacobian_device(self, conductivity, currents=1.0, *, batch_size=None,
                                     include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,

@@ -174,18 +174,19 @@ class Mesh:
         mesh and the parent cell of each child (adtlert/mesh/core.py:326-337, 689-698)."""
 
         self._require_triangles("uniform refinement")
-        points, midpoint, _ = edge_midpoint_builder(self.nodes)
-        cells, parents = [], []
-        for parent, (n0, n1, n2) in enumerate(self.cells.tolist()):
-            m01, m12, m20 = midpoint(n0, n1), midpoint(n1, n2), midpoint(n2, n0)
-            cells += [[n0, m01, m20], [n1, m12, m01], [n2, m20, m12], [m01, m12, m20]]
-            parents += [parent] * 4
-        surface = self.surface_node_ids.tolist()
-        refined_surface = [surface[0]]
-        for a, b in zip(surface[:-1], surface[1:]):
-            refined_surface += [midpoint(a, b), b]
-        refined = Mesh.from_arrays(np.asarray(points), np.asarray(cells), surface_node_ids=np.asarray(refined_surface))
-        return refined, np.asarray(parents, dtype=np.int64)
+        c = self.cells
+        surface = self.surface_node_ids
+        pairs = np.concatenate((c[:, [0, 1, 1, 2, 2, 0]].reshape(-1, 2),
+                                np.stack((surface[:-1], surface[1:]), axis=1)))
+        points, ids = midpoint_nodes(self.nodes, pairs)
+        m01, m12, m20 = ids[:3 * len(c)].reshape(-1, 3).T
+        n0, n1, n2 = c.T
+        cells = np.stack((np.stack((n0, m01, m20), 1), np.stack((n1, m12, m01), 1), np.stack((n2, m20, m12), 1),
+                          np.stack((m01, m12, m20), 1)), axis=1).reshape(-1, 3)
+        refined_surface = np.empty(max(2 * len(surface) - 1, 0), dtype=np.int64)
+        refined_surface[0::2], refined_surface[1::2] = surface, ids[3 * len(c):]
+        refined = Mesh.from_arrays(points, cells, surface_node_ids=refined_surface)
+        return refined, np.repeat(np.arange(len(c), dtype=np.int64), 4)
 
     def expand_columnar_cells(self, tol: float = 1e-6) -> tuple[Mesh, np.ndarray] | None:
         """Complete single-triangle terrain strips into triangulated quads, or ``None`` when the
@@ -204,27 +205,35 @@ class Mesh:
         ``(a, b, m_ab)`` (adtlert/mesh/core.py:543-555, 738-744)."""
 
         self._require_triangles("quadratic topology")
-        points, midpoint, _ = edge_midpoint_builder(self.nodes)
-        cells = [[n0, n1, n2, midpoint(n0, n1), midpoint(n1, n2), midpoint(n2, n0)] for n0, n1, n2 in self.cells.tolist()]
-        boundary = [[a, b, midpoint(a, b)] for a, b in self.boundary_edges.tolist()]
-        return np.asarray(points), np.asarray(cells, dtype=np.int64), np.asarray(boundary, dtype=np.int64)
+        c, boundary = self.cells, self.boundary_edges
+        pairs = np.concatenate((c[:, [0, 1, 1, 2, 2, 0]].reshape(-1, 2), boundary))
+        points, ids = midpoint_nodes(self.nodes, pairs)
+        cells = np.hstack((c, ids[:3 * len(c)].reshape(-1, 3)))
+        return points, cells, np.column_stack((boundary, ids[3 * len(c):]))
 
 
-def edge_midpoint_builder(nodes):
-    """A growing node list and ``midpoint(a, b)``, which appends each edge's midpoint once
-    (adtlert/mesh/core.py:27-44)."""
+def first_use_numbers(keys: np.ndarray, start: int) -> tuple[np.ndarray, np.ndarray]:
+    """Number the distinct values of a key sequence ``start, start + 1, ...`` in the order of
+    their first occurrence. Returns each key's number and, per number, the position of its first
+    occurrence (the sequence the reference's incremental node builders produce)."""
 
-    points = [np.asarray(p, dtype=float) for p in np.asarray(nodes, dtype=float)]
-    index: dict[tuple[int, int], int] = {}
+    unique, first, inverse = np.unique(np.asarray(keys, dtype=np.int64), return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")
+    rank = np.empty(len(unique), dtype=np.int64)
+    rank[order] = np.arange(len(unique))
+    return start + rank[inverse.reshape(-1)], first[order]
 
-    def midpoint(a: int, b: int) -> int:
-        key = (a, b) if a < b else (b, a)
-        if key not in index:
-            index[key] = len(points)
-            points.append(0.5 * (points[key[0]] + points[key[1]]))
-        return index[key]
 
-    return points, midpoint, index
+def midpoint_nodes(nodes, pairs) -> tuple[np.ndarray, np.ndarray]:
+    """Append one midpoint node per distinct edge of ``pairs`` (M x 2 node ids, in use order),
+    numbered in the order of first use; returns the grown node array and each pair's midpoint id
+    (the edge-midpoint builder of adtlert/mesh/core.py:27-44)."""
+
+    nodes = np.asarray(nodes, dtype=float)
+    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    lo, hi = pairs.min(axis=1), pairs.max(axis=1)
+    ids, first = first_use_numbers(lo * len(nodes) + hi, len(nodes))
+    return np.vstack((nodes, 0.5 * (nodes[lo[first]] + nodes[hi[first]]))), ids
 
 
 def _orient_ccw(nodes, triangle: list[int]) -> list[int]:

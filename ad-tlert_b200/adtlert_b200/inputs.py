@@ -34,6 +34,16 @@ def check_finite(values: Tensor, context: str) -> None:
         raise FloatingPointError(f"{context} produced non-finite values")
 
 
+def finite_flag(values: Tensor) -> Tensor:
+    """A one-element boolean on ``values``' device, True iff every entry is finite, computed with
+    one read and no full-size temporary: the float64 sum of float32 values cannot overflow (below
+    2**970 entries), and an inf or NaN entry makes it inf or NaN."""
+
+    if values.dtype in (torch.float32, torch.float16, torch.bfloat16):
+        return torch.isfinite(values.sum(dtype=torch.float64))
+    return torch.isfinite(values).all()
+
+
 def cell_vector(values, count: int, dtype: torch.dtype = FLOAT_DTYPE) -> Tensor:
     vector = torch.as_tensor(values, dtype=dtype)
     if vector.ndim == 0:
