@@ -96,6 +96,7 @@ struct adt_plan {
   double* k2 = nullptr;         // [W]
   double* weights = nullptr;    // [W]
   int* abmn = nullptr;          // [D][4]
+  int2* row_entries = nullptr;  // [2][D] (A | B << 8 | M << 16 | N << 24, d): sorted by (A, B, M, N), then in row order
   int* rcv_dofs = nullptr;      // [E][RW] solver order
   double* rcv_w = nullptr;      // [E][RW]
   int* src_ptr = nullptr;       // [E+1]
@@ -140,6 +141,7 @@ struct adt_plan {
   int device = 0;
   int sms = 148;                // multiprocessors of the device
   bool jacobian_tc = true;      // tensor-core Jacobian where it applies
+  bool jacobian_direct = true;  // direct-form Jacobian for single-wavenumber operators
   int* tc_error = nullptr;      // device flag raised by a tensor-core block that timed out
   int* tc_error_host = nullptr; // pinned copy, refreshed after each tensor-core launch
   cudaStream_t copy_stream = nullptr;        // device-to-host copies of Jacobian column chunks

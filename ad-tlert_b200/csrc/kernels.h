@@ -134,6 +134,8 @@ __global__ void integrated_kernel(const float* fields, const double* weights, co
 __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, int E,
                            double* current);
 cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s);
+int jacobian_direct_cells(int R, int E, int K);
+cudaError_t launch_jacobian_direct(const JacobianArgs& a, const int2* rows, cudaStream_t s);
 bool jacobian_tc_supported(int E, int W, int R, int K, int rows);
 cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaStream_t s);
 __global__ void cell_gradient_kernel(CellGradientArgs a);

@@ -312,7 +312,11 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   adt_plan* p = new adt_plan();
   cudaGetDevice(&p->device);
   cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device);
-  if (const char* choice = std::getenv("ADTLERT_B200_JACOBIAN")) p->jacobian_tc = std::strcmp(choice, "fma") != 0;
+  if (const char* choice = std::getenv("ADTLERT_B200_JACOBIAN")) {
+    // "fma": the CUDA-core Gram kernel everywhere; "tc": tensor cores wherever they apply
+    p->jacobian_tc = std::strcmp(choice, "fma") != 0;
+    p->jacobian_direct = std::strcmp(choice, "fma") != 0 && std::strcmp(choice, "tc") != 0;
+  }
   configure_solver_kernels();
   auto bail = [&](adt_status st) {
     g_create_error = p->error;
@@ -354,6 +358,24 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   ADT_UP(&p->k2, hp.k2);
   ADT_UP(&p->weights, pr->weights, (size_t)W);
   ADT_UP(&p->abmn, pr->abmn, (size_t)D * 4);
+  if (E <= 255) {  // packed measurement rows of the direct-form Jacobian
+    std::vector<int> order(D);
+    std::iota(order.begin(), order.end(), 0);
+    const int32_t* q = pr->abmn;
+    std::stable_sort(order.begin(), order.end(), [q](int x, int y) {
+      return std::lexicographical_compare(q + 4 * x, q + 4 * x + 4, q + 4 * y, q + 4 * y + 4);
+    });
+    auto pack = [q](int d) {
+      return make_int2((int)((uint32_t)q[4 * d] | (uint32_t)q[4 * d + 1] << 8 | (uint32_t)q[4 * d + 2] << 16 |
+                             (uint32_t)q[4 * d + 3] << 24), d);
+    };
+    std::vector<int2> entries(2 * (size_t)D);
+    for (int i = 0; i < D; ++i) {
+      entries[i] = pack(order[i]);
+      entries[(size_t)D + i] = pack(i);
+    }
+    ADT_UP(&p->row_entries, entries);
+  }
   ADT_UP(&p->rcv_dofs, hp.rcv_dofs);
   ADT_UP(&p->rcv_w, hp.rcv_w);
   ADT_UP(&p->src_ptr, pr->source_cell_ptr, (size_t)E + 1);
@@ -393,7 +415,7 @@ adt_status adt_plan_destroy(adt_plan* p) {
   if (!p) return ADT_OK;
   void* ptrs[] = {p->csr_ptr, p->csr_col, p->csr_row, p->contrib_ptr, p->contrib, p->stiffness,
                   p->mass, p->bmass, p->bcoef, p->cell_dofs, p->parent, p->bcells, p->bdofs,
-                  p->cell_bptr, p->cell_blist, p->k2, p->weights, p->abmn, p->rcv_dofs,
+                  p->cell_bptr, p->cell_blist, p->k2, p->weights, p->abmn, p->row_entries, p->rcv_dofs,
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
                   p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
@@ -713,6 +735,18 @@ adt_status launch_normal_jacobian(adt_plan* p, const float* fields, int row_begi
   a.c_begin = c_begin;
   a.c_end = c_end;
   a.ldo = ldo;
+  if (p->jacobian_direct && p->W == 1 && p->row_entries) {
+    if (const int cells = jacobian_direct_cells(p->R, p->E, p->K)) {
+      a.cells_per_block = cells;
+      // all rows: sorted by current pair; a row range: in row order
+      const bool all_rows = row_begin == 0 && row_count == p->D;
+      const int2* rows = all_rows ? p->row_entries : p->row_entries + p->D + row_begin;
+      const cudaError_t err = launch_jacobian_direct(a, rows, s);
+      p->launches++;
+      if (err != cudaSuccess) return fail(p, ADT_CUDA_ERROR, std::string("direct jacobian: ") + cudaGetErrorString(err));
+      return ADT_OK;
+    }
+  }
   if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count)) {
     a.cells_per_block = 0;
     const cudaError_t err = launch_jacobian_tc(a, p->tc_error, p->sms, s);

@@ -1,7 +1,9 @@
-"""The tensor-core (tcgen05) Jacobian against the CUDA-core Jacobian kernel and the FP64 oracle.
+"""The tensor-core (tcgen05) and direct-form Jacobians against the CUDA-core Gram kernel and the
+FP64 oracle.
 
-``ADTLERT_B200_JACOBIAN=fma`` at plan creation selects the CUDA-core kernel; both must agree to
-float32 accuracy on 2.5D sections (12 and 48 electrodes) and a 3D box."""
+``ADTLERT_B200_JACOBIAN=fma`` at plan creation selects the CUDA-core Gram kernel and ``tc`` the
+tensor cores wherever they apply; by default single-wavenumber (3D) operators take the direct
+form. All must agree to float32 accuracy on 2.5D sections (12 and 48 electrodes) and 3D boxes."""
 
 import os
 
@@ -9,7 +11,7 @@ import numpy as np
 import pytest
 import torch
 
-from adtlert_b200 import ERTForward2p5D, ERTForward3D, Mesh, Mesh3D, Survey, synthetic
+from adtlert_b200 import ERTForward2p5D, ERTForward3D, Mesh, Mesh3D, Survey, _native, synthetic
 from cases import case3d_inputs, case_inputs
 from conftest import assert_close
 from oracle.ert2p5d import Oracle2p5D
@@ -17,14 +19,16 @@ from oracle.ert2p5d import Oracle2p5D
 pytestmark = pytest.mark.gpu
 
 
-def _pair(make):
-    tc = make()
-    os.environ["ADTLERT_B200_JACOBIAN"] = "fma"
+def _with_choice(choice, make):
+    os.environ["ADTLERT_B200_JACOBIAN"] = choice
     try:
-        fma = make()
+        return make()
     finally:
         del os.environ["ADTLERT_B200_JACOBIAN"]
-    return tc, fma
+
+
+def _pair(make):
+    return make(), _with_choice("fma", make)
 
 
 def test_tensor_core_jacobian_matches_the_cuda_core_kernel_2p5d():
@@ -50,13 +54,27 @@ def test_tensor_core_jacobian_on_the_benchmark_section():
     assert torch.equal(a, tc.jacobian(sigma)), "bitwise repeatable"
 
 
-def test_tensor_core_jacobian_3d():
-    inputs = case3d_inputs("tet_mixed")
+@pytest.mark.parametrize("name", ["tet_mixed", "tet_p2_mixed"])
+def test_direct_and_tensor_core_jacobians_3d(name):
+    inputs = case3d_inputs(name)
     mesh = Mesh3D.from_arrays(inputs["nodes"], inputs["cells"])
     survey = Survey.from_arrays(inputs["electrodes"], inputs["measurements"])
-    tc, fma = _pair(lambda: ERTForward3D(mesh, survey))
+    options = {"element_order": inputs["order"], "boundary_mode": inputs["boundary"]}
+    make = lambda: ERTForward3D(mesh, survey, **options)  # noqa: E731
+    direct, fma = _pair(make)
+    tc = _with_choice("tc", make)
     sigma = torch.as_tensor(inputs["sigma"], dtype=torch.float32)
-    assert_close(tc.jacobian(sigma), fma.jacobian(sigma), 2e-6, "tcgen05 vs FMA jacobian (3D)")
+    reference = fma.jacobian(sigma)
+    assert_close(direct.jacobian(sigma), reference, 2e-6, f"direct vs FMA jacobian ({name})")
+    assert_close(tc.jacobian(sigma), reference, 2e-6, f"tcgen05 vs FMA jacobian ({name})")
+    # a row range takes the rows in their own order instead of the plan's sorted order
+    fields = direct._fields(sigma)
+    D, C = reference.shape
+    start, count = D // 3, D - D // 3 - 1
+    part = torch.full((count, C), float("nan"), device="cuda")
+    direct._call("adt_normal_jacobian", _native.ptr(fields), start, count, _native.ptr(part), direct._stream())
+    full = direct._jacobian_device(fields, False, None)
+    assert torch.equal(part, full[start:start + count])
 
 
 def test_tensor_core_jacobian_with_more_rows_than_the_offset_table():
@@ -74,7 +92,6 @@ def test_tensor_core_jacobian_with_more_rows_than_the_offset_table():
 
 
 def test_jacobian_to_host_in_column_chunks_is_the_device_jacobian():
-    from adtlert_b200 import _native
     nodes, cells, electrodes, abmn = synthetic.flat_section()
     mesh, survey = Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, abmn)
     sigma = torch.as_tensor(synthetic.layered_model(nodes, cells, 3), dtype=torch.float32)
