@@ -4,6 +4,11 @@
 columns, 20 layers of 0.5 m then 20 geometrically graded layers to 40 m depth (121 x 41 =
 4961 nodes, 9600 triangles), 48 surface electrodes at 2 m spacing from x = 13 m, and a
 dipole-dipole survey with a <= 6, n <= 8 (1232 rows; a <= 6, n <= 3 gives 612).
+
+``box_section`` + ``grid_survey`` + ``ellipsoid_model`` build the 3D workload: a 60 m x 40 m x
+20 m box of structured tetrahedra (60 x 40 x 17 hexahedra of six tetrahedra: 244,800 cells,
+45,018 nodes), a 12 x 8 surface grid of electrodes at 4 m spacing, 4000 dipole-dipole rows
+along the grid's x and y lines, and a 100 ohm-m background with three seeded ellipsoids.
 """
 
 from __future__ import annotations
@@ -70,4 +75,59 @@ def layered_model(nodes, cells, seed: int) -> np.ndarray:
         radius, contrast = rng.uniform(3.0, 8.0), 10.0 ** rng.uniform(-1.0, 1.0)
         r2 = (centers[:, 0] - x0) ** 2 + (centers[:, 1] - z0) ** 2
         rho = rho * contrast ** np.exp(-r2 / (2.0 * radius * radius))
+    return (1.0 / rho).astype(np.float32)
+
+
+def box_section(nx: int = 60, ny: int = 40, nz: int = 17, size=(60.0, 40.0, 20.0)):
+    """Box [0, sx] x [0, sy] x [-sz, 0] of nx x ny x nz hexahedra, each split into six
+    tetrahedra around its main diagonal: (nodes, cells)."""
+
+    xs, ys, zs = np.linspace(0, size[0], nx + 1), np.linspace(0, size[1], ny + 1), np.linspace(-size[2], 0, nz + 1)
+    gx, gy, gz = np.meshgrid(xs, ys, zs, indexing="ij")
+    nodes = np.column_stack((gx.ravel(), gy.ravel(), gz.ravel()))
+    index = np.arange(nodes.shape[0]).reshape(nx + 1, ny + 1, nz + 1)
+    corners = np.stack([
+        index[:-1, :-1, :-1], index[1:, :-1, :-1], index[1:, 1:, :-1], index[:-1, 1:, :-1],
+        index[:-1, :-1, 1:], index[1:, :-1, 1:], index[1:, 1:, 1:], index[:-1, 1:, 1:],
+    ], axis=-1).reshape(-1, 8)
+    fans = ((1, 2, 6), (2, 3, 6), (3, 7, 6), (7, 4, 6), (4, 5, 6), (5, 1, 6))
+    cells = np.stack([corners[:, [0, a, b, c]] for a, b, c in fans], axis=1).reshape(-1, 4)
+    return nodes, cells.astype(np.int64)
+
+
+def grid_survey(rows: int = 4000, seed: int = 4, shape=(12, 8), spacing: float = 4.0, origin=(8.0, 6.0)):
+    """Surface electrodes on a grid and ``rows`` distinct dipole-dipole quadrupoles drawn (seeded)
+    from the dipoles of neighbouring electrodes along the grid's x and y lines."""
+
+    gx, gy = np.meshgrid(origin[0] + spacing * np.arange(shape[0]), origin[1] + spacing * np.arange(shape[1]),
+                         indexing="ij")
+    count = shape[0] * shape[1]
+    electrodes = np.column_stack((gx.ravel(), gy.ravel(), np.zeros(count)))
+    idx = np.arange(count).reshape(shape)
+    dipoles = [(idx[i, j], idx[i + 1, j]) for i in range(shape[0] - 1) for j in range(shape[1])]
+    dipoles += [(idx[i, j], idx[i, j + 1]) for i in range(shape[0]) for j in range(shape[1] - 1)]
+    if rows > len(dipoles) * (len(dipoles) - 1):
+        raise ValueError("more rows than distinct dipole pairs")
+    rng = np.random.default_rng(seed)
+    quads: set[tuple[int, int, int, int]] = set()
+    while len(quads) < rows:
+        (a, b), (m, n) = dipoles[rng.integers(len(dipoles))], dipoles[rng.integers(len(dipoles))]
+        if len({a, b, m, n}) == 4:
+            quads.add((int(a), int(b), int(m), int(n)))
+    return electrodes, np.asarray(sorted(quads), dtype=np.int64)
+
+
+def ellipsoid_model(nodes, cells, seed: int, footprint=((8.0, 52.0), (6.0, 34.0))) -> np.ndarray:
+    """Float32 conductivity: 100 ohm-m background with three ellipsoids (semi-axes U(2,8) m,
+    centres inside the electrode footprint at depth U(2,12) m, resistivity log-uniform in
+    10-1000 ohm-m) at cell centroids."""
+
+    rng = np.random.default_rng(seed)
+    centers = nodes[cells].mean(axis=1)
+    rho = np.full(len(cells), 100.0)
+    for _ in range(3):
+        c = np.array([rng.uniform(*footprint[0]), rng.uniform(*footprint[1]), -rng.uniform(2.0, 12.0)])
+        axes = rng.uniform(2.0, 8.0, 3)
+        inside = np.sum(((centers - c) / axes) ** 2, axis=1) <= 1.0
+        rho[inside] = 10.0 ** rng.uniform(1.0, 3.0)
     return (1.0 / rho).astype(np.float32)

@@ -401,6 +401,8 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   p->panel_ptr = hp.panel_ptr;
   ADT_UP(&p->owners, hp.bowners);
   p->nfixed = (int)hp.fixed.size();
+  if (p->tiled && cudaMalloc(&p->partials, sizeof(double) * 2 * (size_t)p->sms * kTile * kTile) != cudaSuccess)
+    return bail(fail(p, ADT_OOM, "split workspace allocation failed"));
   if (cudaMalloc(&p->tc_error, sizeof(int)) != cudaSuccess || cudaMemset(p->tc_error, 0, sizeof(int)) != cudaSuccess ||
       cudaHostAlloc(&p->tc_error_host, sizeof(int), cudaHostAllocDefault) != cudaSuccess)
     return bail(fail(p, ADT_OOM, "error flag allocation failed"));
@@ -419,7 +421,7 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
                   p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
-                  p->fixed, p->owners, p->titems, p->update_items, p->tc_error};
+                  p->fixed, p->owners, p->titems, p->update_items, p->tc_error, p->partials};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->tc_error_host) cudaFreeHost(p->tc_error_host);

@@ -951,22 +951,23 @@ __device__ __forceinline__ void stage(double* tile, const Operand& op, int rows,
   }
 }
 
-// acc[r][s] += sum_{c < depth} A(ty + 16 r, c) B(tx + 16 s, c) for A rows < ra, B rows < rb.
-// `sm` holds 4 * kKC * kTLD doubles; entered and left by all threads (ends with a barrier).
+// acc[r][s] += sum_{d0 <= c < depth} A(ty + 16 r, c) B(tx + 16 s, c) for A rows < ra, B rows
+// < rb (d0 a multiple of kKC). `sm` holds 4 * kKC * kTLD doubles; entered and left by all
+// threads (ends with a barrier).
 __device__ void gemm_nt(double (&acc)[4][4], const Operand& A, int ra, const Operand& B, int rb,
-                        int depth, double* sm) {
-  if (depth <= 0) return;
+                        int depth, double* sm, int d0 = 0) {
+  if (depth <= d0) return;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int chunks = (depth + kKC - 1) / kKC;
+  const int chunks = (depth - d0 + kKC - 1) / kKC;
   auto a_tile = [&](int b) { return sm + b * 2 * kKC * kTLD; };
   auto b_tile = [&](int b) { return sm + b * 2 * kKC * kTLD + kKC * kTLD; };
-  stage(a_tile(0), A, ra, depth, 0);
-  stage(b_tile(0), B, rb, depth, 0);
+  stage(a_tile(0), A, ra, depth, d0);
+  stage(b_tile(0), B, rb, depth, d0);
   async_commit();
   for (int ch = 0; ch < chunks; ++ch) {
     if (ch + 1 < chunks) {
-      stage(a_tile((ch + 1) & 1), A, ra, depth, (ch + 1) * kKC);
-      stage(b_tile((ch + 1) & 1), B, rb, depth, (ch + 1) * kKC);
+      stage(a_tile((ch + 1) & 1), A, ra, depth, d0 + (ch + 1) * kKC);
+      stage(b_tile((ch + 1) & 1), B, rb, depth, d0 + (ch + 1) * kKC);
       async_commit();
       async_wait<1>();
     } else {
@@ -1081,9 +1082,24 @@ tiled_scatter_kernel(const int* __restrict__ items, int begin, const int64_t* __
   }
 }
 
+// Depth chunks (of kKC) of one update item: its own columns [0, 64k), then each pull's depth.
+__device__ __forceinline__ int update_chunks(const TaskView& v, int seg, int k, const int64_t* pulls) {
+  int n = (kTile * k) / kKC;
+  if (seg == SEG_J)
+    for (int64_t u = v.pull0; u < v.pull1; ++u) n += ((int)pulls[u * P_FIELDS + P_ME] + kKC - 1) / kKC;
+  return n;
+}
+
+// Panel k update of tile (i, k) of segment seg: acc = row_i(c < 64k) row_k^T (+ the Schur pulls
+// for rows of j). With `splits` == 1 the block subtracts acc from the tile and, for the diagonal
+// item, factors it. With splits > 1 the item's depth chunks are divided evenly over blockIdx.z
+// and each block stores its partial acc in `partials` (tile (item, z) of the launch: rows < ni,
+// columns < mk at [((system * items + item) * splits + z) * 4096 + a * 64 + b]); the diagonal
+// and triangular-solve launches sum them.
 __global__ void __launch_bounds__(kTT)
 tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
-                    const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride) {
+                    const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride,
+                    int splits, double* __restrict__ partials) {
   chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
@@ -1093,19 +1109,39 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
   const int ni = min(kTile, v.rows(seg) - kTile * i), mk = min(kTile, v.mj - kTile * k);
   double acc[4][4];
   zero_acc(acc);
+  // this block's chunk range [lo, hi) of the item's depth chunks (all of them when unsplit)
+  int lo = 0, hi = 1 << 30;
+  if (splits > 1) {
+    const int n = update_chunks(v, seg, k, pulls), z = blockIdx.z;
+    lo = (int)((int64_t)n * z / splits);
+    hi = (int)((int64_t)n * (z + 1) / splits);
+  }
+  // sum over one depth segment of `chunks` chunks starting at chunk `base` of the item
+  auto segment = [&](const Operand& A, const Operand& B, int depth, int base) {
+    const int chunks = (depth + kKC - 1) / kKC;
+    const int c0 = max(lo - base, 0), c1 = min(hi - base, chunks);
+    if (c1 > c0) gemm_nt(acc, A, ni, B, mk, min(depth, c1 * kKC), sm, c0 * kKC);
+    return base + chunks;
+  };
+  int base = 0;
   if (k > 0)
-    gemm_nt(acc, v.segment(f, seg, kTile * i, 0), ni, v.segment(f, SEG_J, kTile * k, 0), mk, kTile * k, sm);
+    base = segment(v.segment(f, seg, kTile * i, 0), v.segment(f, SEG_J, kTile * k, 0), kTile * k, base);
   if (seg == SEG_J) {
     for (int64_t u = v.pull0; u < v.pull1; ++u) {
       const int64_t* pl = pulls + u * P_FIELDS;
       const int me = (int)pl[P_ME];
       const double* x = f + pl[P_OFF];
       if (pl[P_TYPE] == 0)  // U_e (me x mj): (U^T U)[a][b] = sum_r U[r][a] U[r][b]
-        gemm_nt(acc, operand(x + kTile * i, 1, v.mj), ni, operand(x + kTile * k, 1, v.mj), mk, me, sm);
+        base = segment(operand(x + kTile * i, 1, v.mj), operand(x + kTile * k, 1, v.mj), me, base);
       else  // V_e (mj x me): (V V^T)[a][b] = sum_r V[a][r] V[b][r]
-        gemm_nt(acc, operand(x + (int64_t)kTile * i * me, me, 1), ni,
-                operand(x + (int64_t)kTile * k * me, me, 1), mk, me, sm);
+        base = segment(operand(x + (int64_t)kTile * i * me, me, 1), operand(x + (int64_t)kTile * k * me, me, 1),
+                       me, base);
     }
+  }
+  if (splits > 1) {
+    double* out = partials + ((int64_t)(blockIdx.y * gridDim.x + blockIdx.x) * splits + blockIdx.z) * kTile * kTile;
+    put_acc(acc, out, kTile, 1, ni, mk, false, false);  // stores -acc
+    return;
   }
   const Operand c = v.segment(f, seg, kTile * i, kTile * k);
   const bool diagonal = seg == SEG_J && i == k;
@@ -1128,9 +1164,42 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
   }
 }
 
+// Split panels: the diagonal item adds its partials (stored negated, summed in split order) to
+// the lower triangle of the diagonal tile and factors it; the launch's other items return.
+__global__ void __launch_bounds__(kTT)
+tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
+                      double* __restrict__ factors, int64_t stride, int splits,
+                      const double* __restrict__ partials) {
+  chain_wait();
+  extern __shared__ double sm[];
+  const int* it = items + 4 * (begin + blockIdx.x);
+  const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
+  if (it[1] != SEG_J || it[2] != k) return;
+  double* f = factors + (int64_t)blockIdx.y * stride;
+  const int mk = min(kTile, v.mj - kTile * k);
+  double* dm = sm;
+  double* rinv = dm + kTile * kTLD;
+  double* diag = f + v.loff + (int64_t)kTile * k * v.mj + kTile * k;
+  const double* part = partials + (int64_t)(blockIdx.y * gridDim.x + blockIdx.x) * splits * kTile * kTile;
+  for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
+    const int r = idx / mk, col = idx - r * mk;
+    double x = diag[(int64_t)r * v.mj + col];
+    if (col <= r)
+      for (int z = 0; z < splits; ++z) x += part[(int64_t)z * kTile * kTile + r * kTile + col];
+    dm[r * kTLD + col] = x;
+  }
+  __syncthreads();
+  cholesky<kTLD>(dm, mk, rinv);
+  for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
+    const int r = idx / mk, col = idx - r * mk;
+    diag[(int64_t)r * v.mj + col] = dm[r * kTLD + col];
+  }
+}
+
 __global__ void __launch_bounds__(kTT)
 tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
-                    double* __restrict__ factors, int64_t stride) {
+                    double* __restrict__ factors, int64_t stride, int splits,
+                    const double* __restrict__ partials) {
   chain_wait();
   extern __shared__ double sm[];
   double* dm = sm;                // diagonal tile -> L_kk
@@ -1152,9 +1221,13 @@ tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64
   const int ni = min(kTile, v.rows(seg) - kTile * i);
   const Operand t = v.segment(f, seg, kTile * i, kTile * k);
   double* tb = const_cast<double*>(t.base);
+  const double* part = partials + (int64_t)(blockIdx.y * gridDim.x + blockIdx.x) * splits * kTile * kTile;
   for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
     const int a = idx / mk, c = idx - a * mk;
-    tt[c * kTLD + a] = tb[a * t.rs + c * t.cs];
+    double x = tb[a * t.rs + c * t.cs];
+    if (splits > 1)  // the panel update's partials (stored negated), in split order
+      for (int z = 0; z < splits; ++z) x += part[(int64_t)z * kTile * kTile + a * kTile + c];
+    tt[c * kTLD + a] = x;
   }
   __syncthreads();
   lower_solve(dm, kTLD, rinv, tt, kTLD, mk, ni);  // L_kk X^T = T^T
@@ -1322,7 +1395,17 @@ constexpr size_t kSubstituteSmem = sizeof(double) * (2 * kTile * kTLD + kTile) +
 void configure_tiled() {
   cudaFuncSetAttribute(tiled_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
   cudaFuncSetAttribute(tiled_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
+  cudaFuncSetAttribute(tiled_diagonal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
   cudaFuncSetAttribute(tiled_substitute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubstituteSmem);
+}
+
+// Depth splits of a panel launch of `tiles` items x `systems`: 1 when the launch fills the GPU
+// (two blocks per SM), else the largest of 2, 4, 8 that keeps it within that (the partials of at
+// most 2 x SMs tiles fit the plan's workspace).
+int panel_splits(int tiles, int systems, int sms) {
+  int splits = 1;
+  while (splits < 8 && (int64_t)tiles * systems * splits * 2 <= 2 * (int64_t)sms) splits *= 2;
+  return splits;
 }
 
 void factor_tiled(adt_plan* p, int systems, const double* values, double* factors, cudaStream_t s) {
@@ -1336,10 +1419,16 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
     for (int k = 0; k < p->panel_ptr[level + 1] - p->panel_ptr[level]; ++k) {
       auto [pb, pe] = range(3 * L + p->panel_ptr[level] + k);
       if (pe == pb) continue;
-      launch_chained(tiled_update_kernel, dim3(pe - pb, systems), kTT, kUpdateSmem, s, p->titems, pb, k, p->tasks, p->pulls,
-                                                                         factors, p->factor_stride);
+      const int splits = panel_splits(pe - pb, systems, p->sms);
+      launch_chained(tiled_update_kernel, dim3(pe - pb, systems, splits), kTT, kUpdateSmem, s, p->titems, pb, k, p->tasks,
+                     p->pulls, factors, p->factor_stride, splits, p->partials);
+      if (splits > 1) {
+        launch_chained(tiled_diagonal_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks,
+                       factors, p->factor_stride, splits, (const double*)p->partials);
+        p->launches++;
+      }
       launch_chained(tiled_factor_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks, factors,
-                                                                           p->factor_stride);
+                     p->factor_stride, splits, (const double*)p->partials);
       p->launches += 2;
     }
     auto [fb, fe] = range(L + level);

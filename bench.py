@@ -14,6 +14,12 @@ quadrature + ABMN measurement, and the 1232 x 9600 normal-quadrupole Jacobian.
   the page-locked result buffers, whose first allocation is a one-time cost.
 * ``--impl reference``: the reference's CPU path (FP64 oracle fields + the C restatement of the
   reference kernel on all host threads), one model per step.
+* ``--workload box3d``: the same metric for the 3D operator (``ERTForward3D.jacobian(sigma,
+  batch_size=32)``, series_batch_steps=1): 60 m x 40 m x 20 m box of 244,800 P1 tetrahedra,
+  12 x 8 surface electrodes, 4000 dipole-dipole rows (192 field columns with singularity
+  removal); a step is one fresh model's factorization, current + receiver fields and the 4000 x
+  244,800 Jacobian (3.9 GB, larger than L2, so no flush is needed). Its CPU baseline is the FP64
+  oracle's fields for one model plus the reference contraction on a sample of rows.
 
 Multi-GPU (torchrun): every rank runs its own models (time-lapse steps are independent), no
 collective on the data path; value = all ranks' entries / max-over-ranks time ("weak").
@@ -49,6 +55,9 @@ def parse_args():
     parser.add_argument("--e2e-steps", type=int, default=None)
     parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg (profiling runs)")
+    parser.add_argument("--workload", choices=("flat", "box3d", "box3d-small"), default="flat",
+                        help="flat: the 2.5D headline section; box3d: the 3D box (244,800 tetrahedra, 96 electrodes, "
+                             "4000 rows); box3d-small: the same survey on 36,000 tetrahedra (profiling captures)")
     return parser.parse_args()
 
 
@@ -161,6 +170,17 @@ def run_reference(args, rank: int, world: int) -> dict:
     from oracle import baseline
     from oracle.ert2p5d import Oracle2p5D
 
+    if args.workload in BOX3D:
+        nodes, cells, electrodes, rows = box3d_workload(args.workload)
+        base = box3d_cpu_baseline(nodes, cells, electrodes, rows)
+        value = base["value"]
+        return {
+            "metric": "jacobian_entries_per_second", "value": value, "unit": "entries/s", "n_gpus": world,
+            "steps": 1, "warmup": 0, "ms_per_step": 1e3 * len(rows) * len(cells) / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": box3d_config(len(rows), len(cells), len(nodes), 192, world), "cpu_baseline": base,
+            "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
     nodes, cells, electrodes, rows = workload(args.max_n)
     oracle = Oracle2p5D(nodes, cells, electrodes, rows)
     D, C = len(rows), len(cells)
@@ -207,6 +227,197 @@ def config(D, C, W, E, world) -> dict:
         "l2": "flushed between steps (256 MiB write, outside the timed events)",
         "parallelism": f"replicas x{world} (independent models per rank)",
     }
+
+
+BOX3D = {"box3d": (60, 40, 17), "box3d-small": (30, 20, 10)}
+
+
+def box3d_workload(name: str):
+    from adtlert_b200 import synthetic
+
+    nodes, cells = synthetic.box_section(*BOX3D[name])
+    electrodes, rows = synthetic.grid_survey()
+    return nodes, cells, electrodes, rows
+
+
+def box3d_config(D, C, N, columns, world) -> dict:
+    return {
+        "workload": f"3D jacobian(batch_size=32): {C} P1 tetrahedra, {N} nodes, 96 electrodes (12 x 8 grid), "
+                    f"{D} dipole-dipole rows, {columns} field columns; fresh model per step",
+        "rows": D,
+        "cells": C,
+        "nodes": N,
+        "field_columns": columns,
+        "l2": "inputs larger than L2 (the 3.9 GB Jacobian); no flush",
+        "parallelism": f"replicas x{world} (independent models per rank)",
+    }
+
+
+def run_box3d(args, rank: int, world: int) -> dict | None:
+    from adtlert_b200 import ERTForward3D, Mesh3D, Survey, _native, synthetic
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    nodes, cells, electrodes, rows = box3d_workload(args.workload)
+    forward = ERTForward3D.from_mesh_survey(Mesh3D.from_arrays(nodes, cells), Survey.from_arrays(electrodes, rows),
+                                            series_batch_steps=1)
+    lib, plan = forward._lib, forward._plan
+    N, D, C, cols = forward.N, forward.D, forward.C, forward.columns
+    stream = torch.cuda.current_stream(device)
+    handle = _native.stream_handle(device)
+    models = torch.as_tensor(np.stack([synthetic.ellipsoid_model(nodes, cells, 1000 * rank + i)
+                                       for i in range(args.warmup + args.steps)]), device=device)
+    fields = torch.empty((1, 1, N, cols), dtype=torch.float32, device=device)
+    normal = torch.empty((1, D), dtype=torch.float64, device=device)
+    recip = torch.empty_like(normal)
+    J = torch.empty((D, C), dtype=torch.float32, device=device)
+    slot = 15
+
+    def call(name, *a):
+        _native.check(getattr(lib, name)(plan, *a), plan, name)
+
+    stages = (
+        ("factorize", lambda i: call("adt_factorize", slot, _native.ptr(models[i]), 1, handle)),
+        ("solve_fields", lambda i: call("adt_solve_fields", slot, _native.ptr(models[i]), 1, _native.ptr(fields), handle)),
+        ("measure", lambda i: call("adt_measure", _native.ptr(fields), 1, _native.ptr(normal), _native.ptr(recip), None,
+                                   handle)),
+        ("normal_jacobian", lambda i: call("adt_normal_jacobian", _native.ptr(fields), 0, D, _native.ptr(J), handle)),
+    )
+
+    def step(i):
+        for _, fn in stages:
+            fn(i)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = forward.kernel_launches()
+    with ClockSampler(device.index) as clocks:
+        for k in range(args.steps):
+            events[k][0].record(stream)
+            step(args.warmup + k)
+            events[k][1].record(stream)
+        torch.cuda.synchronize(device)
+    launches = forward.kernel_launches() - launches0
+    barrier(world)
+    torch.cuda.synchronize(device)
+    elapsed_max = max_over_ranks(sum(a.elapsed_time(b) for a, b in events) / 1e3, world)
+    value = world * D * C * args.steps / elapsed_max
+    clock = clocks.summary()
+
+    stage_ms, stage_launches = {}, {}
+    for name, fn in stages:
+        total = 0.0
+        reps = 3
+        for k in range(reps):
+            i = args.warmup + (k % args.steps)
+            for other_name, other in stages:
+                if other_name == name:
+                    break
+                other(i)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            before = forward.kernel_launches()
+            a.record(stream)
+            fn(i)
+            b.record(stream)
+            stage_launches[name] = forward.kernel_launches() - before
+            torch.cuda.synchronize(device)
+            total += a.elapsed_time(b)
+        stage_ms[name] = total / reps
+    info = forward.plan_info
+    K, R = cells.shape[1], info["features"]
+    algorithmic = {
+        # J write + current/receiver fields read + cell dofs + per-cell template factors + ABMN
+        "normal_jacobian": 4 * D * C + 4 * N * cols + 4 * K * C + 4 * R * K * C + 16 * D,
+        # CSR values read, dense factors written
+        "factorize": 8 * info["nnz"] + 8 * info["factor_doubles_per_system"],
+        # factors read by the forward and backward solves, right-hand side and fields
+        "solve_fields": 2 * 8 * info["factor_doubles_per_system"] + 3 * 8 * N * cols,
+        "measure": 4 * N * cols + 16 * D,
+    }
+    peaks = measured_peaks()
+
+    def roofline(name):
+        count = max(1, stage_launches[name])
+        per_launch_s = stage_ms[name] / 1e3 / count
+        achieved = algorithmic[name] / count / per_launch_s / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": name,
+                "algorithmic_bytes_per_launch": algorithmic[name] / count, "launch_ms": per_launch_s * 1e3,
+                "peak_source": peaks["source"]}
+
+    # end to end: pinned host model in, J (page-locked) out; the untimed calls fill the field cache
+    # and allocate the page-locked result buffers
+    e2e_steps = args.e2e_steps or 3
+    e2e_warmup = max(3, min(args.warmup, forward.normal_field_cache_max_entries + 2))
+    host_models = [torch.as_tensor(synthetic.ellipsoid_model(nodes, cells, 50_000 + 1000 * rank + i)).pin_memory()
+                   for i in range(e2e_steps + e2e_warmup)]
+    for i in range(e2e_warmup):
+        out = forward.jacobian(host_models[i], batch_size=32)
+        del out
+    torch.cuda.synchronize(device)
+    barrier(world)
+    start = time.perf_counter()
+    for i in range(e2e_steps):
+        out = forward.jacobian(host_models[e2e_warmup + i], batch_size=32)
+        del out
+    torch.cuda.synchronize(device)
+    e2e_time = max_over_ranks(time.perf_counter() - start, world)
+    e2e = {"value": world * D * C * e2e_steps / e2e_time, "unit": "entries/s", "h2d_bytes_per_step": 4 * C,
+           "d2h_bytes_per_step": 4 * D * C, "ms_per_step": 1e3 * e2e_time / e2e_steps, "warmup_calls": e2e_warmup}
+    if rank != 0:
+        return None
+    result = {
+        "metric": "jacobian_entries_per_second",
+        "value": value,
+        "unit": "entries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 fields / f64 factorization",
+        "data": "synthetic (seeded 100 ohm-m background with three ellipsoids)",
+        "config": box3d_config(D, C, N, cols, world),
+        "roofline": roofline(max(stage_ms, key=stage_ms.get)),
+        "sensitivity_roofline": roofline("normal_jacobian"),
+        "stages_ms": stage_ms,
+        "clocks": clock,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = box3d_cpu_baseline(nodes, cells, electrodes, rows)
+    return result
+
+
+def box3d_cpu_baseline(nodes, cells, electrodes, rows, sample_rows: int = 64) -> dict:
+    """The FP64 oracle's fields (SciPy SuperLU) for one model plus the reference contraction on
+    a sample of rows, extrapolated to the full Jacobian."""
+
+    sys.path.insert(0, str(ROOT))
+    from adtlert_b200 import synthetic
+    from oracle.ert3d import Oracle3D
+
+    sample = np.linspace(0, len(rows) - 1, sample_rows).astype(int)
+    oracle = Oracle3D(nodes, cells, electrodes, rows[sample])
+    sigma = synthetic.ellipsoid_model(nodes, cells, 90_000).astype(float)
+    start = time.perf_counter()
+    oracle.jacobian(sigma)
+    total = time.perf_counter() - start
+    start = time.perf_counter()
+    oracle.fields(sigma)
+    fields_s = time.perf_counter() - start
+    rows_s = max(total - fields_s, 0.0) / sample_rows
+    full = fields_s + rows_s * len(rows)
+    D, C = len(rows), len(cells)
+    return {"value": D * C / full, "unit": "entries/s", "cores": 1, "kind": "port",
+            "sample": f"one model: FP64 SuperLU fields {fields_s:.1f} s + reference contraction of {sample_rows} of "
+                      f"{D} rows ({total - fields_s:.1f} s), extrapolated to {D} x {C}"}
 
 
 def run_b200(args, rank: int, world: int) -> dict | None:
@@ -403,7 +614,7 @@ def main():
             print(json.dumps(run_reference(args, rank, world)), flush=True)
         return
     rank, world = dist_setup(args)
-    result = run_b200(args, rank, world)
+    result = run_box3d(args, rank, world) if args.workload in BOX3D else run_b200(args, rank, world)
     if result is not None:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import subprocess
+import types
 from pathlib import Path
 
 import numpy as np
@@ -337,11 +338,25 @@ def _items(hp, r):
     return hp.titems.reshape(-1, 4)[b:e]
 
 
-def replay_factor_tiled(hp: HostPlan, values: np.ndarray) -> np.ndarray:
+SMS = 148  # multiprocessors of a B200: the tiled factorization's split rule depends on it
+
+
+def panel_splits(tiles: int, systems: int, sms: int = SMS) -> int:
+    """Depth splits of a panel launch, as the host code chooses them."""
+
+    splits = 1
+    while splits < 8 and tiles * systems * splits * 2 <= 2 * sms:
+        splits *= 2
+    return splits
+
+
+def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms: int = SMS) -> np.ndarray:
     """Factor storage of one system as the tiled kernels write it (items, tiles and offsets as
-    the device indexes them)."""
+    the device indexes them). Panel launches of few tiles split their depth: the partial tiles
+    live in a workspace of 2 x ``sms`` tiles, indexed here past the factor storage."""
 
     f = np.full(hp.factor_stride, np.nan)
+    space = types.SimpleNamespace(size=f.size + 2 * sms * TILE * TILE)  # factors, then the workspace
     L = hp.levels
     tasks = [_Task(r) for r in hp.tasks]
     for level in range(L):
@@ -381,6 +396,40 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray) -> np.ndarray:
         panels = hp.panel_ptr[level + 1] - hp.panel_ptr[level]
         for k in range(panels):
             items = _items(hp, 3 * L + hp.panel_ptr[level] + k)
+            splits = panel_splits(len(items), systems, sms)
+            assert splits == 1 or len(items) * systems * splits <= 2 * sms, "split workspace overflow"
+
+            def partial(n, z, rows, cols, splits=splits):
+                # the first system's partial tile (n, z); later systems follow at items * splits tiles
+                start = f.size + (n * splits + z) * TILE * TILE
+                return _strided(space, start, TILE, 1, rows, cols, "partial")
+
+            def split_panel(updates, k=k, splits=splits):
+                launch = _Launch("diagonal")
+                for n, (v, seg, i, idx, acc) in enumerate(updates):
+                    if seg == SEG_J and i == k:
+                        ni, mk = acc.shape
+                        launch.item([idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
+                launch.check()
+                launch = _Launch("triangular solve")
+                for n, (v, seg, i, idx, acc) in enumerate(updates):
+                    if not (seg == SEG_J and i == k):
+                        mk = min(TILE, v.mj - TILE * k)
+                        didx = _strided(f, v.loff + TILE * k * v.mj + TILE * k, v.mj, 1, mk, mk, "diag")
+                        ni = acc.shape[0]
+                        launch.item([didx, idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
+                launch.check()
+                for v, seg, i, idx, acc in updates:
+                    if seg == SEG_J and i == k:
+                        mask = np.tril(np.ones(acc.shape, bool))
+                        f[idx[mask]] -= acc[mask]
+                        f[idx] = np.linalg.cholesky(np.where(mask, f[idx], f[idx].T))
+                for v, seg, i, idx, acc in updates:
+                    if not (seg == SEG_J and i == k):
+                        mk = min(TILE, v.mj - TILE * k)
+                        didx = _strided(f, v.loff + TILE * k * v.mj + TILE * k, v.mj, 1, mk, mk, "diag")
+                        f[idx] = sla.solve_triangular(np.tril(f[didx]), (f[idx] - acc).T, lower=True).T
+
             launch = _Launch("update")
             updates = []
             for t, seg, i, _ in items:  # update launch: reads, then the item's own tile
@@ -406,9 +455,16 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray) -> np.ndarray:
                         acc += f[ia] @ f[ib].T
                         reads += [ia, ib]
                 idx = _strided(f, *v.segment(seg, TILE * i, TILE * k), ni, mk, "C tile")
-                launch.item(reads, [idx])
                 updates.append((v, seg, i, idx, acc))
+                if splits == 1:
+                    launch.item(reads, [idx])
+                    continue
+                for z in range(splits):
+                    launch.item(reads, [partial(len(updates) - 1, z, ni, mk)])
             launch.check()
+            if splits > 1:
+                split_panel(updates)
+                continue
             for v, seg, i, idx, acc in updates:
                 if seg == SEG_J and i == k:  # lower part, then the in-place Cholesky of the tile
                     mask = np.tril(np.ones(acc.shape, bool))

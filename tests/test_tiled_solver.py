@@ -14,7 +14,7 @@ from adtlert_b200.ert3d import build_problem_3d
 from adtlert_b200.geometry3d import Mesh3D
 from cases import box_tetrahedra, structured_section
 from conftest import assert_close
-from host_plan import HostPlan, replay_assembly, replay_factor_tiled, replay_solve_tiled
+from host_plan import SMS, HostPlan, panel_splits, replay_assembly, replay_factor_tiled, replay_solve_tiled
 
 
 def _section_plan():
@@ -55,11 +55,16 @@ def test_tiled_factor_and_solve_match_a_sparse_lu(build):
     hp = HostPlan(problem.struct())
     assert hp.status == 0, hp.error
     assert hp.tiled == 1 and hp.max_m > 64, "the case must exercise the tiled solver"
-    factors = replay_factor_tiled(hp, values)
     A = sp.csr_matrix((values, (hp.csr_row, hp.csr_col)), shape=(hp.N, hp.N)).tocsc()
     rhs = np.random.default_rng(0).standard_normal((hp.N, 70))
     expected = spl.splu(A).solve(rhs)
-    assert_close(replay_solve_tiled(hp, factors, rhs), expected, 1e-9, "tiled solve")
+    # panels split over 2-8 depth ranges (few tiles per launch on 148 SMs), and never split
+    splits = {panel_splits(len(hp.titems.reshape(-1, 4)[b:e]), 1)
+              for b, e in hp.tranges.reshape(-1, 2)[3 * hp.levels:]}
+    assert max(splits) > 1
+    for sms in (SMS, 1):
+        factors = replay_factor_tiled(hp, values, sms=sms)
+        assert_close(replay_solve_tiled(hp, factors, rhs), expected, 1e-9, f"tiled solve ({sms} SMs)")
 
 
 def test_tiled_items_cover_every_tile_once():
