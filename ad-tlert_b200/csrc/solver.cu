@@ -18,6 +18,8 @@
 // tiles while the next pull's operands stream into shared memory with cp.async (one barrier per
 // pull); Cholesky and triangular solves are blocked by 8 (the diagonal part in registers, the
 // rest as register-tiled updates) and multiply by reciprocal diagonals.
+#include <type_traits>
+
 #include "adt_internal.h"
 
 namespace adt {
@@ -939,12 +941,14 @@ __device__ __forceinline__ Operand operand(const double* base, int64_t rs, int64
 template <int N>
 __device__ __forceinline__ void async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Stage depth chunk [c0, c0 + kKC) of rows [0, rows) of `op` as tile[c][a] (zero outside).
+// Stage depth chunk [c0, c0 + kKC) of rows [0, rows) of `op` as tile[c][a] for a < SPAN (zero
+// outside).
+template <int SPAN = kTile>
 __device__ __forceinline__ void stage(double* tile, const Operand& op, int rows, int depth, int c0) {
   const bool depth_fast = op.cs == 1;
-  for (int idx = threadIdx.x; idx < kKC * kTile; idx += blockDim.x) {
-    const int a = depth_fast ? idx / kKC : idx % kTile;
-    const int c = depth_fast ? idx % kKC : idx / kTile;
+  for (int idx = threadIdx.x; idx < kKC * SPAN; idx += blockDim.x) {
+    const int a = depth_fast ? idx / kKC : idx % SPAN;
+    const int c = depth_fast ? idx % kKC : idx / SPAN;
     double* dst = tile + c * kTLD + a;
     if (a < rows && c0 + c < depth) async_copy8(dst, op.base + a * op.rs + (int64_t)(c0 + c) * op.cs);
     else *dst = 0.0;
@@ -952,9 +956,10 @@ __device__ __forceinline__ void stage(double* tile, const Operand& op, int rows,
 }
 
 // acc[r][s] += sum_{d0 <= c < depth} A(ty + 16 r, c) B(tx + 16 s, c) for A rows < ra, B rows
-// < rb (d0 a multiple of kKC). `sm` holds 4 * kKC * kTLD doubles; entered and left by all
-// threads (ends with a barrier).
-__device__ void gemm_nt(double (&acc)[4][4], const Operand& A, int ra, const Operand& B, int rb,
+// < rb (d0 a multiple of kKC); the output has 64 rows and 16 NQ columns. `sm` holds
+// 4 * kKC * kTLD doubles; entered and left by all threads (ends with a barrier).
+template <int NQ>
+__device__ void gemm_nt(double (&acc)[4][NQ], const Operand& A, int ra, const Operand& B, int rb,
                         int depth, double* sm, int d0 = 0) {
   if (depth <= d0) return;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -962,12 +967,12 @@ __device__ void gemm_nt(double (&acc)[4][4], const Operand& A, int ra, const Ope
   auto a_tile = [&](int b) { return sm + b * 2 * kKC * kTLD; };
   auto b_tile = [&](int b) { return sm + b * 2 * kKC * kTLD + kKC * kTLD; };
   stage(a_tile(0), A, ra, depth, d0);
-  stage(b_tile(0), B, rb, depth, d0);
+  stage<16 * NQ>(b_tile(0), B, rb, depth, d0);
   async_commit();
   for (int ch = 0; ch < chunks; ++ch) {
     if (ch + 1 < chunks) {
       stage(a_tile((ch + 1) & 1), A, ra, depth, d0 + (ch + 1) * kKC);
-      stage(b_tile((ch + 1) & 1), B, rb, depth, d0 + (ch + 1) * kKC);
+      stage<16 * NQ>(b_tile((ch + 1) & 1), B, rb, depth, d0 + (ch + 1) * kKC);
       async_commit();
       async_wait<1>();
     } else {
@@ -978,37 +983,39 @@ __device__ void gemm_nt(double (&acc)[4][4], const Operand& A, int ra, const Ope
     const double* bt = b_tile(ch & 1);
 #pragma unroll 4
     for (int c = 0; c < kKC; ++c) {
-      double a[4], b[4];
+      double a[4], b[NQ];
 #pragma unroll
       for (int r = 0; r < 4; ++r) a[r] = at[c * kTLD + ty + 16 * r];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) b[q] = bt[c * kTLD + tx + 16 * q];
+      for (int q = 0; q < NQ; ++q) b[q] = bt[c * kTLD + tx + 16 * q];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+        for (int q = 0; q < NQ; ++q) acc[r][q] = fma(a[r], b[q], acc[r][q]);
     }
     __syncthreads();
   }
 }
 
-__device__ __forceinline__ void zero_acc(double (&acc)[4][4]) {
+template <int NQ>
+__device__ __forceinline__ void zero_acc(double (&acc)[4][NQ]) {
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+    for (int q = 0; q < NQ; ++q) acc[r][q] = 0.0;
 }
 
 // C(a, b) = C(a, b) - acc (subtract) or -acc (store) for a < rows, b < cols (and b <= a when
 // `lower`), C(a, b) at c[a * rs + b * cs].
-__device__ __forceinline__ void put_acc(const double (&acc)[4][4], double* c, int64_t rs, int64_t cs,
+template <int NQ>
+__device__ __forceinline__ void put_acc(const double (&acc)[4][NQ], double* c, int64_t rs, int64_t cs,
                                         int rows, int cols, bool subtract, bool lower) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
     const int a = ty + 16 * r;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < NQ; ++q) {
       const int b = tx + 16 * q;
       if (a < rows && b < cols && (!lower || b <= a)) {
         double* dst = c + a * rs + b * cs;
@@ -1255,7 +1262,8 @@ tiled_fill_kernel(const int* __restrict__ items, int begin, const int64_t* __res
   put_acc(acc, f + v.fill + (int64_t)kTile * qi * v.mp + kTile * pi, v.mp, 1, nq, np, false, false);
 }
 
-// b_j -= sum of the pulls (U_e^T y_e or V_e y_e) on tile rows i of j, columns [c0, c0 + 64).
+// b_j -= sum of the pulls (U_e^T y_e or V_e y_e) on tile rows i of j, columns [c0, c0 + 16 NQ).
+template <int NQ>
 __global__ void __launch_bounds__(kTT)
 tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                             const int64_t* __restrict__ pulls, const double* __restrict__ factors,
@@ -1268,9 +1276,9 @@ tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int6
   const int i = it[1];
   const double* f = factors + (int64_t)blockIdx.y * stride;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
-  const int c0 = blockIdx.z * kTile, nc = min(kTile, nrhs - c0);
+  const int c0 = blockIdx.z * 16 * NQ, nc = min(16 * NQ, nrhs - c0);
   const int ni = min(kTile, v.mj - kTile * i);
-  double acc[4][4];
+  double acc[4][NQ];
   zero_acc(acc);
   for (int64_t u = v.pull0; u < v.pull1; ++u) {
     const int64_t* pl = pulls + u * P_FIELDS;
@@ -1283,7 +1291,8 @@ tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int6
   put_acc(acc, x + (int64_t)(v.offj + kTile * i) * nrhs + c0, nrhs, 1, ni, nc, true, false);
 }
 
-// y_j -= U_p x_p + V_q^T x_q on tile rows i of j, columns [c0, c0 + 64).
+// y_j -= U_p x_p + V_q^T x_q on tile rows i of j, columns [c0, c0 + 16 NQ).
+template <int NQ>
 __global__ void __launch_bounds__(kTT)
 tiled_backward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                              const double* __restrict__ factors, int64_t stride,
@@ -1296,9 +1305,9 @@ tiled_backward_update_kernel(const int* __restrict__ items, int begin, const int
   const int i = it[1];
   const double* f = factors + (int64_t)blockIdx.y * stride;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride;
-  const int c0 = blockIdx.z * kTile, nc = min(kTile, nrhs - c0);
+  const int c0 = blockIdx.z * 16 * NQ, nc = min(16 * NQ, nrhs - c0);
   const int ni = min(kTile, v.mj - kTile * i);
-  double acc[4][4];
+  double acc[4][NQ];
   zero_acc(acc);
   if (v.p >= 0)
     gemm_nt(acc, operand(f + v.uoff + (int64_t)kTile * i * v.mp, v.mp, 1), ni,
@@ -1309,8 +1318,9 @@ tiled_backward_update_kernel(const int* __restrict__ items, int begin, const int
   put_acc(acc, x + (int64_t)(v.offj + kTile * i) * nrhs + c0, nrhs, 1, ni, nc, true, false);
 }
 
-// Substitutions with L_j on columns [c0, c0 + 64) of one task: forward (L y = b, left-looking
-// over tile rows), and backward (L^T x = y) when `backward`; `forward` may be off.
+// Substitutions with L_j on columns [c0, c0 + 16 NQ) of one task: forward (L y = b,
+// left-looking over tile rows), and backward (L^T x = y) when `backward`; `forward` may be off.
+template <int NQ>
 __global__ void __launch_bounds__(kTT)
 tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
                         const double* __restrict__ factors, int64_t stride, double* __restrict__ rhs,
@@ -1325,7 +1335,7 @@ tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
   const double* f = factors + (int64_t)blockIdx.y * stride;
   const double* l = f + v.loff;
   double* x = rhs + (int64_t)blockIdx.y * rhs_stride + (int64_t)v.offj * nrhs;
-  const int c0 = blockIdx.z * kTile, nc = min(kTile, nrhs - c0);
+  const int c0 = blockIdx.z * 16 * NQ, nc = min(16 * NQ, nrhs - c0);
   const int tiles = (v.mj + kTile - 1) / kTile;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   auto load_diag = [&](int r, int nr) {
@@ -1335,12 +1345,12 @@ tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
     }
   };
   // bt = x rows of tile r minus acc
-  auto load_rows = [&](int r, int nr, const double (&acc)[4][4]) {
+  auto load_rows = [&](int r, int nr, const double (&acc)[4][NQ]) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int a = ty + 16 * i;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < NQ; ++q) {
         const int b = tx + 16 * q;
         if (a < nr && b < nc) bt[a * kTLD + b] = x[(int64_t)(kTile * r + a) * nrhs + c0 + b] - acc[i][q];
       }
@@ -1352,7 +1362,7 @@ tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
       x[(int64_t)(kTile * r + a) * nrhs + c0 + b] = bt[a * kTLD + b];
     }
   };
-  double acc[4][4];
+  double acc[4][NQ];
   if (forward) {
     for (int r = 0; r < tiles; ++r) {
       const int nr = min(kTile, v.mj - kTile * r);
@@ -1396,7 +1406,8 @@ void configure_tiled() {
   cudaFuncSetAttribute(tiled_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
   cudaFuncSetAttribute(tiled_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
   cudaFuncSetAttribute(tiled_diagonal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
-  cudaFuncSetAttribute(tiled_substitute_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubstituteSmem);
+  for (auto kernel : {tiled_substitute_kernel<4>, tiled_substitute_kernel<2>, tiled_substitute_kernel<1>})
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubstituteSmem);
 }
 
 // Depth splits of a panel launch of `tiles` items x `systems`: 1 when the launch fills the GPU
@@ -1440,27 +1451,52 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
   }
 }
 
+// Column strip of the tiled solve launches, in units of 16 columns (4: a full tile), narrowed
+// while the launch would leave most SMs idle.
+int tiled_strip(int blocks, int nrhs, int sms) {
+  int nq = 4;
+  while (nq > 1 && (int64_t)blocks * ((nrhs + 16 * nq - 1) / (16 * nq)) < 2 * (int64_t)sms) nq /= 2;
+  return nq;
+}
+
+template <typename F>
+void with_strip(int nq, F&& f) {
+  if (nq == 4) f(std::integral_constant<int, 4>());
+  else if (nq == 2) f(std::integral_constant<int, 2>());
+  else f(std::integral_constant<int, 1>());
+}
+
 void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s) {
   const int L = p->levels;
   const int64_t rhs_stride = (int64_t)p->N * nrhs;
-  const int strips = (nrhs + kTile - 1) / kTile;
   auto range = [&](int r) { return std::make_pair(p->tranges[2 * r], p->tranges[2 * r + 1]); };
+  auto strips = [&](int nq) { return (nrhs + 16 * nq - 1) / (16 * nq); };
   for (int level = 0; level < L; ++level) {
-    auto [b, e] = range(2 * L + level);
-    launch_chained(tiled_forward_update_kernel, dim3(e - b, systems, strips), kTT, kGemmSmem, s, 
-        p->titems, b, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    const auto [rb, re] = range(2 * L + level);
+    const int b = rb, e = re;
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    launch_chained(tiled_substitute_kernel, dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s, 
-        t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 1, level == L - 1);
+    with_strip(tiled_strip((e - b) * systems, nrhs, p->sms), [&](auto nq) {
+      launch_chained(tiled_forward_update_kernel<nq()>, dim3(e - b, systems, strips(nq())), kTT, kGemmSmem, s,
+                     p->titems, b, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    });
+    with_strip(tiled_strip((t1 - t0) * systems, nrhs, p->sms), [&](auto nq) {
+      launch_chained(tiled_substitute_kernel<nq()>, dim3(t1 - t0, systems, strips(nq())), kTT, kSubstituteSmem, s,
+                     t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 1, level == L - 1);
+    });
     p->launches += 2;
   }
   for (int level = L - 2; level >= 0; --level) {
-    auto [b, e] = range(2 * L + level);
-    launch_chained(tiled_backward_update_kernel, dim3(e - b, systems, strips), kTT, kGemmSmem, s, 
-        p->titems, b, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    const auto [rb, re] = range(2 * L + level);
+    const int b = rb, e = re;
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    launch_chained(tiled_substitute_kernel, dim3(t1 - t0, systems, strips), kTT, kSubstituteSmem, s, 
-        t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 0, 1);
+    with_strip(tiled_strip((e - b) * systems, nrhs, p->sms), [&](auto nq) {
+      launch_chained(tiled_backward_update_kernel<nq()>, dim3(e - b, systems, strips(nq())), kTT, kGemmSmem, s,
+                     p->titems, b, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs);
+    });
+    with_strip(tiled_strip((t1 - t0) * systems, nrhs, p->sms), [&](auto nq) {
+      launch_chained(tiled_substitute_kernel<nq()>, dim3(t1 - t0, systems, strips(nq())), kTT, kSubstituteSmem, s,
+                     t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 0, 1);
+    });
     p->launches += 2;
   }
 }
