@@ -923,6 +923,8 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
 constexpr int kTT = kSolverThreads;  // threads of the tiled kernels (16 x 16 micro-tile grid)
 constexpr int kKC = 16;              // reduction depth staged per step
 constexpr int kTLD = kTile + 1;      // leading dimension of the shared tiles
+constexpr int kSLD = kTile + 8;      // leading dimension of the GEMM staging tiles (== 8 mod 16)
+constexpr int kStage = 4 * kKC * kSLD;  // doubles of GEMM staging (two buffers of A and B chunks)
 
 // Element (a, c) of a strided operand: base[a * rs + c * cs].
 struct Operand {
@@ -949,23 +951,35 @@ __device__ __forceinline__ void stage(double* tile, const Operand& op, int rows,
   for (int idx = threadIdx.x; idx < kKC * SPAN; idx += blockDim.x) {
     const int a = depth_fast ? idx / kKC : idx % SPAN;
     const int c = depth_fast ? idx % kKC : idx / SPAN;
-    double* dst = tile + c * kTLD + a;
+    double* dst = tile + c * kSLD + a;
     if (a < rows && c0 + c < depth) async_copy8(dst, op.base + a * op.rs + (int64_t)(c0 + c) * op.cs);
     else *dst = 0.0;
   }
 }
 
 // acc[r][s] += sum_{d0 <= c < depth} A(ty + 16 r, c) B(tx + 16 s, c) for A rows < ra, B rows
-// < rb (d0 a multiple of kKC); the output has 64 rows and 16 NQ columns. `sm` holds
-// 4 * kKC * kTLD doubles; entered and left by all threads (ends with a barrier).
+// < rb (d0 a multiple of kKC); the output has 64 rows and 16 NQ columns. The products run on
+// the FP64 tensor cores (mma.sync m8n8k4): warp w owns rows 16 (w & 3) + [0, 16) and columns
+// 8 NQ (w >> 2) + [0, 8 NQ) as 2 x NQ tiles of 8 x 8; the fragments are added to `acc` through
+// shared memory at the end. Operand chunks are staged depth-major (tile[c][a], leading
+// dimension 72, so a fragment load of 4 depths x 8 rows takes two wavefronts) with cp.async,
+// double-buffered. `sm` holds kStage doubles; entered and left by all threads (ends with a
+// barrier).
 template <int NQ>
 __device__ void gemm_nt(double (&acc)[4][NQ], const Operand& A, int ra, const Operand& B, int rb,
                         int depth, double* sm, int d0 = 0) {
   if (depth <= d0) return;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = 16 * (warp & 3), n0 = 8 * NQ * (warp >> 2);
   const int chunks = (depth - d0 + kKC - 1) / kKC;
-  auto a_tile = [&](int b) { return sm + b * 2 * kKC * kTLD; };
-  auto b_tile = [&](int b) { return sm + b * 2 * kKC * kTLD + kKC * kTLD; };
+  auto a_tile = [&](int b) { return sm + b * 2 * kKC * kSLD; };
+  auto b_tile = [&](int b) { return sm + b * 2 * kKC * kSLD + kKC * kSLD; };
+  double frag[2][NQ][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) frag[i][j][0] = frag[i][j][1] = 0.0;
   stage(a_tile(0), A, ra, depth, d0);
   stage<16 * NQ>(b_tile(0), B, rb, depth, d0);
   async_commit();
@@ -979,22 +993,39 @@ __device__ void gemm_nt(double (&acc)[4][NQ], const Operand& A, int ra, const Op
       async_wait<0>();
     }
     __syncthreads();
-    const double* at = a_tile(ch & 1);
-    const double* bt = b_tile(ch & 1);
-#pragma unroll 4
-    for (int c = 0; c < kKC; ++c) {
-      double a[4], b[NQ];
+    const double* at = a_tile(ch & 1) + t * kSLD + m0 + g;
+    const double* bt = b_tile(ch & 1) + t * kSLD + n0 + g;
 #pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = at[c * kTLD + ty + 16 * r];
+    for (int k = 0; k < kKC; k += 4) {
+      double a[2], b[NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) b[q] = bt[c * kTLD + tx + 16 * q];
+      for (int i = 0; i < 2; ++i) a[i] = at[k * kSLD + 8 * i];
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int j = 0; j < NQ; ++j) b[j] = bt[k * kSLD + 8 * j];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < NQ; ++j) dmma(frag[i][j], a[i], b[j]);
     }
     __syncthreads();
   }
+  // fragments -> the block's accumulator layout, through the (now idle) staging buffer
+  double* out = sm;  // [64][kTLD]
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+      double* row = out + (m0 + 8 * i + g) * kTLD + n0 + 8 * j + 2 * t;
+      row[0] = frag[i][j][0];
+      row[1] = frag[i][j][1];
+    }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) acc[r][q] += out[(ty + 16 * r) * kTLD + tx + 16 * q];
+  __syncthreads();
 }
 
 template <int NQ>
@@ -1155,7 +1186,7 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
   put_acc(acc, const_cast<double*>(c.base), c.rs, c.cs, ni, mk, true, diagonal);
   if (!diagonal) return;
   // factor the updated diagonal tile in shared memory (after the staging buffers' last use)
-  double* dm = sm + 4 * kKC * kTLD;
+  double* dm = sm + kStage;
   double* rinv = dm + kTile * kTLD;
   double* diag = const_cast<double*>(c.base);
   __syncthreads();
@@ -1397,7 +1428,8 @@ tiled_substitute_kernel(int task_begin, const int64_t* __restrict__ tasks,
   }
 }
 
-constexpr size_t kGemmSmem = sizeof(double) * 4 * kKC * kTLD;
+constexpr size_t kGemmSmem = sizeof(double) * kStage;
+static_assert(kStage >= kTile * kTLD, "the GEMM staging buffer holds the accumulator exchange");
 constexpr size_t kUpdateSmem = kGemmSmem + sizeof(double) * (kTile * kTLD + kTile);
 constexpr size_t kFactorSmem = sizeof(double) * (2 * kTile * kTLD + kTile);
 constexpr size_t kSubstituteSmem = sizeof(double) * (2 * kTile * kTLD + kTile) + kGemmSmem;
