@@ -35,13 +35,14 @@ def check_finite(values: Tensor, context: str) -> None:
 
 
 def finite_flag(values: Tensor) -> Tensor:
-    """A one-element boolean on ``values``' device, True iff every entry is finite, computed with
-    one read and no full-size temporary: the float64 sum of float32 values cannot overflow (below
-    2**970 entries), and an inf or NaN entry makes it inf or NaN."""
+    """A one-element boolean on ``values``' device, True iff every entry is finite, computed in
+    one read with no full-size temporary: the minimum and maximum are finite exactly when every
+    entry is (min/max propagate NaN, and an infinite entry is an extreme)."""
 
-    if values.dtype in (torch.float32, torch.float16, torch.bfloat16):
-        return torch.isfinite(values.sum(dtype=torch.float64))
-    return torch.isfinite(values).all()
+    if values.numel() == 0:
+        return torch.ones((), dtype=torch.bool, device=values.device)
+    low, high = torch.aminmax(values)
+    return torch.isfinite(low) & torch.isfinite(high)
 
 
 def cell_vector(values, count: int, dtype: torch.dtype = FLOAT_DTYPE) -> Tensor:

@@ -8,7 +8,7 @@ from adtlert_b200.inputs import cell_vector, check_finite, conductivity_model, f
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-def test_finite_flag_agrees_with_an_elementwise_scan(dtype):
+def test_finite_flag_detects_every_non_finite_kind(dtype):
     rng = np.random.default_rng(0)
     values = torch.as_tensor(rng.standard_normal((37, 53)), dtype=dtype)
     assert bool(finite_flag(values))
@@ -24,7 +24,7 @@ def test_finite_flag_agrees_with_an_elementwise_scan(dtype):
     assert bool(finite_flag(torch.empty((0, 5), dtype=dtype)))
 
 
-def test_finite_flag_float64_uses_the_elementwise_scan():
+def test_finite_flag_at_the_float64_maximum():
     big = torch.full((4,), torch.finfo(torch.float64).max, dtype=torch.float64)
     assert bool(finite_flag(big))
 
