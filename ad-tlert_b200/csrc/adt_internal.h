@@ -97,6 +97,8 @@ struct adt_plan {
   double* weights = nullptr;    // [W]
   int* abmn = nullptr;          // [D][4]
   double* partials = nullptr;   // tiled solver: split-depth partial tiles (2 x SMs tiles of 64 x 64)
+  double* inverses = nullptr;   // tiled solver: L_kk^-1 per task of a level and system (grown on use)
+  size_t inverses_capacity = 0; // doubles
   int2* row_entries = nullptr;  // [2][D] (A | B << 8 | M << 16 | N << 24, d): sorted by (A, B, M, N), then in row order
   int* rcv_dofs = nullptr;      // [E][RW] solver order
   double* rcv_w = nullptr;      // [E][RW]

@@ -421,7 +421,7 @@ adt_status adt_plan_destroy(adt_plan* p) {
                   p->rcv_w, p->src_ptr, p->src_cells, p->features, p->fscale, p->model_ptr,
                   p->model_list, p->tasks, p->pulls, p->pair_ptr, p->pair_list, p->rdof_ptr,
                   p->rdof_rcv, p->rdof_w, p->rdof_dof, p->primary, p->refrhs, p->scratch, p->pot,
-                  p->fixed, p->owners, p->titems, p->update_items, p->tc_error, p->partials};
+                  p->fixed, p->owners, p->titems, p->update_items, p->tc_error, p->partials, p->inverses};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->tc_error_host) cudaFreeHost(p->tc_error_host);

@@ -1120,6 +1120,24 @@ tiled_scatter_kernel(const int* __restrict__ items, int begin, const int64_t* __
   }
 }
 
+// L^-1 of the factored m x m diagonal tile in `dm` (rinv = 1 / diagonal) through the scratch
+// tile `x` (64 x kTLD), stored 64 x 64 row-major at `out` (zero above the diagonal and past m):
+// the triangular-solve launch of the panel applies it as a GEMM. Entered by all threads; ends
+// with a barrier.
+__device__ void store_inverse(const double* dm, const double* rinv, double* x, int m, double* out) {
+  for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+    const int r = idx / kTile, c = idx - r * kTile;
+    x[r * kTLD + c] = (r == c && r < m) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  lower_solve(dm, kTLD, rinv, x, kTLD, m, m);  // columns of the identity: exact zeros above
+  for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+    const int r = idx / kTile, c = idx - r * kTile;
+    out[idx] = (r < m && c < m) ? x[r * kTLD + c] : 0.0;
+  }
+  __syncthreads();
+}
+
 // Depth chunks (of kKC) of one update item: its own columns [0, 64k), then each pull's depth.
 __device__ __forceinline__ int update_chunks(const TaskView& v, int seg, int k, const int64_t* pulls) {
   int n = (kTile * k) / kKC;
@@ -1137,7 +1155,8 @@ __device__ __forceinline__ int update_chunks(const TaskView& v, int seg, int k, 
 __global__ void __launch_bounds__(kTT)
 tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                     const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride,
-                    int splits, double* __restrict__ partials) {
+                    int splits, double* __restrict__ partials, double* __restrict__ inverses, int t0,
+                    int level_tasks) {
   chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
@@ -1200,6 +1219,8 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
     const int r = idx / mk, col = idx - r * mk;
     diag[(int64_t)r * v.mj + col] = dm[r * kTLD + col];
   }
+  store_inverse(dm, rinv, sm, mk,
+                inverses + ((int64_t)blockIdx.y * level_tasks + (it[0] - t0)) * kTile * kTile);
 }
 
 // Split panels: the diagonal item adds its partials (stored negated, summed in split order) to
@@ -1207,7 +1228,8 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
 __global__ void __launch_bounds__(kTT)
 tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                       double* __restrict__ factors, int64_t stride, int splits,
-                      const double* __restrict__ partials) {
+                      const double* __restrict__ partials, double* __restrict__ inverses, int t0,
+                      int level_tasks) {
   chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
@@ -1216,7 +1238,8 @@ tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int
   double* f = factors + (int64_t)blockIdx.y * stride;
   const int mk = min(kTile, v.mj - kTile * k);
   double* dm = sm;
-  double* rinv = dm + kTile * kTLD;
+  double* x = dm + kTile * kTLD;
+  double* rinv = x + kTile * kTLD;
   double* diag = f + v.loff + (int64_t)kTile * k * v.mj + kTile * k;
   const double* part = partials + (int64_t)(blockIdx.y * gridDim.x + blockIdx.x) * splits * kTile * kTile;
   for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
@@ -1232,30 +1255,34 @@ tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int
     const int r = idx / mk, col = idx - r * mk;
     diag[(int64_t)r * v.mj + col] = dm[r * kTLD + col];
   }
+  store_inverse(dm, rinv, x, mk, inverses + ((int64_t)blockIdx.y * level_tasks + (it[0] - t0)) * kTile * kTile);
 }
 
+// Tile (i, k) below the diagonal: X = T L_kk^-T, with T = the updated tile (plus the panel
+// update's partials when split) and L_kk^-1 from the panel's diagonal step, as one shared-memory
+// GEMM (rows of U_p^T / V_q and of L_j alike).
 __global__ void __launch_bounds__(kTT)
 tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                     double* __restrict__ factors, int64_t stride, int splits,
-                    const double* __restrict__ partials) {
+                    const double* __restrict__ partials, const double* __restrict__ inverses, int t0,
+                    int level_tasks) {
   chain_wait();
   extern __shared__ double sm[];
-  double* dm = sm;                // diagonal tile -> L_kk
-  double* tt = dm + kTile * kTLD; // transposed tile below
-  double* rinv = tt + kTile * kTLD;
+  double* li = sm;                 // L_kk^-1
+  double* tt = li + kTile * kTLD;  // transposed tile
+  double* xo = tt + kTile * kTLD;  // result
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
   const int seg = it[1], i = it[2];
+  if (seg == SEG_J && i == k) return;  // factored by the diagonal step
   double* f = factors + (int64_t)blockIdx.y * stride;
-  if (seg == SEG_J && i == k) return;  // factored by the update launch
   const int mk = min(kTile, v.mj - kTile * k);
-  const double* diag = f + v.loff + (int64_t)kTile * k * v.mj + kTile * k;
-  for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
-    const int r = idx / mk, c = idx - r * mk;
-    dm[r * kTLD + c] = diag[(int64_t)r * v.mj + c];
+  const double* inv = inverses + ((int64_t)blockIdx.y * level_tasks + (it[0] - t0)) * kTile * kTile;
+  for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+    const int r = idx / kTile, c = idx - r * kTile;
+    li[r * kTLD + c] = inv[idx];
+    xo[r * kTLD + c] = 0.0;
   }
-  __syncthreads();
-  reciprocal_diagonal(dm, kTLD, mk, rinv);
   const int ni = min(kTile, v.rows(seg) - kTile * i);
   const Operand t = v.segment(f, seg, kTile * i, kTile * k);
   double* tb = const_cast<double*>(t.base);
@@ -1268,10 +1295,11 @@ tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64
     tt[c * kTLD + a] = x;
   }
   __syncthreads();
-  lower_solve(dm, kTLD, rinv, tt, kTLD, mk, ni);  // L_kk X^T = T^T
+  tile_gemm<true, true>(xo, kTLD, tt, kTLD, li, kTLD, ni, mk, mk, 1.0);  // X[a][b] = sum_c T[a][c] Linv[b][c]
+  __syncthreads();
   for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
     const int a = idx / mk, c = idx - a * mk;
-    tb[a * t.rs + c * t.cs] = tt[c * kTLD + a];
+    tb[a * t.rs + c * t.cs] = xo[a * kTLD + c];
   }
 }
 
@@ -1432,11 +1460,12 @@ constexpr size_t kGemmSmem = sizeof(double) * kStage;
 static_assert(kStage >= kTile * kTLD, "the GEMM staging buffer holds the accumulator exchange");
 constexpr size_t kUpdateSmem = kGemmSmem + sizeof(double) * (kTile * kTLD + kTile);
 constexpr size_t kFactorSmem = sizeof(double) * (2 * kTile * kTLD + kTile);
+constexpr size_t kTileSolveSmem = sizeof(double) * 3 * kTile * kTLD;
 constexpr size_t kSubstituteSmem = sizeof(double) * (2 * kTile * kTLD + kTile) + kGemmSmem;
 
 void configure_tiled() {
   cudaFuncSetAttribute(tiled_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
-  cudaFuncSetAttribute(tiled_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
+  cudaFuncSetAttribute(tiled_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSolveSmem);
   cudaFuncSetAttribute(tiled_diagonal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
   for (auto kernel : {tiled_substitute_kernel<4>, tiled_substitute_kernel<2>, tiled_substitute_kernel<1>})
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubstituteSmem);
@@ -1459,19 +1488,21 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
     launch_chained(tiled_scatter_kernel, dim3(e - b, systems), kTT, 0, s, p->titems, b, p->tasks, p->csr_ptr, p->csr_row,
                                                              p->csr_col, p->nnz, values, factors, p->factor_stride);
     p->launches++;
+    const int t0 = p->level_begin[level], level_tasks = p->level_begin[level + 1] - t0;
     for (int k = 0; k < p->panel_ptr[level + 1] - p->panel_ptr[level]; ++k) {
       auto [pb, pe] = range(3 * L + p->panel_ptr[level] + k);
       if (pe == pb) continue;
       const int splits = panel_splits(pe - pb, systems, p->sms);
       launch_chained(tiled_update_kernel, dim3(pe - pb, systems, splits), kTT, kUpdateSmem, s, p->titems, pb, k, p->tasks,
-                     p->pulls, factors, p->factor_stride, splits, p->partials);
+                     p->pulls, factors, p->factor_stride, splits, p->partials, p->inverses, t0, level_tasks);
       if (splits > 1) {
         launch_chained(tiled_diagonal_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks,
-                       factors, p->factor_stride, splits, (const double*)p->partials);
+                       factors, p->factor_stride, splits, (const double*)p->partials, p->inverses, t0, level_tasks);
         p->launches++;
       }
-      launch_chained(tiled_factor_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks, factors,
-                     p->factor_stride, splits, (const double*)p->partials);
+      launch_chained(tiled_factor_kernel, dim3(pe - pb, systems), kTT, kTileSolveSmem, s, p->titems, pb, k, p->tasks,
+                     factors, p->factor_stride, splits, (const double*)p->partials, (const double*)p->inverses, t0,
+                     level_tasks);
       p->launches += 2;
     }
     auto [fb, fe] = range(L + level);
@@ -1657,7 +1688,22 @@ void configure_solver_kernels() {
 
 adt_status factorize_systems(adt_plan* p, int systems, const double* values, double* factors,
                              cudaStream_t s) {
-  if (p->tiled) factor_tiled(p, systems, values, factors, s);
+  if (p->tiled) {
+    // L_kk^-1 of every task of a level and system, for the panels' triangular solves
+    int widest = 0;
+    for (int level = 0; level < p->levels; ++level)
+      widest = std::max(widest, p->level_begin[level + 1] - p->level_begin[level]);
+    const size_t need = (size_t)widest * systems * kTile * kTile;
+    if (p->inverses_capacity < need) {
+      if (p->inverses) cudaFree(p->inverses);
+      p->inverses = nullptr;
+      p->inverses_capacity = 0;
+      if (cudaMalloc(&p->inverses, need * sizeof(double)) != cudaSuccess)
+        return fail(p, ADT_OOM, "tiled solver workspace allocation failed");
+      p->inverses_capacity = need;
+    }
+    factor_tiled(p, systems, values, factors, s);
+  }
   else if (p->max_m <= 32) factor_levels<32>(p, systems, values, factors, s);
   else if (p->max_m <= 48) factor_levels<48>(p, systems, values, factors, s);
   else factor_levels<64>(p, systems, values, factors, s);

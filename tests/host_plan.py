@@ -356,7 +356,10 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms:
     live in a workspace of 2 x ``sms`` tiles, indexed here past the factor storage."""
 
     f = np.full(hp.factor_stride, np.nan)
-    space = types.SimpleNamespace(size=f.size + 2 * sms * TILE * TILE)  # factors, then the workspace
+    widest = int(np.max(np.diff(hp.level_begin)))
+    inverse_base = f.size + 2 * sms * TILE * TILE
+    # factors, the split partials, then L_kk^-1 per task of a level
+    space = types.SimpleNamespace(size=inverse_base + widest * TILE * TILE)
     L = hp.levels
     tasks = [_Task(r) for r in hp.tasks]
     for level in range(L):
@@ -398,6 +401,10 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms:
             items = _items(hp, 3 * L + hp.panel_ptr[level] + k)
             splits = panel_splits(len(items), systems, sms)
             assert splits == 1 or len(items) * systems * splits <= 2 * sms, "split workspace overflow"
+            t0 = int(hp.level_begin[level])
+
+            def inverse(t):
+                return _strided(space, inverse_base + (int(t) - t0) * TILE * TILE, TILE, 1, TILE, TILE, "inverse")
 
             def partial(n, z, rows, cols, splits=splits):
                 # the first system's partial tile (n, z); later systems follow at items * splits tiles
@@ -406,18 +413,17 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms:
 
             def split_panel(updates, k=k, splits=splits):
                 launch = _Launch("diagonal")
-                for n, (v, seg, i, idx, acc) in enumerate(updates):
+                for n, ((t, _, _, _), (v, seg, i, idx, acc)) in enumerate(zip(items, updates)):
                     if seg == SEG_J and i == k:
                         ni, mk = acc.shape
-                        launch.item([idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
+                        launch.item([idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx, inverse(t)])
                 launch.check()
                 launch = _Launch("triangular solve")
-                for n, (v, seg, i, idx, acc) in enumerate(updates):
+                for n, ((t, _, _, _), (v, seg, i, idx, acc)) in enumerate(zip(items, updates)):
                     if not (seg == SEG_J and i == k):
                         mk = min(TILE, v.mj - TILE * k)
-                        didx = _strided(f, v.loff + TILE * k * v.mj + TILE * k, v.mj, 1, mk, mk, "diag")
                         ni = acc.shape[0]
-                        launch.item([didx, idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
+                        launch.item([inverse(t), idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
                 launch.check()
                 for v, seg, i, idx, acc in updates:
                     if seg == SEG_J and i == k:
@@ -457,7 +463,7 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms:
                 idx = _strided(f, *v.segment(seg, TILE * i, TILE * k), ni, mk, "C tile")
                 updates.append((v, seg, i, idx, acc))
                 if splits == 1:
-                    launch.item(reads, [idx])
+                    launch.item(reads, [idx, inverse(t)] if seg == SEG_J and i == k else [idx])
                     continue
                 for z in range(splits):
                     launch.item(reads, [partial(len(updates) - 1, z, ni, mk)])
@@ -482,7 +488,7 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms:
                 didx = _strided(f, v.loff + TILE * k * v.mj + TILE * k, v.mj, 1, mk, mk, "diag")
                 ni = min(TILE, v.rows(seg) - TILE * i)
                 idx = _strided(f, *v.segment(seg, TILE * i, TILE * k), ni, mk, "tile")
-                launch.item([didx], [idx])
+                launch.item([inverse(t)], [idx])
                 solves.append((didx, idx))
             launch.check()
             for didx, idx in solves:
