@@ -943,19 +943,40 @@ __device__ __forceinline__ Operand operand(const double* base, int64_t rs, int64
 template <int N>
 __device__ __forceinline__ void async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Stage depth chunk [c0, c0 + kKC) of rows [0, rows) of `op` as tile[c][a] for a < SPAN (zero
-// outside).
-template <int SPAN = kTile>
-__device__ __forceinline__ void stage(double* tile, const Operand& op, int rows, int depth, int c0) {
-  const bool depth_fast = op.cs == 1;
-  for (int idx = threadIdx.x; idx < kKC * SPAN; idx += blockDim.x) {
-    const int a = depth_fast ? idx / kKC : idx % SPAN;
-    const int c = depth_fast ? idx % kKC : idx / SPAN;
-    double* dst = tile + c * kSLD + a;
-    if (a < rows && c0 + c < depth) async_copy8(dst, op.base + a * op.rs + (int64_t)(c0 + c) * op.cs);
-    else *dst = 0.0;
+// The elements one thread copies for every depth chunk of an operand: rows a < SPAN of the
+// chunk, kKC depths each, kTT threads. Addresses are formed once per GEMM call; a chunk only adds
+// its depth offset.
+template <int SPAN>
+struct StagePlan {
+  static constexpr int kPer = (kKC * SPAN + kTT - 1) / kTT;
+  const double* src[kPer];
+  int dst[kPer];
+  int depth_of[kPer];  // the element's depth within a chunk; -1: row past the operand or unused
+  int64_t step;        // source advance per chunk
+  __device__ StagePlan(const Operand& op, int rows, int d0) {
+    const bool depth_fast = op.cs == 1;
+    step = (int64_t)kKC * op.cs;
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      const int idx = threadIdx.x + e * kTT;
+      const int a = depth_fast ? idx / kKC : idx % SPAN;
+      const int c = depth_fast ? idx % kKC : idx / SPAN;
+      const bool used = idx < kKC * SPAN;
+      dst[e] = c * kSLD + a;
+      depth_of[e] = used && a < rows ? c : -1;
+      src[e] = op.base + (int64_t)a * op.rs + (int64_t)(d0 + c) * op.cs;
+    }
   }
-}
+  // chunk ch (depths d0 + ch * kKC + [0, kKC)) into tile; zero outside the operand or depth
+  __device__ __forceinline__ void copy(double* tile, int ch, int limit) const {
+#pragma unroll
+    for (int e = 0; e < kPer; ++e) {
+      if (threadIdx.x + e * kTT >= kKC * SPAN) continue;
+      if (depth_of[e] >= 0 && depth_of[e] + ch * kKC < limit) async_copy8(tile + dst[e], src[e] + ch * step);
+      else tile[dst[e]] = 0.0;
+    }
+  }
+};
 
 // acc[r][s] += sum_{d0 <= c < depth} A(ty + 16 r, c) B(tx + 16 s, c) for A rows < ra, B rows
 // < rb (d0 a multiple of kKC); the output has 64 rows and 16 NQ columns. The products run on
@@ -973,20 +994,23 @@ __device__ void gemm_nt(double (&acc)[4][NQ], const Operand& A, int ra, const Op
   const int g = lane >> 2, t = lane & 3;
   const int m0 = 16 * (warp & 3), n0 = 8 * NQ * (warp >> 2);
   const int chunks = (depth - d0 + kKC - 1) / kKC;
+  const int limit = depth - d0;  // depths past it read as zero
   auto a_tile = [&](int b) { return sm + b * 2 * kKC * kSLD; };
   auto b_tile = [&](int b) { return sm + b * 2 * kKC * kSLD + kKC * kSLD; };
+  const StagePlan<kTile> pa(A, ra, d0);
+  const StagePlan<16 * NQ> pb(B, rb, d0);
   double frag[2][NQ][2];
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
     for (int j = 0; j < NQ; ++j) frag[i][j][0] = frag[i][j][1] = 0.0;
-  stage(a_tile(0), A, ra, depth, d0);
-  stage<16 * NQ>(b_tile(0), B, rb, depth, d0);
+  pa.copy(a_tile(0), 0, limit);
+  pb.copy(b_tile(0), 0, limit);
   async_commit();
   for (int ch = 0; ch < chunks; ++ch) {
     if (ch + 1 < chunks) {
-      stage(a_tile((ch + 1) & 1), A, ra, depth, d0 + (ch + 1) * kKC);
-      stage<16 * NQ>(b_tile((ch + 1) & 1), B, rb, depth, d0 + (ch + 1) * kKC);
+      pa.copy(a_tile((ch + 1) & 1), ch + 1, limit);
+      pb.copy(b_tile((ch + 1) & 1), ch + 1, limit);
       async_commit();
       async_wait<1>();
     } else {
@@ -1323,7 +1347,7 @@ tiled_fill_kernel(const int* __restrict__ items, int begin, const int64_t* __res
 
 // b_j -= sum of the pulls (U_e^T y_e or V_e y_e) on tile rows i of j, columns [c0, c0 + 16 NQ).
 template <int NQ>
-__global__ void __launch_bounds__(kTT)
+__global__ void __launch_bounds__(kTT, 2)
 tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                             const int64_t* __restrict__ pulls, const double* __restrict__ factors,
                             int64_t stride, double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
@@ -1352,7 +1376,7 @@ tiled_forward_update_kernel(const int* __restrict__ items, int begin, const int6
 
 // y_j -= U_p x_p + V_q^T x_q on tile rows i of j, columns [c0, c0 + 16 NQ).
 template <int NQ>
-__global__ void __launch_bounds__(kTT)
+__global__ void __launch_bounds__(kTT, 2)
 tiled_backward_update_kernel(const int* __restrict__ items, int begin, const int64_t* __restrict__ tasks,
                              const double* __restrict__ factors, int64_t stride,
                              double* __restrict__ rhs, int64_t rhs_stride, int nrhs) {
