@@ -5,6 +5,12 @@ columns, 20 layers of 0.5 m then 20 geometrically graded layers to 40 m depth (1
 4961 nodes, 9600 triangles), 48 surface electrodes at 2 m spacing from x = 13 m, and a
 dipole-dipole survey with a <= 6, n <= 8 (1232 rows; a <= 6, n <= 3 gives 612).
 
+``terrain_section`` + ``correlated_model`` build the 2.5D terrain workload: a 200 m x 50 m
+section of 40,000 P1 triangles under a surface that is a seeded sum of three sinusoids, interior
+node columns jittered so the mesh is not a columnar strip mesh, 96 surface electrodes at 1 m,
+2538 mixed Wenner-Schlumberger + dipole-dipole rows, and a log-normal resistivity with a 5 m
+correlation length.
+
 ``box_section`` + ``grid_survey`` + ``ellipsoid_model`` build the 3D workload: a 60 m x 40 m x
 20 m box of structured tetrahedra (60 x 40 x 17 hexahedra of six tetrahedra: 244,800 cells,
 45,018 nodes), a 12 x 8 surface grid of electrodes at 4 m spacing, 4000 dipole-dipole rows
@@ -131,3 +137,71 @@ def ellipsoid_model(nodes, cells, seed: int, footprint=((8.0, 52.0), (6.0, 34.0)
         inside = np.sum(((centers - c) / axes) ** 2, axis=1) <= 1.0
         rho[inside] = 10.0 ** rng.uniform(1.0, 3.0)
     return (1.0 / rho).astype(np.float32)
+
+
+def wenner_schlumberger(count: int, max_a: int, max_n: int) -> np.ndarray:
+    """ABMN rows A = i, M = i + n a, N = i + (n + 1) a, B = i + (2n + 1) a."""
+
+    rows = [
+        (i, i + (2 * n + 1) * a, i + n * a, i + (n + 1) * a)
+        for a in range(1, max_a + 1)
+        for n in range(1, max_n + 1)
+        for i in range(count)
+        if i + (2 * n + 1) * a < count
+    ]
+    return np.asarray(rows, dtype=np.int64).reshape(-1, 4)
+
+
+def terrain_section(seed: int = 7):
+    """The terrain workload: (nodes, cells, surface node ids, electrode positions, ABMN rows).
+
+    x from 0 to 200 m in 1 m columns, 100 layers graded from 0.2 m at the surface to 50 m depth,
+    each quad split into two triangles (40,000 cells); the surface is z(x) = sum_i A_i sin(2 pi x
+    / L_i + p_i) with A_i ~ U(0, 5/3) m, L_i ~ U(20, 100) m, p_i ~ U(0, 2 pi), every layer
+    follows it, and interior nodes move by U(-0.05, 0.05) m in x. Electrodes: the 96 surface
+    nodes from x = 52 m; rows: Wenner-Schlumberger a <= 2, n <= 6 and dipole-dipole a <= 3,
+    n <= 6 (2538).
+    """
+
+    rng = np.random.default_rng(seed)
+    xs = np.arange(201, dtype=float)
+    steps = np.geomspace(0.2, 1.0, 100)
+    depths = np.concatenate(([0.0], np.cumsum(steps * 50.0 / steps.sum())))
+    amp, length, phase = rng.uniform(0.0, 5.0 / 3.0, 3), rng.uniform(20.0, 100.0, 3), rng.uniform(0.0, 2 * np.pi, 3)
+
+    def surface(x):
+        return sum(a * np.sin(2 * np.pi * x / w + p) for a, w, p in zip(amp, length, phase))
+
+    gx, gd = np.meshgrid(xs, depths)
+    gz = surface(gx) - gd
+    jitter = rng.uniform(-0.05, 0.05, gx.shape)
+    jitter[0, :] = jitter[-1, :] = jitter[:, 0] = jitter[:, -1] = 0.0  # surface, base and sides stay
+    nodes = np.column_stack(((gx + jitter).ravel(), gz.ravel()))
+    index = np.arange(nodes.shape[0]).reshape(gx.shape)
+    ul, ur = index[:-1, :-1].ravel(), index[:-1, 1:].ravel()
+    ll, lr = index[1:, :-1].ravel(), index[1:, 1:].ravel()
+    cells = np.stack((np.stack((ul, ll, ur), 1), np.stack((ur, ll, lr), 1)), 1).reshape(-1, 3)
+    surface_ids = index[0]
+    electrodes = nodes[surface_ids[52:148]]
+    rows = np.concatenate((wenner_schlumberger(96, 2, 6), dipole_dipole(96, 3, 6)))
+    return nodes, cells.astype(np.int64), surface_ids.astype(np.int64), electrodes, rows
+
+
+def correlated_model(nodes, cells, seed: int, correlation: float = 5.0, spacing: float = 0.5) -> np.ndarray:
+    """Float32 conductivity 1 / rho with log10 rho ~ N(2, 0.4^2): white noise on a ``spacing`` grid
+    over the mesh's bounding box, Gaussian-filtered in Fourier space to the ``correlation`` length,
+    rescaled to unit variance and sampled at the nearest grid point of every cell centroid."""
+
+    rng = np.random.default_rng(seed)
+    lo, hi = nodes.min(axis=0), nodes.max(axis=0)
+    shape = tuple(int(np.ceil((h - l) / spacing)) + 1 for l, h in zip(lo, hi))
+    noise = rng.standard_normal(shape)
+    kx = np.fft.fftfreq(shape[0], spacing)[:, None]
+    kz = np.fft.fftfreq(shape[1], spacing)[None, :]
+    kernel = np.exp(-2.0 * (np.pi * correlation) ** 2 * (kx ** 2 + kz ** 2))
+    field = np.real(np.fft.ifft2(np.fft.fft2(noise) * kernel))
+    field = (field - field.mean()) / field.std()
+    centers = nodes[cells].mean(axis=1)
+    ij = np.clip(np.rint((centers - lo) / spacing).astype(int), 0, np.array(shape) - 1)
+    log_rho = 2.0 + 0.4 * field[ij[:, 0], ij[:, 1]]
+    return (1.0 / 10.0 ** log_rho).astype(np.float32)

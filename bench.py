@@ -14,6 +14,13 @@ quadrature + ABMN measurement, and the 1232 x 9600 normal-quadrupole Jacobian.
   the page-locked result buffers, whose first allocation is a one-time cost.
 * ``--impl reference``: the reference's CPU path (FP64 oracle fields + the C restatement of the
   reference kernel on all host threads), one model per step.
+* ``--workload terrain``: the same metric on the 2.5D terrain section (200 m x 50 m, 40,000 P1
+  triangles under a three-sinusoid surface with jittered interior columns, 96 electrodes at 1 m,
+  2538 Wenner-Schlumberger + dipole-dipole rows, numerical geometric factors, 19 wavenumbers;
+  fields on the H2-refined discretization of 160,000 triangles, 80,601 dofs); a step is one fresh
+  correlated log-normal model's fields and the 2538 x 40,000 Jacobian summed from the refined
+  cells. The line also carries the exact vjp and jvp times. No CPU baseline is run (the
+  reference's set-up alone solves 19 x 96 systems of 321,201 dofs).
 * ``--workload box3d``: the same metric for the 3D operator (``ERTForward3D.jacobian(sigma,
   batch_size=32)``, series_batch_steps=1): 60 m x 40 m x 20 m box of 244,800 P1 tetrahedra,
   12 x 8 surface electrodes, 4000 dipole-dipole rows (192 field columns with singularity
@@ -55,9 +62,11 @@ def parse_args():
     parser.add_argument("--e2e-steps", type=int, default=None)
     parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg (profiling runs)")
-    parser.add_argument("--workload", choices=("flat", "box3d", "box3d-small"), default="flat",
-                        help="flat: the 2.5D headline section; box3d: the 3D box (244,800 tetrahedra, 96 electrodes, "
-                             "4000 rows); box3d-small: the same survey on 36,000 tetrahedra (profiling captures)")
+    parser.add_argument("--workload", choices=("flat", "terrain", "box3d", "box3d-small"), default="flat",
+                        help="flat: the 2.5D headline section; terrain: the 2.5D terrain section (40,000 triangles, "
+                             "96 electrodes, 2538 rows, numerical geometric factors); box3d: the 3D box (244,800 "
+                             "tetrahedra, 96 electrodes, 4000 rows); box3d-small: the same survey on 36,000 "
+                             "tetrahedra (profiling captures)")
     return parser.parse_args()
 
 
@@ -170,6 +179,9 @@ def run_reference(args, rank: int, world: int) -> dict:
     from oracle import baseline
     from oracle.ert2p5d import Oracle2p5D
 
+    if args.workload == "terrain":
+        return {"impl": "reference", "unavailable": "no CPU run of the terrain workload: the reference's set-up "
+                                                    "alone solves 19 x 96 FP64 systems of 321,201 dofs"}
     if args.workload in BOX3D:
         nodes, cells, electrodes, rows = box3d_workload(args.workload)
         base = box3d_cpu_baseline(nodes, cells, electrodes, rows)
@@ -227,6 +239,186 @@ def config(D, C, W, E, world) -> dict:
         "l2": "flushed between steps (256 MiB write, outside the timed events)",
         "parallelism": f"replicas x{world} (independent models per rank)",
     }
+
+
+def terrain_config(D, C, N, W, E, world) -> dict:
+    return {
+        "workload": f"2.5D terrain jacobian(): {C} P1 triangles (H2-refined to {4 * C}, {N} dofs), {E} electrodes, "
+                    f"{D} Wenner-Schlumberger + dipole-dipole rows, {W} wavenumbers, numerical geometric factors; "
+                    f"fresh model per step",
+        "rows": D,
+        "cells": C,
+        "dofs": N,
+        "wavenumbers": W,
+        "electrodes": E,
+        "l2": "inputs larger than L2 (19 x 80,601 x 96 fields, the 406 MB Jacobian); no flush",
+        "parallelism": f"replicas x{world} (independent models per rank)",
+    }
+
+
+def run_terrain(args, rank: int, world: int) -> dict | None:
+    from adtlert_b200 import ERTForward2p5D, Mesh, Survey, _native, synthetic
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    nodes, cells, surface, electrodes, rows = synthetic.terrain_section()
+    forward = ERTForward2p5D.from_mesh_survey(Mesh.from_arrays(nodes, cells, surface_node_ids=surface),
+                                              Survey.from_arrays(electrodes, rows),
+                                              topographic_geometric_factor_mode="numerical")
+    lib, plan = forward._lib, forward._plan
+    W, N, E, D, C, Cd = forward.W, forward.N, forward.E, forward.D, forward.C, forward.Cd
+    stream = torch.cuda.current_stream(device)
+    handle = _native.stream_handle(device)
+    models = torch.as_tensor(np.stack([synthetic.correlated_model(nodes, cells, 1000 * rank + i)
+                                       for i in range(args.warmup + args.steps)]), device=device)
+    fields = torch.empty((1, W, N, E), dtype=torch.float32, device=device)
+    normal = torch.empty((1, D), dtype=torch.float64, device=device)
+    recip = torch.empty_like(normal)
+    Jd = torch.empty((D, Cd), dtype=torch.float32, device=device)
+    columns = forward._columns(None, None, discretization=True)
+    slot = 15
+
+    def call(name, *a):
+        _native.check(getattr(lib, name)(plan, *a), plan, name)
+
+    def sensitivity(i):
+        call("adt_normal_jacobian", _native.ptr(fields), 0, D, _native.ptr(Jd), handle)
+        forward._aggregate(Jd, columns)
+
+    stages = (
+        ("factorize", lambda i: call("adt_factorize_fields", slot, _native.ptr(models[i]), 1, handle)),
+        ("solve_fields", lambda i: call("adt_solve_fields", slot, _native.ptr(models[i]), 1, _native.ptr(fields), handle)),
+        ("measure", lambda i: call("adt_measure", _native.ptr(fields), 1, _native.ptr(normal), _native.ptr(recip), None,
+                                   handle)),
+        ("normal_jacobian", sensitivity),
+    )
+    result = timed_stages(args, rank, world, forward, stages, device, stream)
+    if result is None:
+        return None
+    value_s, stage_ms, stage_launches, clock, launches = result
+    info = forward.plan_info
+    K, R = 3, info["features"]
+    algorithmic = {
+        # J on the refined cells written, summed into model cells; fields, dofs, factors, ABMN read
+        "normal_jacobian": 4 * D * Cd + 4 * D * Cd + 4 * D * C + 4 * W * N * E + 4 * K * Cd + 4 * R * K * Cd + 16 * D,
+        "factorize": 8 * W * info["nnz"] + 8 * W * info["factor_doubles_per_system"] + 8 * W * N * E,
+        "solve_fields": 8 * W * info["factor_doubles_per_system"] + 2 * 8 * W * N * E + 4 * W * N * E,
+        "measure": 4 * W * E * E * 3 + 16 * D,
+    }
+    peaks = measured_peaks()
+
+    def roofline(name):
+        count = max(1, stage_launches[name])
+        per_launch_s = stage_ms[name] / 1e3 / count
+        achieved = algorithmic[name] / count / per_launch_s / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": name,
+                "algorithmic_bytes_per_launch": algorithmic[name] / count, "launch_ms": per_launch_s * 1e3,
+                "peak_source": peaks["source"]}
+
+    # exact derivatives of the resistances through the public API (factorization cached)
+    sigma = models[args.warmup].cpu()
+    g = torch.as_tensor(np.random.default_rng(5).standard_normal(D))
+    delta = sigma * torch.as_tensor(np.random.default_rng(6).standard_normal(C) * 1e-2, dtype=torch.float32)
+    forward.vjp(sigma, g), forward.jvp(sigma, delta)
+    torch.cuda.synchronize(device)
+    start = time.perf_counter()
+    forward.vjp(sigma, g)
+    torch.cuda.synchronize(device)
+    vjp_ms = 1e3 * (time.perf_counter() - start)
+    start = time.perf_counter()
+    forward.jvp(sigma, delta)
+    torch.cuda.synchronize(device)
+    jvp_ms = 1e3 * (time.perf_counter() - start)
+
+    e2e_steps = args.e2e_steps or 3
+    e2e_warmup = max(args.warmup, forward.normal_field_cache_max_entries + 2)
+    host_models = [torch.as_tensor(synthetic.correlated_model(nodes, cells, 50_000 + 1000 * rank + i)).pin_memory()
+                   for i in range(e2e_steps + e2e_warmup)]
+    for i in range(e2e_warmup):
+        out = forward.jacobian(host_models[i])
+    torch.cuda.synchronize(device)
+    barrier(world)
+    start = time.perf_counter()
+    for i in range(e2e_steps):
+        out = forward.jacobian(host_models[e2e_warmup + i])
+    torch.cuda.synchronize(device)
+    e2e_time = max_over_ranks(time.perf_counter() - start, world)
+    assert out.shape == (D, C)
+    if rank != 0:
+        return None
+    return {
+        "metric": "jacobian_entries_per_second",
+        "value": world * D * C * args.steps / value_s,
+        "unit": "entries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * value_s / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 fields / f64 factorization",
+        "data": "synthetic (seeded log-normal resistivity, 5 m correlation length)",
+        "config": terrain_config(D, C, N, W, E, world),
+        "roofline": roofline(max(stage_ms, key=stage_ms.get)),
+        "sensitivity_roofline": roofline("normal_jacobian"),
+        "stages_ms": stage_ms,
+        "vjp_ms": vjp_ms,
+        "jvp_ms": jvp_ms,
+        "clocks": clock,
+        "e2e": {"value": world * D * C * e2e_steps / e2e_time, "unit": "entries/s", "h2d_bytes_per_step": 4 * C,
+                "d2h_bytes_per_step": 4 * D * C + 1, "ms_per_step": 1e3 * e2e_time / e2e_steps,
+                "warmup_calls": e2e_warmup},
+        "gpu_launches": int(launches),
+        "cpu_baseline": None,
+    }
+
+
+def timed_stages(args, rank, world, forward, stages, device, stream):
+    """Warm-up, the timed steps (CUDA events per step, max over ranks) and a per-stage breakdown:
+    (elapsed seconds, stage ms, stage launches, clock summary, launches in the timed region)."""
+
+    def step(i):
+        for _, fn in stages:
+            fn(i)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    torch.cuda.synchronize(device)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = forward.kernel_launches()
+    with ClockSampler(device.index) as clocks:
+        for k in range(args.steps):
+            events[k][0].record(stream)
+            step(args.warmup + k)
+            events[k][1].record(stream)
+        torch.cuda.synchronize(device)
+    launches = forward.kernel_launches() - launches0
+    barrier(world)
+    torch.cuda.synchronize(device)
+    elapsed = max_over_ranks(sum(a.elapsed_time(b) for a, b in events) / 1e3, world)
+    clock = clocks.summary()
+    stage_ms, stage_launches = {}, {}
+    for name, fn in stages:
+        total = 0.0
+        for k in range(3):
+            i = args.warmup + (k % args.steps)
+            for other_name, other in stages:
+                if other_name == name:
+                    break
+                other(i)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            before = forward.kernel_launches()
+            a.record(stream)
+            fn(i)
+            b.record(stream)
+            stage_launches[name] = forward.kernel_launches() - before
+            torch.cuda.synchronize(device)
+            total += a.elapsed_time(b)
+        stage_ms[name] = total / 3
+    return elapsed, stage_ms, stage_launches, clock, launches
 
 
 BOX3D = {"box3d": (60, 40, 17), "box3d-small": (30, 20, 10)}
@@ -614,7 +806,12 @@ def main():
             print(json.dumps(run_reference(args, rank, world)), flush=True)
         return
     rank, world = dist_setup(args)
-    result = run_box3d(args, rank, world) if args.workload in BOX3D else run_b200(args, rank, world)
+    if args.workload in BOX3D:
+        result = run_box3d(args, rank, world)
+    elif args.workload == "terrain":
+        result = run_terrain(args, rank, world)
+    else:
+        result = run_b200(args, rank, world)
     if result is not None:
         print(json.dumps(result), flush=True)
     if world > 1:
