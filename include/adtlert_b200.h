@@ -167,11 +167,13 @@ adt_status adt_integrated_potentials(adt_plan* plan, const float* fields, float*
 /* Normal-quadrupole sensitivity rows [row_begin, row_begin+row_count) of one model,
  * out[d][c] = -sum_w w_w (u_M - u_N)^T (K_c + k_w^2 M_c) (u_A - u_B) over discretization cells.
  * Replaces: normal_sensitivity (adtlert/forward/kernels.py:132-268) as called by
- * _normal_jacobian (ert2p5d.py:984-1010). The electrode Grams run on the tensor cores (tcgen05,
- * TF32 with a hi/lo split) for up to 64 electrodes, otherwise (or when the environment variable
- * ADTLERT_B200_JACOBIAN=fma is set at plan creation) on FP32 FMA. A tensor-core launch whose
- * MMAs do not complete within its bounded wait writes NaN into its cells' columns, and the
- * plan's next adt_normal_jacobian call returns ADT_TIMEOUT. */
+ * _normal_jacobian (ert2p5d.py:984-1010). Single-wavenumber (3D) operators compute every entry
+ * directly from per-cell features (no electrode Gram); otherwise the electrode Grams run on the
+ * tensor cores (tcgen05, TF32 with a hi/lo split) for up to 64 field columns, else on FP32 FMA.
+ * The environment variable ADTLERT_B200_JACOBIAN, read at plan creation, overrides the choice:
+ * "fma" takes the FP32 Gram kernel everywhere, "tc" the tensor cores wherever they apply. A
+ * tensor-core launch whose MMAs do not complete within its bounded wait writes NaN into its
+ * cells' columns, and the plan's next adt_normal_jacobian call returns ADT_TIMEOUT. */
 adt_status adt_normal_jacobian(adt_plan* plan, const float* fields, int32_t row_begin,
                                int32_t row_count, float* jacobian, adt_stream stream);
 
