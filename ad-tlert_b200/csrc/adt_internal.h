@@ -127,6 +127,7 @@ struct adt_plan {
   bool tiled = false;
   int* titems = nullptr;
   std::vector<int> tranges, panel_ptr;
+  std::vector<int> panel_width;  // per tiled item range: widest column panel of its items (0: not a panel)
   // primary field
   double* primary = nullptr;    // [W][N][E] solver order
   double* refrhs = nullptr;     // [W][N][E]

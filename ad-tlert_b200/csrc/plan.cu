@@ -399,6 +399,16 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   p->tiled = hp.tiled;
   p->tranges = hp.tranges;
   p->panel_ptr = hp.panel_ptr;
+  // the column width of every panel range: min(64, m_j - 64 k) over its items' tasks
+  p->panel_width.assign(hp.tranges.size() / 2, 0);
+  for (int level = 0; hp.tiled && level < hp.levels; ++level)
+    for (int k = 0; k < hp.panel_ptr[level + 1] - hp.panel_ptr[level]; ++k) {
+      const int r = 3 * hp.levels + hp.panel_ptr[level] + k;
+      for (int it = hp.tranges[2 * r]; it < hp.tranges[2 * r + 1]; ++it) {
+        const int64_t mj = hp.task_rows[(size_t)hp.titems[4 * (size_t)it] * T_FIELDS + T_MJ];
+        p->panel_width[r] = std::max<int>(p->panel_width[r], (int)std::min<int64_t>(kTile, mj - (int64_t)kTile * k));
+      }
+    }
   ADT_UP(&p->owners, hp.bowners);
   p->nfixed = (int)hp.fixed.size();
   if (p->tiled && cudaMalloc(&p->partials, sizeof(double) * 2 * (size_t)p->sms * kTile * kTile) != cudaSuccess)

@@ -1171,11 +1171,12 @@ __device__ __forceinline__ int update_chunks(const TaskView& v, int seg, int k, 
 }
 
 // Panel k update of tile (i, k) of segment seg: acc = row_i(c < 64k) row_k^T (+ the Schur pulls
-// for rows of j). With `splits` == 1 the block subtracts acc from the tile and, for the diagonal
+// for rows of j), 64 rows by the panel's 16 NQ columns. With `splits` == 1 the block subtracts acc from the tile and, for the diagonal
 // item, factors it. With splits > 1 the item's depth chunks are divided evenly over blockIdx.z
 // and each block stores its partial acc in `partials` (tile (item, z) of the launch: rows < ni,
 // columns < mk at [((system * items + item) * splits + z) * 4096 + a * 64 + b]); the diagonal
 // and triangular-solve launches sum them.
+template <int NQ>
 __global__ void __launch_bounds__(kTT)
 tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                     const int64_t* __restrict__ pulls, double* __restrict__ factors, int64_t stride,
@@ -1188,7 +1189,7 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
   const int seg = it[1], i = it[2];
   double* f = factors + (int64_t)blockIdx.y * stride;
   const int ni = min(kTile, v.rows(seg) - kTile * i), mk = min(kTile, v.mj - kTile * k);
-  double acc[4][4];
+  double acc[4][NQ];  // columns of the panel: 16 NQ >= its width
   zero_acc(acc);
   // this block's chunk range [lo, hi) of the item's depth chunks (all of them when unsplit)
   int lo = 0, hi = 1 << 30;
@@ -1488,11 +1489,19 @@ constexpr size_t kTileSolveSmem = sizeof(double) * 3 * kTile * kTLD;
 constexpr size_t kSubstituteSmem = sizeof(double) * (2 * kTile * kTLD + kTile) + kGemmSmem;
 
 void configure_tiled() {
-  cudaFuncSetAttribute(tiled_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
+  for (auto kernel : {tiled_update_kernel<4>, tiled_update_kernel<2>, tiled_update_kernel<1>})
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem);
   cudaFuncSetAttribute(tiled_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSolveSmem);
   cudaFuncSetAttribute(tiled_diagonal_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem);
   for (auto kernel : {tiled_substitute_kernel<4>, tiled_substitute_kernel<2>, tiled_substitute_kernel<1>})
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSubstituteSmem);
+}
+
+template <typename F>
+void with_strip(int nq, F&& f) {
+  if (nq == 4) f(std::integral_constant<int, 4>());
+  else if (nq == 2) f(std::integral_constant<int, 2>());
+  else f(std::integral_constant<int, 1>());
 }
 
 // Depth splits of a panel launch of `tiles` items x `systems`: 1 when the launch fills the GPU
@@ -1514,11 +1523,16 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
     p->launches++;
     const int t0 = p->level_begin[level], level_tasks = p->level_begin[level + 1] - t0;
     for (int k = 0; k < p->panel_ptr[level + 1] - p->panel_ptr[level]; ++k) {
-      auto [pb, pe] = range(3 * L + p->panel_ptr[level] + k);
+      const auto [rb, re] = range(3 * L + p->panel_ptr[level] + k);
+      const int pb = rb, pe = re;
       if (pe == pb) continue;
       const int splits = panel_splits(pe - pb, systems, p->sms);
-      launch_chained(tiled_update_kernel, dim3(pe - pb, systems, splits), kTT, kUpdateSmem, s, p->titems, pb, k, p->tasks,
-                     p->pulls, factors, p->factor_stride, splits, p->partials, p->inverses, t0, level_tasks);
+      const int width = p->panel_width[3 * L + p->panel_ptr[level] + k];
+      with_strip(width <= 16 ? 1 : width <= 32 ? 2 : 4, [&](auto nq) {
+        launch_chained(tiled_update_kernel<nq()>, dim3(pe - pb, systems, splits), kTT, kUpdateSmem, s, p->titems, pb, k,
+                       p->tasks, p->pulls, factors, p->factor_stride, splits, p->partials, p->inverses, t0,
+                       level_tasks);
+      });
       if (splits > 1) {
         launch_chained(tiled_diagonal_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks,
                        factors, p->factor_stride, splits, (const double*)p->partials, p->inverses, t0, level_tasks);
@@ -1539,19 +1553,15 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
 }
 
 // Column strip of the tiled solve launches, in units of 16 columns (4: a full tile), narrowed
-// while the launch would leave most SMs idle.
+// while the launch would leave most SMs idle. (Narrowing a launch that fills the GPU to pad
+// fewer columns, e.g. 96 as three strips of 32, was measured slower: 32.8 -> 36.8 ms at the
+// terrain section.)
 int tiled_strip(int blocks, int nrhs, int sms) {
   int nq = 4;
   while (nq > 1 && (int64_t)blocks * ((nrhs + 16 * nq - 1) / (16 * nq)) < 2 * (int64_t)sms) nq /= 2;
   return nq;
 }
 
-template <typename F>
-void with_strip(int nq, F&& f) {
-  if (nq == 4) f(std::integral_constant<int, 4>());
-  else if (nq == 2) f(std::integral_constant<int, 2>());
-  else f(std::integral_constant<int, 1>());
-}
 
 void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, double* rhs, cudaStream_t s) {
   const int L = p->levels;
