@@ -29,6 +29,8 @@ SYMBOLS = (
     "adt_solve_fields",
     "adt_solve",
     "adt_factorize_wavenumbers",
+    "adt_forward",
+    "adt_jacobian",
     "adt_measure",
     "adt_integrated_potentials",
     "adt_normal_jacobian",
@@ -128,6 +130,8 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_solve_fields": (status, [_p, _i32, _p, _i32, _p, _p]),
         "adt_solve": (status, [_p, _i32, _i32, _i32, _p, _p]),
         "adt_factorize_wavenumbers": (status, [_p, _i32, _p, _i32, _i32, _p]),
+        "adt_forward": (status, [_p, _i32, _p, _i32, _p, _p, _p, _p]),
+        "adt_jacobian": (status, [_p, _i32, _p, _p, _i32, _i32, _p, _p]),
         "adt_measure": (status, [_p, _p, _i32, _p, _p, _p, _p]),
         "adt_integrated_potentials": (status, [_p, _p, _p, _p]),
         "adt_normal_jacobian": (status, [_p, _p, _i32, _i32, _p, _p]),

@@ -696,6 +696,20 @@ adt_status adt_solve(adt_plan* p, int32_t slot, int32_t systems, int32_t nrhs, d
   return check_launch(p, "solve");
 }
 
+adt_status adt_forward(adt_plan* p, int32_t slot, const float* sigma, int32_t models, float* fields,
+                       double* normal, double* reciprocal, adt_stream stream) {
+  if (adt_status st = adt_factorize_fields(p, slot, sigma, models, stream)) return st;
+  if (adt_status st = adt_solve_fields(p, slot, sigma, models, fields, stream)) return st;
+  return adt_measure(p, fields, models, normal, reciprocal, nullptr, stream);
+}
+
+adt_status adt_jacobian(adt_plan* p, int32_t slot, const float* sigma, float* fields, int32_t row_begin,
+                        int32_t row_count, float* jacobian, adt_stream stream) {
+  if (adt_status st = adt_factorize_fields(p, slot, sigma, 1, stream)) return st;
+  if (adt_status st = adt_solve_fields(p, slot, sigma, 1, fields, stream)) return st;
+  return adt_normal_jacobian(p, fields, row_begin, row_count, jacobian, stream);
+}
+
 adt_status adt_measure(adt_plan* p, const float* fields, int32_t models, double* normal,
                        double* reciprocal, double* potentials, adt_stream stream) {
   if (!p || !fields || !normal || !reciprocal || models <= 0)

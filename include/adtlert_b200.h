@@ -155,6 +155,20 @@ adt_status adt_factorize_wavenumbers(adt_plan* plan, int32_t slot, const float* 
 adt_status adt_solve(adt_plan* plan, int32_t slot, int32_t systems, int32_t nrhs, double* rhs,
                      adt_stream stream);
 
+/* One call for the forward of S models: adt_factorize_fields + adt_solve_fields into `fields`
+ * [S][W][N][E] + adt_measure (normal and reciprocal resistances [S][D], float64). The slot keeps
+ * the factorization, so adt_vjp / adt_jvp / adt_adjoint_jacobian may follow. Replaces: the
+ * field and measurement phases of solve() / resistance() (adtlert/forward/ert2p5d.py:532-589). */
+adt_status adt_forward(adt_plan* plan, int32_t slot, const float* sigma, int32_t models, float* fields,
+                       double* normal, double* reciprocal, adt_stream stream);
+
+/* One call for the normal Jacobian of one model: adt_factorize_fields + adt_solve_fields into
+ * `fields` [W][N][E] + adt_normal_jacobian of rows [row_begin, row_begin+row_count) into
+ * jacobian [row_count][C]. Replaces: jacobian(conductivity) with the default normal sensitivity
+ * (adtlert/forward/ert2p5d.py:971-1010) up to the host copy. */
+adt_status adt_jacobian(adt_plan* plan, int32_t slot, const float* sigma, float* fields, int32_t row_begin,
+                        int32_t row_count, float* jacobian, adt_stream stream);
+
 /* Normal and reciprocal transfer resistances of S models (and, if not NULL, the E*E electrode
  * potentials per model). Replaces: _integrate + _normal_reciprocal (ert2p5d.py:560-589). */
 adt_status adt_measure(adt_plan* plan, const float* fields, int32_t models, double* normal,

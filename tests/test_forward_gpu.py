@@ -284,3 +284,35 @@ def test_fused_forward_substitution_gives_the_two_phase_fields():
     for name, value in (("fused", fused), ("again", again), ("elsewhere", elsewhere)):
         assert torch.isfinite(value).all()
         assert_close(value, two_phase, 1e-6, f"{name} fields vs factorize + solve_fields")
+
+
+def test_one_call_forward_and_jacobian_entry_points():
+    """adt_forward / adt_jacobian equal the step-by-step calls they compose, bitwise."""
+
+    from adtlert_b200 import _native
+
+    nodes, cells, electrodes, rows = synthetic.flat_section()
+    forward = ERTForward2p5D.from_mesh_survey(Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, rows))
+    W, N, E, D, C = forward.W, forward.N, forward.E, forward.D, forward.C
+    models = torch.as_tensor(np.stack([synthetic.layered_model(nodes, cells, s) for s in (4, 5)]), device="cuda")
+    handle = forward._stream()
+
+    def run(name, *args):
+        forward._call(name, *args)
+
+    fields = torch.empty((2, W, N, E), device="cuda")
+    normal = torch.empty((2, D), dtype=torch.float64, device="cuda")
+    recip = torch.empty_like(normal)
+    run("adt_forward", 14, _native.ptr(models), 2, _native.ptr(fields), _native.ptr(normal), _native.ptr(recip), handle)
+    fields2, normal2, recip2 = torch.empty_like(fields), torch.empty_like(normal), torch.empty_like(recip)
+    run("adt_factorize_fields", 13, _native.ptr(models), 2, handle)
+    run("adt_solve_fields", 13, _native.ptr(models), 2, _native.ptr(fields2), handle)
+    run("adt_measure", _native.ptr(fields2), 2, _native.ptr(normal2), _native.ptr(recip2), None, handle)
+    assert torch.equal(fields, fields2) and torch.equal(normal, normal2) and torch.equal(recip, recip2)
+
+    one = models[1]
+    J = torch.empty((D - 10, C), device="cuda")
+    run("adt_jacobian", 14, _native.ptr(one), _native.ptr(fields[0]), 10, D - 10, _native.ptr(J), handle)
+    expected = torch.empty_like(J)
+    run("adt_normal_jacobian", _native.ptr(fields2[1]), 10, D - 10, _native.ptr(expected), handle)
+    assert torch.equal(J, expected)
