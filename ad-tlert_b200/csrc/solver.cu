@@ -923,7 +923,7 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
 constexpr int kTT = kSolverThreads;  // threads of the tiled kernels (16 x 16 micro-tile grid)
 constexpr int kKC = 16;              // reduction depth staged per step
 constexpr int kTLD = kTile + 1;      // leading dimension of the shared tiles
-constexpr int kSLD = kTile + 8;      // leading dimension of the GEMM staging tiles (== 8 mod 16)
+constexpr int kSLD = kTile + 4;      // leading dimension of the GEMM staging tiles (== 4 mod 16)
 constexpr int kStage = 4 * kKC * kSLD;  // doubles of GEMM staging (two buffers of A and B chunks)
 
 // Element (a, c) of a strided operand: base[a * rs + c * cs].
@@ -962,7 +962,7 @@ struct StagePlan {
       const int a = depth_fast ? idx / kKC : idx % SPAN;
       const int c = depth_fast ? idx % kKC : idx / SPAN;
       const bool used = idx < kKC * SPAN;
-      dst[e] = c * kSLD + a;
+      dst[e] = c * kSLD + a;  // see gemm_nt
       depth_of[e] = used && a < rows ? c : -1;
       src[e] = op.base + (int64_t)a * op.rs + (int64_t)(d0 + c) * op.cs;
     }
@@ -982,10 +982,14 @@ struct StagePlan {
 // < rb (d0 a multiple of kKC); the output has 64 rows and 16 NQ columns. The products run on
 // the FP64 tensor cores (mma.sync m8n8k4): warp w owns rows 16 (w & 3) + [0, 16) and columns
 // 8 NQ (w >> 2) + [0, 8 NQ) as 2 x NQ tiles of 8 x 8; the fragments are added to `acc` through
-// shared memory at the end. Operand chunks are staged depth-major (tile[c][a], leading
-// dimension 72, so a fragment load of 4 depths x 8 rows takes two wavefronts) with cp.async,
-// double-buffered. `sm` holds kStage doubles; entered and left by all threads (ends with a
-// barrier).
+// shared memory at the end. Operand chunks are staged depth-major with cp.async,
+// double-buffered: element (a, c) at tile[c * 68 + a]. 8-byte accesses are served per half-warp,
+// and with a leading dimension of 4 mod 16 doubles the 4 depths x 4 rows of a half-warp's
+// fragment load hit 16 distinct banks. (The leading dimension 72, with 2-way conflicted
+// fragment loads, was 10 % slower on the terrain section; an XOR swizzle of the rows by depth,
+// which spreads the staging writes of depth-contiguous operands, was slower again there and
+// gained 1 ms at the 3D box.) `sm` holds kStage doubles; entered and left by all threads (ends
+// with a barrier).
 template <int NQ>
 __device__ void gemm_nt(double (&acc)[4][NQ], const Operand& A, int ra, const Operand& B, int rb,
                         int depth, double* sm, int d0 = 0) {
@@ -1017,15 +1021,16 @@ __device__ void gemm_nt(double (&acc)[4][NQ], const Operand& A, int ra, const Op
       async_wait<0>();
     }
     __syncthreads();
-    const double* at = a_tile(ch & 1) + t * kSLD + m0 + g;
-    const double* bt = b_tile(ch & 1) + t * kSLD + n0 + g;
+    const double* at = a_tile(ch & 1) + t * kSLD + m0;
+    const double* bt = b_tile(ch & 1) + t * kSLD + n0;
 #pragma unroll
     for (int k = 0; k < kKC; k += 4) {
+      const int row = k * kSLD + g;
       double a[2], b[NQ];
 #pragma unroll
-      for (int i = 0; i < 2; ++i) a[i] = at[k * kSLD + 8 * i];
+      for (int i = 0; i < 2; ++i) a[i] = at[row + 8 * i];
 #pragma unroll
-      for (int j = 0; j < NQ; ++j) b[j] = bt[k * kSLD + 8 * j];
+      for (int j = 0; j < NQ; ++j) b[j] = bt[row + 8 * j];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
