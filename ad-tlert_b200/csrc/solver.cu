@@ -1254,12 +1254,13 @@ tiled_update_kernel(const int* __restrict__ items, int begin, int k, const int64
 }
 
 // Split panels: the diagonal item adds its partials (stored negated, summed in split order) to
-// the lower triangle of the diagonal tile and factors it; the launch's other items return.
+// the lower triangle of the diagonal tile and factors it; the launch's other items return. (The
+// tiles below solve with L_kk by substitution: a split panel has few of them, and forming
+// L_kk^-1 here would lengthen the panel's critical path.)
 __global__ void __launch_bounds__(kTT)
 tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                       double* __restrict__ factors, int64_t stride, int splits,
-                      const double* __restrict__ partials, double* __restrict__ inverses, int t0,
-                      int level_tasks) {
+                      const double* __restrict__ partials) {
   chain_wait();
   extern __shared__ double sm[];
   const int* it = items + 4 * (begin + blockIdx.x);
@@ -1268,8 +1269,7 @@ tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int
   double* f = factors + (int64_t)blockIdx.y * stride;
   const int mk = min(kTile, v.mj - kTile * k);
   double* dm = sm;
-  double* x = dm + kTile * kTLD;
-  double* rinv = x + kTile * kTLD;
+  double* rinv = dm + kTile * kTLD;
   double* diag = f + v.loff + (int64_t)kTile * k * v.mj + kTile * k;
   const double* part = partials + (int64_t)(blockIdx.y * gridDim.x + blockIdx.x) * splits * kTile * kTile;
   for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
@@ -1285,12 +1285,12 @@ tiled_diagonal_kernel(const int* __restrict__ items, int begin, int k, const int
     const int r = idx / mk, col = idx - r * mk;
     diag[(int64_t)r * v.mj + col] = dm[r * kTLD + col];
   }
-  store_inverse(dm, rinv, x, mk, inverses + ((int64_t)blockIdx.y * level_tasks + (it[0] - t0)) * kTile * kTile);
 }
 
 // Tile (i, k) below the diagonal: X = T L_kk^-T, with T = the updated tile (plus the panel
-// update's partials when split) and L_kk^-1 from the panel's diagonal step, as one shared-memory
-// GEMM (rows of U_p^T / V_q and of L_j alike).
+// update's partials when split). Unsplit panels (many tiles) apply L_kk^-1 from the panel's
+// diagonal step as one shared-memory GEMM; split panels (few tiles) solve with L_kk by blocked
+// substitution. Rows of U_p^T / V_q and of L_j alike.
 __global__ void __launch_bounds__(kTT)
 tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64_t* __restrict__ tasks,
                     double* __restrict__ factors, int64_t stride, int splits,
@@ -1298,20 +1298,28 @@ tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64
                     int level_tasks) {
   chain_wait();
   extern __shared__ double sm[];
-  double* li = sm;                 // L_kk^-1
+  double* li = sm;                 // L_kk^-1 (unsplit) or L_kk (split)
   double* tt = li + kTile * kTLD;  // transposed tile
-  double* xo = tt + kTile * kTLD;  // result
+  double* xo = tt + kTile * kTLD;  // result (unsplit) or 1 / diag(L_kk) (split)
   const int* it = items + 4 * (begin + blockIdx.x);
   const TaskView v(tasks + (int64_t)it[0] * T_FIELDS);
   const int seg = it[1], i = it[2];
   if (seg == SEG_J && i == k) return;  // factored by the diagonal step
   double* f = factors + (int64_t)blockIdx.y * stride;
   const int mk = min(kTile, v.mj - kTile * k);
-  const double* inv = inverses + ((int64_t)blockIdx.y * level_tasks + (it[0] - t0)) * kTile * kTile;
-  for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
-    const int r = idx / kTile, c = idx - r * kTile;
-    li[r * kTLD + c] = inv[idx];
-    xo[r * kTLD + c] = 0.0;
+  if (splits == 1) {
+    const double* inv = inverses + ((int64_t)blockIdx.y * level_tasks + (it[0] - t0)) * kTile * kTile;
+    for (int idx = threadIdx.x; idx < kTile * kTile; idx += blockDim.x) {
+      const int r = idx / kTile, c = idx - r * kTile;
+      li[r * kTLD + c] = inv[idx];
+      xo[r * kTLD + c] = 0.0;
+    }
+  } else {
+    const double* diag = f + v.loff + (int64_t)kTile * k * v.mj + kTile * k;
+    for (int idx = threadIdx.x; idx < mk * mk; idx += blockDim.x) {
+      const int r = idx / mk, c = idx - r * mk;
+      li[r * kTLD + c] = diag[(int64_t)r * v.mj + c];
+    }
   }
   const int ni = min(kTile, v.rows(seg) - kTile * i);
   const Operand t = v.segment(f, seg, kTile * i, kTile * k);
@@ -1325,11 +1333,20 @@ tiled_factor_kernel(const int* __restrict__ items, int begin, int k, const int64
     tt[c * kTLD + a] = x;
   }
   __syncthreads();
-  tile_gemm<true, true>(xo, kTLD, tt, kTLD, li, kTLD, ni, mk, mk, 1.0);  // X[a][b] = sum_c T[a][c] Linv[b][c]
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
-    const int a = idx / mk, c = idx - a * mk;
-    tb[a * t.rs + c * t.cs] = xo[a * kTLD + c];
+  if (splits == 1) {
+    tile_gemm<true, true>(xo, kTLD, tt, kTLD, li, kTLD, ni, mk, mk, 1.0);  // X[a][b] = sum_c T[a][c] Linv[b][c]
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
+      const int a = idx / mk, c = idx - a * mk;
+      tb[a * t.rs + c * t.cs] = xo[a * kTLD + c];
+    }
+  } else {
+    reciprocal_diagonal(li, kTLD, mk, xo);
+    lower_solve(li, kTLD, xo, tt, kTLD, mk, ni);  // L_kk X^T = T^T
+    for (int idx = threadIdx.x; idx < ni * mk; idx += blockDim.x) {
+      const int a = idx / mk, c = idx - a * mk;
+      tb[a * t.rs + c * t.cs] = tt[c * kTLD + a];
+    }
   }
 }
 
@@ -1540,7 +1557,7 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
       });
       if (splits > 1) {
         launch_chained(tiled_diagonal_kernel, dim3(pe - pb, systems), kTT, kFactorSmem, s, p->titems, pb, k, p->tasks,
-                       factors, p->factor_stride, splits, (const double*)p->partials, p->inverses, t0, level_tasks);
+                       factors, p->factor_stride, splits, (const double*)p->partials);
         p->launches++;
       }
       launch_chained(tiled_factor_kernel, dim3(pe - pb, systems), kTT, kTileSolveSmem, s, p->titems, pb, k, p->tasks,

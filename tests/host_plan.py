@@ -416,14 +416,15 @@ def replay_factor_tiled(hp: HostPlan, values: np.ndarray, systems: int = 1, sms:
                 for n, ((t, _, _, _), (v, seg, i, idx, acc)) in enumerate(zip(items, updates)):
                     if seg == SEG_J and i == k:
                         ni, mk = acc.shape
-                        launch.item([idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx, inverse(t)])
+                        launch.item([idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
                 launch.check()
                 launch = _Launch("triangular solve")
                 for n, ((t, _, _, _), (v, seg, i, idx, acc)) in enumerate(zip(items, updates)):
                     if not (seg == SEG_J and i == k):
                         mk = min(TILE, v.mj - TILE * k)
                         ni = acc.shape[0]
-                        launch.item([inverse(t), idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
+                        didx = _strided(f, v.loff + TILE * k * v.mj + TILE * k, v.mj, 1, mk, mk, "diag")
+                        launch.item([didx, idx] + [partial(n, z, ni, mk) for z in range(splits)], [idx])
                 launch.check()
                 for v, seg, i, idx, acc in updates:
                     if seg == SEG_J and i == k:
