@@ -2,8 +2,9 @@
 
 Every product is checked with the reference test suite's metric (max-norm relative error,
 adtlert tests/test_forward_gpu.py:18-27) at the float32 tolerance of 1e-4, against (a) the
-reference's own float32 outputs on identical inputs and (b) the float64 oracle; relational checks (half-space, scaling, dot tests, finite differences, reciprocity,
-repeatability) follow the reference's tests.
+reference's own float32 outputs on identical inputs and (b) the float64 oracle; relational
+checks (half-space, scaling, dot tests, finite differences, reciprocity, repeatability) follow
+the reference's tests.
 """
 
 import numpy as np
