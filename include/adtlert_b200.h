@@ -8,7 +8,10 @@
  * the direct solver are host arrays copied into the plan once; the plan owns that device
  * memory. Every other array crossing this boundary is a caller-owned DEVICE pointer (for
  * example a PyTorch CUDA tensor); work is enqueued on the caller's stream and the entry points
- * return without synchronizing unless stated. Entry points are not thread-safe per plan.
+ * return without synchronizing unless stated. Entry points are not thread-safe per plan, and
+ * the work of one plan must be ordered on the GPU (one stream, or streams the caller
+ * synchronizes): factorizations share the plan's solver workspaces (split-depth partial tiles,
+ * diagonal-tile inverses) whatever their slot.
  *
  * Layouts (row-major, C order):
  *   sigma      [S][model_cells]                       float32 (conductivity, S models)
