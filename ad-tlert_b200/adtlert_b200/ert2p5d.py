@@ -739,7 +739,7 @@ class ERTForward2p5D:
             include_robin_boundary_derivative=include_robin_boundary_derivative,
             normal_sensitivity=normal_sensitivity, jacobian_cell_parameter_ids=jacobian_cell_parameter_ids,
             jacobian_parameter_count=jacobian_parameter_count)
-        return response, _to_host(jacobian).to(self.dtype)
+        return response, _to_host(jacobian.to(self.dtype))  # widened on the device: exact, and cheaper
 
     def _solve_with_jacobian_device(self, conductivity, currents=1.0, *, batch_size=None,
                                     include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
@@ -779,7 +779,10 @@ class ERTForward2p5D:
         with self._deferred_checks():
             fields = self._fields(conductivity)
             columns = self._columns(None, None, discretization=True)
-            host = self._jacobian_to_host(fields) if columns is None else _to_host(self._jacobian_device(fields, columns))
+            if columns is None:
+                host = self._jacobian_to_host(fields)
+            else:  # float64 results (terrain) are widened on the device, not over the host's memory
+                host = _to_host(self._jacobian_device(fields, columns).to(self.dtype))
         return host.to(self.dtype)
 
     def _jacobian_to_host(self, fields: _Fields) -> Tensor:

@@ -367,7 +367,7 @@ def run_terrain(args, rank: int, world: int) -> dict | None:
         "jvp_ms": jvp_ms,
         "clocks": clock,
         "e2e": {"value": world * D * C * e2e_steps / e2e_time, "unit": "entries/s", "h2d_bytes_per_step": 4 * C,
-                "d2h_bytes_per_step": 4 * D * C + 1, "ms_per_step": 1e3 * e2e_time / e2e_steps,
+                "d2h_bytes_per_step": forward.dtype.itemsize * D * C + 1, "ms_per_step": 1e3 * e2e_time / e2e_steps,
                 "warmup_calls": e2e_warmup},
         "gpu_launches": int(launches),
         "cpu_baseline": None,
