@@ -1,8 +1,8 @@
 """Log-space response and Jacobian of an operator (adtlert/forward/modeling.py:137-162).
 
 ``d log(rhoa) / d log(rho) = k J_R (-sigma) / rhoa``: the row factor k / rhoa and the column
-factor -sigma are applied by one kernel while the Jacobian is still on the device, so only the
-final matrix crosses to the host.
+factor -sigma are applied by one kernel while the Jacobian is still on the device, and the
+result is widened to float64 there, so only the final matrix crosses to the host.
 """
 
 from __future__ import annotations
@@ -35,4 +35,5 @@ def log_response_and_jacobian(operator, conductivity, *, chain=None, **solve_kwa
     lib = _native.load_library()
     _native.check(lib.adt_scale_rows_columns(_native.ptr(jacobian), rows, columns, _native.ptr(row), _native.ptr(column),
                                              _native.stream_handle(device)), None, "adt_scale_rows_columns")
-    return np.log(np.asarray(response.apparent_resistivity, dtype=float)), _to_host(jacobian).numpy().astype(float)
+    # widened to float64 on the device (exact), so the host receives the final array
+    return np.log(np.asarray(response.apparent_resistivity, dtype=float)), _to_host(jacobian.to(torch.float64)).numpy()
