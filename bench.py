@@ -110,52 +110,87 @@ def barrier(world: int) -> None:
 
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled every 10 ms through NVML (read-only queries) while
+    the GPU works: the sampler is started before the warm-up steps and stopped after the timed
+    steps. The GPU is addressed by its PCI bus id, so the samples belong to the device torch
+    uses whatever CUDA_VISIBLE_DEVICES or the CUDA device ordering is. Falls back to nvidia-smi
+    (same PCI id, 100 ms) when NVML cannot be loaded."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device_index: int):
-        self.device_index = device_index
-        self.proc = None
-        self.path = None
+    def __init__(self, device_index: int, period_s: float = 0.010):
+        props = torch.cuda.get_device_properties(device_index)
+        self.pci = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+        self.period_s = period_s
+        self.samples: list[tuple[float, int, int]] = []  # (sm MHz, max MHz, reasons mask)
+        self._stop = None
+        self._thread = None
+        self._proc = None
+        self._path = None
+
+    def _nvml_loop(self, handle, nvml):
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)),
+                                     int(nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM)),
+                                     int(nvml.nvmlDeviceGetCurrentClocksEventReasons(handle))))
+            except Exception:  # noqa: BLE001 - a failed query only loses a sample
+                pass
+            self._stop.wait(self.period_s)
 
     def __enter__(self):
-        handle, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(handle)
+        import threading
+
+        self._stop = threading.Event()
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL,
-            )
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            handle = nvml.nvmlDeviceGetHandleByPciBusId(self.pci)
+            self._thread = threading.Thread(target=self._nvml_loop, args=(handle, nvml), daemon=True)
+            self._thread.start()
+            return self
+        except Exception:  # noqa: BLE001
+            self._thread = None
+        handle, self._path = tempfile.mkstemp(suffix=".csv")
+        os.close(handle)
+        fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.pci}", f"--query-gpu={fields}",
+                                           "--format=csv,noheader,nounits", "-lms", "100"],
+                                          stdout=open(self._path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
-            self.proc = None
+            self._proc = None
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                self.proc.wait(timeout=5)
+                self._proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._proc.kill()
+            try:
+                for line in Path(self._path).read_text().splitlines():
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 6 and parts[0].replace(".", "").isdigit():
+                        mask = sum(bit for (_, bit), flag in zip(self.REASONS, parts[2:6]) if flag.lower().startswith("active"))
+                        self.samples.append((float(parts[0]), int(float(parts[1])), mask))
+            finally:
+                Path(self._path).unlink(missing_ok=True)
 
     def summary(self) -> dict:
-        rows = []
-        try:
-            for line in Path(self.path).read_text().splitlines():
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
-                    rows.append(parts)
-        finally:
-            Path(self.path).unlink(missing_ok=True)
-        if not rows:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        sm = [float(r[1]) for r in rows]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({name for r in rows for name, flag in zip(names, r[5:9]) if flag.lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({name for _, _, mask in self.samples for name, bit in self.REASONS if mask & bit})
+        return {"sm_mhz": statistics.median(s for s, _, _ in self.samples), "sm_max_mhz": float(self.samples[0][1]),
+                "reasons": reasons, "samples": len(self.samples), "pci_bus_id": self.pci,
+                "window": "warm-up and timed steps, 10 ms NVML samples"}
 
 
 def measured_peaks() -> dict:
@@ -382,14 +417,14 @@ def timed_stages(args, rank, world, forward, stages, device, stream):
         for _, fn in stages:
             fn(i)
 
-    for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize(device)
-    barrier(world)
-    torch.cuda.synchronize(device)
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    launches0 = forward.kernel_launches()
     with ClockSampler(device.index) as clocks:
+        for i in range(args.warmup):
+            step(i)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        torch.cuda.synchronize(device)
+        launches0 = forward.kernel_launches()
         for k in range(args.steps):
             events[k][0].record(stream)
             step(args.warmup + k)
@@ -479,14 +514,14 @@ def run_box3d(args, rank: int, world: int) -> dict | None:
         for _, fn in stages:
             fn(i)
 
-    for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize(device)
-    barrier(world)
-    torch.cuda.synchronize(device)
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    launches0 = forward.kernel_launches()
     with ClockSampler(device.index) as clocks:
+        for i in range(args.warmup):
+            step(i)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        torch.cuda.synchronize(device)
+        launches0 = forward.kernel_launches()
         for k in range(args.steps):
             events[k][0].record(stream)
             step(args.warmup + k)
@@ -655,14 +690,14 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         for _, fn in stages:
             fn(i)
 
-    for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize(device)
-    barrier(world)
-    torch.cuda.synchronize(device)
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    launches0 = forward.kernel_launches()
     with ClockSampler(device.index) as clocks:
+        for i in range(args.warmup):
+            step(i)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        torch.cuda.synchronize(device)
+        launches0 = forward.kernel_launches()
         for k in range(args.steps):
             flush.fill_(float(k))
             events[k][0].record(stream)
@@ -771,8 +806,79 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "gpu_launches": int(launches),
     }
     if world == 1 and not args.no_cpu_baseline:
+        result["reference_kernel"] = reference_kernel(forward, fields, J, handle, flush, device, stream)
         result["cpu_baseline"] = cpu_baseline(args, nodes, cells, electrodes, rows)
     return result
+
+
+def reference_kernel(forward, fields, J, handle, flush, device, stream, reps: int = 20) -> dict:
+    """The reference's own GPU kernel (normal_sensitivity<float, 3>, adtlert/forward/kernels.py:132-178,
+    built by nvcc for sm_100 from the reference's source into oracle/_ref) on the same fields,
+    timed beside this library's Jacobian kernel in the same process (CUDA events, L2 flushed
+    before every launch, median of ``reps``): once as one launch over all rows, once as the
+    reference's jacobian() issues it (64-row launches and a torch.cat, ert2p5d.py:984-1010)."""
+
+    sys.path.insert(0, str(ROOT))
+    from adtlert_b200 import _native
+    from oracle import reference_kernel as refk
+
+    if not refk.available():
+        return {"unavailable": "oracle/_ref not built (the reference tree is needed at build time)"}
+    W, N, E, D, C = forward.W, forward.N, forward.E, forward.D, forward.C
+    phi, a, b, m, n, cells, templates = refk.operator_inputs(forward, fields)
+    out = torch.empty((D, C), dtype=torch.float32, device=device)
+    chunk = min(D, 64) if C >= 4096 else D
+
+    def one_launch():
+        refk.normal_sensitivity(phi, a, b, m, n, cells, templates, out, stream)
+
+    def reference_chunking():
+        parts = []
+        for start in range(0, D, chunk):
+            part = torch.empty((min(chunk, D - start), C), dtype=torch.float32, device=device)
+            sl = slice(start, start + part.shape[0])
+            refk.normal_sensitivity(phi, a[sl], b[sl], m[sl], n[sl], cells, templates, part, stream)
+            parts.append(part)
+        return torch.cat(parts)
+
+    def ours():
+        _native.check(forward._lib.adt_normal_jacobian(forward._plan, _native.ptr(fields), 0, D, _native.ptr(J), handle),
+                      forward._plan, "adt_normal_jacobian")
+
+    times = {"one": [], "chunked": [], "ours": []}
+    for rep in range(reps + 3):
+        for name, fn in (("one", one_launch), ("chunked", reference_chunking), ("ours", ours)):
+            flush.fill_(float(rep))
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            fn()
+            end.record(stream)
+            torch.cuda.synchronize(device)
+            if rep >= 3:
+                times[name].append(start.elapsed_time(end))
+    chunked = reference_chunking()
+    one_launch()
+    torch.cuda.synchronize(device)
+    scale = float(out.abs().max())
+    parity = float((out - J).abs().max()) / scale
+    parity_chunked = float((chunked - out).abs().max()) / scale
+    ms = {name: statistics.median(v) for name, v in times.items()}
+    algorithmic = 4 * D * C + 4 * W * N * E + 4 * 3 * C + 4 * 9 * W * C + 16 * D  # J, fields, dofs, templates, ABMN
+    peak = measured_peaks()["hbm_gbs"]
+    return {
+        "kernel": "reference normal_sensitivity<float, 3> (its source, nvcc -gencode arch=compute_100,code=sm_100, "
+                  "blocks of 32 cells x 4 rows)",
+        "ms_one_launch": ms["one"],
+        "ms_reference_chunking": ms["chunked"],
+        "launches_reference_chunking": -(-D // chunk),
+        "ms_ours": ms["ours"],
+        "ratio_one_launch": ms["one"] / ms["ours"],
+        "ratio_reference_chunking": ms["chunked"] / ms["ours"],
+        "hbm_frac_reference_one_launch": algorithmic / (ms["one"] * 1e-3) / 1e9 / peak,
+        "parity_max_rel_vs_ours": parity,
+        "parity_chunked_vs_one_launch": parity_chunked,
+        "timing": f"median of {reps} launches each, L2 flushed before every launch, CUDA events on the launching stream",
+    }
 
 
 def cpu_baseline(args, nodes, cells, electrodes, rows) -> dict:

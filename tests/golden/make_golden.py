@@ -1,7 +1,8 @@
 """Generate the golden vectors that pin the CPU oracle to AD-TLERT's own implementation.
 
-This script runs the reference package (``adtlert``, read from ``/root/reference``) on the CPU
-with three substitutions that leave its arithmetic untouched:
+This script runs the reference package (``adtlert``, from the AD-TLERT project root named by
+the ``ADTLERT_REFERENCE`` environment variable) on the CPU with three substitutions that leave
+its arithmetic untouched:
 
 1. its CUDA device constant is replaced by ``cpu`` (every torch op then runs on the host);
 2. the cuDSS batched solve (``adtlert/forward/cudss.py:63-122``) is replaced by SciPy's
@@ -14,7 +15,8 @@ with three substitutions that leave its arithmetic untouched:
 stub module stands in for it. Each precision runs in its own interpreter because the
 reference fixes ``FLOAT_DTYPE`` at import (``adtlert/utils/dtypes.py:10-23``).
 
-Usage: ``python tests/golden/make_golden.py`` (writes ``tests/golden/*.npz``).
+Usage: ``ADTLERT_REFERENCE=<AD-TLERT project root> python tests/golden/make_golden.py`` (writes
+``tests/golden/*.npz``).
 """
 
 from __future__ import annotations
@@ -26,7 +28,7 @@ import tempfile
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path("/root/reference")
+REFERENCE = Path(os.environ.get("ADTLERT_REFERENCE", ""))
 
 sys.path.insert(0, str(HERE))
 from cases import CASES, CASES3D, case3d_inputs, case_inputs  # noqa: E402
@@ -193,6 +195,8 @@ def main() -> None:
         _, _, name, precision = sys.argv
         _child(name, precision, os.environ["GOLDEN_TARGET"])
         return
+    if not (REFERENCE / "adtlert").is_dir():
+        raise SystemExit("set ADTLERT_REFERENCE to the AD-TLERT project root (the folder holding adtlert/)")
     with tempfile.TemporaryDirectory() as stub:
         _stub_meshio(Path(stub))
         only = sys.argv[1:]
