@@ -44,6 +44,8 @@ SYMBOLS = (
     "adt_boundary_jacobian",
     "adt_measure_static",
     "adt_scale_rows_columns",
+    "adt_fingerprint",
+    "adt_fingerprint_host",
     "adt_kernel_launches",
 )
 
@@ -145,6 +147,8 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_boundary_jacobian": (status, [_p, _p, _i32, _i32, _p, _p]),
         "adt_measure_static": (status, [_p, _p, _i32, _p, _p, _p]),
         "adt_scale_rows_columns": (status, [_p, _i32, _i32, _p, _p, _p]),
+        "adt_fingerprint": (status, [_p, _p, _i64, _i32, _p, _p]),
+        "adt_fingerprint_host": (status, [_p, _i64, _i32, _p]),
         "adt_kernel_launches": (_i64, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():

@@ -1,9 +1,17 @@
-"""PyTorch autograd bridge (semantics of adtlert/forward/autograd.py:17-207).
+"""Differentiable apparent resistivity over this library's operators.
 
-Forward returns apparent resistivity on the input's device and dtype; backward calls the
-operator's ``vjp_series`` (adjoint kernels reusing the forward factorization, no Jacobian is
-formed); forward-mode AD calls ``jvp``. Gradients flow to the conductivity and to scalar or
-per-datum currents; second derivatives are not supported.
+Observable contract of the reference bridge (adtlert/forward/autograd.py:17-207), kept as is:
+``apparent_resistivity_autograd(conductivity, forward_operator, currents=1.0)`` takes one model
+``(cells,)`` or a series ``(steps, cells)``, returns ``k R / I`` on the conductivity's device
+and dtype, back-propagates to the conductivity and to scalar, one-element or per-datum currents
+(once differentiable), supports forward-mode AD, and raises the same TypeError / ValueError
+messages for bad arguments.
+
+How it gets there is this library's: a conductivity that lives on the GPU stays there. Its
+resistances, the adjoint (exact VJP, reusing the forward factorization; no Jacobian is formed)
+and the tangents come from the operator's device-resident entry points, so neither the model,
+nor the resistances, nor the gradient crosses to the host. A CPU conductivity goes through the
+operator's public methods, whose results are CPU tensors, exactly like the reference's path.
 """
 
 from __future__ import annotations
@@ -17,102 +25,126 @@ from .ert2p5d import ERTForward2p5D
 from .ert3d import ERTForward3D
 from .inputs import FLOAT_DTYPE
 
-
-def _operators():
-    return (ERTForward2p5D, ERTForward3D)
+Tensor = torch.Tensor
 
 
-def _validate_inputs(conductivity, currents, forward_operator) -> None:
-    if not isinstance(forward_operator, _operators()):
+def _checked(conductivity, currents, operator) -> None:
+    """The reference's argument checks, with its exception types and messages."""
+
+    if not isinstance(operator, (ERTForward2p5D, ERTForward3D)):
         raise TypeError("forward_operator must be an ERTForward2p5D or ERTForward3D instance")
-    if not isinstance(conductivity, torch.Tensor) or not conductivity.is_floating_point():
+    if not isinstance(conductivity, Tensor) or not conductivity.is_floating_point():
         raise TypeError("conductivity must be a floating-point torch.Tensor")
-    cells = forward_operator.C
+    cells, data = operator.C, operator.D
     if conductivity.ndim not in (1, 2) or conductivity.shape[-1] != cells:
         raise ValueError(
-            f"conductivity must have shape ({cells},) or (n_steps, {cells}), got {tuple(conductivity.shape)}"
-        )
-    if not bool(torch.all(torch.isfinite(conductivity))) or bool(torch.any(conductivity <= 0.0)):
+            f"conductivity must have shape ({cells},) or (n_steps, {cells}), got {tuple(conductivity.shape)}")
+    low, high = torch.aminmax(conductivity.detach())
+    if not (bool(torch.isfinite(low)) and bool(torch.isfinite(high))) or float(low) <= 0.0:
         raise ValueError("conductivity must contain finite positive values")
-    if not isinstance(currents, torch.Tensor) or not currents.is_floating_point():
+    if not isinstance(currents, Tensor) or not currents.is_floating_point():
         raise TypeError("currents must be a floating-point torch.Tensor")
-    count = forward_operator.D
-    if tuple(currents.shape) not in {(), (1,), (count,)}:
-        raise ValueError(f"currents must be scalar or have shape ({count},), got {tuple(currents.shape)}")
-    if not bool(torch.all(torch.isfinite(currents))) or bool(torch.any(currents == 0.0)):
+    if tuple(currents.shape) not in {(), (1,), (data,)}:
+        raise ValueError(f"currents must be scalar or have shape ({data},), got {tuple(currents.shape)}")
+    if not bool(torch.isfinite(currents).all()) or bool((currents == 0.0).any()):
         raise ValueError("currents must contain finite non-zero values")
 
 
-def _reduce_current_gradient(gradient: torch.Tensor, shape: torch.Size) -> torch.Tensor:
-    if len(shape) == 0:
-        return gradient.sum()
+class _Evaluation:
+    """Where one call's arithmetic happens: the operator's GPU for CUDA conductivities, the host
+    (through the public CPU methods) otherwise."""
+
+    def __init__(self, operator, on_gpu: bool) -> None:
+        self.operator = operator
+        self.on_gpu = on_gpu
+        self.device = operator.device if on_gpu else torch.device("cpu")
+
+    def models(self, conductivity: Tensor) -> Tensor:
+        series = conductivity.detach().reshape(-1, self.operator.C)
+        return series.to(self.device, FLOAT_DTYPE).contiguous()
+
+    def factors(self) -> Tensor:
+        return self.operator._geometric_factors().to(self.device)
+
+    def resistances(self, models: Tensor) -> Tensor:
+        if self.on_gpu:
+            return self.operator._resistances_device(models)
+        return self.operator.resistance_series(models)
+
+    def vjp(self, models: Tensor, cotangents: Tensor) -> Tensor:
+        if self.on_gpu:
+            return self.operator._vjp_device(models, cotangents)
+        return self.operator.vjp_series(models, cotangents)
+
+    def jvp(self, model: Tensor, direction: Tensor) -> Tensor:
+        if self.on_gpu:
+            return self.operator._jvp_device(model, direction)
+        return self.operator.jvp(model, direction)
+
+
+def _current_gradient(per_datum: Tensor, shape: torch.Size) -> Tensor:
+    """Gradient of the currents from the per-datum gradient, reduced to the currents' shape."""
+
     if tuple(shape) == (1,):
-        return gradient.sum().reshape(shape)
-    return gradient
+        return per_datum.sum().reshape(1)
+    if len(shape) == 0:
+        return per_datum.sum()
+    return per_datum
 
 
 class ERT2p5DApparentResistivityFunction(torch.autograd.Function):
-    """Apparent resistivity of one model ``(n_cells,)`` or a series ``(n_steps, n_cells)``."""
+    """Apparent resistivity of one model ``(cells,)`` or a series ``(steps, cells)``, for a 2.5D
+    or a 3D operator."""
 
     @staticmethod
     def forward(ctx: Any, conductivity, currents, forward_operator):
-        _validate_inputs(conductivity, currents, forward_operator)
-        conductivity_work = conductivity.detach().to(device="cpu", dtype=FLOAT_DTYPE)
-        currents_work = currents.detach().to(device="cpu", dtype=FLOAT_DTYPE)
-        geometric_scale = forward_operator._geometric_factors().detach()
-        resistance = forward_operator.resistance_series(
-            conductivity_work.reshape(-1, conductivity_work.shape[-1])
-        ).reshape(*conductivity_work.shape[:-1], -1)
-        apparent_resistivity = geometric_scale * resistance / currents_work
-        ctx.forward_operator = forward_operator
-        ctx.conductivity_device, ctx.conductivity_dtype = conductivity.device, conductivity.dtype
-        ctx.currents_device, ctx.currents_dtype = currents.device, currents.dtype
-        ctx.currents_shape = currents.shape
-        saved = (conductivity_work, currents_work, apparent_resistivity, geometric_scale)
-        ctx.save_for_backward(*saved)
-        ctx.save_for_forward(*saved)
-        return apparent_resistivity.to(device=conductivity.device, dtype=conductivity.dtype)
+        _checked(conductivity, currents, forward_operator)
+        run = _Evaluation(forward_operator, conductivity.is_cuda)
+        models = run.models(conductivity)
+        resistance = run.resistances(models)
+        factors = run.factors().to(resistance.dtype)
+        current = currents.detach().to(run.device, resistance.dtype)
+        apparent = factors * resistance / current
+        ctx.run = run
+        ctx.input_shape, ctx.input_kind = conductivity.shape, (conductivity.device, conductivity.dtype)
+        ctx.current_shape, ctx.current_kind = currents.shape, (currents.device, currents.dtype)
+        kept = (models, current, apparent, factors)
+        ctx.save_for_backward(*kept)
+        ctx.save_for_forward(*kept)
+        device, dtype = ctx.input_kind
+        return apparent.reshape(*conductivity.shape[:-1], -1).to(device=device, dtype=dtype)
 
     @staticmethod
     @once_differentiable
     def backward(ctx: Any, grad_output):
-        conductivity, currents, apparent_resistivity, geometric_scale = ctx.saved_tensors
-        output_cotangent = grad_output.detach().to(device="cpu", dtype=FLOAT_DTYPE)
-        conductivity_gradient = None
+        models, current, apparent, factors = ctx.saved_tensors
+        upstream = grad_output.detach().reshape(apparent.shape).to(apparent.device, apparent.dtype)
+        conductivity_grad = currents_grad = None
         if ctx.needs_input_grad[0]:
-            resistance_cotangent = output_cotangent * geometric_scale / currents
-            conductivity_gradient = ctx.forward_operator.vjp_series(
-                conductivity.reshape(-1, conductivity.shape[-1]),
-                resistance_cotangent.reshape(-1, resistance_cotangent.shape[-1]),
-            ).reshape(conductivity.shape)
-            conductivity_gradient = conductivity_gradient.to(device=ctx.conductivity_device, dtype=ctx.conductivity_dtype)
-        currents_gradient = None
+            gradient = ctx.run.vjp(models, upstream * factors / current)
+            device, dtype = ctx.input_kind
+            conductivity_grad = gradient.reshape(ctx.input_shape).to(device=device, dtype=dtype)
         if ctx.needs_input_grad[1]:
-            expanded = -output_cotangent * apparent_resistivity / currents
-            currents_gradient = _reduce_current_gradient(expanded.reshape(-1, expanded.shape[-1]).sum(0), ctx.currents_shape)
-            currents_gradient = currents_gradient.to(device=ctx.currents_device, dtype=ctx.currents_dtype)
-        return conductivity_gradient, currents_gradient, None
+            per_datum = (-upstream * apparent / current).sum(dim=0)
+            device, dtype = ctx.current_kind
+            currents_grad = _current_gradient(per_datum, ctx.current_shape).to(device=device, dtype=dtype)
+        return conductivity_grad, currents_grad, None
 
     @staticmethod
     def jvp(ctx: Any, conductivity_tangent, currents_tangent, forward_operator_tangent):
         del forward_operator_tangent
-        conductivity, currents, apparent_resistivity, geometric_scale = ctx.saved_tensors
-        tangent = torch.zeros_like(apparent_resistivity)
+        models, current, apparent, factors = ctx.saved_tensors
+        run = ctx.run
+        tangent = torch.zeros_like(apparent)
         if conductivity_tangent is not None:
-            direction = conductivity_tangent.detach().to(device="cpu", dtype=FLOAT_DTYPE)
-            resistance_tangent = torch.stack([
-                ctx.forward_operator.jvp(model, step)
-                for model, step in zip(
-                    conductivity.reshape(-1, conductivity.shape[-1]),
-                    direction.reshape(-1, conductivity.shape[-1]),
-                    strict=True,
-                )
-            ]).reshape(apparent_resistivity.shape)
-            tangent = tangent + geometric_scale * resistance_tangent / currents
+            directions = conductivity_tangent.detach().reshape(models.shape).to(run.device, FLOAT_DTYPE)
+            resistance_tangent = torch.stack([run.jvp(model, direction).to(run.device, apparent.dtype)
+                                              for model, direction in zip(models, directions, strict=True)])
+            tangent = tangent + factors * resistance_tangent / current
         if currents_tangent is not None:
-            current_direction = currents_tangent.detach().to(device="cpu", dtype=FLOAT_DTYPE)
-            tangent = tangent - apparent_resistivity * current_direction / currents
-        return tangent.to(device=ctx.conductivity_device, dtype=ctx.conductivity_dtype)
+            tangent = tangent - apparent * currents_tangent.detach().to(run.device, apparent.dtype) / current
+        device, dtype = ctx.input_kind
+        return tangent.reshape(*ctx.input_shape[:-1], -1).to(device=device, dtype=dtype)
 
 
 ERT3DApparentResistivityFunction = ERT2p5DApparentResistivityFunction
@@ -120,9 +152,9 @@ ERTApparentResistivityFunction = ERT2p5DApparentResistivityFunction
 
 
 def apparent_resistivity_autograd(conductivity, forward_operator, currents=1.0):
-    """Differentiable apparent resistivity; output on the conductivity's device and dtype."""
+    """Differentiable apparent resistivity; the output is on the conductivity's device and dtype."""
 
-    if not isinstance(conductivity, torch.Tensor):
+    if not isinstance(conductivity, Tensor):
         raise TypeError("conductivity must be a torch.Tensor")
-    current_tensor = torch.as_tensor(currents, device=conductivity.device, dtype=conductivity.dtype)
-    return ERT2p5DApparentResistivityFunction.apply(conductivity, current_tensor, forward_operator)
+    currents = torch.as_tensor(currents, device=conductivity.device, dtype=conductivity.dtype)
+    return ERT2p5DApparentResistivityFunction.apply(conductivity, currents, forward_operator)

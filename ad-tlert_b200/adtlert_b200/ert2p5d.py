@@ -37,7 +37,7 @@ from .fem import (
     wavenumber_bounds,
 )
 from .discretization import Discretization, build_discretization, exact_node_indices
-from .field_cache import FieldCache, factorization_name, newest_batches_first
+from .field_store import FieldStore, adjoint_batches, batch_name, model_fingerprints
 from .geometry import Mesh, Survey, geometric_factors, locate_points
 from .inputs import (
     FLOAT_DTYPE,
@@ -330,7 +330,7 @@ class ERTForward2p5D:
         self.device = torch.device("cuda", torch.cuda.current_device())
         self._lib = _native.load_library()
         self._cache: dict = {}
-        self._field_cache = FieldCache(self.normal_field_cache_max_entries)
+        self._field_cache = FieldStore(self.normal_field_cache_max_entries, self._fingerprints)
         self._pending_checks = None  # (device flag, context) pairs read back with a host result
         self._solver = _Slots()
         self._plan = None
@@ -598,8 +598,11 @@ class ERTForward2p5D:
             context = next(what for flag, what in pending if not bool(flag))
             raise FloatingPointError(f"{context} produced non-finite values")
 
+    def _fingerprints(self, models: Tensor) -> list[bytes]:
+        return model_fingerprints(self._lib, self._plan, models, self._stream())
+
     def _fields_series(self, models: Tensor):
-        return self._field_cache.solve_series(models, self.series_batch_steps, self._solve_fields)
+        return self._field_cache.fields(models, self.series_batch_steps, self._solve_fields)
 
     def _fields(self, conductivity) -> _Fields:
         return self._fields_series(self._sigma(conductivity)[None])[0][0]
@@ -664,9 +667,15 @@ class ERTForward2p5D:
         return self._geometric_factors() * self.resistance(conductivity) / current
 
     def resistance_series(self, conductivities) -> Tensor:
-        fields, _ = self._fields_series(self._series(conductivities))
+        return self._resistances_device(self._series(conductivities)).cpu()
+
+    def _resistances_device(self, models: Tensor) -> Tensor:
+        """Reciprocity-averaged resistances (S, D) of validated models (S, C), left on the GPU in
+        the operator's result dtype."""
+
+        fields, _ = self._fields_series(models)
         normal, reciprocal, _ = self._transfers(self._stack(fields))
-        return self._combine(normal.cpu(), reciprocal.cpu()).to(self.dtype)
+        return self._combine(normal, reciprocal).to(self.dtype)
 
     def apparent_resistivity_series(self, conductivities, currents=1.0) -> Tensor:
         current = torch.as_tensor(currents, dtype=FLOAT_DTYPE)
@@ -754,7 +763,7 @@ class ERTForward2p5D:
             jacobian = self._jacobian_device(fields, columns)
         else:
             key = self._field_cache.key(self._sigma(conductivity))
-            slot = self._factorize(self._sigma(conductivity).to(self.device)[None].contiguous(), factorization_name([key]))
+            slot = self._factorize(self._sigma(conductivity).to(self.device)[None].contiguous(), batch_name([key]))
             rows = []
             for start in range(0, self.D, batch):
                 count = min(batch, self.D - start)
@@ -807,33 +816,44 @@ class ERTForward2p5D:
     def vjp_series(self, conductivities, cotangents) -> Tensor:
         models = self._series(conductivities)
         cotangents = cotangent_series(cotangents, models.shape[0], self.D)
+        gradient = self._vjp_device(models, cotangents).cpu().to(self.dtype)
+        check_finite(gradient, "conductivity gradient")
+        return gradient
+
+    def _vjp_device(self, models: Tensor, cotangents: Tensor) -> Tensor:
+        """Exact VJPs (S, C) float32 on the GPU of validated models (S, C) and resistance
+        cotangents (S, D) on any device."""
+
         fields, keys = self._fields_series(models)
         gradients: dict[int, Tensor] = {}
-        for batch in newest_batches_first(len(fields), self.series_batch_steps):
+        for batch in adjoint_batches(len(fields), self.series_batch_steps):
             totals = self._stack([fields[step] for step in batch])
             normal, reciprocal, _ = self._transfers(totals)
             slot = self._factorize(models[batch].to(self.device, torch.float32).contiguous(),
-                                   factorization_name([keys[step] for step in batch]))
+                                   batch_name([keys[step] for step in batch]))
             cot = cotangents[batch].to(self.device, torch.float64).contiguous()
             grad = torch.empty((len(batch), self.C), dtype=torch.float32, device=self.device)
             self._call("adt_vjp", slot, _native.ptr(totals), _native.ptr(normal), _native.ptr(reciprocal),
                        _native.ptr(cot), len(batch), _native.ptr(grad), self._stream())
             for i, step in enumerate(batch):
                 gradients[step] = grad[i]
-        gradient = torch.stack([gradients[step] for step in range(len(fields))]).cpu().to(self.dtype)
-        check_finite(gradient, "conductivity gradient")
-        return gradient
+        return torch.stack([gradients[step] for step in range(len(fields))])
 
     def jvp(self, conductivity, delta_conductivity) -> Tensor:
-        sigma = self._sigma(conductivity)
+        out = self._jvp_device(self._sigma(conductivity), cell_vector(delta_conductivity, self.C))
+        check_finite(out, "tangent fields")
+        return out.cpu().to(self.dtype)
+
+    def _jvp_device(self, sigma: Tensor, direction: Tensor) -> Tensor:
+        """Resistance tangent (D,) float64 on the GPU of a validated model and direction (C,)."""
+
         fields, normal, reciprocal = self._measure(sigma)
-        direction = cell_vector(delta_conductivity, self.C).to(self.device, torch.float32).contiguous()
-        slot = self._factorize(sigma.to(self.device)[None].contiguous(), factorization_name([self._field_cache.key(sigma)]))
+        direction = direction.to(self.device, torch.float32).contiguous()
+        slot = self._factorize(sigma.to(self.device)[None].contiguous(), batch_name([self._field_cache.key(sigma)]))
         out = torch.empty(self.D, dtype=torch.float64, device=self.device)
         self._call("adt_jvp", slot, _native.ptr(fields.total), _native.ptr(normal), _native.ptr(reciprocal),
                    _native.ptr(direction), _native.ptr(out), self._stream())
-        check_finite(out, "tangent fields")
-        return out.cpu().to(self.dtype)
+        return out
 
     def normal_vjp(self, conductivity, cotangent, *, cell_parameter_ids=None, parameter_count=None) -> Tensor:
         columns = self._columns(cell_parameter_ids, parameter_count)

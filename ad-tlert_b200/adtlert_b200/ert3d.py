@@ -29,7 +29,7 @@ import torch
 
 from . import _native
 from .ert2p5d import _checked_to_host, _Slots, _survey_arrays
-from .field_cache import FieldCache
+from .field_store import FieldStore, model_fingerprints
 from .geometry3d import (
     Mesh3D,
     p2_shape_values,
@@ -273,8 +273,8 @@ class ERTForward3D:
         self.singularity_removal = bool(singularity_removal)
         self.element_order = int(element_order)
         self.series_batch_steps = int(series_batch_steps)
-        self._field_cache = FieldCache(normal_field_cache_max_entries)
-        self.normal_field_cache_max_entries = self._field_cache.max_entries
+        self._field_cache = FieldStore(normal_field_cache_max_entries, self._fingerprints)
+        self.normal_field_cache_max_entries = self._field_cache.capacity
         self.device = torch.device("cuda", torch.cuda.current_device())
         self._lib = _native.load_library()
         self._cache: dict = {}
@@ -342,8 +342,11 @@ class ERTForward3D:
         check_finite(fields, "node fields")
         return [fields[i] for i in range(batch)]
 
+    def _fingerprints(self, models: Tensor) -> list[bytes]:
+        return model_fingerprints(self._lib, self._plan, models, self._stream())
+
     def _fields_series(self, models: Tensor):
-        return self._field_cache.solve_series(models, self.series_batch_steps, self._solve_fields)
+        return self._field_cache.fields(models, self.series_batch_steps, self._solve_fields)
 
     def _fields(self, conductivity) -> Tensor:
         return self._fields_series(self._sigma(conductivity)[None])[0][0]
@@ -413,10 +416,15 @@ class ERTForward3D:
         return self.resistance_series(self._sigma(conductivity)[None])[0]
 
     def resistance_series(self, conductivities) -> Tensor:
-        fields, _ = self._fields_series(self._series(conductivities))
-        resistance = self._resistances(self._stack(fields)).cpu().to(FLOAT_DTYPE)
+        resistance = self._resistances_device(self._series(conductivities)).cpu()
         check_finite(resistance, "resistances")
         return resistance
+
+    def _resistances_device(self, models: Tensor) -> Tensor:
+        """Resistances (S, D) of validated models (S, C), left on the GPU in the result dtype."""
+
+        fields, _ = self._fields_series(models)
+        return self._resistances(self._stack(fields)).to(FLOAT_DTYPE)
 
     def apparent_resistivity_values(self, conductivity, currents=1.0) -> Tensor:
         factors = self._geometric_factors()
@@ -475,20 +483,29 @@ class ERTForward3D:
 
         models = self._series(conductivities)
         cotangents = cotangent_series(cotangents, models.shape[0], self.D)
-        fields, _ = self._fields_series(models)
-        rows = [self._cell_products(f, c.to(self.device, torch.float64).contiguous(), True)[0]
-                for f, c in zip(fields, cotangents, strict=True)]
-        gradient = torch.stack(rows).cpu()
+        gradient = self._vjp_device(models, cotangents).cpu()
         check_finite(gradient, "conductivity gradient")
         return gradient
 
+    def _vjp_device(self, models: Tensor, cotangents: Tensor) -> Tensor:
+        """Exact VJPs (S, C) float32 on the GPU of validated models and cotangents (S, D)."""
+
+        fields, _ = self._fields_series(models)
+        rows = [self._cell_products(f, c.to(self.device, torch.float64).contiguous(), True)[0]
+                for f, c in zip(fields, cotangents, strict=True)]
+        return torch.stack(rows)
+
     def jvp(self, conductivity, delta_conductivity) -> Tensor:
-        fields = self._fields(conductivity)
-        direction = cell_vector(delta_conductivity, self.C, torch.float64)
-        result = self._data_products(fields, direction.to(self.device, torch.float32).contiguous(), True)
+        result = self._jvp_device(self._sigma(conductivity), cell_vector(delta_conductivity, self.C, torch.float64))
         result = result.cpu().to(FLOAT_DTYPE)
         check_finite(result, "resistance jvp")
         return result
+
+    def _jvp_device(self, sigma: Tensor, direction: Tensor) -> Tensor:
+        """Resistance tangent (D,) float64 on the GPU of a validated model and direction (C,)."""
+
+        fields = self._fields(sigma)
+        return self._data_products(fields, direction.to(self.device, torch.float32).contiguous(), True)
 
     def normal_vjp(self, conductivity, cotangent, *, cell_parameter_ids=None, parameter_count=None) -> Tensor:
         cotangent = measurement_vector(cotangent, self.D, FLOAT_DTYPE)

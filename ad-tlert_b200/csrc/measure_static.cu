@@ -18,7 +18,12 @@
 // In host code the array's name is only a host-side stand-in, not a device address, so the device
 // address is fetched with cudaGetSymbolAddress once per device (with that device current) and
 // cached. That happens during the first call on each device, so make that first call before any
-// stream capture.
+// stream capture. The cached address belongs to the device's primary context as it was then: a
+// cudaDeviceReset (or any teardown of that context) after the first call is not supported, since
+// the reloaded module may place the array elsewhere.
+//
+// Both kernels are launched like the rest of the library (adt::launch_chained: programmatic
+// stream serialization; each kernel waits on the grid before it as its first statement).
 #include <mutex>
 
 #include "adt_internal.h"
@@ -58,9 +63,11 @@ adt_status static_table(adt_plan* p, int device, double** out) {
   return ADT_OK;
 }
 
-inline int grid_for(int64_t work) {
+// Blocks of 256 threads for `work` grid-stride items: at most 32 per multiprocessor.
+inline int grid_for(int64_t work, int sms) {
   const int64_t blocks = (work + 255) / 256;
-  return (int)(blocks < 1 ? 1 : (blocks > 148 * 32 ? 148 * 32 : blocks));
+  const int64_t cap = (int64_t)sms * 32;
+  return (int)(blocks < 1 ? 1 : (blocks > cap ? cap : blocks));
 }
 
 }  // namespace
@@ -97,8 +104,8 @@ extern "C" adt_status adt_measure_static(adt_plan* p, const float* fields, int32
   a.D = p->D;
   a.combine = 0;
   cudaStream_t s = (cudaStream_t)stream;
-  adt::potentials_kernel<<<grid_for((int64_t)need), 256, 0, s>>>(a, models, table);
-  adt::transfers_kernel<<<grid_for((int64_t)models * p->D), 256, 0, s>>>(a, models, table);
+  adt::launch_chained(adt::potentials_kernel, grid_for((int64_t)need, p->sms), 256, 0, s, a, models, table);
+  adt::launch_chained(adt::transfers_kernel, grid_for((int64_t)models * p->D, p->sms), 256, 0, s, a, models, table);
   p->launches += 2;
   return adt::check_launch(p, "static measure");
 }

@@ -1693,9 +1693,9 @@ void factor_levels_rhs(adt_plan* p, int systems, const double* values, double* f
 
 // Column strip of the substitution kernels: the full tile unless that leaves most SMs idle.
 template <int MAXM>
-int strip_for(int blocks, int nrhs) {
+int strip_for(int blocks, int nrhs, int sms) {
   int strip = MAXM;
-  while (strip > 16 && (int64_t)blocks * ((nrhs + strip - 1) / strip) < 2 * 148) strip /= 2;
+  while (strip > 16 && (int64_t)blocks * ((nrhs + strip - 1) / strip) < 2 * sms) strip /= 2;
   return strip;
 }
 
@@ -1705,7 +1705,7 @@ void backward_levels(adt_plan* p, int systems, int nrhs, const double* factors, 
   const int64_t rhs_stride = (int64_t)p->N * nrhs;
   for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs);
+    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, p->sms);
     launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
                    backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
@@ -1718,14 +1718,14 @@ void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, dou
   for (int level = 0; level < p->levels; ++level) {  // forward: eager updates only
     const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
     if (i1 <= i0) continue;
-    const int strip = strip_for<MAXM>((i1 - i0) * systems, nrhs);
+    const int strip = strip_for<MAXM>((i1 - i0) * systems, nrhs, p->sms);
     launch_chained(forward_update_kernel<MAXM>, dim3(i1 - i0, systems, (nrhs + strip - 1) / strip), kSolverThreads, forward_update_smem<MAXM>(), s, 
         p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
   }
   for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs);
+    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, p->sms);
     launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads, backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs,
                                                               rhs_stride, nrhs, strip);
     p->launches++;

@@ -263,7 +263,8 @@ adt_status adt_boundary_jacobian(adt_plan* plan, const float* fields, int32_t ro
  * 65,536 doubles (512 KiB) per device, held until exit, so models * (E+1)^2 must not exceed
  * 65,536 (larger requests return ADT_INVALID_ARG). All calls share that array: calls that overlap
  * on the GPU race and must be ordered by the caller. The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress), so make it before any stream capture. */
+ * array's device address (cudaGetSymbolAddress), so make it before any stream capture; the address
+ * is cached, so a device reset after that first call is not supported. */
 adt_status adt_measure_static(adt_plan* plan, const float* fields, int32_t models, double* normal,
                               double* reciprocal, adt_stream stream);
 
@@ -275,6 +276,18 @@ adt_status adt_measure_static(adt_plan* plan, const float* fields, int32_t model
 adt_status adt_scale_rows_columns(float* values, int32_t rows, int32_t columns,
                                   const double* row_scale, const double* column_scale,
                                   adt_stream stream);
+
+/* Content fingerprints of `models` consecutive models of bytes_per_model bytes each (a multiple
+ * of 4, the data 4-byte aligned): two uint64 per model, the keys of the operators' field caches
+ * (two 64-bit sums of a mixed word stream; identical for identical bytes, different models
+ * collide with probability about 2^-128). adt_fingerprint reads device memory and writes the
+ * device array `fingerprints` [models][2] on `stream`; adt_fingerprint_host computes the same
+ * bits from host memory on the calling thread. Replaces the blake2b digest of FieldCache.key
+ * (adtlert/forward/field_cache.py:54-59), which first copies a device model to the host. */
+adt_status adt_fingerprint(adt_plan* plan, const void* models_data, int64_t bytes_per_model, int32_t models,
+                           uint64_t* fingerprints, adt_stream stream);
+adt_status adt_fingerprint_host(const void* models_data, int64_t bytes_per_model, int32_t models,
+                                uint64_t* fingerprints);
 
 /* Number of kernels this library has launched since the plan was created. */
 int64_t adt_kernel_launches(const adt_plan* plan);
