@@ -46,6 +46,9 @@ SYMBOLS = (
     "adt_scale_rows_columns",
     "adt_fingerprint",
     "adt_fingerprint_host",
+    "adt_gn_workspace_bytes",
+    "adt_gn_step",
+    "adt_gn_regularize",
     "adt_kernel_launches",
 )
 
@@ -149,6 +152,10 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_scale_rows_columns": (status, [_p, _i32, _i32, _p, _p, _p]),
         "adt_fingerprint": (status, [_p, _p, _i64, _i32, _p, _p]),
         "adt_fingerprint_host": (status, [_p, _i64, _i32, _p]),
+        "adt_gn_workspace_bytes": (status, [_i32, _i32, _i32, _i32, _p]),
+        "adt_gn_step": (status, [_p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, ctypes.c_double, ctypes.c_double,
+                                 _i32, ctypes.c_double, _p, _p, ctypes.c_size_t, _i32, _p]),
+        "adt_gn_regularize": (status, [_p, _i32, _i32, _p, _p, _p, ctypes.c_double, ctypes.c_double, _p, _p, _p]),
         "adt_kernel_launches": (_i64, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():

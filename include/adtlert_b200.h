@@ -289,6 +289,37 @@ adt_status adt_fingerprint(adt_plan* plan, const void* models_data, int64_t byte
 adt_status adt_fingerprint_host(const void* models_data, int64_t bytes_per_model, int32_t models,
                                 uint64_t* fingerprints);
 
+/* Gauss-Newton step of a time-lapse window of `steps` models (rows x columns log Jacobians each):
+ * solves min ||A x - b|| by `iterations` CGLS iterations on the device (stopping early, with the
+ * rest of the launched iterations doing nothing, once gamma / gamma_0 < tolerance), where
+ *   A = [ W J_t (per model) ; sqrt(spatial) R (per model) ; sqrt(temporal) D_t ],
+ *   b = [ data_rhs ; -sqrt(spatial) R m ; -sqrt(temporal) D_t m ],
+ * W = diag(data_weights), R the first-order neighbour differences given as symmetric neighbour
+ * lists (neighbour_ptr[columns+1], neighbour_cells, neighbour_weights = squared row weights; each
+ * neighbouring pair listed from both cells), D_t the first difference between consecutive models.
+ * Device arrays: jacobian [steps][rows][columns] float32 (16-byte aligned; columns a multiple of
+ * 4, at most 16384), data_weights and data_rhs [steps][rows] float64, models and step
+ * [steps][columns] float64. The caller provides `workspace` (256-byte aligned, the size that
+ * adt_gn_workspace_bytes gives for the same sizes and `multiprocessors`); nothing is allocated.
+ * Replaces: the gauss_newton_cgls linearized step with gpu_cgls of
+ * adtlert/inversion/core.py:204-216 (_data_system, objective.py:56-80; RegularizationTerms.blocks,
+ * terms.py:75-186; _gpu_cgls, optimizers.py:314-360), without forming the stacked sparse matrix. */
+adt_status adt_gn_workspace_bytes(int32_t steps, int32_t rows, int32_t columns, int32_t multiprocessors,
+                                  size_t* bytes);
+adt_status adt_gn_step(adt_plan* plan, const float* jacobian, int32_t steps, int32_t rows, int32_t columns,
+                       const double* data_weights, const double* data_rhs, const double* models,
+                       const int32_t* neighbour_ptr, const int32_t* neighbour_cells,
+                       const double* neighbour_weights, double spatial, double temporal, int32_t iterations,
+                       double tolerance, double* step, void* workspace, size_t workspace_bytes,
+                       int32_t multiprocessors, adt_stream stream);
+/* out = (spatial R^T R + temporal D_t^T D_t) models for [steps][columns] float64 device arrays
+ * (the regularization part of A^T A; the line search of the Gauss-Newton iteration evaluates its
+ * quadratic from it). Replaces the regularization rows of _line_search_tau
+ * (adtlert/inversion/objective.py:168-192). */
+adt_status adt_gn_regularize(adt_plan* plan, int32_t steps, int32_t columns, const int32_t* neighbour_ptr,
+                             const int32_t* neighbour_cells, const double* neighbour_weights, double spatial,
+                             double temporal, const double* models, double* out, adt_stream stream);
+
 /* Number of kernels this library has launched since the plan was created. */
 int64_t adt_kernel_launches(const adt_plan* plan);
 
