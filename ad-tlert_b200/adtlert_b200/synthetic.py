@@ -205,3 +205,15 @@ def correlated_model(nodes, cells, seed: int, correlation: float = 5.0, spacing:
     ij = np.clip(np.rint((centers - lo) / spacing).astype(int), 0, np.array(shape) - 1)
     log_rho = 2.0 + 0.4 * field[ij[:, 0], ij[:, 1]]
     return (1.0 / 10.0 ** log_rho).astype(np.float32)
+
+
+def infiltration_series(nodes, cells, steps: int = 365, seed: int = 0, max_depth: float = 8.0) -> np.ndarray:
+    """(steps, cells) float64 resistivity of the time-lapse workload: the seeded layered model
+    with an infiltration front whose depth grows monotonically, f(t) = max_depth (t / (steps -
+    1))^0.7, and the resistivity above the front multiplied by one factor c ~ U(0.3, 0.7)."""
+
+    base = 1.0 / layered_model(nodes, cells, seed).astype(float)
+    depth = -nodes[cells].mean(axis=1)[:, 1]
+    factor = np.random.default_rng(seed + 7919).uniform(0.3, 0.7)
+    fronts = max_depth * (np.arange(steps) / max(steps - 1, 1)) ** 0.7
+    return np.where(depth[None, :] < fronts[:, None], base[None, :] * factor, base[None, :])

@@ -402,3 +402,14 @@ class TimeLapseResult:
     final_log_models: Tensor  # (S, C): mean of the windows' log models per step
     covered: Tensor           # (S,) steps some inverted window contains
     windows: list[dict]
+
+
+def window_share(count: int, rank: int, world: int) -> list[int]:
+    """Window indices of ``rank`` when ``world`` ranks split ``count`` independent windows:
+    contiguous, as equal as possible, every window in exactly one share."""
+
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must lie in [0, world)")
+    short, longer = divmod(int(count), int(world))
+    start = rank * short + min(rank, longer)
+    return list(range(start, start + short + (1 if rank < longer else 0)))

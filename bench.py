@@ -62,11 +62,14 @@ def parse_args():
     parser.add_argument("--e2e-steps", type=int, default=None)
     parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg (profiling runs)")
-    parser.add_argument("--workload", choices=("flat", "terrain", "box3d", "box3d-small"), default="flat",
+    parser.add_argument("--windows", type=int, default=None,
+                        help="timelapse workload: invert only the first K windows of this rank's share")
+    parser.add_argument("--workload", choices=("flat", "terrain", "box3d", "box3d-small", "timelapse"), default="flat",
                         help="flat: the 2.5D headline section; terrain: the 2.5D terrain section (40,000 triangles, "
                              "96 electrodes, 2538 rows, numerical geometric factors); box3d: the 3D box (244,800 "
                              "tetrahedra, 96 electrodes, 4000 rows); box3d-small: the same survey on 36,000 "
-                             "tetrahedra (profiling captures)")
+                             "tetrahedra (profiling captures); timelapse: the 363-window Gauss-Newton inversion of "
+                             "365 time steps on the flat section (windows/s)")
     return parser.parse_args()
 
 
@@ -214,6 +217,8 @@ def run_reference(args, rank: int, world: int) -> dict:
     from oracle import baseline
     from oracle.ert2p5d import Oracle2p5D
 
+    if args.workload == "timelapse":
+        return timelapse_reference(args, world)
     if args.workload == "terrain":
         return {"impl": "reference", "unavailable": "no CPU run of the terrain workload: the reference's set-up "
                                                     "alone solves 19 x 96 FP64 systems of 321,201 dofs"}
@@ -262,6 +267,37 @@ def run_reference(args, rank: int, world: int) -> dict:
         "cpu_baseline": {"value": value, "unit": "entries/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def timelapse_reference(args, world: int) -> dict:
+    """The reference's driver restated by the FP64 oracle (SciPy SuperLU fields, dense
+    Jacobians, CSR CGLS) on the host cores: one full window (window 100, up to 15 iterations)."""
+
+    sys.path.insert(0, str(ROOT))
+    from adtlert_b200 import synthetic
+    from oracle.ert2p5d import Oracle2p5D
+    from oracle.timelapse import OracleTimeLapse
+
+    nodes, cells, electrodes, rows = synthetic.flat_section()
+    rho = synthetic.infiltration_series(nodes, cells, TIMELAPSE_STEPS, seed=0)
+    operator = Oracle2p5D(nodes, cells, electrodes, rows)
+    clean = np.stack([operator.apparent_resistivity(1.0 / rho[t]) for t in range(100, 103)])
+    noise = np.random.default_rng(1).standard_normal((TIMELAPSE_STEPS, len(rows)))[100:103]
+    observed = clean * np.exp(TIMELAPSE_NOISE * noise)
+    initial = np.tile(np.log(np.median(observed, axis=1))[:, None], (1, len(cells)))
+    oracle = OracleTimeLapse(nodes, cells, electrodes, rows, data_std=float(np.log1p(TIMELAPSE_NOISE)))
+    start = time.perf_counter()
+    _, _, chi2, _ = oracle.invert_window(np.log(observed), initial)
+    seconds = time.perf_counter() - start
+    value = 1.0 / seconds
+    sample = f"window 100 of 363: {len(chi2)} Gauss-Newton iterations of the FP64 oracle driver, {seconds:.1f} s"
+    return {"metric": "windows_per_second", "value": value, "unit": "windows/s", "n_gpus": world, "steps": 1,
+            "warmup": 0, "ms_per_step": 1e3 * seconds, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": timelapse_config(363, world, len(rows), len(cells)),
+            "cpu_baseline": {"value": value, "unit": "windows/s", "cores": int(torch.get_num_threads()), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def config(D, C, W, E, world) -> dict:
@@ -902,6 +938,137 @@ def cpu_baseline(args, nodes, cells, electrodes, rows) -> dict:
             "sample": f"{count} models x full jacobian ({D} x {C}): FP64 SuperLU fields + C contraction, {total:.1f} s"}
 
 
+TIMELAPSE_STEPS = 365
+TIMELAPSE_NOISE = 0.02
+
+
+def timelapse_workload():
+    """Flat section, 365-step infiltration series and its noisy observed apparent resistivities
+    (FEM of every step by this library, times exp(0.02 N(0, 1)), seed 1)."""
+
+    from adtlert_b200 import ERTForward2p5D, Mesh, Survey, synthetic
+
+    nodes, cells, electrodes, rows = synthetic.flat_section()
+    forward = ERTForward2p5D.from_mesh_survey(Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, rows))
+    rho = synthetic.infiltration_series(nodes, cells, TIMELAPSE_STEPS, seed=0)
+    clean = np.concatenate([forward.apparent_resistivity_series(torch.as_tensor(1.0 / rho[i:i + 8], dtype=torch.float32))
+                            .numpy() for i in range(0, TIMELAPSE_STEPS, 8)]).astype(float)
+    observed = clean * np.exp(TIMELAPSE_NOISE * np.random.default_rng(1).standard_normal(clean.shape))
+    initial = np.tile(np.log(np.median(observed, axis=1))[:, None], (1, len(cells)))
+    return forward, nodes, cells, electrodes, rows, rho, clean, observed, initial
+
+
+def timelapse_config(windows, world, D, C) -> dict:
+    return {
+        "workload": f"time-lapse Gauss-Newton inversion: {TIMELAPSE_STEPS} steps on the 2.5D flat section ({C} cells, "
+                    f"{D} rows, 17 wavenumbers), {windows} windows of 3 steps, first-order spatial (50) and temporal "
+                    f"(10) smoothness, CGLS 60 iterations, line search, at most 15 iterations per window",
+        "windows": windows,
+        "steps": TIMELAPSE_STEPS,
+        "cells": C,
+        "rows": D,
+        "noise": "2 % multiplicative (data_std log1p(0.02))",
+        "l2": "inputs larger than L2 (three 47 MB Jacobians per window, re-read by every CGLS iteration); no flush",
+        "parallelism": f"windows split across {world} rank(s) (window_share), no collective on the data path",
+    }
+
+
+def run_timelapse(args, rank: int, world: int) -> dict | None:
+    from adtlert_b200.timelapse import WindowedInversion, WindowSettings, window_share, window_starts
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    forward, nodes, cells, electrodes, rows, rho, clean, observed, initial = timelapse_workload()
+    D, C = forward.D, forward.C
+    settings = WindowSettings(data_std=float(np.log1p(TIMELAPSE_NOISE)))
+    starts = window_starts(TIMELAPSE_STEPS, 3)
+    mine = window_share(len(starts), rank, world)
+    if args.windows is not None:
+        mine = mine[:args.windows]
+    observed_log = torch.as_tensor(np.log(observed), device=device)
+    initial_log = torch.as_tensor(initial, device=device)
+    inversion = WindowedInversion(forward, settings)
+    stream = torch.cuda.current_stream(device)
+    with ClockSampler(device.index) as clocks:
+        for index in starts[-min(2, len(starts)):]:  # untimed warm-up windows, then a cold cache
+            inversion.invert_window(observed_log[index:index + 3], initial_log[index:index + 3])
+        inversion.linearize = type(inversion.linearize)(forward)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        launches0 = forward.kernel_launches()
+        begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        wall = time.perf_counter()
+        begin.record(stream)
+        result = inversion.run(np.log(observed), initial, windows=mine)  # host arrays in
+        end.record(stream)
+        host_models = result.final_log_models.cpu()  # host result out
+        wall = time.perf_counter() - wall
+    launches = forward.kernel_launches() - launches0
+    elapsed = max_over_ranks(begin.elapsed_time(end) / 1e3, world)
+    total_windows = len(mine) * world if args.windows is not None else len(starts)
+    iterations = [w["iterations"] for w in result.windows]
+    chi2 = [w["final_chi2"] for w in result.windows]
+    covered = result.covered.cpu().numpy()
+    final = result.final_log_models[result.covered]
+    predicted, _ = inversion.linearize(final, jacobian=False)
+    predicted = np.exp(predicted.cpu().numpy())
+    rms_observed = float(np.sqrt(np.mean((predicted / observed[covered] - 1.0) ** 2)))
+    rms_clean = float(np.sqrt(np.mean((predicted / clean[covered] - 1.0) ** 2)))
+    if rank != 0:
+        return None
+    line = {
+        "metric": "windows_per_second",
+        "value": total_windows / elapsed,
+        "unit": "windows/s",
+        "n_gpus": world,
+        "steps": len(mine),
+        "warmup": 2,
+        "ms_per_step": 1e3 * elapsed / max(len(mine), 1),
+        "higher_is_better": True,
+        "scaling": "strong" if args.windows is None else "weak",
+        "vs_baseline": None,
+        "dtype": "f32 Jacobians and fields / f64 factorization and CGLS vectors",
+        "data": "synthetic (seeded layered base model, infiltration front to 8 m, 2 % noise)",
+        "config": timelapse_config(total_windows, world, D, C),
+        "misfit": {"final_chi2_mean": float(np.mean(chi2)), "final_chi2_max": float(np.max(chi2)),
+                   "rhoa_rms_rel_error_vs_observed": rms_observed, "rhoa_rms_rel_error_vs_noise_free": rms_clean,
+                   "iterations_mean": float(np.mean(iterations)), "iterations_max": int(np.max(iterations))},
+        "linearized_models": inversion.linearize.evaluations,
+        "e2e": {"value": total_windows / max_over_ranks(wall, world), "unit": "windows/s",
+                "h2d_bytes_per_step": int((observed.nbytes + initial.nbytes) / max(len(mine), 1)),
+                "d2h_bytes_per_step": int(host_models.numel() * 8 / max(len(mine), 1)),
+                "note": "the same run, wall clock, observed data and initial models copied from host arrays and "
+                        "the combined models read back"},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(launches),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = timelapse_cpu_baseline(nodes, cells, electrodes, rows, observed, initial,
+                                                      float(np.mean(iterations)))
+    return line
+
+
+def timelapse_cpu_baseline(nodes, cells, electrodes, rows, observed, initial, iterations_per_window: float) -> dict:
+    """The FP64 oracle restatement of the reference's driver (SciPy SuperLU fields, dense
+    Jacobians, SciPy/torch CSR CGLS on the host) timed on one window for 2 Gauss-Newton
+    iterations, extrapolated to windows/s with the GPU run's mean iterations per window."""
+
+    sys.path.insert(0, str(ROOT))
+    from oracle.timelapse import OracleTimeLapse
+
+    oracle = OracleTimeLapse(nodes, cells, electrodes, rows, max_iterations=2, data_std=float(np.log1p(TIMELAPSE_NOISE)),
+                             step_tolerance=0.0)
+    start = time.perf_counter()
+    _, _, chi2, taus = oracle.invert_window(np.log(observed[100:103]), initial[100:103])
+    seconds = time.perf_counter() - start
+    per_iteration = seconds / len(chi2)
+    per_window = per_iteration * max(iterations_per_window, 1.0)
+    threads = int(torch.get_num_threads())
+    return {"value": 1.0 / per_window, "unit": "windows/s", "cores": threads, "kind": "port",
+            "sample": f"window 100, {len(chi2)} Gauss-Newton iterations of the FP64 oracle driver in {seconds:.1f} s "
+                      f"({per_iteration:.1f} s per iteration incl. the first linearization), extrapolated to "
+                      f"{iterations_per_window:.1f} iterations per window"}
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -912,7 +1079,9 @@ def main():
             print(json.dumps(run_reference(args, rank, world)), flush=True)
         return
     rank, world = dist_setup(args)
-    if args.workload in BOX3D:
+    if args.workload == "timelapse":
+        result = run_timelapse(args, rank, world)
+    elif args.workload in BOX3D:
         result = run_box3d(args, rank, world)
     elif args.workload == "terrain":
         result = run_terrain(args, rank, world)
