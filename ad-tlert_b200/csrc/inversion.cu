@@ -19,10 +19,10 @@
 // iteration stops turns the rest of the launched iterations into no-ops, so the host never waits
 // inside the loop):
 //   normal_data_kernel   per block, a range of rows of one model: q_d = w_d (J_d . p_t), then
-//                        partial += J_d w_d q_d, kept in registers; written once per block.
+//                        partial += J_d w_d q_d, in float64 registers; written once per block.
 //   normal_reduce_kernel u = sum of the block partials (fixed order) + ls L p_t + lt T^T T p,
 //                        with L = R^T R from neighbour lists; block partials of p.u.
-//   cgls_update_kernel   one block: alpha, x, s, gamma', beta, p (and its float copy).
+//   cgls_update_kernel   one block: alpha, x, s, gamma', beta, p.
 // Every reduction runs in a fixed order, so a step is bitwise repeatable.
 #include "adt_internal.h"
 
@@ -45,8 +45,7 @@ struct Workspace {
   double* s;
   double* p;
   double* u;
-  float* p32;
-  float* partial;
+  double* partial;
   double* dots;
   int ctas_per_model;
   int reduce_blocks;
@@ -73,8 +72,7 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
   char* s = take(n * sizeof(double));
   char* p = take(n * sizeof(double));
   char* u = take(n * sizeof(double));
-  char* p32 = take(n * sizeof(float));
-  char* partial = take((size_t)T * per * C * sizeof(float));
+  char* partial = take((size_t)T * per * C * sizeof(double));
   char* dots = take((size_t)reduce_blocks * sizeof(double));
   (void)D;
   if (w) {
@@ -82,8 +80,7 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
     w->s = reinterpret_cast<double*>(s);
     w->p = reinterpret_cast<double*>(p);
     w->u = reinterpret_cast<double*>(u);
-    w->p32 = reinterpret_cast<float*>(p32);
-    w->partial = reinterpret_cast<float*>(partial);
+    w->partial = reinterpret_cast<double*>(partial);
     w->dots = reinterpret_cast<double*>(dots);
     w->ctas_per_model = per;
     w->reduce_blocks = reduce_blocks;
@@ -103,27 +100,29 @@ __device__ __forceinline__ void axpy4(float4& acc, float4 a, float s) {
 }
 
 // Data pass. `given` (T x D) replaces the row products q_d when not null (A^T b: q = b_data).
+// J is read as float32 (streamed once), every product and sum is float64: CGLS truncated at
+// tens of iterations is sensitive to rounding in A^T A p (float32 rounding of it alone moves the
+// least-squares residual after 60 iterations by ~6e-4), so only the matrix is float32.
 template <int VEC>
 __global__ void __launch_bounds__(kPassThreads) normal_data_kernel(
-    const float* __restrict__ J, int D, int C, const double* __restrict__ weights, const float* __restrict__ vec,
-    const double* __restrict__ given, int ctas_per_model, float* __restrict__ partial,
+    const float* __restrict__ J, int D, int C, const double* __restrict__ weights, const double* __restrict__ vec,
+    const double* __restrict__ given, int ctas_per_model, double* __restrict__ partial,
     const CglsState* __restrict__ state) {
   adt::chain_wait();
   if (state != nullptr && state->done) return;
+  extern __shared__ double pvec[];  // p_t (C doubles) when the rows' products are formed here
   const int t = blockIdx.x / ctas_per_model, k = blockIdx.x % ctas_per_model;
   const int rows_per = (D + ctas_per_model - 1) / ctas_per_model;
   const int d0 = k * rows_per, d1 = min(D, d0 + rows_per);
   const int C4 = C >> 2;
+  if (given == nullptr)
+    for (int c = threadIdx.x; c < C; c += kPassThreads) pvec[c] = vec[(size_t)t * C + c];
+  __syncthreads();
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float4* p4 = reinterpret_cast<const float4*>(vec + (size_t)t * C);
-  float4 pv[VEC], acc[VEC];
+  double acc[VEC][4];
 #pragma unroll
-  for (int v = 0; v < VEC; ++v) {
-    const int idx = threadIdx.x + v * kPassThreads;
-    pv[v] = (given == nullptr && idx < C4) ? p4[idx] : zero;
-    acc[v] = zero;
-  }
-  __shared__ float red[2][kPassThreads / 32];
+  for (int v = 0; v < VEC; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.0;
+  __shared__ double red[2][kPassThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int parity = 0;
   for (int d = d0; d < d1; ++d) {
@@ -135,32 +134,50 @@ __global__ void __launch_bounds__(kPassThreads) normal_data_kernel(
       r[v] = idx < C4 ? __ldcs(row + idx) : zero;
     }
     const double w = weights[(size_t)t * D + d];
-    float q;
+    double q;
     if (given != nullptr) {
-      q = (float)given[(size_t)t * D + d];
+      q = given[(size_t)t * D + d];
     } else {
-      float dot = 0.f;
+      double dot = 0.0;
 #pragma unroll
-      for (int v = 0; v < VEC; ++v) dot += dot4(r[v], pv[v]);
+      for (int v = 0; v < VEC; ++v) {
+        const int idx = threadIdx.x + v * kPassThreads;
+        if (idx < C4) {
+          const double* pc = pvec + 4 * idx;
+          dot = fma((double)r[v].x, pc[0], dot);
+          dot = fma((double)r[v].y, pc[1], dot);
+          dot = fma((double)r[v].z, pc[2], dot);
+          dot = fma((double)r[v].w, pc[3], dot);
+        }
+      }
 #pragma unroll
       for (int offset = 16; offset > 0; offset >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, offset);
       if (lane == 0) red[parity][warp] = dot;
       __syncthreads();
-      dot = 0.f;
+      dot = 0.0;
 #pragma unroll
       for (int i = 0; i < kPassThreads / 32; ++i) dot += red[parity][i];
       parity ^= 1;
-      q = (float)(w * (double)dot);
+      q = w * dot;
     }
-    const float wq = (float)(w * (double)q);
+    const double wq = w * q;
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) axpy4(acc[v], r[v], wq);
+    for (int v = 0; v < VEC; ++v) {
+      acc[v][0] = fma((double)r[v].x, wq, acc[v][0]);
+      acc[v][1] = fma((double)r[v].y, wq, acc[v][1]);
+      acc[v][2] = fma((double)r[v].z, wq, acc[v][2]);
+      acc[v][3] = fma((double)r[v].w, wq, acc[v][3]);
+    }
   }
-  float4* out = reinterpret_cast<float4*>(partial + (size_t)blockIdx.x * C);
+  double* out = partial + (size_t)blockIdx.x * C;
 #pragma unroll
   for (int v = 0; v < VEC; ++v) {
     const int idx = threadIdx.x + v * kPassThreads;
-    if (idx < C4) out[idx] = acc[v];
+    if (idx < C4) {
+      double2* pair = reinterpret_cast<double2*>(out + 4 * idx);
+      pair[0] = make_double2(acc[v][0], acc[v][1]);
+      pair[1] = make_double2(acc[v][2], acc[v][3]);
+    }
   }
 }
 
@@ -182,7 +199,7 @@ __device__ __forceinline__ double block_sum(double value, double* shared) {
 // u = (sum of the data partials) + spatial L v_t + temporal T^T T v, element (t, c) per thread;
 // with `dot_with`, per-block partials of dot_with . u. `partial` may be null (regularizer only).
 __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
-    const float* __restrict__ partial, int ctas_per_model, int T, int C, const double* __restrict__ v,
+    const double* __restrict__ partial, int ctas_per_model, int T, int C, const double* __restrict__ v,
     const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_cell, const double* __restrict__ nbr_w2,
     double spatial, double temporal, const double* __restrict__ dot_with, double* __restrict__ u,
     double* __restrict__ dots, const CglsState* __restrict__ state) {
@@ -196,7 +213,7 @@ __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
     const int t = (int)(i / C), c = (int)(i % C);
     double sum = 0.0;
     if (partial != nullptr)
-      for (int k = 0; k < ctas_per_model; ++k) sum += (double)partial[((size_t)t * ctas_per_model + k) * C + c];
+      for (int k = 0; k < ctas_per_model; ++k) sum += partial[((size_t)t * ctas_per_model + k) * C + c];
     const double* vt = v + (size_t)t * C;
     const double vc = vt[c];
     double lap = 0.0;
@@ -217,7 +234,7 @@ __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
 // x = 0, s = p = A^T b (in u), gamma = gamma_0 = s.s.
 __global__ void __launch_bounds__(kUpdateThreads) cgls_start_kernel(CglsState* st, int64_t n, const double* __restrict__ u,
                                                                     double* __restrict__ x, double* __restrict__ s,
-                                                                    double* __restrict__ p, float* __restrict__ p32) {
+                                                                    double* __restrict__ p) {
   adt::chain_wait();
   __shared__ double shared[kUpdateThreads / 32];
   double ss = 0.0;
@@ -226,7 +243,6 @@ __global__ void __launch_bounds__(kUpdateThreads) cgls_start_kernel(CglsState* s
     x[i] = 0.0;
     s[i] = value;
     p[i] = value;
-    p32[i] = (float)value;
     ss += value * value;
   }
   const double gamma = block_sum<kUpdateThreads>(ss, shared);
@@ -241,7 +257,7 @@ __global__ void __launch_bounds__(kUpdateThreads) cgls_start_kernel(CglsState* s
 __global__ void __launch_bounds__(kUpdateThreads) cgls_update_kernel(CglsState* st, int64_t n,
                                                                      const double* __restrict__ dots, int blocks,
                                                                      double* __restrict__ x, double* __restrict__ s,
-                                                                     double* __restrict__ p, float* __restrict__ p32,
+                                                                     double* __restrict__ p,
                                                                      const double* __restrict__ u, double tolerance) {
   adt::chain_wait();
   __shared__ double shared[kUpdateThreads / 32];
@@ -285,18 +301,24 @@ __global__ void __launch_bounds__(kUpdateThreads) cgls_update_kernel(CglsState* 
   for (int64_t i = threadIdx.x; i < n; i += kUpdateThreads) {
     const double value = s[i] + beta * p[i];
     p[i] = value;
-    p32[i] = (float)value;
   }
 }
 
 template <int VEC>
-void launch_data(const float* J, int T, int D, int C, const double* weights, const float* vec, const double* given,
+void launch_data(const float* J, int T, int D, int C, const double* weights, const double* vec, const double* given,
                  const Workspace& w, const CglsState* state, cudaStream_t s) {
-  adt::launch_chained(normal_data_kernel<VEC>, dim3(T * w.ctas_per_model), dim3(kPassThreads), 0, s, J, D, C, weights,
-                      vec, given, w.ctas_per_model, w.partial, state);
+  const size_t smem = given == nullptr ? (size_t)C * sizeof(double) : 0;
+  static bool raised = false;  // the dynamic shared-memory limit, raised once per instantiation
+  if (!raised) {
+    cudaFuncSetAttribute(normal_data_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         4 * kPassThreads * VEC * (int)sizeof(double));
+    raised = true;
+  }
+  adt::launch_chained(normal_data_kernel<VEC>, dim3(T * w.ctas_per_model), dim3(kPassThreads), smem, s, J, D, C,
+                      weights, vec, given, w.ctas_per_model, w.partial, state);
 }
 
-bool data_pass(const float* J, int T, int D, int C, const double* weights, const float* vec, const double* given,
+bool data_pass(const float* J, int T, int D, int C, const double* weights, const double* vec, const double* given,
                const Workspace& w, const CglsState* state, cudaStream_t s) {
   const int vec_per_thread = ((C >> 2) + kPassThreads - 1) / kPassThreads;
   switch (vec_per_thread) {
@@ -346,22 +368,22 @@ extern "C" adt_status adt_gn_step(adt_plan* p, const float* jacobian, int32_t st
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t n = (int64_t)steps * columns;
   // s_0 = A^T b = J^T W b_data - ls L m - lt T^T T m
-  data_pass(jacobian, steps, rows, columns, data_weights, w.p32, data_rhs, w, nullptr, s);
-  adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s, (const float*)w.partial,
+  data_pass(jacobian, steps, rows, columns, data_weights, w.p, data_rhs, w, nullptr, s);
+  adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s, (const double*)w.partial,
                       w.ctas_per_model, (int)steps, (int)columns, models, neighbour_ptr, neighbour_cells,
                       neighbour_weights, -spatial, -temporal, (const double*)nullptr, w.u, w.dots,
                       (const CglsState*)nullptr);
   adt::launch_chained(cgls_start_kernel, dim3(1), dim3(kUpdateThreads), 0, s, w.state, n, (const double*)w.u, step,
-                      w.s, w.p, w.p32);
+                      w.s, w.p);
   p->launches += 3;
   for (int it = 0; it < iterations; ++it) {
-    data_pass(jacobian, steps, rows, columns, data_weights, w.p32, nullptr, w, w.state, s);
+    data_pass(jacobian, steps, rows, columns, data_weights, w.p, nullptr, w, w.state, s);
     adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s,
-                        (const float*)w.partial, w.ctas_per_model, (int)steps, (int)columns, (const double*)w.p,
+                        (const double*)w.partial, w.ctas_per_model, (int)steps, (int)columns, (const double*)w.p,
                         neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal, (const double*)w.p, w.u,
                         w.dots, (const CglsState*)w.state);
     adt::launch_chained(cgls_update_kernel, dim3(1), dim3(kUpdateThreads), 0, s, w.state, n, (const double*)w.dots,
-                        w.reduce_blocks, step, w.s, w.p, w.p32, (const double*)w.u, tolerance);
+                        w.reduce_blocks, step, w.s, w.p, (const double*)w.u, tolerance);
     p->launches += 3;
   }
   return adt::check_launch(p, "gauss-newton step");
@@ -376,7 +398,7 @@ extern "C" adt_status adt_gn_regularize(adt_plan* p, int32_t steps, int32_t colu
     return adt::fail(p, ADT_INVALID_ARG, "adt_gn_regularize: invalid arguments");
   const int64_t n = (int64_t)steps * columns;
   adt::launch_chained(normal_reduce_kernel, dim3((unsigned)((n + kReduceThreads - 1) / kReduceThreads)),
-                      dim3(kReduceThreads), 0, (cudaStream_t)stream, (const float*)nullptr, 0, (int)steps,
+                      dim3(kReduceThreads), 0, (cudaStream_t)stream, (const double*)nullptr, 0, (int)steps,
                       (int)columns, models, neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal,
                       (const double*)nullptr, out, (double*)nullptr, (const CglsState*)nullptr);
   p->launches += 1;
