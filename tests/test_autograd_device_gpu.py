@@ -75,7 +75,7 @@ def test_cuda_series_goes_forward_and_backward_on_the_device(forward, monkeypatc
     assert op.kernel_launches() > launches
     assert out_gpu.device.type == "cuda" and gpu.grad.device.type == "cuda"
     assert max(large, default=0) < op.C, f"a host copy of {max(large)} elements was made"
-    assert_close(out_gpu.cpu(), out_cpu.detach(), 1e-6, "apparent resistivity, GPU vs CPU path")
+    assert_close(out_gpu.detach().cpu(), out_cpu.detach(), 1e-6, "apparent resistivity, GPU vs CPU path")
     assert_close(gpu.grad.cpu(), cpu.grad, 1e-5, "conductivity gradient, GPU vs CPU path")
 
 
