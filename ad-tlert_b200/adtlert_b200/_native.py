@@ -49,6 +49,14 @@ SYMBOLS = (
     "adt_gn_workspace_bytes",
     "adt_gn_step",
     "adt_gn_regularize",
+    "adt_mlp_gemm_splits",
+    "adt_mlp_gemm",
+    "adt_mlp_epilogue",
+    "adt_mlp_loss",
+    "adt_mlp_bias_grad",
+    "adt_mlp_adam",
+    "adt_mlp_transpose",
+    "adt_mlp_to_bf16",
     "adt_kernel_launches",
 )
 
@@ -156,6 +164,15 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_gn_step": (status, [_p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, ctypes.c_double, ctypes.c_double,
                                  _i32, ctypes.c_double, _p, _p, ctypes.c_size_t, _i32, _p]),
         "adt_gn_regularize": (status, [_p, _i32, _i32, _p, _p, _p, ctypes.c_double, ctypes.c_double, _p, _p, _p]),
+        "adt_mlp_gemm_splits": (_i32, [_i32, _i32, _i32, _i32]),
+        "adt_mlp_gemm": (status, [_p, _p, _i32, _i32, _i32, _i32, _p, ctypes.c_size_t, _p, _p]),
+        "adt_mlp_epilogue": (status, [_i32, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p]),
+        "adt_mlp_loss": (status, [_p, _p, _i32, _i32, _i32, _p, _p, _p, _p]),
+        "adt_mlp_bias_grad": (status, [_p, _i32, _i32, _p, _p]),
+        "adt_mlp_adam": (status, [_p, _p, _p, _p, _i64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, ctypes.c_float, _p, _p]),
+        "adt_mlp_transpose": (status, [_p, _i32, _i32, _p, _p]),
+        "adt_mlp_to_bf16": (status, [_p, _i64, _p, _p]),
         "adt_kernel_launches": (_i64, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():

@@ -303,19 +303,27 @@ class WindowedInversion:
         return (residual * residual).sum() + (models * self.regularized(models)).sum()
 
     # ---------------------------------------------------------------- one window
-    def invert_window(self, observed_log: Tensor, initial_log: Tensor, screen=None) -> WindowResult:
+    def invert_window(self, observed_log: Tensor, initial_log: Tensor, screen=None,
+                      previous: Tensor | None = None) -> WindowResult:
         """Gauss-Newton iterations of one window (adtlert/inversion/core.py:81-300): observed
         ``(T, D)`` log data, initial ``(T, C)`` log models. With ``screen`` (a surrogate screen,
         see surrogate.py) the line search runs on the screen's predictions and only the accepted
         model is solved by the FEM, which falls back to the plain candidate evaluation whenever
-        that model does not lower the objective."""
+        that model does not lower the objective; the screen may also start the window from
+        ``previous`` (the preceding window's final models) instead of ``initial_log``."""
 
         s, f = self.settings, self.forward
         observed = observed_log.to(self.device, torch.float64)
         T = int(observed.shape[0])
         weights = torch.full((T, f.D), 1.0 / float(s.data_std), dtype=torch.float64, device=self.device)
         models = self._clip(initial_log.to(self.device, torch.float64)).contiguous()
-        predicted, J = self.linearize(models)
+        start, bound = (models, None) if screen is None else screen.window_start(self, observed, models, previous)
+        predicted, J = self.linearize(start)
+        if bound is not None and float(self.objective(start, predicted, observed, weights)) > bound:
+            screen.reject_start()  # the FEM does not confirm the screened start
+            predicted, J = self.linearize(models)
+        else:
+            models = start
         result = WindowResult(models, predicted, [])
         scale = max(math.sqrt(models.numel()), 1.0)
         for _ in range(s.max_iterations):
@@ -373,10 +381,13 @@ class WindowedInversion:
         total = torch.zeros_like(initial)
         count = torch.zeros(steps, dtype=torch.float64, device=self.device)
         reports = []
+        previous, previous_start = None, None
         for index in chosen:
             start = starts[index]
             end = start + window_size
-            window = self.invert_window(observed[start:end], initial[start:end], screen)
+            warm = previous if previous_start == start - 1 else None
+            window = self.invert_window(observed[start:end], initial[start:end], screen, warm)
+            previous, previous_start = window.log_models, start
             total[start:end] += window.log_models
             count[start:end] += 1.0
             reports.append({"window": index, "start": start, "iterations": len(window.chi2),

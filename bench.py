@@ -62,6 +62,8 @@ def parse_args():
     parser.add_argument("--e2e-steps", type=int, default=None)
     parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg (profiling runs)")
+    parser.add_argument("--no-surrogate", action="store_true", help="timelapse workload: plain FEM pass only")
+    parser.add_argument("--training-models", type=int, default=20_000, help="timelapse workload: surrogate training set")
     parser.add_argument("--windows", type=int, default=None,
                         help="timelapse workload: invert only the first K windows of this rank's share")
     parser.add_argument("--workload", choices=("flat", "terrain", "box3d", "box3d-small", "timelapse"), default="flat",
@@ -973,7 +975,90 @@ def timelapse_config(windows, world, D, C) -> dict:
     }
 
 
+def timed_inversion(inversion, observed, initial, windows, screen, device, world):
+    """One pass over ``windows``: CUDA-event time (max over ranks), wall time with host arrays in
+    and host models out, the result, and the library launches."""
+
+    stream = torch.cuda.current_stream(device)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    launches0 = inversion.forward.kernel_launches()
+    begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    wall = time.perf_counter()
+    begin.record(stream)
+    result = inversion.run(np.log(observed), initial, windows=windows, screen=screen)  # host arrays in
+    end.record(stream)
+    host_models = result.final_log_models.cpu()  # host result out
+    wall = time.perf_counter() - wall
+    launches = inversion.forward.kernel_launches() - launches0
+    return max_over_ranks(begin.elapsed_time(end) / 1e3, world), max_over_ranks(wall, world), result, launches, host_models
+
+
+def inversion_misfit(inversion, result, observed, clean) -> dict:
+    covered = result.covered.cpu().numpy()
+    predicted, _ = inversion.linearize(result.final_log_models[result.covered], jacobian=False)
+    predicted = np.exp(predicted.cpu().numpy())
+    iterations = [w["iterations"] for w in result.windows]
+    chi2 = [w["final_chi2"] for w in result.windows]
+    return {"final_chi2_mean": float(np.mean(chi2)), "final_chi2_max": float(np.max(chi2)),
+            "rhoa_rms_rel_error_vs_observed": float(np.sqrt(np.mean((predicted / observed[covered] - 1.0) ** 2))),
+            "rhoa_rms_rel_error_vs_noise_free": float(np.sqrt(np.mean((predicted / clean[covered] - 1.0) ** 2))),
+            "iterations_mean": float(np.mean(iterations)), "iterations_max": int(np.max(iterations)),
+            "linearized_models": inversion.linearize.evaluations}, predicted
+
+
+def train_surrogate(forward, count: int, device) -> tuple:
+    """Training set from the FEM, the trained surrogate, and its report (times, held-out error,
+    GEMM throughput of a training step measured with CUDA events)."""
+
+    from adtlert_b200.surrogate import Surrogate, training_set
+
+    torch.cuda.synchronize(device)
+    start = time.perf_counter()
+    models, data = training_set(forward, count + 1024, seed=11)
+    torch.cuda.synchronize(device)
+    data_s = time.perf_counter() - start
+    surrogate = Surrogate(forward, seed=0)
+    start = time.perf_counter()
+    history = surrogate.fit(models[:count], data[:count], epochs=30)
+    torch.cuda.synchronize(device)
+    train_s = time.perf_counter() - start
+    held_out = surrogate.predict_log10(models[count:])
+    error = (10.0 ** (held_out - data[count:]) - 1.0).double()
+    # one training step timed alone: FLOPs of its 11 GEMMs over the step's device time
+    net = surrogate.mlp
+    x16 = surrogate._inputs(models[:net.batch], net.batch)
+    xt16 = x16.T.contiguous()
+    target = surrogate._targets(data[:net.batch], net.batch)
+    for _ in range(3):
+        net.gradients(x16, xt16, target)
+    stream = torch.cuda.current_stream(device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    a.record(stream)
+    for _ in range(reps):
+        net.gradients(x16, xt16, target)
+    b.record(stream)
+    torch.cuda.synchronize(device)
+    step_ms = a.elapsed_time(b) / reps
+    sizes = net.sizes
+    # forward, weight gradient and input gradient GEMMs (no input gradient for the first layer)
+    flops = sum(2.0 * net.batch * sizes[i] * sizes[i + 1] * (3 if i > 0 else 2) for i in range(len(sizes) - 1))
+    peak = measured_peaks()["bf16_tflops"]
+    achieved = flops / (step_ms * 1e-3) / 1e12
+    net.check_error()
+    report = {"training_models": count, "held_out_models": 1024, "epochs": len(history), "data_seconds": data_s,
+              "train_seconds": train_s, "final_train_mse_standardized": history[-1],
+              "held_out_rhoa_rms_rel_error": float(torch.sqrt((error ** 2).mean())),
+              "held_out_rhoa_max_rel_error": float(error.abs().max()),
+              "forward_backward_ms": step_ms, "forward_backward_gflop": flops / 1e9,
+              "gemm_tflops": achieved, "tensor_frac_of_measured_bf16_peak": achieved / peak,
+              "network": "6144-1024-1024-1024-1232 (padded 1280), GELU, BF16 weights/activations, FP32 accumulate, Adam"}
+    return surrogate, report
+
+
 def run_timelapse(args, rank: int, world: int) -> dict | None:
+    from adtlert_b200.surrogate import SurrogateScreen
     from adtlert_b200.timelapse import WindowedInversion, WindowSettings, window_share, window_starts
 
     device = torch.device("cuda", torch.cuda.current_device())
@@ -984,66 +1069,72 @@ def run_timelapse(args, rank: int, world: int) -> dict | None:
     mine = window_share(len(starts), rank, world)
     if args.windows is not None:
         mine = mine[:args.windows]
-    observed_log = torch.as_tensor(np.log(observed), device=device)
-    initial_log = torch.as_tensor(initial, device=device)
-    inversion = WindowedInversion(forward, settings)
-    stream = torch.cuda.current_stream(device)
-    with ClockSampler(device.index) as clocks:
-        for index in starts[-min(2, len(starts)):]:  # untimed warm-up windows, then a cold cache
-            inversion.invert_window(observed_log[index:index + 3], initial_log[index:index + 3])
-        inversion.linearize = type(inversion.linearize)(forward)
-        torch.cuda.synchronize(device)
-        barrier(world)
-        launches0 = forward.kernel_launches()
-        begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        wall = time.perf_counter()
-        begin.record(stream)
-        result = inversion.run(np.log(observed), initial, windows=mine)  # host arrays in
-        end.record(stream)
-        host_models = result.final_log_models.cpu()  # host result out
-        wall = time.perf_counter() - wall
-    launches = forward.kernel_launches() - launches0
-    elapsed = max_over_ranks(begin.elapsed_time(end) / 1e3, world)
     total_windows = len(mine) * world if args.windows is not None else len(starts)
-    iterations = [w["iterations"] for w in result.windows]
-    chi2 = [w["final_chi2"] for w in result.windows]
-    covered = result.covered.cpu().numpy()
-    final = result.final_log_models[result.covered]
-    predicted, _ = inversion.linearize(final, jacobian=False)
-    predicted = np.exp(predicted.cpu().numpy())
-    rms_observed = float(np.sqrt(np.mean((predicted / observed[covered] - 1.0) ** 2)))
-    rms_clean = float(np.sqrt(np.mean((predicted / clean[covered] - 1.0) ** 2)))
+    with ClockSampler(device.index) as clocks:
+        warm = WindowedInversion(forward, settings)  # untimed warm-up windows on a separate cache
+        for index in starts[-2:]:
+            warm.invert_window(torch.as_tensor(np.log(observed[index:index + 3])), torch.as_tensor(initial[index:index + 3]))
+        plain = WindowedInversion(forward, settings)
+        plain_s, plain_wall, plain_result, plain_launches, _ = timed_inversion(plain, observed, initial, mine, None,
+                                                                               device, world)
+        plain_misfit, plain_predicted = inversion_misfit(plain, plain_result, observed, clean)
+        screened_line = None
+        if not args.no_surrogate:
+            surrogate, report = train_surrogate(forward, args.training_models, device)
+            screened = WindowedInversion(forward, settings)
+            screen = SurrogateScreen(surrogate)
+            launches_before = surrogate.mlp.launches
+            s_s, s_wall, s_result, s_launches, _ = timed_inversion(screened, observed, initial, mine, screen, device,
+                                                                   world)
+            s_misfit, s_predicted = inversion_misfit(screened, s_result, observed, clean)
+            iterations = sum(w["iterations"] for w in s_result.windows)
+            screened_line = (s_s, s_wall, s_launches + surrogate.mlp.launches - launches_before, s_misfit, report,
+                             screen.counts, iterations, s_predicted)
     if rank != 0:
         return None
     line = {
         "metric": "windows_per_second",
-        "value": total_windows / elapsed,
+        "value": total_windows / plain_s,
         "unit": "windows/s",
         "n_gpus": world,
         "steps": len(mine),
         "warmup": 2,
-        "ms_per_step": 1e3 * elapsed / max(len(mine), 1),
+        "ms_per_step": 1e3 * plain_s / max(len(mine), 1),
         "higher_is_better": True,
         "scaling": "strong" if args.windows is None else "weak",
         "vs_baseline": None,
-        "dtype": "f32 Jacobians and fields / f64 factorization and CGLS vectors",
+        "dtype": "f32 Jacobians and fields / f64 factorization and CGLS / bf16 surrogate",
         "data": "synthetic (seeded layered base model, infiltration front to 8 m, 2 % noise)",
         "config": timelapse_config(total_windows, world, D, C),
-        "misfit": {"final_chi2_mean": float(np.mean(chi2)), "final_chi2_max": float(np.max(chi2)),
-                   "rhoa_rms_rel_error_vs_observed": rms_observed, "rhoa_rms_rel_error_vs_noise_free": rms_clean,
-                   "iterations_mean": float(np.mean(iterations)), "iterations_max": int(np.max(iterations))},
-        "linearized_models": inversion.linearize.evaluations,
-        "e2e": {"value": total_windows / max_over_ranks(wall, world), "unit": "windows/s",
+        "misfit": plain_misfit,
+        "e2e": {"value": total_windows / plain_wall, "unit": "windows/s",
                 "h2d_bytes_per_step": int((observed.nbytes + initial.nbytes) / max(len(mine), 1)),
-                "d2h_bytes_per_step": int(host_models.numel() * 8 / max(len(mine), 1)),
+                "d2h_bytes_per_step": int(initial.nbytes / max(len(mine), 1)),
                 "note": "the same run, wall clock, observed data and initial models copied from host arrays and "
                         "the combined models read back"},
         "clocks": clocks.summary(),
-        "gpu_launches": int(launches),
+        "gpu_launches": int(plain_launches),
     }
+    if screened_line is not None:
+        s_s, s_wall, s_launches, s_misfit, report, counts, iterations, s_predicted = screened_line
+        line["value"] = total_windows / s_s
+        line["ms_per_step"] = 1e3 * s_s / max(len(mine), 1)
+        line["misfit"] = s_misfit
+        line["e2e"]["value"] = total_windows / s_wall
+        line["gpu_launches"] = int(s_launches)
+        line["plain_fem"] = {"value": total_windows / plain_s, "e2e": total_windows / plain_wall,
+                             "misfit": plain_misfit, "gpu_launches": int(plain_launches)}
+        line["speedup_vs_plain_fem"] = plain_s / s_s
+        line["screened_vs_plain_rhoa_rms_rel_difference"] = float(
+            np.sqrt(np.mean((s_predicted / plain_predicted - 1.0) ** 2)))
+        line["surrogate"] = report
+        line["screening"] = dict(counts, iterations=iterations,
+                                 fallback_rate=(counts["line_search_fallbacks"] + counts["warm_start_fallbacks"])
+                                 / max(1, counts["line_search_screened"] + counts["line_search_fallbacks"]
+                                       + counts["warm_starts"]))
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = timelapse_cpu_baseline(nodes, cells, electrodes, rows, observed, initial,
-                                                      float(np.mean(iterations)))
+                                                      plain_misfit["iterations_mean"])
     return line
 
 

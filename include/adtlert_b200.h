@@ -320,6 +320,40 @@ adt_status adt_gn_regularize(adt_plan* plan, int32_t steps, int32_t columns, con
                              const int32_t* neighbour_cells, const double* neighbour_weights, double spatial,
                              double temporal, const double* models, double* out, adt_stream stream);
 
+/* Kernels of the learned apparent-resistivity surrogate (BF16 operands, FP32 accumulation). No
+ * counterpart in the reference, whose inversion evaluates every line-search and window candidate
+ * with the FEM (adtlert/inversion/core.py:224-257, objective.py:168-192); the surrogate screens
+ * those candidates and the FEM still judges every accepted model. Device pointers; BF16 arrays
+ * are passed as void*.
+ * adt_mlp_gemm: partial[s][m][n] = sum over split s's K range of a[m][k] b[n][k] (a: m x k, b:
+ *   n x k, row-major BF16, 16-byte aligned; m, n multiples of 128, k of 64), on tcgen05 tensor
+ *   cores; `splits` must be the value adt_mlp_gemm_splits returns for these sizes (it fills the
+ *   multiprocessors and gives every split at least one 64-wide K chunk); partial holds at least
+ *   splits*m*n floats; *error is set to 1 when a bounded wait inside the kernel ran out.
+ * adt_mlp_epilogue: sums the splits in order and applies mode 0 (z = sum + bias -> z_out; y =
+ *   gelu(z) -> row_out and, if not NULL, col_out[n][m]), 1 (f32_out = sum + bias), 2 (g = sum *
+ *   gelu'(z_in) -> row_out, col_out) or 3 (f32_out = sum); gelu is the tanh form.
+ * adt_mlp_loss: g = 2 (pred - target) / (m n_valid) on columns < n_valid (0 beyond) -> g_row,
+ *   g_col (transposed); sums[(m / 32) (n / 32)] receives per-tile squared-error sums.
+ * adt_mlp_bias_grad: db[n] = sum_m g_col[n][m]. adt_mlp_adam: one Adam step on FP32 parameters
+ *   (correction1 = 1 / (1 - beta1^t), correction2 = 1 / (1 - beta2^t)), writing the BF16 copy if
+ *   params_bf16 is not NULL. adt_mlp_transpose: out[c][r] = in[r][c] (BF16, sides multiples of
+ *   32). adt_mlp_to_bf16: FP32 -> BF16 (round to nearest even). */
+int32_t adt_mlp_gemm_splits(int32_t m, int32_t n, int32_t k, int32_t multiprocessors);
+adt_status adt_mlp_gemm(const void* a, const void* b, int32_t m, int32_t n, int32_t k, int32_t splits,
+                        float* partial, size_t partial_floats, int32_t* error, adt_stream stream);
+adt_status adt_mlp_epilogue(int32_t mode, const float* partial, int32_t splits, int32_t m, int32_t n,
+                            const float* bias, const void* z_in, void* z_out, void* row_out, void* col_out,
+                            float* f32_out, adt_stream stream);
+adt_status adt_mlp_loss(const float* pred, const float* target, int32_t m, int32_t n, int32_t n_valid,
+                        void* g_row, void* g_col, float* sums, adt_stream stream);
+adt_status adt_mlp_bias_grad(const void* g_col, int32_t n, int32_t m, float* db, adt_stream stream);
+adt_status adt_mlp_adam(float* params, const float* grads, float* first, float* second, int64_t count, float lr,
+                        float beta1, float beta2, float eps, float correction1, float correction2,
+                        void* params_bf16, adt_stream stream);
+adt_status adt_mlp_transpose(const void* in, int32_t rows, int32_t cols, void* out, adt_stream stream);
+adt_status adt_mlp_to_bf16(const float* in, int64_t count, void* out, adt_stream stream);
+
 /* Number of kernels this library has launched since the plan was created. */
 int64_t adt_kernel_launches(const adt_plan* plan);
 

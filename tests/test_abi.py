@@ -13,7 +13,7 @@ HEADER = ROOT / "include" / "adtlert_b200.h"
 
 def declared_symbols():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:adt_status|int64_t)\s+(adt_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:adt_status|int64_t|int32_t)\s+(adt_\w+)\s*\(", text, flags=re.M)))
 
 
 def test_header_declares_the_binding_symbols():
