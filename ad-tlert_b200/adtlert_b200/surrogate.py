@@ -57,7 +57,7 @@ class MLP:
                  seed: int = 0, device=None) -> None:
         if inputs % 64 or hidden % 128 or batch % 128:
             raise ValueError("inputs must be a multiple of 64, hidden and batch multiples of 128")
-        self.device = torch.device(device or ("cuda", torch.cuda.current_device()))
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.lib = _native.load_library()
         self.inputs, self.outputs, self.hidden, self.batch = inputs, outputs, hidden, batch
         self.padded = _pad(outputs, 128)
