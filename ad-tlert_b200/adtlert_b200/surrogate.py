@@ -328,9 +328,10 @@ class SurrogateScreen:
     back to the reference's start.
     """
 
-    def __init__(self, surrogate: Surrogate, *, warm_start: bool = True) -> None:
+    def __init__(self, surrogate: Surrogate, *, warm_start: bool = True, line_search: bool = True) -> None:
         self.surrogate = surrogate
         self.warm_start = warm_start
+        self.line_search = line_search
         self.counts = {"line_search_screened": 0, "line_search_fallbacks": 0, "warm_starts": 0,
                        "warm_start_fallbacks": 0, "surrogate_batches": 0}
 
@@ -345,6 +346,8 @@ class SurrogateScreen:
     def screened_step(self, inv, models, step, candidate, predicted, observed, weights, result):
         from .timelapse import line_search_tau
 
+        if not self.line_search:
+            return None
         steps = int(models.shape[0])
         surrogate = self.surrogate.predict(torch.cat([models, candidate]))
         self.counts["surrogate_batches"] += 1
