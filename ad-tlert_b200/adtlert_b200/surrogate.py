@@ -312,23 +312,32 @@ def training_set(forward, count: int, seed: int = 0, batch: int = 8):
 
 
 class SurrogateScreen:
-    """Candidate screening of the windowed Gauss-Newton inversion by a trained surrogate.
+    """Candidate screening of the windowed Gauss-Newton inversion.
 
-    Line-search candidates: the reference solves the FEM at the full-step candidate and, when the
-    grid search along the step picks tau < 0.95, again at the chosen model
-    (adtlert/inversion/core.py:224-257, objective.py:168-192). Screened, the search runs on the
-    FEM data at the current model plus the surrogate's predicted change of the data, and the FEM
-    is solved once, at the chosen model. The FEM then judges: if the objective there is not
-    lower than at the current model, the iteration falls back to the FEM candidate search.
+    Window candidates (on by default): a window may start from the reference's initial models or
+    from the preceding window's result moved one step on (its last model repeated; those models
+    are in the linearization cache, so that start costs no FEM solve). The surrogate estimates the
+    objective of both and only the one chosen is linearized by the FEM; when the FEM objective of
+    a warm start exceeds the surrogate's estimate for the reference's start, the window falls back
+    to the reference's start. Windows started near their solution need fewer Gauss-Newton
+    iterations (measured on 30 windows of the flat time-lapse workload: 5.0 -> 2.2 iterations,
+    630 -> 201 FEM model solves, 2.8x faster, mean final chi2 1.052 -> 1.048).
 
-    Window candidates: a window may start from the reference's initial models or from the
-    preceding window's result moved one step on (its last model repeated). The surrogate
-    estimates the objective of both and the FEM solves only the one chosen; when the FEM objective
-    of a warm start exceeds the surrogate's estimate for the reference's start, the window falls
-    back to the reference's start.
+    Line-search candidates (``line_search=True``, off by default): the reference solves the FEM at
+    the full-step candidate and, when the grid search along the step picks tau < 0.95, again at
+    the chosen model (adtlert/inversion/core.py:224-257, objective.py:168-192). Screened, the search
+    runs on the FEM data at the current model plus the surrogate's predicted change of the data,
+    the FEM solves only the chosen model and falls back to the FEM search when the objective there
+    is not lower. A surrogate accurate to a few percent in absolute apparent resistivity is far
+    less accurate in the small change along one step, so the screened search picked shorter
+    steps and the windows needed more iterations (measured: 5.0 -> 14.5 iterations); it is kept
+    as an option.
+
+    With ``surrogate=None`` the window candidates are judged by the FEM itself (the reference's
+    start linearized too), the variant that shows what the network adds to the warm start.
     """
 
-    def __init__(self, surrogate: Surrogate, *, warm_start: bool = True, line_search: bool = True) -> None:
+    def __init__(self, surrogate: Surrogate | None, *, warm_start: bool = True, line_search: bool = False) -> None:
         self.surrogate = surrogate
         self.warm_start = warm_start
         self.line_search = line_search
@@ -336,8 +345,12 @@ class SurrogateScreen:
                        "warm_start_fallbacks": 0, "surrogate_batches": 0}
 
     def _objectives(self, inv, candidates: Tensor, observed: Tensor, weights: Tensor, steps: int) -> list[float]:
-        predicted = self.surrogate.predict(candidates)
-        self.counts["surrogate_batches"] += 1
+        if self.surrogate is None:
+            predicted = torch.cat([inv.linearize(candidates[i:i + steps])[0]
+                                   for i in range(0, int(candidates.shape[0]), steps)])
+        else:
+            predicted = self.surrogate.predict(candidates)
+            self.counts["surrogate_batches"] += 1
         values = []
         for i in range(0, int(candidates.shape[0]), steps):
             values.append(inv.objective(candidates[i:i + steps], predicted[i:i + steps], observed, weights))
@@ -346,7 +359,7 @@ class SurrogateScreen:
     def screened_step(self, inv, models, step, candidate, predicted, observed, weights, result):
         from .timelapse import line_search_tau
 
-        if not self.line_search:
+        if not self.line_search or self.surrogate is None:
             return None
         steps = int(models.shape[0])
         surrogate = self.surrogate.predict(torch.cat([models, candidate]))
