@@ -35,6 +35,7 @@ SYMBOLS = (
     "adt_integrated_potentials",
     "adt_normal_jacobian",
     "adt_normal_jacobian_to_host",
+    "adt_set_jacobian_wait_limit",
     "adt_aggregate_columns",
     "adt_vjp",
     "adt_adjoint_jacobian",
@@ -173,6 +174,7 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
                                   ctypes.c_float, ctypes.c_float, _p, _p]),
         "adt_mlp_transpose": (status, [_p, _i32, _i32, _p, _p]),
         "adt_mlp_to_bf16": (status, [_p, _i64, _p, _p]),
+        "adt_set_jacobian_wait_limit": (status, [_p, ctypes.c_uint32]),
         "adt_kernel_launches": (_i64, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():

@@ -83,6 +83,8 @@ struct JacobianArgs {
   int W, N, E, C, K, R, row_begin, rows, cells_per_block;
   int c_begin, c_end;     // cells computed: [c_begin, c_end)
   int64_t ldo;            // row stride of out
+  unsigned first_wait_polls = 0;  // tensor-core kernel: 0 = the default bounded wait for each MMA
+                                  // chain; n > 0 = give up after n non-blocking polls (tests)
 };
 
 struct CellGradientArgs {

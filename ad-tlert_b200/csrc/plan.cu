@@ -775,6 +775,7 @@ adt_status launch_normal_jacobian(adt_plan* p, const float* fields, int row_begi
   }
   if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count)) {
     a.cells_per_block = 0;
+    a.first_wait_polls = p->tc_first_wait_polls;
     const cudaError_t err = launch_jacobian_tc(a, p->tc_error, p->sms, s);
     p->launches++;
     if (err != cudaSuccess)
@@ -1062,3 +1063,13 @@ adt_status adt_scale_rows_columns(float* values, int32_t rows, int32_t columns,
 int64_t adt_kernel_launches(const adt_plan* p) { return p ? p->launches : 0; }
 
 }  // extern "C"
+
+extern "C" adt_status adt_set_jacobian_wait_limit(adt_plan* p, uint32_t polls) {
+  if (!p) return ADT_INVALID_ARG;
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(p, ADT_CUDA_ERROR, "cudaDeviceSynchronize failed");
+  p->tc_first_wait_polls = polls;
+  if (p->tc_error && cudaMemset(p->tc_error, 0, sizeof(int)) != cudaSuccess)
+    return fail(p, ADT_CUDA_ERROR, "resetting the tensor-core error flag failed");
+  if (p->tc_error_host) *p->tc_error_host = 0;
+  return ADT_OK;
+}

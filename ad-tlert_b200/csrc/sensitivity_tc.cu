@@ -84,6 +84,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
 __device__ __forceinline__ void tmem_load8(uint32_t addr, uint32_t (&v)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
@@ -326,10 +338,17 @@ __global__ void __launch_bounds__(kTcThreads, 2) jacobian_tc_kernel(JacobianArgs
                    ::"r"(smem_addr(bar)) : "memory");
     }
 
-    // (3) bounded wait for the MMAs
+    // (3) bounded wait for the MMAs (a plan option may shorten it to a few non-blocking polls,
+    //     so that a test can make it run out; the drain below keeps the full limit)
     uint32_t polls = 0;
-    while (!mbar_try_wait(smem_addr(bar), phase)) {
-      if (++polls >= kTcWaitLimit) { failed = true; break; }
+    if (a.first_wait_polls == 0) {
+      while (!mbar_try_wait(smem_addr(bar), phase)) {
+        if (++polls >= kTcWaitLimit) { failed = true; break; }
+      }
+    } else {
+      while (!mbar_test_wait(smem_addr(bar), phase)) {
+        if (++polls >= a.first_wait_polls) { failed = true; break; }
+      }
     }
     phase ^= 1u;
     failed = __syncthreads_or(failed);

@@ -194,6 +194,13 @@ adt_status adt_integrated_potentials(adt_plan* plan, const float* fields, float*
 adt_status adt_normal_jacobian(adt_plan* plan, const float* fields, int32_t row_begin,
                                int32_t row_count, float* jacobian, adt_stream stream);
 
+/* Failure detection of the tensor-core Jacobian: with polls > 0 each block waits for its MMA
+ * chain with at most `polls` non-blocking polls before it gives up (NaN columns, ADT_TIMEOUT on
+ * the plan's next adt_normal_jacobian), while the wait that guards the release of its tensor
+ * memory keeps the full limit; polls = 0 restores the default wait. Synchronizes the device and
+ * clears the plan's timeout flag. No counterpart in the reference (its kernel has no wait). */
+adt_status adt_set_jacobian_wait_limit(adt_plan* plan, uint32_t polls);
+
 /* The whole normal Jacobian of one model (the adt_normal_jacobian product for rows 0 .. D-1)
  * into host_jacobian [D][C] float32, which must be page-locked (cudaHostAlloc / pinned), through
  * device_jacobian (same layout, on the device). J is computed on `stream` in `chunks` column
