@@ -145,6 +145,7 @@ struct adt_plan {
   int device = 0;
   int sms = 148;                // multiprocessors of the device
   bool jacobian_tc = true;      // tensor-core Jacobian where it applies
+  bool jacobian_pipe = true;    // its warp-role pipelined form where that applies
   bool jacobian_direct = true;  // direct-form Jacobian for single-wavenumber operators
   unsigned tc_first_wait_polls = 0;  // 0: default MMA wait of the tensor-core Jacobian; n: n polls
   int* tc_error = nullptr;      // device flag raised by a tensor-core block that timed out

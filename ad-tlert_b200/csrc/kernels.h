@@ -140,6 +140,10 @@ int jacobian_direct_cells(int R, int E, int K);
 cudaError_t launch_jacobian_direct(const JacobianArgs& a, const int2* rows, cudaStream_t s);
 bool jacobian_tc_supported(int E, int W, int R, int K, int rows);
 cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaStream_t s);
+// Pipelined tensor-core kernel (warp roles): the Gram batch (pairs per row store) it would use
+// for these sizes, 0 when it does not apply.
+int jacobian_tcpipe_batch(int E, int W, int R, int K, int rows);
+cudaError_t launch_jacobian_tcpipe(const JacobianArgs& a, int batch, int* error, int sms, cudaStream_t s);
 __global__ void cell_gradient_kernel(CellGradientArgs a);
 __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a);
 __global__ void add_kernel(double* y, const double* x, int64_t count);

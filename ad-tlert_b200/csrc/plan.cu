@@ -314,8 +314,11 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
   cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, p->device);
   if (const char* choice = std::getenv("ADTLERT_B200_JACOBIAN")) {
     // "fma": the CUDA-core Gram kernel everywhere; "tc": tensor cores wherever they apply
+    // "tc1": the tensor-core kernel without warp roles (for comparison)
     p->jacobian_tc = std::strcmp(choice, "fma") != 0;
-    p->jacobian_direct = std::strcmp(choice, "fma") != 0 && std::strcmp(choice, "tc") != 0;
+    p->jacobian_direct = std::strcmp(choice, "fma") != 0 && std::strcmp(choice, "tc") != 0 &&
+                         std::strcmp(choice, "tc1") != 0;
+    p->jacobian_pipe = std::strcmp(choice, "tc1") != 0;
   }
   configure_solver_kernels();
   auto bail = [&](adt_status st) {
@@ -776,7 +779,9 @@ adt_status launch_normal_jacobian(adt_plan* p, const float* fields, int row_begi
   if (p->jacobian_tc && jacobian_tc_supported(p->E, p->W, p->R, p->K, row_count)) {
     a.cells_per_block = 0;
     a.first_wait_polls = p->tc_first_wait_polls;
-    const cudaError_t err = launch_jacobian_tc(a, p->tc_error, p->sms, s);
+    const int batch = p->jacobian_pipe ? jacobian_tcpipe_batch(p->E, p->W, p->R, p->K, row_count) : 0;
+    const cudaError_t err = batch > 0 ? launch_jacobian_tcpipe(a, batch, p->tc_error, p->sms, s)
+                                      : launch_jacobian_tc(a, p->tc_error, p->sms, s);
     p->launches++;
     if (err != cudaSuccess)
       return fail(p, ADT_CUDA_ERROR, std::string("tensor-core jacobian: ") + cudaGetErrorString(err));
