@@ -6,17 +6,20 @@
 // G[N][B]). What changes is how the per-pair chain overlaps. One persistent block per SM:
 //
 //   producer warps 0-7   build the features of pair j into operand stage j % 2 (thread: cell,
-//                        half of the wavenumbers, electrode; tables read straight from global
-//                        memory), then thread 0 issues pair j's MMAs into accumulator j % 2
-//                        (TMEM columns 0 or 128) and commits them to mma_done[j % 2].
-//   epilogue warps 8-11  wait for mma_done[j % 2], read the two Grams back (warp w: TMEM lanes
-//                        32 (w - 8) ..), release the accumulator (acc_free[j % 2], one arrival
-//                        per thread), and after `batch` pairs write every row of the batch's
-//                        2 batch consecutive cells at once (32 bytes per row for 4 pairs).
+//                        half of the wavenumbers, electrode), from registers loaded one pair
+//                        ahead (cell dofs two pairs ahead, so the dependent field loads are
+//                        issued a whole pair early); then thread 0 issues pair j's MMAs into
+//                        accumulator j % 4 (TMEM columns 128 (j % 4)) and commits them to
+//                        stage_free[j % 2] and acc_full[j % 4].
+//   epilogue warps 8-15  wait for acc_full[j % 4], read the Grams back (warp 8 + w: TMEM lanes
+//                        32 (w % 4) .., the columns of cell w / 4; 16-column loads, one wait),
+//                        release the accumulator (acc_free[j % 4]), and after `batch` pairs
+//                        write every row of the batch's 2 batch consecutive cells at once (32
+//                        bytes per row for 4 pairs).
 //
-// So pair j + 1's features, pair j's MMAs and pair j - 1's readback and rows run at the same
-// time. A stage is rebuilt only after the MMAs that read it completed (mma_done), an accumulator
-// rewritten only after its readback (acc_free). Every wait is bounded: a role that gives up
+// So the features of pair j + 1, the MMAs of pair j and the readback and rows of up to three
+// earlier pairs run at the same time. A stage is rebuilt only after the MMAs that read it
+// completed, an accumulator rewritten only after its readback. Every wait is bounded: a role that gives up
 // raises the block's abort flag (the other role stops at its next wait), the block writes NaN
 // into its columns and raises the caller's error flag, and before tensor memory is freed it
 // waits (again bounded) for the last MMAs it issued.
@@ -29,9 +32,10 @@ namespace {
 
 using namespace tc;
 
-constexpr int kPipeThreads = 384;       // 8 producer warps + 4 epilogue warps
+constexpr int kPipeThreads = 512;       // 8 producer warps + 8 epilogue warps
 constexpr int kProducerThreads = 256;
-constexpr int kEpilogueThreads = 128;
+constexpr int kEpilogueThreads = 256;
+constexpr int kAccumulators = 4;        // TMEM accumulators of 128 columns
 constexpr int kPipeM = 128;
 constexpr int kPipeRowTable = 4096;     // rows whose Gram offsets stay in shared memory
 constexpr uint32_t kPipeWaitLimit = 1u << 20;
@@ -55,7 +59,7 @@ __host__ __device__ inline PipeLayout pipe_layout(int E, int W, int R, int batch
   l.feat = 2 * l.stage + (size_t)kPipeM * 16;  // + the rows the M = 128 MMA reads past the end
   l.gram = (size_t)batch * 2 * l.GS * 4;
   l.offs = (size_t)rows * 8;
-  const size_t tail = 4 * 8 + 16 + (size_t)W * R * 4 + 64;  // barriers, TMEM slot, flags, scales
+  const size_t tail = 10 * 8 + 16 + (size_t)W * R * 4 + 64;  // barriers, TMEM slot, flags, scales
   l.total = ((l.feat + l.gram + 15) / 16 * 16) + l.offs + tail;
   return l;
 }
@@ -78,6 +82,20 @@ __device__ __forceinline__ bool pipe_wait(uint64_t* bar, uint32_t parity, volati
   return false;
 }
 
+__device__ __forceinline__ void tmem_load16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+}
+
+__device__ __forceinline__ void commit_to(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
 __device__ __forceinline__ void named_sync(int id, int threads) {
   asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(threads) : "memory");
 }
@@ -94,12 +112,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   float* gram = reinterpret_cast<float*>(pipe_sm + L.feat);  // [batch][2][GS]
   short4* offs = reinterpret_cast<short4*>(pipe_sm + (L.feat + L.gram + 15) / 16 * 16);
   uint64_t* bars = reinterpret_cast<uint64_t*>(
-      (reinterpret_cast<uintptr_t>(offs + a.rows) + 15) & ~uintptr_t(15));  // mma_done[2], acc_free[2]
-  uint64_t* mma_done = bars;
-  uint64_t* acc_free = bars + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
+      (reinterpret_cast<uintptr_t>(offs + a.rows) + 15) & ~uintptr_t(15));
+  uint64_t* stage_free = bars;      // [2]  MMAs of the pair in stage s completed
+  uint64_t* acc_full = bars + 2;    // [4]  MMAs of the pair in accumulator k completed
+  uint64_t* acc_free = bars + 6;    // [4]  accumulator k read back
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  int* stage_flag = reinterpret_cast<int*>(tmem_slot + 2);  // producers: stage wait failed
+  int* stage_flag = reinterpret_cast<int*>(tmem_slot + 2);  // producers' broadcast of abort
+  int* epilogue_flag = reinterpret_cast<int*>(tmem_slot + 3);
   float* scale = reinterpret_cast<float*>(tmem_slot + 4);   // [WT][R]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int pairs_total = (a.c_end - a.c_begin + 1) / 2;
@@ -108,17 +128,19 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   const int pairs = my_supers * batch;  // pairs of this block, including empty ones at the end
 
   if (tid == 0) {
-    mbar_init(mma_done + 0, 1);
-    mbar_init(mma_done + 1, 1);
-    mbar_init(acc_free + 0, kEpilogueThreads);
-    mbar_init(acc_free + 1, kEpilogueThreads);
+    for (int i = 0; i < 2; ++i) mbar_init(stage_free + i, 1);
+    for (int i = 0; i < kAccumulators; ++i) {
+      mbar_init(acc_full + i, 1);
+      mbar_init(acc_free + i, kEpilogueThreads);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *abort = 0;
     *stage_flag = 0;
+    *epilogue_flag = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(tmem_slot)),
-                 "r"(256u)
+                 "r"(128u * kAccumulators)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -148,37 +170,51 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   if (warp < kProducerThreads / 32) {
     // ---------------------------------------------------------------- producers
     // thread (cell ci, half hf, electrode e): wavenumbers 0 .. 7 (hf = 0: chunks 0 .. 2R - 1) or
-    // 8 .. WT - 1 (hf = 1: chunks 2R .. KC - 1); field loads first, whole 16-byte chunks stored
+    // 8 .. WT - 1 (hf = 1: chunks 2R .. KC - 1); whole 16-byte chunks stored
     constexpr int WH = 8, WB = WT - WH, CH0 = WH * R / 4;
     static_assert(WB >= WH && WB <= 16 && (WH * R) % 4 == 0, "two halves of at most 16 wavenumbers");
     const int ci = tid >> 7, hf = (tid >> 6) & 1, e = tid & 63;
+    const bool on = e < E;
+    const int w0 = hf * WH, wn = hf ? WB : WH;
+    auto cell_of = [&](int j) {
+      return a.c_begin + 2 * ((blockIdx.x + (j / batch) * gridDim.x) * batch + j % batch) + ci;
+    };
+    auto load_dofs = [&](int j, int (&d)[K]) {
+      const int c = cell_of(j);
+      const bool valid = on && j < pairs && c < a.c_end;
+#pragma unroll
+      for (int k = 0; k < K; ++k) d[k] = valid ? __ldg(a.cell_dofs + (int64_t)c * K + k) : -1;
+    };
+    float x[WB][K], cf[R][K];
+    int dnext[K];
+    auto load_pair = [&](int j, const int (&d)[K]) {  // fields and template factors of pair j
+      const int c = cell_of(j);
+      const bool valid = on && j < pairs && c < a.c_end;
+#pragma unroll
+      for (int f = 0; f < R; ++f)
+#pragma unroll
+        for (int k = 0; k < K; ++k) cf[f][k] = valid ? __ldg(a.features + ((int64_t)c * R + f) * K + k) : 0.f;
+#pragma unroll
+      for (int jj = 0; jj < WB; ++jj)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          x[jj][k] = (jj < wn && d[k] >= 0) ? __ldg(a.fields + ((int64_t)(w0 + jj) * a.N + d[k]) * E + e) : 0.f;
+    };
+    {
+      int d0[K];
+      load_dofs(0, d0);
+      load_pair(0, d0);
+      load_dofs(1, dnext);
+    }
     for (int j = 0; j < pairs; ++j) {
       const int s = j & 1;
       if (tid == 0) {  // stage s is free once pair j - 2's MMAs completed
-        if (j >= 2 && !pipe_wait(mma_done + s, ((j >> 1) & 1) ^ 1u, abort)) *abort = 1;
+        if (j >= 2 && !pipe_wait(stage_free + s, ((j >> 1) & 1) ^ 1u, abort)) *abort = 1;
         *stage_flag = *abort;
       }
       named_sync(1, kProducerThreads);
       if (*stage_flag) break;
-      const int super = blockIdx.x + (j / batch) * gridDim.x;
-      const int c = a.c_begin + 2 * (super * batch + j % batch) + ci;
-      if (e < E) {
-        const bool valid = c < a.c_end;
-        int dof[K];
-        float cf[R][K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) dof[k] = valid ? __ldg(a.cell_dofs + (int64_t)c * K + k) : -1;
-#pragma unroll
-        for (int f = 0; f < R; ++f)
-#pragma unroll
-          for (int k = 0; k < K; ++k) cf[f][k] = valid ? __ldg(a.features + ((int64_t)c * R + f) * K + k) : 0.f;
-        const int w0 = hf * WH, wn = hf ? WB : WH;
-        float x[WB][K];
-#pragma unroll
-        for (int jj = 0; jj < WB; ++jj)
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-            x[jj][k] = (jj < wn && dof[k] >= 0) ? __ldg(a.fields + ((int64_t)(w0 + jj) * a.N + dof[k]) * E + e) : 0.f;
+      if (on) {
         const int nch = hf ? L.KC - CH0 : CH0;
         unsigned char* row_feat = feat + (size_t)s * L.stage + ((size_t)(hf * CH0) * L.RW + ci * L.Ep + e) * 16;
         float hi[4] = {0.f, 0.f, 0.f, 0.f}, lo[4] = {0.f, 0.f, 0.f, 0.f};
@@ -213,10 +249,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
           }
         }
       }
+      // prefetch: fields of pair j + 1 (its dofs arrived during pair j), dofs of pair j + 2
+      load_pair(j + 1, dnext);
+      load_dofs(j + 2, dnext);
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       named_sync(1, kProducerThreads);
-      if (tid == 0) {  // accumulator s is free once pair j - 2 was read back
-        if (j >= 2 && !pipe_wait(acc_free + s, ((j >> 1) & 1) ^ 1u, abort)) *abort = 1;
+      if (tid == 0) {  // accumulator j % 4 is free once pair j - 4 was read back
+        const int acc_index = j % kAccumulators;
+        if (j >= kAccumulators && !pipe_wait(acc_free + acc_index, ((j >> 2) & 1) ^ 1u, abort)) *abort = 1;
         if (!*abort) {
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
           const uint32_t base = smem_addr(feat + (size_t)s * L.stage);
@@ -224,7 +264,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
           uint64_t dl = operand_desc(base + (uint32_t)L.part, (uint32_t)L.RW * 16, 128);
           const uint64_t step = (uint64_t)(2 * L.RW * 16) >> 4;
           const uint32_t idesc = tf32_idesc(kPipeM, L.RW);
-          const uint32_t acc = tmem + (uint32_t)(s * 128);
+          const uint32_t acc = tmem + (uint32_t)(acc_index * 128);
           for (int ks = 0; ks < L.KS; ++ks) {
             mma_tf32(acc, dh, dh, idesc, ks > 0 ? 1u : 0u);
             mma_tf32(acc, dh, dl, idesc, 1u);
@@ -232,27 +272,30 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
             dh += step;
             dl += step;
           }
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                           smem_addr(mma_done + s))
-                       : "memory");
+          commit_to(stage_free + s);
+          commit_to(acc_full + acc_index);
           issued = j + 1;
         }
       }
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    const int et = tid - kProducerThreads, ew = warp - kProducerThreads / 32;  // TMEM lane quarter ew
-    int* epilogue_flag = stage_flag + 1;
+    const int et = tid - kProducerThreads, ew = warp - kProducerThreads / 32;
+    const int lq = ew & 3, hh = ew >> 2;  // TMEM lane quarter lq, columns of cell hh
+    const int first = 32 * lq - hh * L.Ep;  // lane 0's row within cell hh
+    const bool busy = first < E && first + 32 > 0;  // warp-uniform: some rows of cell hh here
+    const int lr = first + lane;
+    const bool mine = lr >= 0 && lr < E;
     for (int j = 0; j < pairs; ++j) {
-      const int s = j & 1, q = j % batch;
+      const int acc_index = j % kAccumulators, q = j % batch;
       if (et == 0) {
         bool done;
         if (a.first_wait_polls == 0) {
-          done = pipe_wait(mma_done + s, (j >> 1) & 1, abort);
+          done = pipe_wait(acc_full + acc_index, (j >> 2) & 1, abort);
         } else {  // failure-detection tests: a few non-blocking polls
           done = false;
           for (unsigned polls = 0; !done && polls < a.first_wait_polls; ++polls)
-            done = mbar_test_wait(smem_addr(mma_done + s), (j >> 1) & 1);
+            done = mbar_test_wait(smem_addr(acc_full + acc_index), (j >> 2) & 1);
         }
         if (!done) *abort = 1;
         *epilogue_flag = *abort;
@@ -260,30 +303,27 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
       named_sync(2, kEpilogueThreads);
       if (*epilogue_flag) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const int row = 32 * ew + lane;  // row of D held by this lane
-      for (int hh = 0; hh < 2; ++hh) {
-        const int first = 32 * ew - hh * L.Ep;  // lane 0's row within cell hh
-        if (first >= E || first + 32 <= 0) continue;  // warp-uniform: no row of cell hh here
-        const int lr = row - hh * L.Ep;
-        const bool mine = lr >= 0 && lr < E;
+      if (busy) {
+        const uint32_t base = tmem + ((uint32_t)(32 * lq) << 16) + (uint32_t)(acc_index * 128 + hh * L.Ep);
         float* g = gram + ((size_t)q * 2 + hh) * L.GS + (size_t)(mine ? lr : 0) * L.GLD;
-        for (int cc = 0; cc < L.Ep; cc += 8) {
-          uint32_t v[8];
-          tmem_load8(tmem + ((uint32_t)(32 * ew) << 16) + (uint32_t)(s * 128 + hh * L.Ep + cc), v);
-          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-          if (mine) {
+        uint32_t v[4][16];
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj)
-              if (cc + jj < E) g[cc + jj] = __uint_as_float(v[jj]);
-          }
+        for (int b = 0; b < 4; ++b)
+          if (16 * b < L.Ep) tmem_load16(base + 16 * b, v[b]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (mine) {
+#pragma unroll
+          for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj)
+              if (16 * b + jj < E) g[16 * b + jj] = __uint_as_float(v[b][jj]);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      mbar_arrive(acc_free + s);
+      mbar_arrive(acc_free + acc_index);
       if (q == batch - 1 || j == pairs - 1) {
         named_sync(2, kEpilogueThreads);  // every Gram of the batch is staged
-        const int super = blockIdx.x + (j / batch) * gridDim.x;
-        const int cfirst = a.c_begin + 2 * super * batch;
+        const int cfirst = a.c_begin + 2 * (blockIdx.x + (j / batch) * gridDim.x) * batch;
         const int ncells = min(2 * (q + 1), a.c_end - cfirst);
         for (int d = et; ncells > 0 && d < a.rows; d += kEpilogueThreads) {
           const short4 o = offs[d];
@@ -315,7 +355,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
       if (issued > 0) {  // the last commit covers every MMA issued; full bounded wait
         const int last = issued - 1;
         for (uint32_t polls = 0; polls < kPipeWaitLimit; ++polls)
-          if (mbar_try_wait(smem_addr(mma_done + (last & 1)), (uint32_t)((last >> 1) & 1))) break;
+          if (mbar_try_wait(smem_addr(stage_free + (last & 1)), (uint32_t)((last >> 1) & 1))) break;
       }
     }
     for (int sg = 0; sg < my_supers; ++sg) {  // NaN in every column of this block
@@ -329,7 +369,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(256u) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(128u * kAccumulators)
+                 : "memory");
 }
 
 template __global__ void jacobian_tcpipe_kernel<3, 5, kPipeStaticW>(JacobianArgs, int, int*);
