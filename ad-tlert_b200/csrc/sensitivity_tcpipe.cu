@@ -8,10 +8,10 @@
 //   producer warps 0-7   build the features of pair j into operand stage j % 2 (thread: cell,
 //                        half of the wavenumbers, electrode), from registers loaded one pair
 //                        ahead (cell dofs two pairs ahead, so the dependent field loads are
-//                        issued a whole pair early); then thread 0 issues pair j's MMAs into
-//                        accumulator j % 4 (TMEM columns 128 (j % 4)) and commits them to
-//                        stage_free[j % 2] and acc_full[j % 4].
-//   epilogue warps 8-15  wait for acc_full[j % 4], read the Grams back (warp 8 + w: TMEM lanes
+//                        issued a whole pair early), and arrive on stage_full[j % 2].
+//   MMA warp 15          one thread issues pair j's MMAs into accumulator j % 4 (TMEM columns
+//                        128 (j % 4)) and commits them to stage_free[j % 2] and acc_full[j % 4].
+//   epilogue warps 8-14  wait for acc_full[j % 4], read the Grams back (warp 8 + w: TMEM lanes
 //                        32 (w % 4) .., the columns of cell w / 4; 16-column loads, one wait),
 //                        release the accumulator (acc_free[j % 4]), and after `batch` pairs
 //                        write every row of the batch's 2 batch consecutive cells at once (32
@@ -32,9 +32,10 @@ namespace {
 
 using namespace tc;
 
-constexpr int kPipeThreads = 512;       // 8 producer warps + 8 epilogue warps
+constexpr int kPipeThreads = 512;       // 8 producer warps, 7 epilogue warps, 1 MMA warp
 constexpr int kProducerThreads = 256;
-constexpr int kEpilogueThreads = 256;
+constexpr int kEpilogueThreads = 224;
+constexpr int kMmaWarp = 15;
 constexpr int kAccumulators = 4;        // TMEM accumulators of 128 columns
 constexpr int kPipeM = 128;
 constexpr int kPipeRowTable = 4096;     // rows whose Gram offsets stay in shared memory
@@ -59,7 +60,7 @@ __host__ __device__ inline PipeLayout pipe_layout(int E, int W, int R, int batch
   l.feat = 2 * l.stage + (size_t)kPipeM * 16;  // + the rows the M = 128 MMA reads past the end
   l.gram = (size_t)batch * 2 * l.GS * 4;
   l.offs = (size_t)rows * 8;
-  const size_t tail = 10 * 8 + 16 + (size_t)W * R * 4 + 64;  // barriers, TMEM slot, flags, scales
+  const size_t tail = 12 * 8 + 16 + (size_t)W * R * 4 + 64;  // barriers, TMEM slot, flags, scales
   l.total = ((l.feat + l.gram + 15) / 16 * 16) + l.offs + tail;
   return l;
 }
@@ -114,11 +115,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   uint64_t* bars = reinterpret_cast<uint64_t*>(
       (reinterpret_cast<uintptr_t>(offs + a.rows) + 15) & ~uintptr_t(15));
   uint64_t* stage_free = bars;      // [2]  MMAs of the pair in stage s completed
-  uint64_t* acc_full = bars + 2;    // [4]  MMAs of the pair in accumulator k completed
-  uint64_t* acc_free = bars + 6;    // [4]  accumulator k read back
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  uint64_t* stage_full = bars + 2;  // [2]  features of the pair in stage s written
+  uint64_t* acc_full = bars + 4;    // [4]  MMAs of the pair in accumulator k completed
+  uint64_t* acc_free = bars + 8;    // [4]  accumulator k read back
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 12);
   volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  int* stage_flag = reinterpret_cast<int*>(tmem_slot + 2);  // producers' broadcast of abort
   int* epilogue_flag = reinterpret_cast<int*>(tmem_slot + 3);
   float* scale = reinterpret_cast<float*>(tmem_slot + 4);   // [WT][R]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -128,14 +129,16 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   const int pairs = my_supers * batch;  // pairs of this block, including empty ones at the end
 
   if (tid == 0) {
-    for (int i = 0; i < 2; ++i) mbar_init(stage_free + i, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(stage_free + i, 1);
+      mbar_init(stage_full + i, kProducerThreads);
+    }
     for (int i = 0; i < kAccumulators; ++i) {
       mbar_init(acc_full + i, 1);
       mbar_init(acc_free + i, kEpilogueThreads);
     }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *abort = 0;
-    *stage_flag = 0;
     *epilogue_flag = 0;
   }
   if (warp == 0) {
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  int issued = 0;  // producer thread 0: pairs whose MMAs were committed
+  int issued = 0;  // MMA thread: pairs whose MMAs were committed
 
   if (warp < kProducerThreads / 32) {
     // ---------------------------------------------------------------- producers
@@ -208,12 +211,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
     }
     for (int j = 0; j < pairs; ++j) {
       const int s = j & 1;
-      if (tid == 0) {  // stage s is free once pair j - 2's MMAs completed
-        if (j >= 2 && !pipe_wait(stage_free + s, ((j >> 1) & 1) ^ 1u, abort)) *abort = 1;
-        *stage_flag = *abort;
+      // stage s is free once pair j - 2's MMAs completed (each thread waits: producers need no
+      // barrier among themselves)
+      if ((j >= 2 && !pipe_wait(stage_free + s, ((j >> 1) & 1) ^ 1u, abort)) || *abort) {
+        *abort = 1;
+        break;
       }
-      named_sync(1, kProducerThreads);
-      if (*stage_flag) break;
       if (on) {
         const int nch = hf ? L.KC - CH0 : CH0;
         unsigned char* row_feat = feat + (size_t)s * L.stage + ((size_t)(hf * CH0) * L.RW + ci * L.Ep + e) * 16;
@@ -249,38 +252,44 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
           }
         }
       }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_arrive(stage_full + s);
       // prefetch: fields of pair j + 1 (its dofs arrived during pair j), dofs of pair j + 2
       load_pair(j + 1, dnext);
       load_dofs(j + 2, dnext);
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      named_sync(1, kProducerThreads);
-      if (tid == 0) {  // accumulator j % 4 is free once pair j - 4 was read back
-        const int acc_index = j % kAccumulators;
-        if (j >= kAccumulators && !pipe_wait(acc_free + acc_index, ((j >> 2) & 1) ^ 1u, abort)) *abort = 1;
-        if (!*abort) {
-          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-          const uint32_t base = smem_addr(feat + (size_t)s * L.stage);
-          uint64_t dh = operand_desc(base, (uint32_t)L.RW * 16, 128);
-          uint64_t dl = operand_desc(base + (uint32_t)L.part, (uint32_t)L.RW * 16, 128);
-          const uint64_t step = (uint64_t)(2 * L.RW * 16) >> 4;
-          const uint32_t idesc = tf32_idesc(kPipeM, L.RW);
-          const uint32_t acc = tmem + (uint32_t)(acc_index * 128);
-          for (int ks = 0; ks < L.KS; ++ks) {
-            mma_tf32(acc, dh, dh, idesc, ks > 0 ? 1u : 0u);
-            mma_tf32(acc, dh, dl, idesc, 1u);
-            mma_tf32(acc, dl, dh, idesc, 1u);
-            dh += step;
-            dl += step;
-          }
-          commit_to(stage_free + s);
-          commit_to(acc_full + acc_index);
-          issued = j + 1;
+    }
+  } else if (warp == kMmaWarp) {
+    // ---------------------------------------------------------------- MMA issue (one thread)
+    if (lane == 0) {
+      for (int j = 0; j < pairs; ++j) {
+        const int s = j & 1, acc_index = j % kAccumulators;
+        if (!pipe_wait(stage_full + s, (j >> 1) & 1, abort) ||
+            (j >= kAccumulators && !pipe_wait(acc_free + acc_index, ((j >> 2) & 1) ^ 1u, abort))) {
+          *abort = 1;
+          break;
         }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t base = smem_addr(feat + (size_t)s * L.stage);
+        uint64_t dh = operand_desc(base, (uint32_t)L.RW * 16, 128);
+        uint64_t dl = operand_desc(base + (uint32_t)L.part, (uint32_t)L.RW * 16, 128);
+        const uint64_t step = (uint64_t)(2 * L.RW * 16) >> 4;
+        const uint32_t idesc = tf32_idesc(kPipeM, L.RW);
+        const uint32_t acc = tmem + (uint32_t)(acc_index * 128);
+        for (int ks = 0; ks < L.KS; ++ks) {
+          mma_tf32(acc, dh, dh, idesc, ks > 0 ? 1u : 0u);
+          mma_tf32(acc, dh, dl, idesc, 1u);
+          mma_tf32(acc, dl, dh, idesc, 1u);
+          dh += step;
+          dl += step;
+        }
+        commit_to(stage_free + s);
+        commit_to(acc_full + acc_index);
+        issued = j + 1;
       }
     }
   } else {
     // ---------------------------------------------------------------- epilogue
-    const int et = tid - kProducerThreads, ew = warp - kProducerThreads / 32;
+    const int et = tid - kProducerThreads, ew = warp - kProducerThreads / 32;  // warps 8 .. 14
     const int lq = ew & 3, hh = ew >> 2;  // TMEM lane quarter lq, columns of cell hh
     const int first = 32 * lq - hh * L.Ep;  // lane 0's row within cell hh
     const bool busy = first < E && first + 32 > 0;  // warp-uniform: some rows of cell hh here
@@ -350,7 +359,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (*abort) {
-    if (tid == 0) {
+    if (warp == kMmaWarp && lane == 0) {
       atomicExch(error, 1);
       if (issued > 0) {  // the last commit covers every MMA issued; full bounded wait
         const int last = issued - 1;
@@ -376,10 +385,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
 template __global__ void jacobian_tcpipe_kernel<3, 5, kPipeStaticW>(JacobianArgs, int, int*);
 
 // The pipelined kernel applies to the flat 2.5D operator's shape (P1 triangles: K = 3, R = 5,
-// the 17-wavenumber quadrature) with at most 64 electrode slots and 4096 rows; the Gram batch is
+// the 17-wavenumber quadrature) with at most 48 electrodes (so TMEM lanes 96-127, whose warp
+// issues the MMAs, hold no Gram row) and 4096 rows; the Gram batch is
 // the largest of 4, 2, 1 pairs whose shared memory fits one block per SM.
 int jacobian_tcpipe_batch(int E, int W, int R, int K, int rows) {
-  if (K != 3 || R != 5 || W != kPipeStaticW || E > kPipeM / 2 || rows > kPipeRowTable) return 0;
+  if (K != 3 || R != 5 || W != kPipeStaticW || E > 48 || rows > kPipeRowTable) return 0;
   for (int batch = 4; batch >= 1; batch >>= 1)
     if (pipe_layout(E, W, R, batch, rows).total <= 227 * 1024) return batch;
   return 0;
