@@ -88,17 +88,6 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
   return offset;
 }
 
-__device__ __forceinline__ float dot4(float4 a, float4 b) {
-  return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
-}
-
-__device__ __forceinline__ void axpy4(float4& acc, float4 a, float s) {
-  acc.x = fmaf(a.x, s, acc.x);
-  acc.y = fmaf(a.y, s, acc.y);
-  acc.z = fmaf(a.z, s, acc.z);
-  acc.w = fmaf(a.w, s, acc.w);
-}
-
 // Data pass. `given` (T x D) replaces the row products q_d when not null (A^T b: q = b_data).
 // J is read as float32 (streamed once), every product and sum is float64: CGLS truncated at
 // tens of iterations is sensitive to rounding in A^T A p (float32 rounding of it alone moves the
