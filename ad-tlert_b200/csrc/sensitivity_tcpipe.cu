@@ -5,20 +5,17 @@
 // S S^T in tensor memory holds both electrode Grams; J[d][c] = -(G[M][A] - G[M][B] - G[N][A] +
 // G[N][B]). What changes is how the per-pair chain overlaps. One persistent block per SM:
 //
-//   producer warps 0-7   two teams: warps 0-3 build the even pairs into operand stage 0, warps
-//                        4-7 the odd pairs into stage 1 (thread: one electrode row of one cell,
-//                        all wavenumbers; the team's next cell dofs loaded a pair ahead), so one
-//                        team's field loads are in flight while the other computes; each thread
-//                        arrives on stage_full[j % 2].
+//   producer warps 0-7   build the features of pair j into operand stage j % 2 (thread: cell,
+//                        half of the wavenumbers, electrode), from registers loaded one pair
+//                        ahead (cell dofs two pairs ahead, so the dependent field loads are
+//                        issued a whole pair early), and arrive on stage_full[j % 2].
 //   MMA warp 15          one thread issues pair j's MMAs into accumulator j % 4 (TMEM columns
 //                        128 (j % 4)) and commits them to stage_free[j % 2] and acc_full[j % 4].
 //   epilogue warps 8-14  wait for acc_full[j % 4], read the Grams back (warp 8 + w: TMEM lanes
 //                        32 (w % 4) .., the columns of cell w / 4; 16-column loads, one wait),
 //                        release the accumulator (acc_free[j % 4]), and after `batch` pairs
 //                        write every row of the batch's 2 batch consecutive cells at once (32
-//                        bytes per row for 4 pairs). The batch's Grams are stored entry-major
-//                        with the cells interleaved, so a row's four entries for all 8 cells
-//                        are eight 16-byte shared-memory loads.
+//                        bytes per row for 4 pairs).
 //
 // So the features of pair j + 1, the MMAs of pair j and the readback and rows of up to three
 // earlier pairs run at the same time. A stage is rebuilt only after the MMAs that read it
@@ -37,7 +34,6 @@ using namespace tc;
 
 constexpr int kPipeThreads = 512;       // 8 producer warps, 7 epilogue warps, 1 MMA warp
 constexpr int kProducerThreads = 256;
-constexpr int kTeamThreads = 128;     // producers per operand stage
 constexpr int kEpilogueThreads = 224;
 constexpr int kMmaWarp = 15;
 constexpr int kAccumulators = 4;        // TMEM accumulators of 128 columns
@@ -114,8 +110,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   const int E = a.E;
   const PipeLayout L = pipe_layout(E, WT, R, batch, a.rows);
   unsigned char* feat = pipe_sm;
-  float* gram = reinterpret_cast<float*>(pipe_sm + L.feat);  // [GS][2 batch]: cells interleaved per entry
-  const int NC = 2 * batch;
+  float* gram = reinterpret_cast<float*>(pipe_sm + L.feat);  // [batch][2][GS]
   short4* offs = reinterpret_cast<short4*>(pipe_sm + (L.feat + L.gram + 15) / 16 * 16);
   uint64_t* bars = reinterpret_cast<uint64_t*>(
       (reinterpret_cast<uintptr_t>(offs + a.rows) + 15) & ~uintptr_t(15));
@@ -136,7 +131,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   if (tid == 0) {
     for (int i = 0; i < 2; ++i) {
       mbar_init(stage_free + i, 1);
-      mbar_init(stage_full + i, kTeamThreads);
+      mbar_init(stage_full + i, kProducerThreads);
     }
     for (int i = 0; i < kAccumulators; ++i) {
       mbar_init(acc_full + i, 1);
@@ -160,9 +155,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
     };
     offs[d] = make_short4(at(q.z, q.x), at(q.z, q.y), at(q.w, q.x), at(q.w, q.y));
   }
-  for (int i = tid; i < NC; i += kPipeThreads) gram[(size_t)(L.GS - 1) * NC + i] = 0.f;  // remote entry
+  for (int i = tid; i < batch * 2; i += kPipeThreads) gram[(size_t)i * L.GS + L.GS - 1] = 0.f;
   // chunks the producers never write (K padding) are zero in both stages
-  constexpr int kWritten = (WT * R + 3) / 4;
+  constexpr int kWritten = 2 * R + ((WT - 8) * R + 3) / 4;
   for (int item = tid; item < (L.KC - kWritten) * L.RW * 4 * 4; item += kPipeThreads) {
     const int per_part = (L.KC - kWritten) * L.RW * 4;
     const int which = item / per_part, rest = item % per_part;  // (stage, part) and float index
@@ -177,12 +172,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
 
   if (warp < kProducerThreads / 32) {
     // ---------------------------------------------------------------- producers
-    // two teams: warps 0-3 build the even pairs (stage 0), warps 4-7 the odd pairs (stage 1), so
-    // one team's field loads are in flight while the other computes. Thread (cell ci, electrode
-    // e) builds its row of the operand for all wavenumbers: chunks 0 .. KC - 1 of row ci Ep + e.
-    static_assert(WT * R <= 88, "the features of a row fit 22 chunks");
-    const int team = warp >> 2, tt = tid & (kTeamThreads - 1), ci = tt >> 6, e = tt & 63;
+    // thread (cell ci, half hf, electrode e): wavenumbers 0 .. 7 (hf = 0: chunks 0 .. 2R - 1) or
+    // 8 .. WT - 1 (hf = 1: chunks 2R .. KC - 1); whole 16-byte chunks stored
+    constexpr int WH = 8, WB = WT - WH, CH0 = WH * R / 4;
+    static_assert(WB >= WH && WB <= 16 && (WH * R) % 4 == 0, "two halves of at most 16 wavenumbers");
+    const int ci = tid >> 7, hf = (tid >> 6) & 1, e = tid & 63;
     const bool on = e < E;
+    const int w0 = hf * WH, wn = hf ? WB : WH;
     auto cell_of = [&](int j) {
       return a.c_begin + 2 * ((blockIdx.x + (j / batch) * gridDim.x) * batch + j % batch) + ci;
     };
@@ -192,64 +188,75 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
 #pragma unroll
       for (int k = 0; k < K; ++k) d[k] = valid ? __ldg(a.cell_dofs + (int64_t)c * K + k) : -1;
     };
+    float x[WB][K], cf[R][K];
     int dnext[K];
-    load_dofs(team, dnext);
-    for (int j = team; j < pairs; j += 2) {
-      const int s = team;  // == j & 1
-      int dof[K];
-#pragma unroll
-      for (int k = 0; k < K; ++k) dof[k] = dnext[k];
-      load_dofs(j + 2, dnext);  // the team's next pair
+    auto load_pair = [&](int j, const int (&d)[K]) {  // fields and template factors of pair j
       const int c = cell_of(j);
-      const bool valid = on && c < a.c_end;
-      float cf[R][K], x[WT][K];
+      const bool valid = on && j < pairs && c < a.c_end;
 #pragma unroll
       for (int f = 0; f < R; ++f)
 #pragma unroll
         for (int k = 0; k < K; ++k) cf[f][k] = valid ? __ldg(a.features + ((int64_t)c * R + f) * K + k) : 0.f;
-      const float* column = a.fields + e;
 #pragma unroll
-      for (int w = 0; w < WT; ++w)
+      for (int jj = 0; jj < WB; ++jj)
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          x[w][k] = dof[k] >= 0 ? __ldg(column + ((int64_t)w * a.N + dof[k]) * E) : 0.f;
-      // stage s is free once pair j - 2's MMAs completed
+          x[jj][k] = (jj < wn && d[k] >= 0) ? __ldg(a.fields + ((int64_t)(w0 + jj) * a.N + d[k]) * E + e) : 0.f;
+    };
+    {
+      int d0[K];
+      load_dofs(0, d0);
+      load_pair(0, d0);
+      load_dofs(1, dnext);
+    }
+    for (int j = 0; j < pairs; ++j) {
+      const int s = j & 1;
+      // stage s is free once pair j - 2's MMAs completed (each thread waits: producers need no
+      // barrier among themselves)
       if ((j >= 2 && !pipe_wait(stage_free + s, ((j >> 1) & 1) ^ 1u, abort)) || *abort) {
         *abort = 1;
         break;
       }
       if (on) {
-        unsigned char* row_feat = feat + (size_t)s * L.stage + (size_t)(ci * L.Ep + e) * 16;
-        float hi[4], lo[4];
+        const int nch = hf ? L.KC - CH0 : CH0;
+        unsigned char* row_feat = feat + (size_t)s * L.stage + ((size_t)(hf * CH0) * L.RW + ci * L.Ep + e) * 16;
+        float hi[4] = {0.f, 0.f, 0.f, 0.f}, lo[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int w = 0; w < WT; ++w) {
+        for (int jj = 0; jj < WB; ++jj) {
 #pragma unroll
           for (int f = 0; f < R; ++f) {
-            const int kl = w * R + f;  // compile-time: chunk kl / 4, lane kl % 4
+            const int kl = jj * R + f;  // compile-time: chunk kl / 4, lane kl % 4
             float v = 0.f;
+            if (jj < wn) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[w][k], v);
-            v *= scale[w * R + f];
+              for (int k = 0; k < K; ++k) v = fmaf(cf[f][k], x[jj][k], v);
+              v *= scale[(w0 + jj) * R + f];
+            }
             hi[kl & 3] = tf32_round(v);
             lo[kl & 3] = v - hi[kl & 3];
-            if ((kl & 3) == 3) {
+            if ((kl & 3) == 3 && (kl >> 2) < nch) {
               const size_t off = (size_t)(kl >> 2) * L.RW * 16;
               *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
               *reinterpret_cast<float4*>(row_feat + L.part + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
             }
           }
         }
-        constexpr int last = WT * R;
-        if constexpr (last % 4 != 0) {  // a partial last chunk: its remaining lanes are padding
+        constexpr int last = WB * R;
+        if constexpr (last % 4 != 0) {
 #pragma unroll
           for (int i = last % 4; i < 4; ++i) hi[i] = lo[i] = 0.f;
-          const size_t off = (size_t)(last >> 2) * L.RW * 16;
-          *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<float4*>(row_feat + L.part + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+          if ((last >> 2) < nch) {
+            const size_t off = (size_t)(last >> 2) * L.RW * 16;
+            *reinterpret_cast<float4*>(row_feat + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<float4*>(row_feat + L.part + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+          }
         }
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       mbar_arrive(stage_full + s);
+      // prefetch: fields of pair j + 1 (its dofs arrived during pair j), dofs of pair j + 2
+      load_pair(j + 1, dnext);
+      load_dofs(j + 2, dnext);
     }
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA issue (one thread)
@@ -307,7 +314,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       if (busy) {
         const uint32_t base = tmem + ((uint32_t)(32 * lq) << 16) + (uint32_t)(acc_index * 128 + hh * L.Ep);
-        float* g = gram + (size_t)(mine ? lr : 0) * L.GLD * NC + (2 * q + hh);  // entry (lr, col) of cell 2q + hh
+        float* g = gram + ((size_t)q * 2 + hh) * L.GS + (size_t)(mine ? lr : 0) * L.GLD;
         uint32_t v[4][16];
 #pragma unroll
         for (int b = 0; b < 4; ++b)
@@ -318,7 +325,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
           for (int b = 0; b < 4; ++b)
 #pragma unroll
             for (int jj = 0; jj < 16; ++jj)
-              if (16 * b + jj < E) g[(size_t)(16 * b + jj) * NC] = __uint_as_float(v[b][jj]);
+              if (16 * b + jj < E) g[16 * b + jj] = __uint_as_float(v[b][jj]);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -330,25 +337,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
         for (int d = et; ncells > 0 && d < a.rows; d += kEpilogueThreads) {
           const short4 o = offs[d];
           float v[8];
-          if (NC == 8) {  // the 8 cells of an entry are 32 contiguous bytes: two float4 loads each
-            const float4* gx = reinterpret_cast<const float4*>(gram + (size_t)o.x * 8);
-            const float4* gy = reinterpret_cast<const float4*>(gram + (size_t)o.y * 8);
-            const float4* gz = reinterpret_cast<const float4*>(gram + (size_t)o.z * 8);
-            const float4* gw = reinterpret_cast<const float4*>(gram + (size_t)o.w * 8);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const float4 X = gx[h], Y = gy[h], Z = gz[h], W = gw[h];
-              v[4 * h + 0] = -((X.x - Y.x) - (Z.x - W.x));
-              v[4 * h + 1] = -((X.y - Y.y) - (Z.y - W.y));
-              v[4 * h + 2] = -((X.z - Y.z) - (Z.z - W.z));
-              v[4 * h + 3] = -((X.w - Y.w) - (Z.w - W.w));
-            }
-          } else {
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-              v[i] = i < ncells ? -((gram[(size_t)o.x * NC + i] - gram[(size_t)o.y * NC + i]) -
-                                    (gram[(size_t)o.z * NC + i] - gram[(size_t)o.w * NC + i]))
-                                : 0.f;
+          for (int i = 0; i < 8; ++i) {
+            const float* gc = gram + (size_t)i * L.GS;
+            v[i] = i < ncells ? -((gc[o.x] - gc[o.y]) - (gc[o.z] - gc[o.w])) : 0.f;
           }
           float* out = a.out + (int64_t)d * a.ldo + cfirst;
           if (ncells == 8 && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
