@@ -843,10 +843,78 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "e2e": e2e,
         "gpu_launches": int(launches),
     }
+    result["operations_ms"] = operation_timings(forward, nodes, cells, device)
     if world == 1 and not args.no_cpu_baseline:
         result["reference_kernel"] = reference_kernel(forward, fields, J, handle, flush, device, stream)
         result["cpu_baseline"] = cpu_baseline(args, nodes, cells, electrodes, rows)
+        result["cpu_operations_ms"] = cpu_operation_timings(nodes, cells, electrodes, rows)
     return result
+
+
+def operation_timings(forward, nodes, cells, device, reps: int = 5) -> dict:
+    """Wall-clock ms (median of ``reps``) of the operator's other public calls on the workload,
+    host tensors in and out (adtlert/forward/ert2p5d.py:697-943): solve of a fresh model (assembly,
+    factorization, fields, measurement) and of a cached one, and the derivative products of a
+    model whose fields are cached."""
+
+    from adtlert_b200 import synthetic
+
+    rng = np.random.default_rng(7)
+    sigma = torch.as_tensor(synthetic.layered_model(nodes, cells, 70_000), dtype=torch.float32)
+    g = torch.as_tensor(rng.standard_normal(forward.D), dtype=torch.float32)
+    delta = sigma * torch.as_tensor(rng.standard_normal(forward.C) * 1e-2, dtype=torch.float32)
+    fresh = [torch.as_tensor(synthetic.layered_model(nodes, cells, 71_000 + i), dtype=torch.float32)
+             for i in range(reps + 2)]
+
+    def timed(fn, count=reps):
+        values = []
+        for i in range(count + 2):
+            torch.cuda.synchronize(device)
+            start = time.perf_counter()
+            fn(i)
+            torch.cuda.synchronize(device)
+            if i >= 2:
+                values.append(1e3 * (time.perf_counter() - start))
+        return statistics.median(values)
+
+    forward.solve(sigma)
+    return {
+        "solve_fresh_model": timed(lambda i: forward.solve(fresh[i])),
+        "solve_cached_fields": timed(lambda i: forward.solve(sigma)),
+        "vjp": timed(lambda i: forward.vjp(sigma, g)),
+        "jvp": timed(lambda i: forward.jvp(sigma, delta)),
+        "normal_vjp": timed(lambda i: forward.normal_vjp(sigma, g)),
+        "normal_jvp": timed(lambda i: forward.normal_jvp(sigma, delta)),
+        "timing": f"wall clock, host tensors in and out, median of {reps} after 2 untimed calls",
+    }
+
+
+def cpu_operation_timings(nodes, cells, electrodes, rows) -> dict:
+    """The same calls on the FP64 oracle (SciPy SuperLU per wavenumber), once each, ms; the
+    oracle keeps no fields between calls, so every call solves its own fields as the reference's
+    CPU path does without a cache."""
+
+    sys.path.insert(0, str(ROOT))
+    from adtlert_b200 import synthetic
+    from oracle.ert2p5d import Oracle2p5D
+
+    oracle = Oracle2p5D(nodes, cells, electrodes, rows)
+    rng = np.random.default_rng(7)
+    sigma = synthetic.layered_model(nodes, cells, 70_000).astype(float)
+    g = rng.standard_normal(len(rows))
+    delta = sigma * rng.standard_normal(len(cells)) * 1e-2
+    out = {}
+    for name, fn in (("solve_fresh_model", lambda: oracle.apparent_resistivity(sigma)),
+                     ("vjp", lambda: oracle.vjp(sigma, g)), ("jvp", lambda: oracle.jvp(sigma, delta)),
+                     ("normal_vjp", lambda: oracle.normal_vjp(sigma, g)),
+                     ("normal_jvp", lambda: oracle.normal_jvp(sigma, delta))):
+        oracle._fields_cache = {}
+        start = time.perf_counter()
+        fn()
+        out[name] = 1e3 * (time.perf_counter() - start)
+    out["cores"] = int(torch.get_num_threads())
+    out["kind"] = "port"
+    return out
 
 
 def reference_kernel(forward, fields, J, handle, flush, device, stream, reps: int = 20) -> dict:
