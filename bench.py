@@ -660,29 +660,44 @@ def run_box3d(args, rank: int, world: int) -> dict | None:
     return result
 
 
-def box3d_cpu_baseline(nodes, cells, electrodes, rows, sample_rows: int = 64) -> dict:
-    """The FP64 oracle's fields (SciPy SuperLU) for one model plus the reference contraction on
-    a sample of rows, extrapolated to the full Jacobian."""
+def box3d_cpu_baseline(nodes, cells, electrodes, rows, sample_rows: int = 256) -> dict:
+    """The FP64 oracle's fields for one model (SciPy SuperLU: one factorization, 192 right-hand
+    sides) plus the reference's per-entry contraction (the C restatement, all host threads) on a
+    sample of rows, extrapolated to the full Jacobian. The contraction takes the current and the
+    receiver fields stacked as the rows of one field array, with A, B pointing at current rows
+    and M, N at receiver rows."""
 
     sys.path.insert(0, str(ROOT))
     from adtlert_b200 import synthetic
+    from oracle import baseline
     from oracle.ert3d import Oracle3D
 
     sample = np.linspace(0, len(rows) - 1, sample_rows).astype(int)
-    oracle = Oracle3D(nodes, cells, electrodes, rows[sample])
+    oracle = Oracle3D(nodes, cells, electrodes, rows)
     sigma = synthetic.ellipsoid_model(nodes, cells, 90_000).astype(float)
     start = time.perf_counter()
-    oracle.jacobian(sigma)
-    total = time.perf_counter() - start
-    start = time.perf_counter()
-    oracle.fields(sigma)
+    current, receiver, _ = oracle.fields(sigma)
     fields_s = time.perf_counter() - start
-    rows_s = max(total - fields_s, 0.0) / sample_rows
-    full = fields_s + rows_s * len(rows)
+    n_cur = current.shape[0]
+    phi = np.vstack((current, receiver))[None]  # (1, S, N)
+    S = phi.shape[1]
+    a, b, m, n = (oracle.abmn[sample, i] for i in range(4))
+    a = np.where(a >= n_cur, S, a)
+    b = np.where(b >= n_cur, S, b)
+    m = np.where(m >= receiver.shape[0], S, m + n_cur)
+    n = np.where(n >= receiver.shape[0], S, n + n_cur)
+    templates = np.where(oracle.pair_keep.reshape(-1, oracle.K, oracle.K), oracle.volume_templates, 0.0)[None]
+    threads = baseline.host_threads()
+    baseline.build()
+    start = time.perf_counter()
+    baseline.normal_sensitivity(phi, a, b, m, n, oracle.dofs, templates, threads)
+    contraction_s = time.perf_counter() - start
     D, C = len(rows), len(cells)
-    return {"value": D * C / full, "unit": "entries/s", "cores": 1, "kind": "port",
-            "sample": f"one model: FP64 SuperLU fields {fields_s:.1f} s + reference contraction of {sample_rows} of "
-                      f"{D} rows ({total - fields_s:.1f} s), extrapolated to {D} x {C}"}
+    full = fields_s + contraction_s * D / sample_rows
+    return {"value": D * C / full, "unit": "entries/s", "cores": threads, "kind": "port",
+            "sample": f"one model: FP64 SuperLU fields {fields_s:.1f} s (SciPy, one thread) + the reference contraction "
+                      f"of {sample_rows} of {D} rows on {threads} threads ({contraction_s:.2f} s), extrapolated to "
+                      f"{D} x {C}"}
 
 
 def run_b200(args, rank: int, world: int) -> dict | None:
