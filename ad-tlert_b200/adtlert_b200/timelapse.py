@@ -272,6 +272,24 @@ class WindowedInversion:
             _native.ptr(step), address, size, self.multiprocessors, f._stream()), f._plan, "adt_gn_step")
         return step
 
+    def _cgls_state(self) -> Tensor:
+        """The last step's device state as int32 words (the workspace's first 16 bytes: done,
+        iterations, error, reserved; the float64 gammas follow)."""
+
+        address, _ = self._workspace_ptr()
+        offset = address - self._workspace.data_ptr()
+        return self._workspace[offset:offset + 16].view(torch.int32)
+
+    def cgls_iterations(self) -> int:
+        """CGLS iterations the last ``gauss_newton_step`` ran before its stop test held. Synchronizes."""
+
+        return int(self._cgls_state()[1].item())
+
+    def _check_cgls(self, error: float) -> None:
+        if error != 0:
+            raise RuntimeError("adt_gn_step: a data pass gave up waiting for its copies of the Jacobian rows "
+                               "(the step is NaN)")
+
     def regularized(self, models: Tensor) -> Tensor:
         """(ls R^T R + lt D^T D) models, (T, C) float64 on the device (adt_gn_regularize)."""
 
@@ -354,7 +372,9 @@ class WindowedInversion:
                 tau, step, models, predicted, J = accepted
             result.taus.append(tau)
             residual = weights * (predicted - observed)
-            chi2, step_sq = torch.stack([(residual * residual).mean(), (step * step).sum()]).cpu().tolist()
+            chi2, step_sq, error = torch.stack([(residual * residual).mean(), (step * step).sum(),
+                                                self._cgls_state()[2].double()]).cpu().tolist()
+            self._check_cgls(error)
             result.chi2.append(chi2)
             if s.target_chi2 is not None and chi2 < s.target_chi2:
                 result.stop_reason = "target_chi2"

@@ -147,6 +147,7 @@ struct adt_plan {
   bool jacobian_tc = true;      // tensor-core Jacobian where it applies
   bool jacobian_pipe = true;    // its warp-role pipelined form where that applies
   bool jacobian_direct = true;  // direct-form Jacobian for single-wavenumber operators
+  bool cgls_ring = true;        // shared-memory ring data pass of adt_gn_step where p and its rows fit
   unsigned tc_first_wait_polls = 0;  // 0: default MMA wait of the tensor-core Jacobian; n: n polls
   int* tc_error = nullptr;      // device flag raised by a tensor-core block that timed out
   int* tc_error_host = nullptr; // pinned copy, refreshed after each tensor-core launch

@@ -18,26 +18,45 @@
 // Kernels of one iteration (all chained on the caller's stream; a device flag set when the
 // iteration stops turns the rest of the launched iterations into no-ops, so the host never waits
 // inside the loop):
-//   normal_data_kernel   per block, a range of rows of one model: q_d = w_d (J_d . p_t), then
-//                        partial += J_d w_d q_d, in float64 registers; written once per block.
+//   normal_ring_kernel   per block, a range of rows of one model, streamed through a shared-memory
+//                        ring by bulk copies: q_d = w_d (J_d . p_t), then partial += J_d w_d q_d,
+//                        in float64 registers; written once per block (normal_data_kernel: the
+//                        same with register loads, where p_t and the ring exceed shared memory).
 //   normal_reduce_kernel u = sum of the block partials (fixed order) + ls L p_t + lt T^T T p,
 //                        with L = R^T R from neighbour lists; block partials of p.u.
-//   cgls_update_kernel   one block: alpha, x, s, gamma', beta, p.
+//   cgls_alpha_kernel    alpha = gamma / p.u, x += alpha p, s -= alpha u; block partials of s.s.
+//   cgls_beta_kernel     gamma' = s.s, the stop test, beta = gamma' / gamma, p = s + beta p.
+// The last two run on every block; each block sums the partials it needs itself, in one order.
 // Every reduction runs in a fixed order, so a step is bitwise repeatable.
+#include <algorithm>
+
 #include "adt_internal.h"
+#include "tcgen05.h"
 
 namespace {
 
 constexpr int kPassThreads = 512;
-constexpr int kReduceThreads = 256;
-constexpr int kUpdateThreads = 1024;
+constexpr int kReduceColumns = 64;  // reduce kernel: 64 elements per block ...
+constexpr int kReduceGroups = 4;    // ... with the data partials of each split over 4 threads
+constexpr int kReduceThreads = kReduceColumns * kReduceGroups;
+constexpr int kUpdateThreads = 256;  // alpha and beta kernels: one element per thread
+constexpr int kStartThreads = 1024;  // start kernel: one block
 constexpr int kMaxVec = 8;  // float4 per thread of the data pass: C <= 4 * 512 * 8 = 16384 columns
+constexpr int kRingSlots = 4;  // most rows of J in the shared-memory ring of one data-pass block
+constexpr uint32_t kRingWaitLimit = 1u << 22;  // mbarrier polls before a ring wait gives up
+constexpr size_t kL2ResidentBytes = 96u << 20;  // J bytes loaded evict-last (kept in L2 between passes)
 
+// Per-step device state. The host clears it before a step; `error` is raised by a data pass that
+// gave up waiting for its row copies (the step is then NaN). gamma = s.s alternates between two
+// slots by iteration parity, so the blocks of one kernel read the old value while block 0 writes
+// the new one.
 struct CglsState {
-  double gamma;
-  double gamma0;
   int done;
   int iterations;
+  int error;
+  int reserved;
+  double gamma0;
+  double gamma[2];
 };
 
 struct Workspace {
@@ -46,22 +65,30 @@ struct Workspace {
   double* p;
   double* u;
   double* partial;
-  double* dots;
+  double* dots;     // per-block partials of p.u (reduce kernel)
+  double* squares;  // per-block partials of s.s (alpha kernel)
   int ctas_per_model;
   int reduce_blocks;
+  int update_blocks;
 };
 
 size_t align256(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
+// Blocks per model of a data pass: both data kernels hold one block per multiprocessor, so the
+// grid is at most one wave (rounding up would leave a second wave of a few blocks that doubles
+// the pass).
 int data_ctas_per_model(int steps, int sms) {
-  const int per = (sms + steps - 1) / steps;
+  const int per = sms / steps;
   return per < 1 ? 1 : per;
 }
+
+int reduce_grid(int64_t n) { return (int)((n + kReduceColumns - 1) / kReduceColumns); }
+int update_grid(int64_t n) { return (int)((n + kUpdateThreads - 1) / kUpdateThreads); }
 
 size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) {
   const size_t n = (size_t)T * C;
   const int per = data_ctas_per_model(T, sms);
-  const int reduce_blocks = (int)((n + kReduceThreads - 1) / kReduceThreads);
+  const int reduce_blocks = reduce_grid((int64_t)n), update_blocks = update_grid((int64_t)n);
   size_t offset = 0;
   auto take = [&](size_t bytes) {
     char* at = base ? base + offset : nullptr;
@@ -74,6 +101,7 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
   char* u = take(n * sizeof(double));
   char* partial = take((size_t)T * per * C * sizeof(double));
   char* dots = take((size_t)reduce_blocks * sizeof(double));
+  char* squares = take((size_t)update_blocks * sizeof(double));
   (void)D;
   if (w) {
     w->state = reinterpret_cast<CglsState*>(state);
@@ -82,8 +110,10 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
     w->u = reinterpret_cast<double*>(u);
     w->partial = reinterpret_cast<double*>(partial);
     w->dots = reinterpret_cast<double*>(dots);
+    w->squares = reinterpret_cast<double*>(squares);
     w->ctas_per_model = per;
     w->reduce_blocks = reduce_blocks;
+    w->update_blocks = update_blocks;
   }
   return offset;
 }
@@ -170,6 +200,191 @@ __global__ void __launch_bounds__(kPassThreads) normal_data_kernel(
   }
 }
 
+// Shared-memory ring data pass, the default wherever p_t and three rows fit in shared memory:
+// the sums of normal_data_kernel, but the rows of J arrive by bulk asynchronous copies
+// (cp.async.bulk, one row per copy, completion counted on one mbarrier per slot) into a ring of
+// 4 slots (3 where 4 do not fit), issued that many rows ahead, so they stream while the block
+// forms a row's dot product, reduces it and accumulates. Thread 0 issues the copies; a slot is
+// refilled after the barrier that ends every thread's reads of it (each thread keeps its slice of
+// the row in registers for the accumulation). p_t is held as two planes of double2, (p0, p1) and
+// (p2, p3) of each group of four columns, so a warp's reads are conflict-free. Rows of models
+// t < l2_resident_models are loaded evict-last and the others evict-first: with three 47 MB
+// Jacobians per window, two stay in the 126 MB L2 from one CGLS iteration to the next instead of
+// all three thrashing it.
+struct RingLayout {
+  size_t rows, bars, total;
+};
+
+__host__ __device__ inline RingLayout ring_layout(int C, int slots) {
+  RingLayout l;
+  l.rows = (size_t)C * sizeof(double);  // p_t first, then the slots
+  l.bars = l.rows + (size_t)slots * C * sizeof(float);
+  l.total = l.bars + (size_t)slots * sizeof(uint64_t);
+  return l;
+}
+
+constexpr size_t kRingSmemLimit = 227 * 1024 - 1024;  // dynamic bytes; the rest is the static reduction buffer
+
+// Ring slots for C columns: 4 where they fit, else 3, else 0 (the register pass).
+inline int ring_slots(int C) {
+  for (int slots = kRingSlots; slots >= 3; --slots)
+    if (ring_layout(C, slots).total <= kRingSmemLimit) return slots;
+  return 0;
+}
+
+__device__ __forceinline__ uint64_t l2_policy(bool keep) {
+  uint64_t policy;
+  if (keep)
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(policy));
+  else
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(policy));
+  return policy;
+}
+
+__device__ __forceinline__ void ring_copy(uint64_t* bar, void* dst, const void* src, uint32_t bytes,
+                                          uint64_t policy) {
+  const uint32_t b = adt::tc::smem_addr(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;\n" ::
+          "r"(adt::tc::smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(b), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ bool ring_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t b = adt::tc::smem_addr(bar);
+  for (uint32_t polls = 0; polls < kRingWaitLimit; ++polls)
+    if (adt::tc::mbar_try_wait(b, parity)) return true;
+  return false;
+}
+
+template <int VEC>
+__global__ void __launch_bounds__(kPassThreads, 1) normal_ring_kernel(
+    const float* __restrict__ J, int D, int C, const double* __restrict__ weights, const double* __restrict__ vec,
+    const double* __restrict__ given, int ctas_per_model, double* __restrict__ partial, CglsState* state,
+    int l2_resident_models, int slots) {
+  adt::chain_wait();
+  if (given == nullptr && state->done) return;
+  extern __shared__ __align__(16) unsigned char ring[];
+  const RingLayout lay = ring_layout(C, slots);
+  const int C4 = C >> 2;
+  double2* pa = reinterpret_cast<double2*>(ring);
+  double2* pb = pa + C4;
+  float* ring_rows = reinterpret_cast<float*>(ring + lay.rows);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + lay.bars);
+  const int t = blockIdx.x / ctas_per_model, k = blockIdx.x % ctas_per_model;
+  const int rows_per = (D + ctas_per_model - 1) / ctas_per_model;
+  const int d0 = k * rows_per, n = max(0, min(D, d0 + rows_per) - d0);
+  const uint32_t row_bytes = (uint32_t)C * sizeof(float);
+  const float* rows0 = J + ((size_t)t * D + d0) * C;
+  const uint64_t policy = l2_policy(t < l2_resident_models);
+  if (threadIdx.x == 0) {
+    for (int slot = 0; slot < slots; ++slot)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(adt::tc::smem_addr(full + slot)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    for (int i = 0; i < min(slots, n); ++i)
+      ring_copy(full + i, ring_rows + (size_t)i * C, rows0 + (size_t)i * C, row_bytes, policy);
+  }
+  if (given == nullptr)
+    for (int i = threadIdx.x; i < C4; i += kPassThreads) {
+      const double* src = vec + (size_t)t * C + 4 * i;
+      pa[i] = make_double2(src[0], src[1]);
+      pb[i] = make_double2(src[2], src[3]);
+    }
+  __syncthreads();
+  auto wait_row = [&](int i) { return ring_wait(full + i % slots, (uint32_t)((i / slots) & 1)); };
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  double acc[VEC][4];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.0;
+  __shared__ double red[2][kPassThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int stalled = -1;  // the row whose copy did not arrive within the wait limit
+  int issued = min(slots, n);
+  for (int i = 0; i < n; ++i) {
+    const int slot = i % slots;
+    const double w = weights[(size_t)t * D + d0 + i];
+    const double given_q = given != nullptr ? given[(size_t)t * D + d0 + i] : 0.0;
+    const bool ready = wait_row(i);
+    const float4* row = reinterpret_cast<const float4*>(ring_rows + (size_t)slot * C);
+    float4 r[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const int idx = threadIdx.x + v * kPassThreads;
+      r[v] = (ready && idx < C4) ? row[idx] : zero;
+    }
+    if (given == nullptr) {
+      double part[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        const int idx = threadIdx.x + v * kPassThreads;
+        if (idx < C4) {
+          const double2 a = pa[idx], b = pb[idx];
+          part[0] = fma((double)r[v].x, a.x, part[0]);
+          part[1] = fma((double)r[v].y, a.y, part[1]);
+          part[2] = fma((double)r[v].z, b.x, part[2]);
+          part[3] = fma((double)r[v].w, b.y, part[3]);
+        }
+      }
+      double dot = (part[0] + part[1]) + (part[2] + part[3]);
+#pragma unroll
+      for (int offset = 16; offset > 0; offset >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, offset);
+      if (lane == 0) red[i & 1][warp] = dot;
+    }
+    // one barrier per row: the block's dot product is complete and every thread holds its slice of
+    // the row in registers, so the slot can take the row `slots` further on
+    if (__syncthreads_or(!ready)) {
+      stalled = i;
+      break;
+    }
+    if (i + slots < n) {
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        ring_copy(full + slot, ring_rows + (size_t)slot * C, rows0 + (size_t)(i + slots) * C, row_bytes, policy);
+      }
+      issued = i + slots + 1;
+    }
+    double q = given_q;
+    if (given == nullptr) {
+      double dot = 0.0;
+#pragma unroll
+      for (int j = 0; j < kPassThreads / 32; ++j) dot += red[i & 1][j];
+      q = w * dot;
+    }
+    const double wq = w * q;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      acc[v][0] = fma((double)r[v].x, wq, acc[v][0]);
+      acc[v][1] = fma((double)r[v].y, wq, acc[v][1]);
+      acc[v][2] = fma((double)r[v].z, wq, acc[v][2]);
+      acc[v][3] = fma((double)r[v].w, wq, acc[v][3]);
+    }
+  }
+  double* out = partial + (size_t)blockIdx.x * C;
+  if (stalled >= 0) {
+    // a copy did not complete within the wait limit: wait (bounded) for the copies still in flight
+    // into this block's shared memory, mark the step and leave NaN in this block's partial
+    if (threadIdx.x == 0) {
+      for (int j = stalled; j < issued; ++j) wait_row(j);
+      atomicExch(&state->error, 1);
+    }
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = nan;
+  }
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    const int idx = threadIdx.x + v * kPassThreads;
+    if (idx < C4) {
+      double2* pair = reinterpret_cast<double2*>(out + 4 * idx);
+      pair[0] = make_double2(acc[v][0], acc[v][1]);
+      pair[1] = make_double2(acc[v][2], acc[v][3]);
+    }
+  }
+  __syncthreads();  // thread 0's waits for in-flight copies end before the block's shared memory is released
+}
+
 // Block sum of one double per thread, in a fixed order (shuffle tree, then warp 0 over the
 // warps in order). The result is valid in thread 0.
 template <int THREADS>
@@ -185,8 +400,24 @@ __device__ __forceinline__ double block_sum(double value, double* shared) {
   return total;
 }
 
-// u = (sum of the data partials) + spatial L v_t + temporal T^T T v, element (t, c) per thread;
-// with `dot_with`, per-block partials of dot_with . u. `partial` may be null (regularizer only).
+// Sum of `count` values in a fixed order (lane l adds values l, l + 32, ..., then a butterfly),
+// identical in every block that calls it; the result is returned to every thread of the block.
+__device__ __forceinline__ double ordered_sum(const double* __restrict__ values, int count, double* shared_total) {
+  if (threadIdx.x < 32) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < count; i += 32) v += values[i];
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_xor_sync(0xffffffffu, v, offset);
+    if (threadIdx.x == 0) *shared_total = v;
+  }
+  __syncthreads();
+  return *shared_total;
+}
+
+// u = (sum of the data partials) + spatial L v_t + temporal T^T T v, kReduceColumns elements (t, c)
+// per block, the data partials of each summed by kReduceGroups threads (every kReduceGroups-th
+// partial) and the group sums added in group order; with `dot_with`, per-block partials of
+// dot_with . u. `partial` may be null (regularizer only).
 __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
     const double* __restrict__ partial, int ctas_per_model, int T, int C, const double* __restrict__ v,
     const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_cell, const double* __restrict__ nbr_w2,
@@ -194,15 +425,23 @@ __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
     double* __restrict__ dots, const CglsState* __restrict__ state) {
   adt::chain_wait();
   if (state != nullptr && state->done) return;
-  __shared__ double shared[kReduceThreads / 32];
+  __shared__ double group_sum[kReduceGroups - 1][kReduceColumns];
+  __shared__ double shared[kReduceColumns / 32];
   const int64_t n = (int64_t)T * C;
-  const int64_t i = (int64_t)blockIdx.x * kReduceThreads + threadIdx.x;
+  const int column = threadIdx.x % kReduceColumns, group = threadIdx.x / kReduceColumns;
+  const int64_t i = (int64_t)blockIdx.x * kReduceColumns + column;
+  const int t = i < n ? (int)(i / C) : 0, c = i < n ? (int)(i % C) : 0;
+  double sum = 0.0;
+  if (partial != nullptr && i < n)
+    for (int k = group; k < ctas_per_model; k += kReduceGroups)
+      sum += partial[((size_t)t * ctas_per_model + k) * C + c];
+  if (group > 0) group_sum[group - 1][column] = sum;
+  __syncthreads();
+  if (group > 0) return;
+#pragma unroll
+  for (int g = 0; g < kReduceGroups - 1; ++g) sum += group_sum[g][column];
   double product = 0.0;
   if (i < n) {
-    const int t = (int)(i / C), c = (int)(i % C);
-    double sum = 0.0;
-    if (partial != nullptr)
-      for (int k = 0; k < ctas_per_model; ++k) sum += partial[((size_t)t * ctas_per_model + k) * C + c];
     const double* vt = v + (size_t)t * C;
     const double vc = vt[c];
     double lap = 0.0;
@@ -214,83 +453,96 @@ __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
     u[i] = value;
     if (dot_with != nullptr) product = dot_with[i] * value;
   }
-  if (dot_with != nullptr) {
-    const double total = block_sum<kReduceThreads>(product, shared);
-    if (threadIdx.x == 0) dots[blockIdx.x] = total;
+  if (dot_with != nullptr) {  // the first kReduceColumns threads (the other groups have left): named barrier
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) product += __shfl_xor_sync(0xffffffffu, product, offset);
+    if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = product;
+    asm volatile("bar.sync 1, %0;\n" ::"n"(kReduceColumns) : "memory");
+    if (threadIdx.x == 0) {
+      double total = 0.0;
+#pragma unroll
+      for (int w = 0; w < kReduceColumns / 32; ++w) total += shared[w];
+      dots[blockIdx.x] = total;
+    }
   }
 }
 
 // x = 0, s = p = A^T b (in u), gamma = gamma_0 = s.s.
-__global__ void __launch_bounds__(kUpdateThreads) cgls_start_kernel(CglsState* st, int64_t n, const double* __restrict__ u,
-                                                                    double* __restrict__ x, double* __restrict__ s,
-                                                                    double* __restrict__ p) {
+__global__ void __launch_bounds__(kStartThreads) cgls_start_kernel(CglsState* st, int64_t n, const double* __restrict__ u,
+                                                                   double* __restrict__ x, double* __restrict__ s,
+                                                                   double* __restrict__ p) {
   adt::chain_wait();
-  __shared__ double shared[kUpdateThreads / 32];
+  __shared__ double shared[kStartThreads / 32];
   double ss = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += kUpdateThreads) {
+  for (int64_t i = threadIdx.x; i < n; i += kStartThreads) {
     const double value = u[i];
     x[i] = 0.0;
     s[i] = value;
     p[i] = value;
     ss += value * value;
   }
-  const double gamma = block_sum<kUpdateThreads>(ss, shared);
+  const double gamma = block_sum<kStartThreads>(ss, shared);
   if (threadIdx.x == 0) {
-    st->gamma = gamma;
+    st->gamma[0] = gamma;
     st->gamma0 = gamma;
     st->done = gamma > 0.0 ? 0 : 1;
     st->iterations = 0;
   }
 }
 
-__global__ void __launch_bounds__(kUpdateThreads) cgls_update_kernel(CglsState* st, int64_t n,
-                                                                     const double* __restrict__ dots, int blocks,
-                                                                     double* __restrict__ x, double* __restrict__ s,
-                                                                     double* __restrict__ p,
-                                                                     const double* __restrict__ u, double tolerance) {
+// Iteration `it`, first half: alpha = gamma / p.u (p.u summed from the reduce partials by every
+// block in the same order), x += alpha p, s -= alpha u, per-block partials of s.s.
+__global__ void __launch_bounds__(kUpdateThreads) cgls_alpha_kernel(CglsState* st, int it, int64_t n,
+                                                                    const double* __restrict__ dots, int dot_count,
+                                                                    double* __restrict__ x, double* __restrict__ s,
+                                                                    const double* __restrict__ p,
+                                                                    const double* __restrict__ u,
+                                                                    double* __restrict__ squares) {
   adt::chain_wait();
-  __shared__ double shared[kUpdateThreads / 32];
-  __shared__ double alpha_s, beta_s;
-  __shared__ int stop_s;
-  if (threadIdx.x == 0) {  // only thread 0 reads or writes the flag in this kernel
-    if (st->done) {
-      stop_s = 1;
-    } else {
-      double pu = 0.0;
-      for (int b = 0; b < blocks; ++b) pu += dots[b];
-      stop_s = pu > 0.0 ? 0 : 1;
-      alpha_s = stop_s ? 0.0 : st->gamma / pu;
-      if (stop_s) st->done = 1;
-    }
+  if (st->done) return;  // set by an earlier kernel, or below by block 0 for the same reason
+  __shared__ double total, shared[kUpdateThreads / 32];
+  const double pu = ordered_sum(dots, dot_count, &total);
+  if (!(pu > 0.0)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+    return;
   }
-  __syncthreads();
-  if (stop_s) return;
-  const double alpha = alpha_s;
-  double ss = 0.0;
-  for (int64_t i = threadIdx.x; i < n; i += kUpdateThreads) {
+  const double alpha = st->gamma[it & 1] / pu;
+  const int64_t i = (int64_t)blockIdx.x * kUpdateThreads + threadIdx.x;
+  double square = 0.0;
+  if (i < n) {
     x[i] += alpha * p[i];
     const double si = s[i] - alpha * u[i];
     s[i] = si;
-    ss += si * si;
+    square = si * si;
   }
-  const double gamma_new = block_sum<kUpdateThreads>(ss, shared);
+  const double block_total = block_sum<kUpdateThreads>(square, shared);
   if (threadIdx.x == 0) {
-    st->iterations += 1;
-    if (!(gamma_new > 0.0) || gamma_new / st->gamma0 < tolerance) {
-      stop_s = 1;
+    squares[blockIdx.x] = block_total;
+    if (blockIdx.x == 0) st->iterations += 1;
+  }
+}
+
+// Iteration `it`, second half: gamma' = s.s (every block sums the partials in the same order),
+// stop when gamma' / gamma_0 < tolerance, else beta = gamma' / gamma and p = s + beta p.
+__global__ void __launch_bounds__(kUpdateThreads) cgls_beta_kernel(CglsState* st, int it, int64_t n,
+                                                                   const double* __restrict__ squares, int count,
+                                                                   const double* __restrict__ s,
+                                                                   double* __restrict__ p, double tolerance) {
+  adt::chain_wait();
+  if (st->done) return;
+  __shared__ double total;
+  const double gamma_new = ordered_sum(squares, count, &total);
+  const bool stop = !(gamma_new > 0.0) || gamma_new / st->gamma0 < tolerance;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (stop)
       st->done = 1;
-    } else {
-      beta_s = gamma_new / st->gamma;
-      st->gamma = gamma_new;
-    }
+    else
+      st->gamma[(it + 1) & 1] = gamma_new;
   }
-  __syncthreads();
-  if (stop_s) return;
-  const double beta = beta_s;
-  for (int64_t i = threadIdx.x; i < n; i += kUpdateThreads) {
-    const double value = s[i] + beta * p[i];
-    p[i] = value;
-  }
+  if (stop) return;
+  const double beta = gamma_new / st->gamma[it & 1];
+  const int64_t i = (int64_t)blockIdx.x * kUpdateThreads + threadIdx.x;
+  if (i < n) p[i] = s[i] + beta * p[i];
 }
 
 template <int VEC>
@@ -307,11 +559,39 @@ void launch_data(const float* J, int T, int D, int C, const double* weights, con
                       weights, vec, given, w.ctas_per_model, w.partial, state);
 }
 
-bool data_pass(const float* J, int T, int D, int C, const double* weights, const double* vec, const double* given,
-               const Workspace& w, const CglsState* state, cudaStream_t s) {
-  const int vec_per_thread = ((C >> 2) + kPassThreads - 1) / kPassThreads;
+template <int VEC>
+void launch_ring(const float* J, int T, int D, int C, const double* weights, const double* vec, const double* given,
+                 const Workspace& w, int slots, cudaStream_t s) {
+  static bool raised = false;
+  if (!raised) {
+    cudaFuncSetAttribute(normal_ring_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRingSmemLimit);
+    raised = true;
+  }
+  const size_t model_bytes = (size_t)D * C * sizeof(float);
+  const int resident = (int)std::min<size_t>((size_t)T, kL2ResidentBytes / model_bytes);
+  adt::launch_chained(normal_ring_kernel<VEC>, dim3(T * w.ctas_per_model), dim3(kPassThreads),
+                      ring_layout(C, slots).total, s, J, D, C, weights, vec, given, w.ctas_per_model, w.partial,
+                      w.state, resident, slots);
+}
+
+// One pass over J: A^T b (given = b_data, `iteration` false) or the product of a CGLS iteration.
+bool data_pass(const adt_plan* p, const float* J, int T, int D, int C, const double* weights, const double* vec,
+               const double* given, const Workspace& w, bool iteration, cudaStream_t s) {
+  const int vec_per_thread = std::max(1, ((C >> 2) + kPassThreads - 1) / kPassThreads);
+  const int slots = p->cgls_ring ? ring_slots(C) : 0;
+  if (slots > 0) {
+    switch (vec_per_thread) {
+      case 1: launch_ring<1>(J, T, D, C, weights, vec, given, w, slots, s); return true;
+      case 2: launch_ring<2>(J, T, D, C, weights, vec, given, w, slots, s); return true;
+      case 3: launch_ring<3>(J, T, D, C, weights, vec, given, w, slots, s); return true;
+      case 4: launch_ring<4>(J, T, D, C, weights, vec, given, w, slots, s); return true;
+      case 5: launch_ring<5>(J, T, D, C, weights, vec, given, w, slots, s); return true;
+      case 6: launch_ring<6>(J, T, D, C, weights, vec, given, w, slots, s); return true;
+      default: break;  // p_t and the ring above the shared-memory limit: the register pass below
+    }
+  }
+  const CglsState* state = iteration ? w.state : nullptr;
   switch (vec_per_thread) {
-    case 0:
     case 1: launch_data<1>(J, T, D, C, weights, vec, given, w, state, s); return true;
     case 2: launch_data<2>(J, T, D, C, weights, vec, given, w, state, s); return true;
     case 3: launch_data<3>(J, T, D, C, weights, vec, given, w, state, s); return true;
@@ -357,23 +637,27 @@ extern "C" adt_status adt_gn_step(adt_plan* p, const float* jacobian, int32_t st
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t n = (int64_t)steps * columns;
   // s_0 = A^T b = J^T W b_data - ls L m - lt T^T T m
-  data_pass(jacobian, steps, rows, columns, data_weights, w.p, data_rhs, w, nullptr, s);
+  cudaMemsetAsync(w.state, 0, sizeof(CglsState), s);
+  data_pass(p, jacobian, steps, rows, columns, data_weights, w.p, data_rhs, w, false, s);
   adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s, (const double*)w.partial,
                       w.ctas_per_model, (int)steps, (int)columns, models, neighbour_ptr, neighbour_cells,
                       neighbour_weights, -spatial, -temporal, (const double*)nullptr, w.u, w.dots,
                       (const CglsState*)nullptr);
-  adt::launch_chained(cgls_start_kernel, dim3(1), dim3(kUpdateThreads), 0, s, w.state, n, (const double*)w.u, step,
+  adt::launch_chained(cgls_start_kernel, dim3(1), dim3(kStartThreads), 0, s, w.state, n, (const double*)w.u, step,
                       w.s, w.p);
   p->launches += 3;
   for (int it = 0; it < iterations; ++it) {
-    data_pass(jacobian, steps, rows, columns, data_weights, w.p, nullptr, w, w.state, s);
+    data_pass(p, jacobian, steps, rows, columns, data_weights, w.p, nullptr, w, true, s);
     adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s,
                         (const double*)w.partial, w.ctas_per_model, (int)steps, (int)columns, (const double*)w.p,
                         neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal, (const double*)w.p, w.u,
                         w.dots, (const CglsState*)w.state);
-    adt::launch_chained(cgls_update_kernel, dim3(1), dim3(kUpdateThreads), 0, s, w.state, n, (const double*)w.dots,
-                        w.reduce_blocks, step, w.s, w.p, (const double*)w.u, tolerance);
-    p->launches += 3;
+    adt::launch_chained(cgls_alpha_kernel, dim3(w.update_blocks), dim3(kUpdateThreads), 0, s, w.state, it, n,
+                        (const double*)w.dots, w.reduce_blocks, step, w.s, (const double*)w.p, (const double*)w.u,
+                        w.squares);
+    adt::launch_chained(cgls_beta_kernel, dim3(w.update_blocks), dim3(kUpdateThreads), 0, s, w.state, it, n,
+                        (const double*)w.squares, w.update_blocks, (const double*)w.s, w.p, tolerance);
+    p->launches += 4;
   }
   return adt::check_launch(p, "gauss-newton step");
 }
@@ -386,9 +670,8 @@ extern "C" adt_status adt_gn_regularize(adt_plan* p, int32_t steps, int32_t colu
   if (steps <= 0 || columns <= 0 || !neighbour_ptr || !models || !out)
     return adt::fail(p, ADT_INVALID_ARG, "adt_gn_regularize: invalid arguments");
   const int64_t n = (int64_t)steps * columns;
-  adt::launch_chained(normal_reduce_kernel, dim3((unsigned)((n + kReduceThreads - 1) / kReduceThreads)),
-                      dim3(kReduceThreads), 0, (cudaStream_t)stream, (const double*)nullptr, 0, (int)steps,
-                      (int)columns, models, neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal,
+  adt::launch_chained(normal_reduce_kernel, dim3((unsigned)reduce_grid(n)), dim3(kReduceThreads), 0,
+                      (cudaStream_t)stream, (const double*)nullptr, 0, (int)steps, (int)columns, models, neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal,
                       (const double*)nullptr, out, (double*)nullptr, (const CglsState*)nullptr);
   p->launches += 1;
   return adt::check_launch(p, "gauss-newton regularizer");

@@ -320,6 +320,10 @@ adt_status adt_plan_create(const adt_problem* pr, adt_plan** out) {
                          std::strcmp(choice, "tc1") != 0;
     p->jacobian_pipe = std::strcmp(choice, "tc1") != 0;
   }
+  if (const char* choice = std::getenv("ADTLERT_B200_CGLS")) {
+    // "registers": the register data pass of the Gauss-Newton step at every size (for comparison)
+    p->cgls_ring = std::strcmp(choice, "registers") != 0;
+  }
   configure_solver_kernels();
   auto bail = [&](adt_status st) {
     g_create_error = p->error;

@@ -25,17 +25,25 @@ from oracle import timelapse as oracle
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def golden():
+def _golden():
     return np.load(ROOT / "tests" / "golden" / "timelapse_small.npz")
 
 
-@pytest.fixture(scope="module")
-def small():
+def _small():
     inputs = case_inputs("tri_flat")
     op = ERTForward2p5D(Mesh.from_arrays(inputs["nodes"], inputs["cells"]),
                         Survey.from_arrays(inputs["electrodes"], inputs["measurements"]))
     return op, inputs
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return _golden()
+
+
+@pytest.fixture(scope="module")
+def small():
+    return _small()
 
 
 def _settings(golden, **overrides):
@@ -95,6 +103,27 @@ def test_device_cgls_on_the_benchmark_section():
     settings = WindowSettings(data_std=float(np.log1p(0.02)), cgls_max_iterations=20)
     step, expected, _, _ = _compare_steps(op, nodes, cells, settings, observed, initial)
     assert_close(step, expected, 1e-5, "20-iteration CGLS step, 3 x 1232 x 9600")
+
+
+def test_register_data_pass_matches_the_oracle():
+    """The register data pass (used where p_t and the row ring exceed shared memory), forced for
+    both sizes through ADTLERT_B200_CGLS=registers in a child process (the choice is read when a
+    plan is created)."""
+
+    import os
+    import subprocess
+    import sys
+
+    script = ("import test_timelapse_gpu as m\n"
+              "m.test_device_cgls_matches_the_oracle(m._small(), m._golden())\n"
+              "m.test_device_cgls_on_the_benchmark_section()\n"
+              "print('register data pass ok')\n")
+    env = dict(os.environ, ADTLERT_B200_CGLS="registers",
+               PYTHONPATH=os.pathsep.join([str(ROOT / "tests"), str(ROOT / "tests" / "golden"), str(ROOT),
+                                           str(ROOT / "ad-tlert_b200"),
+                                           os.environ.get("PYTHONPATH", "")]))
+    done = subprocess.run([sys.executable, "-c", script], env=env, capture_output=True, text=True, timeout=600)
+    assert done.returncode == 0 and "register data pass ok" in done.stdout, done.stdout + done.stderr
 
 
 def test_one_iteration_matches_the_reference(small, golden):
