@@ -59,7 +59,12 @@ SYMBOLS = (
     "adt_mlp_transpose",
     "adt_mlp_to_bf16",
     "adt_kernel_launches",
+    "adt_autotune",
+    "adt_get_tuning",
+    "adt_set_tuning",
 )
+
+JACOBIAN_KERNELS = ("direct", "tc_pipelined", "tc", "fma")
 
 _p = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -113,6 +118,23 @@ class PlanInfo(ctypes.Structure):
         ("factor_doubles_per_system", _i64),
         ("contributions", _i64),
     ]
+
+
+class Tuning(ctypes.Structure):
+    """``adt_tuning``: launch shapes of one plan (and, from ``adt_autotune``, their times)."""
+
+    _fields_ = [
+        ("strip_fill", _i32),
+        ("split_fill", _i32),
+        ("jacobian_kernel", _i32),
+        ("fields_ms", ctypes.c_float),
+        ("jacobian_ms", ctypes.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {"strip_fill": self.strip_fill, "split_fill": self.split_fill,
+                "jacobian_kernel": JACOBIAN_KERNELS[self.jacobian_kernel],
+                "fields_ms": float(self.fields_ms), "jacobian_ms": float(self.jacobian_ms)}
 
 
 _lib = None
@@ -176,6 +198,9 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_mlp_to_bf16": (status, [_p, _i64, _p, _p]),
         "adt_set_jacobian_wait_limit": (status, [_p, ctypes.c_uint32]),
         "adt_kernel_launches": (_i64, [_p]),
+        "adt_autotune": (status, [_p, _i32, _p, _i32, _p, _p, _i32, ctypes.POINTER(Tuning), _p]),
+        "adt_get_tuning": (status, [_p, ctypes.POINTER(Tuning)]),
+        "adt_set_tuning": (status, [_p, ctypes.POINTER(Tuning)]),
     }
     for name, (restype, argtypes) in signatures.items():
         fn = getattr(lib, name)

@@ -27,6 +27,7 @@ import numpy as np
 import torch
 
 from . import _native
+from . import tuning as _tuning
 from .fem import (
     analytic_primary,
     boundary_mass,
@@ -533,6 +534,18 @@ class ERTForward2p5D:
 
     def kernel_launches(self) -> int:
         return int(self._lib.adt_kernel_launches(self._plan))
+
+    def autotune(self, conductivity=None, *, repeats: int = 3, jacobian: bool = True) -> dict:
+        """Choose the plan's launch shapes (solver strips, tiled split depth, Jacobian kernel) by
+        timing them on ``conductivity``; returns the choice and its times (ms)."""
+
+        return _tuning.autotune(self, conductivity, repeats, jacobian)
+
+    def tuning(self) -> dict:
+        return _tuning.tuning(self)
+
+    def set_tuning(self, settings: dict) -> None:
+        _tuning.set_tuning(self, settings)
 
     def _sigma(self, conductivity) -> Tensor:
         return conductivity_model(conductivity, self.C)

@@ -28,6 +28,7 @@ import numpy as np
 import torch
 
 from . import _native
+from . import tuning as _tuning
 from .ert2p5d import _checked_to_host, _Slots, _survey_arrays
 from .field_store import FieldStore, model_fingerprints
 from .geometry3d import (
@@ -319,6 +320,18 @@ class ERTForward3D:
 
     def kernel_launches(self) -> int:
         return int(self._lib.adt_kernel_launches(self._plan))
+
+    def autotune(self, conductivity=None, *, repeats: int = 3, jacobian: bool = True) -> dict:
+        """Choose the plan's launch shapes (solver strips, tiled split depth, Jacobian kernel) by
+        timing them on ``conductivity``; returns the choice and its times (ms)."""
+
+        return _tuning.autotune(self, conductivity, repeats, jacobian)
+
+    def tuning(self) -> dict:
+        return _tuning.tuning(self)
+
+    def set_tuning(self, settings: dict) -> None:
+        _tuning.set_tuning(self, settings)
 
     def _call(self, name: str, *args) -> None:
         _native.check(getattr(self._lib, name)(self._plan, *args), self._plan, name)

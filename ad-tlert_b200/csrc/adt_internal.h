@@ -144,6 +144,9 @@ struct adt_plan {
   int64_t launches = 0;
   int device = 0;
   int sms = 148;                // multiprocessors of the device
+  // launch-shape rules of the solver (chosen by adt_autotune, else these defaults):
+  int strip_fill = 2;           // substitution strips narrow while blocks x strips < strip_fill x SMs
+  int split_fill = 2;           // tiled panels split while tiles x systems x splits x 2 <= split_fill x SMs
   bool jacobian_tc = true;      // tensor-core Jacobian where it applies
   bool jacobian_pipe = true;    // its warp-role pipelined form where that applies
   bool jacobian_direct = true;  // direct-form Jacobian for single-wavenumber operators

@@ -1526,12 +1526,13 @@ void with_strip(int nq, F&& f) {
   else f(std::integral_constant<int, 1>());
 }
 
-// Depth splits of a panel launch of `tiles` items x `systems`: 1 when the launch fills the GPU
-// (two blocks per SM), else the largest of 2, 4, 8 that keeps it within that (the partials of at
-// most 2 x SMs tiles fit the plan's workspace).
-int panel_splits(int tiles, int systems, int sms) {
+// Depth splits of a panel launch of `tiles` items x `systems`: 1 when the launch fills `target`
+// block slots (2 x SMs by default: two blocks per SM; 0 never splits), else the largest of 2, 4,
+// 8 that keeps it within that. `target` is at most 2 x SMs, so the partials of a split launch
+// (tiles x systems x splits <= SMs) fit the plan's workspace of 2 x SMs tiles.
+int panel_splits(int tiles, int systems, int64_t target) {
   int splits = 1;
-  while (splits < 8 && (int64_t)tiles * systems * splits * 2 <= 2 * (int64_t)sms) splits *= 2;
+  while (splits < 8 && (int64_t)tiles * systems * splits * 2 <= target) splits *= 2;
   return splits;
 }
 
@@ -1548,7 +1549,7 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
       const auto [rb, re] = range(3 * L + p->panel_ptr[level] + k);
       const int pb = rb, pe = re;
       if (pe == pb) continue;
-      const int splits = panel_splits(pe - pb, systems, p->sms);
+      const int splits = panel_splits(pe - pb, systems, (int64_t)p->split_fill * p->sms);
       const int width = p->panel_width[3 * L + p->panel_ptr[level] + k];
       with_strip(width <= 16 ? 1 : width <= 32 ? 2 : 4, [&](auto nq) {
         launch_chained(tiled_update_kernel<nq()>, dim3(pe - pb, systems, splits), kTT, kUpdateSmem, s, p->titems, pb, k,
@@ -1578,9 +1579,9 @@ void factor_tiled(adt_plan* p, int systems, const double* values, double* factor
 // while the launch would leave most SMs idle. (Narrowing a launch that fills the GPU to pad
 // fewer columns, e.g. 96 as three strips of 32, was measured slower: 32.8 -> 36.8 ms at the
 // terrain section.)
-int tiled_strip(int blocks, int nrhs, int sms) {
+int tiled_strip(int blocks, int nrhs, int64_t target) {
   int nq = 4;
-  while (nq > 1 && (int64_t)blocks * ((nrhs + 16 * nq - 1) / (16 * nq)) < 2 * (int64_t)sms) nq /= 2;
+  while (nq > 1 && (int64_t)blocks * ((nrhs + 16 * nq - 1) / (16 * nq)) < target) nq /= 2;
   return nq;
 }
 
@@ -1594,11 +1595,11 @@ void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, doub
     const auto [rb, re] = range(2 * L + level);
     const int b = rb, e = re;
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    with_strip(tiled_strip((e - b) * systems, nrhs, p->sms), [&](auto nq) {
+    with_strip(tiled_strip((e - b) * systems, nrhs, (int64_t)p->strip_fill * p->sms), [&](auto nq) {
       launch_chained(tiled_forward_update_kernel<nq()>, dim3(e - b, systems, strips(nq())), kTT, kGemmSmem, s,
                      p->titems, b, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs);
     });
-    with_strip(tiled_strip((t1 - t0) * systems, nrhs, p->sms), [&](auto nq) {
+    with_strip(tiled_strip((t1 - t0) * systems, nrhs, (int64_t)p->strip_fill * p->sms), [&](auto nq) {
       launch_chained(tiled_substitute_kernel<nq()>, dim3(t1 - t0, systems, strips(nq())), kTT, kSubstituteSmem, s,
                      t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 1, level == L - 1);
     });
@@ -1608,11 +1609,11 @@ void solve_tiled(adt_plan* p, int systems, int nrhs, const double* factors, doub
     const auto [rb, re] = range(2 * L + level);
     const int b = rb, e = re;
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    with_strip(tiled_strip((e - b) * systems, nrhs, p->sms), [&](auto nq) {
+    with_strip(tiled_strip((e - b) * systems, nrhs, (int64_t)p->strip_fill * p->sms), [&](auto nq) {
       launch_chained(tiled_backward_update_kernel<nq()>, dim3(e - b, systems, strips(nq())), kTT, kGemmSmem, s,
                      p->titems, b, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs);
     });
-    with_strip(tiled_strip((t1 - t0) * systems, nrhs, p->sms), [&](auto nq) {
+    with_strip(tiled_strip((t1 - t0) * systems, nrhs, (int64_t)p->strip_fill * p->sms), [&](auto nq) {
       launch_chained(tiled_substitute_kernel<nq()>, dim3(t1 - t0, systems, strips(nq())), kTT, kSubstituteSmem, s,
                      t0, p->tasks, factors, p->factor_stride, rhs, rhs_stride, nrhs, 0, 1);
     });
@@ -1691,11 +1692,12 @@ void factor_levels_rhs(adt_plan* p, int systems, const double* values, double* f
   }
 }
 
-// Column strip of the substitution kernels: the full tile unless that leaves most SMs idle.
+// Column strip of the substitution kernels: the full tile unless the launch would have fewer
+// than `target` blocks (2 x SMs by default).
 template <int MAXM>
-int strip_for(int blocks, int nrhs, int sms) {
+int strip_for(int blocks, int nrhs, int64_t target) {
   int strip = MAXM;
-  while (strip > 16 && (int64_t)blocks * ((nrhs + strip - 1) / strip) < 2 * sms) strip /= 2;
+  while (strip > 16 && (int64_t)blocks * ((nrhs + strip - 1) / strip) < target) strip /= 2;
   return strip;
 }
 
@@ -1705,7 +1707,7 @@ void backward_levels(adt_plan* p, int systems, int nrhs, const double* factors, 
   const int64_t rhs_stride = (int64_t)p->N * nrhs;
   for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, p->sms);
+    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, (int64_t)p->strip_fill * p->sms);
     launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
                    backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
@@ -1718,14 +1720,14 @@ void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, dou
   for (int level = 0; level < p->levels; ++level) {  // forward: eager updates only
     const int i0 = p->update_begin[level], i1 = p->update_begin[level + 1];
     if (i1 <= i0) continue;
-    const int strip = strip_for<MAXM>((i1 - i0) * systems, nrhs, p->sms);
+    const int strip = strip_for<MAXM>((i1 - i0) * systems, nrhs, (int64_t)p->strip_fill * p->sms);
     launch_chained(forward_update_kernel<MAXM>, dim3(i1 - i0, systems, (nrhs + strip - 1) / strip), kSolverThreads, forward_update_smem<MAXM>(), s, 
         p->update_items, i0, p->tasks, p->pulls, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
   }
   for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
-    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, p->sms);
+    const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, (int64_t)p->strip_fill * p->sms);
     launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads, backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs,
                                                               rhs_stride, nrhs, strip);
     p->launches++;

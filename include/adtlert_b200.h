@@ -364,6 +364,47 @@ adt_status adt_mlp_to_bf16(const float* in, int64_t count, void* out, adt_stream
 /* Number of kernels this library has launched since the plan was created. */
 int64_t adt_kernel_launches(const adt_plan* plan);
 
+/* Launch shapes of one plan, chosen by measurement. No counterpart in the reference (cuDSS and
+ * its NVRTC kernel choose their own launch shapes); the settings change which blocks compute
+ * what, not the arithmetic of any entry, except that a different split depth reorders the
+ * float64 partial sums of a tiled panel (results stay within rounding of each other).
+ *   strip_fill       substitution launches (forward, backward, tiled strips) narrow their
+ *                    right-hand-side strips while blocks x strips < strip_fill x SMs: 1, 2, 4 or 8
+ *   split_fill       tiled panel launches split their reduction depth while
+ *                    tiles x systems x splits x 2 <= split_fill x SMs: 0 (never), 1 or 2
+ *   jacobian_kernel  ADT_JACOBIAN_* below; a kernel that does not apply to the plan's shapes
+ *                    falls through to the next one in that order
+ *   fields_ms, jacobian_ms  (adt_autotune only) the fastest time of the chosen setting */
+enum {
+  ADT_JACOBIAN_DIRECT = 0,      /* direct form, one wavenumber (3D) */
+  ADT_JACOBIAN_TC_PIPELINED = 1,/* tensor-core Gram with producer / MMA / epilogue warp roles */
+  ADT_JACOBIAN_TC = 2,          /* tensor-core Gram, one block chain per cell group */
+  ADT_JACOBIAN_FMA = 3          /* FP32 CUDA-core Gram */
+};
+typedef struct {
+  int32_t strip_fill;
+  int32_t split_fill;
+  int32_t jacobian_kernel;
+  float fields_ms;
+  float jacobian_ms;
+} adt_tuning;
+
+/* Autotuner of the plan's launch shapes: times adt_factorize_fields + adt_solve_fields of
+ * `models` models `sigma` in slot `slot` for every strip_fill (and, on tiled plans, split_fill),
+ * then adt_normal_jacobian of all rows for every Jacobian kernel that applies, each candidate
+ * once untimed and `repeats` (1..32) times timed with CUDA events on `stream`; keeps the fastest
+ * of each and writes the choice to `out` (may be NULL). On return `fields` ([models][W][dofs][E])
+ * and `jacobian` ([D][cells of the discretization], of the first model; NULL skips the Jacobian)
+ * hold the results of the chosen settings. Synchronizes the stream; allocates what the timed entry points
+ * allocate on first use. Beside the reference's fixed launch geometry (kernels.py:222-268). */
+adt_status adt_autotune(adt_plan* plan, int32_t slot, const float* sigma, int32_t models, float* fields,
+                        float* jacobian, int32_t repeats, adt_tuning* out, adt_stream stream);
+/* The plan's current launch shapes (timing fields zero). */
+adt_status adt_get_tuning(const adt_plan* plan, adt_tuning* out);
+/* Apply saved launch shapes (for example an earlier adt_autotune result on the same device);
+ * out-of-range values are rejected. */
+adt_status adt_set_tuning(adt_plan* plan, const adt_tuning* tuning);
+
 #ifdef __cplusplus
 }
 #endif
