@@ -62,6 +62,10 @@ SYMBOLS = (
     "adt_autotune",
     "adt_get_tuning",
     "adt_set_tuning",
+    "adt_jacobian_graph_create",
+    "adt_graph_launch",
+    "adt_graph_kernels",
+    "adt_graph_destroy",
 )
 
 JACOBIAN_KERNELS = ("direct", "tc_pipelined", "tc", "fma")
@@ -201,6 +205,10 @@ def load_library(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         "adt_autotune": (status, [_p, _i32, _p, _i32, _p, _p, _i32, ctypes.POINTER(Tuning), _p]),
         "adt_get_tuning": (status, [_p, ctypes.POINTER(Tuning)]),
         "adt_set_tuning": (status, [_p, ctypes.POINTER(Tuning)]),
+        "adt_jacobian_graph_create": (status, [_p, _i32, _p, _p, _p, _p, _p, _p, ctypes.POINTER(_p)]),
+        "adt_graph_launch": (status, [_p, _p]),
+        "adt_graph_kernels": (_i64, [_p]),
+        "adt_graph_destroy": (status, [_p]),
     }
     for name, (restype, argtypes) in signatures.items():
         fn = getattr(lib, name)

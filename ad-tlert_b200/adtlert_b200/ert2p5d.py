@@ -28,6 +28,7 @@ import torch
 
 from . import _native
 from . import tuning as _tuning
+from .graph import JacobianGraph
 from .fem import (
     analytic_primary,
     boundary_mass,
@@ -89,11 +90,19 @@ class _Slots:
     def __init__(self) -> None:
         self.slots: dict[int, dict] = {}
         self.factorizations = 0
+        self._next = 0
 
     def lookup(self, models: int) -> dict:
         if models not in self.slots:
-            self.slots[models] = {"slot": len(self.slots), "name": None}
+            self.slots[models] = {"slot": self._next, "name": None}
+            self._next += 1
         return self.slots[models]
+
+    def private(self) -> int:
+        """A slot outside the batch-size table (a captured graph's): never reused by name."""
+
+        self._next += 1
+        return self._next - 1
 
     def holds(self, models: int, name) -> bool:
         entry = self.slots.get(models)
@@ -543,6 +552,11 @@ class ERTForward2p5D:
 
     def tuning(self) -> dict:
         return _tuning.tuning(self)
+
+    def jacobian_graph(self) -> "JacobianGraph":
+        """A CUDA graph of the whole fresh-model ``jacobian()`` chain, replayed per model."""
+
+        return JacobianGraph(self)
 
     def set_tuning(self, settings: dict) -> None:
         _tuning.set_tuning(self, settings)

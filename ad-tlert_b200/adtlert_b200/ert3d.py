@@ -29,6 +29,7 @@ import torch
 
 from . import _native
 from . import tuning as _tuning
+from .graph import JacobianGraph
 from .ert2p5d import _checked_to_host, _Slots, _survey_arrays
 from .field_store import FieldStore, model_fingerprints
 from .geometry3d import (
@@ -329,6 +330,11 @@ class ERTForward3D:
 
     def tuning(self) -> dict:
         return _tuning.tuning(self)
+
+    def jacobian_graph(self) -> "JacobianGraph":
+        """A CUDA graph of the whole fresh-model ``jacobian()`` chain, replayed per model."""
+
+        return JacobianGraph(self)
 
     def set_tuning(self, settings: dict) -> None:
         _tuning.set_tuning(self, settings)

@@ -25,7 +25,7 @@ def autotune(operator, conductivity=None, repeats: int = 3, jacobian: bool = Tru
     sig = sigma.to(operator.device, torch.float32).reshape(1, -1).contiguous()
     entry = operator._solver.lookup(1)
     columns = operator.columns if hasattr(operator, "columns") else operator.E
-    fields = torch.empty((1, operator.W, operator.N, columns), dtype=torch.float32, device=operator.device)
+    fields = torch.empty((1, getattr(operator, "W", 1), operator.N, columns), dtype=torch.float32, device=operator.device)
     cells = getattr(operator, "Cd", operator.C)
     J = torch.empty((operator.D, cells), dtype=torch.float32, device=operator.device) if jacobian else None
     result = _native.Tuning()

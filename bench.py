@@ -62,6 +62,9 @@ def parse_args():
     parser.add_argument("--e2e-steps", type=int, default=None)
     parser.add_argument("--max-n", type=int, default=8, help="dipole-dipole n range (8: 1232 rows, 3: 612)")
     parser.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline leg (profiling runs)")
+    parser.add_argument("--tuning", choices=("auto", "default"), default="auto",
+                        help="auto: launch shapes chosen by the library's autotuner before warm-up; default: the "
+                             "library's built-in rules (fixed launch counts, for profiling captures)")
     parser.add_argument("--no-surrogate", action="store_true", help="timelapse workload: plain FEM pass only")
     parser.add_argument("--training-models", type=int, default=20_000, help="timelapse workload: surrogate training set")
     parser.add_argument("--windows", type=int, default=None,
@@ -349,7 +352,8 @@ def run_terrain(args, rank: int, world: int) -> dict | None:
     Jd = torch.empty((D, Cd), dtype=torch.float32, device=device)
     columns = forward._columns(None, None, discretization=True)
     slot = 15
-    tuned = forward.autotune(torch.as_tensor(synthetic.correlated_model(nodes, cells, 99_999 + rank)), repeats=2)
+    tuned = (forward.autotune(torch.as_tensor(synthetic.correlated_model(nodes, cells, 99_999 + rank)), repeats=2)
+             if args.tuning == "auto" else forward.tuning())
 
     def call(name, *a):
         _native.check(getattr(lib, name)(plan, *a), plan, name)
@@ -572,7 +576,8 @@ def run_box3d(args, rank: int, world: int) -> dict | None:
     recip = torch.empty_like(normal)
     J = torch.empty((D, C), dtype=torch.float32, device=device)
     slot = 15
-    tuned = forward.autotune(torch.as_tensor(synthetic.ellipsoid_model(nodes, cells, 99_999 + rank)), repeats=2)
+    tuned = (forward.autotune(torch.as_tensor(synthetic.ellipsoid_model(nodes, cells, 99_999 + rank)), repeats=2)
+             if args.tuning == "auto" else forward.tuning())
 
     def call(name, *a):
         _native.check(getattr(lib, name)(plan, *a), plan, name)
@@ -760,7 +765,8 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
     slot = 15
     # launch shapes chosen by the library's autotuner on a model outside the timed set
-    tuned = forward.autotune(torch.as_tensor(synthetic.layered_model(nodes, cells, 99_999 + rank)), repeats=3)
+    tuned = (forward.autotune(torch.as_tensor(synthetic.layered_model(nodes, cells, 99_999 + rank)), repeats=3)
+             if args.tuning == "auto" else forward.tuning())
 
     def call(name, *a):
         _native.check(getattr(lib, name)(plan, *a), plan, name)
@@ -804,6 +810,28 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     elapsed_max = max_over_ranks(elapsed, world)
     value = world * D * C * args.steps / elapsed_max
     clock = clocks.summary()
+
+    # the same steps replayed from a captured CUDA graph of the chain (the model copied into the
+    # graph's input buffer inside the timed events)
+    graph = forward.jacobian_graph()
+    for i in range(args.warmup):
+        graph.sigma.copy_(models[i])
+        graph.launch()
+    torch.cuda.synchronize(device)
+    barrier(world)
+    graph_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                    for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        graph_events[k][0].record(stream)
+        graph.sigma.copy_(models[args.warmup + k])
+        graph.launch()
+        graph_events[k][1].record(stream)
+    torch.cuda.synchronize(device)
+    graph_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in graph_events) / 1e3, world)
+    graph_line = {"value": world * D * C * args.steps / graph_s, "unit": "entries/s",
+                  "ms_per_step": 1e3 * graph_s / args.steps, "kernels_per_step": graph.kernels}
+    graph.close()
 
     # per-stage breakdown (same workload, L2 flushed, after the timed region)
     stage_ms, stage_launches = {}, {}
@@ -898,6 +926,7 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "e2e": e2e,
         "gpu_launches": int(launches),
         "autotune": tuned,
+        "graph": graph_line,
     }
     result["operations_ms"] = operation_timings(forward, nodes, cells, device)
     if world == 1 and not args.no_cpu_baseline:

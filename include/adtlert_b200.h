@@ -365,9 +365,10 @@ adt_status adt_mlp_to_bf16(const float* in, int64_t count, void* out, adt_stream
 int64_t adt_kernel_launches(const adt_plan* plan);
 
 /* Launch shapes of one plan, chosen by measurement. No counterpart in the reference (cuDSS and
- * its NVRTC kernel choose their own launch shapes); the settings change which blocks compute
- * what, not the arithmetic of any entry, except that a different split depth reorders the
- * float64 partial sums of a tiled panel (results stay within rounding of each other).
+ * its NVRTC kernel choose their own launch shapes). The settings change which blocks compute
+ * what; a narrower strip or a different split depth can also split a block's float64 reductions
+ * differently, so results of two settings agree to rounding, and each setting is bitwise
+ * repeatable.
  *   strip_fill       substitution launches (forward, backward, tiled strips) narrow their
  *                    right-hand-side strips while blocks x strips < strip_fill x SMs: 1, 2, 4 or 8
  *   split_fill       tiled panel launches split their reduction depth while
@@ -399,6 +400,25 @@ typedef struct {
  * allocate on first use. Beside the reference's fixed launch geometry (kernels.py:222-268). */
 adt_status adt_autotune(adt_plan* plan, int32_t slot, const float* sigma, int32_t models, float* fields,
                         float* jacobian, int32_t repeats, adt_tuning* out, adt_stream stream);
+/* CUDA graph of one fresh-model Jacobian: adt_factorize_fields, adt_solve_fields (one model),
+ * adt_measure and adt_normal_jacobian of all rows (skipped when `jacobian` is NULL), captured
+ * once from a private stream after one uncaptured run on `stream` (which allocates what the
+ * chain grows on first use and synchronizes), then replayed by adt_graph_launch on any stream.
+ * Every launch reads `sigma` ([model_cells]) and writes `fields`, `normal`, `reciprocal` and
+ * `jacobian` at the addresses given here; the caller refreshes `sigma` before a launch. A launch
+ * is refused (ADT_INVALID_ARG) once the plan has reallocated a workspace the graph holds (for
+ * example a later call on the same slot with more models): create the graph again. Destroy
+ * graphs before their plan, after their last launch has completed. Replaces the per-call launch
+ * sequence of jacobian() (adtlert/forward/ert2p5d.py:945-1010) for repeated fresh models. */
+typedef struct adt_graph adt_graph;
+adt_status adt_jacobian_graph_create(adt_plan* plan, int32_t slot, const float* sigma, float* fields,
+                                     double* normal, double* reciprocal, float* jacobian, adt_stream stream,
+                                     adt_graph** graph);
+adt_status adt_graph_launch(adt_graph* graph, adt_stream stream);
+/* Library kernels one launch of the graph runs. */
+int64_t adt_graph_kernels(const adt_graph* graph);
+adt_status adt_graph_destroy(adt_graph* graph);
+
 /* The plan's current launch shapes (timing fields zero). */
 adt_status adt_get_tuning(const adt_plan* plan, adt_tuning* out);
 /* Apply saved launch shapes (for example an earlier adt_autotune result on the same device);
