@@ -37,20 +37,34 @@ __device__ __forceinline__ void async_copy8(double* dst, const double* src) {
 __device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// f(r, c, i) for every entry i = r * cols + c of a rows x cols block that falls to this thread
+// (i = threadIdx.x, threadIdx.x + blockDim.x, ...): the row and column advance by the stride's
+// quotient and remainder, so a call divides twice instead of once per entry.
+template <typename F>
+__device__ __forceinline__ void for_each_entry(int rows, int cols, F&& f) {
+  if (rows <= 0 || cols <= 0) return;
+  const int stride = blockDim.x, dr = stride / cols, dc = stride - dr * cols;
+  int r = threadIdx.x / cols, c = threadIdx.x - r * cols, i = threadIdx.x;
+  while (r < rows) {
+    f(r, c, i);
+    i += stride;
+    r += dr;
+    c += dc;
+    if (c >= cols) {
+      c -= cols;
+      ++r;
+    }
+  }
+}
+
 // rows x cols dense block at src -> tile with leading dimension ld
 __device__ __forceinline__ void async_tile(double* dst, int ld, const double* src, int rows, int cols) {
-  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-    const int r = i / cols, c = i - r * cols;
-    async_copy8(dst + r * ld + c, src + i);
-  }
+  for_each_entry(rows, cols, [&](int r, int c, int i) { async_copy8(dst + r * ld + c, src + i); });
 }
 
 // rows x cols slice of a right-hand-side array (row stride `stride`) -> tile
 __device__ __forceinline__ void async_rows(double* dst, int ld, const double* src, int64_t stride, int rows, int cols) {
-  for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-    const int r = i / cols, c = i - r * cols;
-    async_copy8(dst + r * ld + c, src + r * stride + c);
-  }
+  for_each_entry(rows, cols, [&](int r, int c, int) { async_copy8(dst + r * ld + c, src + r * stride + c); });
 }
 
 // ---- register-tiled products ---------------------------------------------------------------
@@ -480,20 +494,12 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
   const int s0 = csr_ptr[offj], s1 = csr_ptr[offj + mj];
 
   // 1. [D_j | A[j,p] | A[q,j]^T] in shared memory
-  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
-    const int r = i / mj, c = i - r * mj;
-    async_copy8(aug + r * LDA + c, f + t[T_LOFF] + i);
-  }
-  if (p >= 0 && !p_csr)  // A[j,p] (mj x mp): the previous level's fill
-    for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
-      const int r = i / mp, c = i - r * mp;
-      async_copy8(aug + r * LDA + mj + c, f + t[T_LINKP] + i);
-    }
+  async_tile(aug, LDA, f + t[T_LOFF], mj, mj);
+  if (p >= 0 && !p_csr) async_tile(aug + mj, LDA, f + t[T_LINKP], mj, mp);  // A[j,p]: the previous level's fill
   async_commit();
-  for (int i = threadIdx.x; i < mj * (mp + mq); i += blockDim.x) {
-    const int r = i / (mp + mq), c = i - r * (mp + mq);
+  for_each_entry(mj, mp + mq, [&](int r, int c, int) {
     if (p_csr || c >= mp) aug[r * LDA + mj + c] = 0.0;
-  }
+  });
   __syncthreads();
   for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
     const int r = csr_row[s] - offj, c = csr_col[s];
@@ -502,25 +508,20 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
   }
   if (q >= 0 && !q_csr) {  // A[q,j] (mq x mj), stored transposed after A[j,p]
     const double* src = f + t[T_LINKQ];
-    for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
-      const int r = i / mj, k = i - r * mj;
-      aug[k * LDA + mj + mp + r] = src[i];
-    }
+    for_each_entry(mq, mj, [&](int r, int k, int i) { aug[k * LDA + mj + mp + r] = src[i]; });
   }
   async_wait_all();
   __syncthreads();
 
   // 2. copies of the couplings (read by the Schur updates and the fill)
-  if (p >= 0)
-    for (int i = threadIdx.x; i < mj * mp; i += blockDim.x) {
-      const int r = i / mp, c = i - r * mp;
-      f[t[T_RUOFF] + i] = aug[r * LDA + mj + c];
-    }
-  if (q >= 0)
-    for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
-      const int r = i / mj, k = i - r * mj;
-      f[t[T_RVOFF] + i] = aug[k * LDA + mj + mp + r];
-    }
+  if (p >= 0) {
+    double* ru = f + t[T_RUOFF];
+    for_each_entry(mj, mp, [&](int r, int c, int i) { ru[i] = aug[r * LDA + mj + c]; });
+  }
+  if (q >= 0) {
+    double* rv = f + t[T_RVOFF];
+    for_each_entry(mq, mj, [&](int r, int k, int i) { rv[i] = aug[k * LDA + mj + mp + r]; });
+  }
 
   // 3. block Gauss-Jordan in registers
   const int tc = threadIdx.x & 31, tr = threadIdx.x >> 5;
@@ -651,9 +652,9 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
   __syncthreads();
   // 5. fill A[q,p] = -A[q,j] Z_p: the coupling copy (written by this block above) replaces G_j
   //    in shared memory
-  for (int i = threadIdx.x; i < mq * mj; i += blockDim.x) {
-    const int r = i / mj, k = i - r * mj;
-    aug[r * LDA + k] = f[t[T_RVOFF] + i];
+  {
+    const double* rv = f + t[T_RVOFF];
+    for_each_entry(mq, mj, [&](int r, int k, int i) { aug[r * LDA + k] = rv[i]; });
   }
   double* fill = f + t[T_FILL];
   __syncthreads();
@@ -717,10 +718,7 @@ update_level_kernel(const int* __restrict__ items, int item_begin, const int64_t
   }
   __syncthreads();
   subtract_tile(acc, mu, dm, LD, mj, mj, tile(0));
-  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
-    const int r = i / mj, c = i - r * mj;
-    d[i] = dm[r * LD + c];
-  }
+  for_each_entry(mj, mj, [&](int r, int c, int i) { d[i] = dm[r * LD + c]; });
 }
 
 // The Schur updates of one level with the forward substitution of the same level fused in: block
@@ -784,14 +782,8 @@ update_rhs_level_kernel(const int* __restrict__ items, int item_begin, const int
   __syncthreads();
   subtract_tile(accd, md, dm, LD, mj, mj, tile(0));
   subtract_tile(accb, mb, bt, LD, mj, nrhs, tile(0));
-  for (int i = threadIdx.x; i < mj * mj; i += blockDim.x) {
-    const int r = i / mj, c = i - r * mj;
-    d[i] = dm[r * LD + c];
-  }
-  for (int i = threadIdx.x; i < mj * nrhs; i += blockDim.x) {
-    const int r = i / nrhs, c = i - r * nrhs;
-    x[(int64_t)(offj + r) * nrhs + c] = bt[r * LD + c];
-  }
+  for_each_entry(mj, mj, [&](int r, int c, int i) { d[i] = dm[r * LD + c]; });
+  for_each_entry(mj, nrhs, [&](int r, int c, int) { x[(int64_t)(offj + r) * nrhs + c] = bt[r * LD + c]; });
 }
 
 // Eager forward updates after a level: b_j -= Z_j^T b_e / V_j b_e for the pulls [u0, u1) of the
@@ -846,10 +838,7 @@ forward_update_kernel(const int* __restrict__ items, int item_begin, const int64
   }
   __syncthreads();
   subtract_tile(acc, mu, bt, LD, mj, nc, tile(0));
-  for (int i = threadIdx.x; i < mj * nc; i += blockDim.x) {
-    const int r = i / nc, c = i - r * nc;
-    x[(int64_t)(offj + r) * nrhs + c0 + c] = bt[r * LD + c];
-  }
+  for_each_entry(mj, nc, [&](int r, int c, int) { x[(int64_t)(offj + r) * nrhs + c0 + c] = bt[r * LD + c]; });
 }
 
 // Backward level: x_j = G_j b_j - Z_p x_p - V_q^T x_q (the root: x = G b), every operand
@@ -889,8 +878,8 @@ backward_level_kernel(const int64_t* __restrict__ tasks, int task_begin,
   async_commit();
   async_wait_all();
   __syncthreads();
-  for (int i = threadIdx.x; i < mp * nc; i += blockDim.x) xp[(i / nc) * LD + i % nc] *= -1.0;
-  for (int i = threadIdx.x; i < mq * nc; i += blockDim.x) xq[(i / nc) * LD + i % nc] *= -1.0;
+  for_each_entry(mp, nc, [&](int r, int c, int) { xp[r * LD + c] *= -1.0; });
+  for_each_entry(mq, nc, [&](int r, int c, int) { xq[r * LD + c] *= -1.0; });
   __syncthreads();
   const Micro mu(mj, nc);
   double acc[4][4];
