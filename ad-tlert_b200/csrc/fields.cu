@@ -233,38 +233,93 @@ __global__ void adjoint_rhs_kernel(AdjointRhsArgs a) {
 
 // Partial Gram sums for normal_jvp: partial[b][e][f] = sum over this block's slice of (w, n) of
 // weight_w * phi[w][n][e] * y[w][n][f]; a second pass sums the partials in block order.
+// partial[b] = sum over the rows r of chunk b (rows of the W x N row space, in order) of
+// weight_{w(r)} phi[r]^T y[r] (E x E, float64). Rows stream through shared memory `sub` at a
+// time (weighted phi and y, row stride padded to a multiple of 4 with zeros); each thread owns
+// 4 x 4 output tiles and sums its rows in order, so every partial is bitwise repeatable.
 __global__ void gram_partial_kernel(const float* phi, const double* y, const double* weights,
-                                    int W, int N, int E, int chunk, double* partial) {
+                                    int W, int N, int E, int chunk, int sub, double* partial) {
   chain_wait();
-  extern __shared__ double rows[];
+  extern __shared__ double rows_sm[];
+  const int Et = (E + 3) / 4, Ep = 4 * Et, tiles = Et * Et;
+  double* ps = rows_sm;            // [sub][Ep]
+  double* ys = rows_sm + sub * Ep; // [sub][Ep]
   const int64_t total = (int64_t)W * N;
   const int64_t begin = (int64_t)blockIdx.x * chunk;
   const int64_t end = begin + chunk < total ? begin + chunk : total;
   double* out = partial + (int64_t)blockIdx.x * E * E;
-  for (int ef = threadIdx.x; ef < E * E; ef += blockDim.x) {
-    const int e = ef / E, f = ef % E;
-    double acc = 0.0;
-    for (int64_t wn = begin; wn < end; ++wn) {
-      const int w = (int)(wn / N);
-      acc += weights[w] * (double)phi[wn * E + e] * y[wn * E + f];
+  for (int t0 = 0; t0 < tiles; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    const bool active = t < tiles;
+    const int ti = active ? t / Et : 0, tj = active ? t - ti * Et : 0;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int64_t r0 = begin; r0 < end; r0 += sub) {
+      const int rows = (int)(end - r0 < sub ? end - r0 : sub);
+      const int w0 = (int)(r0 / N);
+      const int64_t boundary = (int64_t)(w0 + 1) * N;  // rows at or past it belong to w0 + 1 (sub <= N)
+      __syncthreads();  // the previous rows have been read
+      for (int i = threadIdx.x; i < sub * Ep; i += blockDim.x) {
+        const int r = i / Ep, c = i - r * Ep;
+        const int64_t row = r0 + r;
+        double pv = 0.0, yv = 0.0;
+        if (r < rows && c < E) {
+          const int w = row >= boundary ? w0 + 1 : w0;
+          pv = weights[w] * (double)phi[row * E + c];
+          yv = y[row * E + c];
+        }
+        ps[i] = pv;
+        ys[i] = yv;
+      }
+      __syncthreads();
+      if (active)
+        for (int r = 0; r < rows; ++r) {
+          const double* pr = ps + r * Ep + 4 * ti;
+          const double* yr = ys + r * Ep + 4 * tj;
+          double a[4], b[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            a[k] = pr[k];
+            b[k] = yr[k];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
     }
-    out[ef] = acc;
+    if (active)
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const int i = 4 * ti + u, j = 4 * tj + v;
+          if (i < E && j < E) out[i * E + j] = acc[u][v];
+        }
   }
 }
 
-__global__ void gram_gather_kernel(const double* partial, int blocks, int E, int D,
-                                   const int* abmn, double* out) {
+// gram[ef] = sum over the blocks' partials in block order (fixed order: repeatable).
+__global__ void gram_reduce_kernel(const double* partial, int blocks, int E, double* gram) {
+  chain_wait();
+  const int ef = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ef >= E * E) return;
+  double acc = 0.0;
+  for (int b = 0; b < blocks; ++b) acc += partial[(int64_t)b * E * E + ef];
+  gram[ef] = acc;
+}
+
+// out[d] = -(G[M][A] - G[M][B] - G[N][A] + G[N][B]), slot E (the remote electrode) contributing 0.
+__global__ void gram_gather_kernel(const double* gram, int E, int D, const int* abmn, double* out) {
   chain_wait();
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= D) return;
   const int A = abmn[4 * d], B = abmn[4 * d + 1], M = abmn[4 * d + 2], N = abmn[4 * d + 3];
-  auto gram = [&](int i, int j) -> double {
-    if (i >= E || j >= E) return 0.0;
-    double acc = 0.0;
-    for (int b = 0; b < blocks; ++b) acc += partial[((int64_t)b * E + i) * E + j];
-    return -acc;
-  };
-  out[d] = gram(M, A) - gram(M, B) - gram(N, A) + gram(N, B);
+  auto g = [&](int i, int j) -> double { return (i >= E || j >= E) ? 0.0 : gram[(int64_t)i * E + j]; };
+  out[d] = -(g(M, A) - g(M, B) - g(N, A) + g(N, B));
 }
 
 // integrated[e][orig] = sum_w weight_w fields[w][pos(orig)][e]

@@ -128,11 +128,14 @@ __global__ void transfers_kernel(MeasureArgs a, int models, const double* pot);
 __global__ void pair_kernel(PairArgs a);
 __global__ void adjoint_rhs_kernel(AdjointRhsArgs a);
 __global__ void gram_partial_kernel(const float* phi, const double* y, const double* weights,
-                                    int W, int N, int E, int chunk, double* partial);
-__global__ void gram_gather_kernel(const double* partial, int blocks, int E, int D,
-                                   const int* abmn, double* out);
+                                    int W, int N, int E, int chunk, int sub, double* partial);
+__global__ void gram_reduce_kernel(const double* partial, int blocks, int E, double* gram);
+__global__ void gram_gather_kernel(const double* gram, int E, int D, const int* abmn, double* out);
 __global__ void integrated_kernel(const float* fields, const double* weights, const int* iperm,
                                   int W, int N, int E, float* integrated);
+constexpr int kMixTileRows = 64;  // field rows per block of mix_tiled_kernel
+__global__ void mix_tiled_kernel(const double* pairs, const float* phi, int64_t rows, int E, double* current);
+size_t mix_tiled_smem(int E);
 __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, int E,
                            double* current);
 cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s);
@@ -144,7 +147,7 @@ cudaError_t launch_jacobian_tc(const JacobianArgs& a, int* error, int sms, cudaS
 // for these sizes, 0 when it does not apply.
 int jacobian_tcpipe_batch(int E, int W, int R, int K, int rows);
 cudaError_t launch_jacobian_tcpipe(const JacobianArgs& a, int batch, int* error, int sms, cudaStream_t s);
-__global__ void cell_gradient_kernel(CellGradientArgs a);
+cudaError_t launch_cell_gradient(const CellGradientArgs& a, int blocks, cudaStream_t s);
 __global__ void boundary_jacobian_kernel(BoundaryJacobianArgs a);
 __global__ void add_kernel(double* y, const double* x, int64_t count);
 __global__ void scale_rows_columns_kernel(float* values, int rows, int columns, const double* row_scale,

@@ -284,7 +284,7 @@ void launch_cell_gradient(adt_plan* p, const void* x, bool x_double, int x_cols,
   a.x_cols = x_cols;
   a.q_per_model = q_per_model;
   const int64_t warps = (int64_t)models * q_per_model * p->C;
-  launch_chained(cell_gradient_kernel, (int)((warps + 7) / 8), 256, 0, s, a);
+  launch_cell_gradient(a, (int)((warps + 7) / 8), s);
   p->launches++;
 }
 
@@ -994,7 +994,14 @@ adt_status adt_normal_vjp(adt_plan* p, const float* fields, const double* cotang
   double* current = (double*)(base + cv.offsets[ix]);
   double* g = (double*)(base + cv.offsets[ig]);
   launch_pairs(p, cotangent, nullptr, nullptr, 1, true, false, 0, false, pairs, s);
-  launch_chained(mix_kernel, grid_for((int64_t)p->W * p->N * p->E), 256, 0, s, pairs, fields, p->W, p->N, p->E, current);
+  if (mix_tiled_smem(p->E) <= 48 * 1024) {
+    const int64_t rows = (int64_t)p->W * p->N;
+    launch_chained(mix_tiled_kernel, (int)((rows + kMixTileRows - 1) / kMixTileRows), 256, mix_tiled_smem(p->E), s,
+                   pairs, fields, rows, p->E, current);
+  } else {
+    launch_chained(mix_kernel, grid_for((int64_t)p->W * p->N * p->E), 256, 0, s, pairs, fields, p->W, p->N, p->E,
+                   current);
+  }
   p->launches++;
   launch_cell_gradient(p, current, true, p->E, nullptr, fields, false, p->weights, 1, 1, robin != 0, g, s);
   launch_to_model_cells(p, g, 1, gradient, s);
@@ -1008,20 +1015,28 @@ adt_status adt_normal_jvp(adt_plan* p, const float* fields, const float* directi
   const int64_t rows = (int64_t)p->W * p->N;
   const int chunk = 256;
   const int blocks = (int)((rows + chunk - 1) / chunk);
+  // rows staged per pass: two float64 row blocks of the padded width within 48 KB, at most N
+  const int Ep = (p->E + 3) / 4 * 4;
+  const int sub = std::max(1, std::min({64, p->N, 48 * 1024 / (16 * Ep)}));
   Carve cv;
   const size_t iv = cv.add((size_t)p->W * p->nnz * sizeof(double));
   const size_t iy = cv.add((size_t)p->W * p->N * p->E * sizeof(double));
   const size_t ip = cv.add((size_t)blocks * p->E * p->E * sizeof(double));
+  const size_t ig = cv.add((size_t)p->E * p->E * sizeof(double));
   char* base = (char*)scratch(p, cv.total);
   if (!base) return fail(p, ADT_OOM, "scratch allocation failed");
   double* values = (double*)(base + cv.offsets[iv]);
   double* y = (double*)(base + cv.offsets[iy]);
   double* partial = (double*)(base + cv.offsets[ip]);
+  double* gram = (double*)(base + cv.offsets[ig]);
   launch_assemble(p, direction, p->W, values, robin != 0, false, s);
   launch_spmm<float>(p, values, false, fields, true, nullptr, nullptr, 1.0, p->W, y, s);
-  launch_chained(gram_partial_kernel, blocks, 256, 0, s, fields, y, p->weights, p->W, p->N, p->E, chunk, partial);
+  launch_chained(gram_partial_kernel, blocks, 256, (size_t)2 * sub * Ep * sizeof(double), s, fields, y, p->weights,
+                 p->W, p->N, p->E, chunk, sub, partial);
   p->launches++;
-  launch_chained(gram_gather_kernel, (p->D + 255) / 256, 256, 0, s, partial, blocks, p->E, p->D, p->abmn, out);
+  launch_chained(gram_reduce_kernel, (p->E * p->E + 255) / 256, 256, 0, s, partial, blocks, p->E, gram);
+  p->launches++;
+  launch_chained(gram_gather_kernel, (p->D + 255) / 256, 256, 0, s, gram, p->E, p->D, p->abmn, out);
   p->launches++;
   return check_launch(p, "normal jvp");
 }

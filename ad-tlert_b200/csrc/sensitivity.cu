@@ -213,9 +213,12 @@ cudaError_t launch_jacobian(const JacobianArgs& a, size_t smem, cudaStream_t s) 
 // One warp per (cotangent q, cell): g[q][c] = -sum_w sum_e x_we^T (K + k_w^2 M) y_we over the
 // cell's dofs (x scaled by x_scale[w], y by y_scale[w]), plus the mixed-boundary term
 // -sum_w sum_e x^T (alpha_w[b] Mb) y over the cell's boundary elements when `robin`.
-// Lanes own electrodes; the lane sums are combined by a fixed shuffle tree.
+// Lanes own electrodes; the lane sums are combined by a fixed shuffle tree. KT > 0 fixes the
+// element's dof count at compile time (P1 triangles and tetrahedra, Q1 quads: the dof values
+// stay in registers); KT = 0 takes a.K.
 // Replaces _cell_gradient (adtlert/forward/ert2p5d.py:765-825).
-__global__ void cell_gradient_kernel(CellGradientArgs a) {
+template <int KT>
+__global__ void __launch_bounds__(256, 3) cell_gradient_kernel_t(CellGradientArgs a) {
   chain_wait();
   const int warps = blockDim.x / 32;
   const int64_t warp_id = (int64_t)blockIdx.x * warps + threadIdx.x / 32;
@@ -224,7 +227,8 @@ __global__ void cell_gradient_kernel(CellGradientArgs a) {
   if (warp_id >= count * a.C) return;
   const int q = (int)(warp_id / a.C), c = (int)(warp_id % a.C);
   const int s = q / a.q_per_model, ql = q % a.q_per_model;
-  const int K = a.K, K2 = K * K;
+  const int K = KT > 0 ? KT : a.K, K2 = K * K;
+  constexpr int KA = KT > 0 ? KT : 16;
   const int* dofs = a.cell_dofs + (int64_t)c * K;
   double acc = 0.0;
   for (int w = 0; w < a.W; ++w) {
@@ -233,7 +237,8 @@ __global__ void cell_gradient_kernel(CellGradientArgs a) {
     const double ys = a.y_scale ? a.y_scale[w] : 1.0;
     const double k2 = a.k2[w];
     for (int e = lane; e < a.E; e += 32) {
-      double xv[16], yv[16];
+      double xv[KA], yv[KA];
+#pragma unroll
       for (int k = 0; k < K; ++k) {
         const int64_t xi = (t * a.N + dofs[k]) * a.x_cols + (int64_t)ql * a.E + e;
         const int64_t yi = (t * a.N + dofs[k]) * a.E + e;
@@ -243,8 +248,10 @@ __global__ void cell_gradient_kernel(CellGradientArgs a) {
       const double* st = a.stiffness + (int64_t)c * K2;
       const double* ms = a.mass + (int64_t)c * K2;
       double sum = 0.0;
+#pragma unroll
       for (int i = 0; i < K; ++i) {
         double row = 0.0;
+#pragma unroll
         for (int j = 0; j < K; ++j) row += (st[i * K + j] + k2 * ms[i * K + j]) * yv[j];
         sum += xv[i] * row;
       }
@@ -273,6 +280,14 @@ __global__ void cell_gradient_kernel(CellGradientArgs a) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
   if (lane == 0) a.out[(int64_t)q * a.C + c] = -acc;
+}
+
+cudaError_t launch_cell_gradient(const CellGradientArgs& a, int blocks, cudaStream_t s) {
+  switch (a.K) {
+    case 3: return launch_chained(cell_gradient_kernel_t<3>, blocks, 256, 0, s, a);
+    case 4: return launch_chained(cell_gradient_kernel_t<4>, blocks, 256, 0, s, a);
+    default: return launch_chained(cell_gradient_kernel_t<0>, blocks, 256, 0, s, a);
+  }
 }
 
 // Mixed-boundary part of the Jacobian, added to rows already holding the volume part: one thread
@@ -363,6 +378,62 @@ __global__ void mix_kernel(const double* pairs, const float* phi, int W, int N, 
     current[idx] = acc;
   }
 }
+
+// mix_kernel for E <= 64 as register-tiled products: a block takes 64 rows of the (W N) x E field
+// matrix, stages them (as float64) and the E x E pair matrix in shared memory, and every thread
+// forms a 4 x 4 tile of current = rows x pairs, summing f = 0 .. E-1 in order with fused
+// multiply-adds -- the same operations in the same order as mix_kernel.
+__global__ void __launch_bounds__(256) mix_tiled_kernel(const double* pairs, const float* phi, int64_t rows, int E,
+                                                        double* current) {
+  chain_wait();
+  extern __shared__ double mix_sm[];
+  const int Et = (E + 3) / 4, Ep = 4 * Et;
+  double* pm = mix_sm;                 // [E][Ep] pairs, zero-padded columns
+  double* xs = mix_sm + E * Ep;        // [kMixTileRows][E] rows
+  const int64_t r0 = (int64_t)blockIdx.x * kMixTileRows;
+  const int nr = (int)(rows - r0 < kMixTileRows ? rows - r0 : kMixTileRows);
+  for (int i = threadIdx.x; i < E * Ep; i += blockDim.x) {
+    const int f = i / Ep, e = i - f * Ep;
+    pm[i] = e < E ? pairs[f * E + e] : 0.0;
+  }
+  for (int i = threadIdx.x; i < kMixTileRows * E; i += blockDim.x) {
+    const int r = i / E;
+    xs[i] = r < nr ? (double)phi[r0 * E + i] : 0.0;
+  }
+  __syncthreads();
+  const int tiles = (kMixTileRows / 4) * Et;
+  for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
+    const int tr = t / Et, te = t - tr * Et;
+    double acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+    for (int f = 0; f < E; ++f) {
+      double x[4], y[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = xs[(4 * tr + u) * E + f];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) y[v] = pm[f * Ep + 4 * te + v];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(y[v], x[u], acc[u][v]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = 4 * tr + u;
+      if (r >= nr) continue;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int e = 4 * te + v;
+        if (e < E) current[(r0 + r) * E + e] = acc[u][v];
+      }
+    }
+  }
+}
+
+size_t mix_tiled_smem(int E) { return sizeof(double) * ((size_t)E * ((E + 3) / 4 * 4) + (size_t)kMixTileRows * E); }
 
 // out[r][col] = sum over the column's cells (fixed order) of in[r][cell].
 __global__ void aggregate_kernel(const double* in, int rows, int C, int columns, const int* ptr,
