@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
   if (tid == 0) {
     for (int i = 0; i < 2; ++i) {
       mbar_init(stage_free + i, 1);
-      mbar_init(stage_full + i, kProducerThreads);
+      mbar_init(stage_full + i, 4 * E);  // the active producers (4 E <= 192)
     }
     for (int i = 0; i < kAccumulators; ++i) {
       mbar_init(acc_full + i, 1);
@@ -172,12 +172,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
 
   if (warp < kProducerThreads / 32) {
     // ---------------------------------------------------------------- producers
-    // thread (cell ci, half hf, electrode e): wavenumbers 0 .. 7 (hf = 0: chunks 0 .. 2R - 1) or
-    // 8 .. WT - 1 (hf = 1: chunks 2R .. KC - 1); whole 16-byte chunks stored
+    // thread tid < 4 E: (cell ci, half hf, electrode e), packed so that whole warps work and the
+    // rest (warps past 4 E threads) leave the role at once; wavenumbers 0 .. 7 (hf = 0: chunks
+    // 0 .. 2R - 1) or 8 .. WT - 1 (hf = 1: chunks 2R .. KC - 1); whole 16-byte chunks stored
     constexpr int WH = 8, WB = WT - WH, CH0 = WH * R / 4;
     static_assert(WB >= WH && WB <= 16 && (WH * R) % 4 == 0, "two halves of at most 16 wavenumbers");
-    const int ci = tid >> 7, hf = (tid >> 6) & 1, e = tid & 63;
-    const bool on = e < E;
+    const int ci = tid / (2 * E), hf = (tid / E) & 1, e = tid % E;
+    const bool on = tid < 4 * E;
     const int w0 = hf * WH, wn = hf ? WB : WH;
     auto cell_of = [&](int j) {
       return a.c_begin + 2 * ((blockIdx.x + (j / batch) * gridDim.x) * batch + j % batch) + ci;
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) jacobian_tcpipe_kernel(Jacobi
       load_pair(0, d0);
       load_dofs(1, dnext);
     }
-    for (int j = 0; j < pairs; ++j) {
+    for (int j = 0; on && j < pairs; ++j) {  // idle producer threads leave at once
       const int s = j & 1;
       // stage s is free once pair j - 2's MMAs completed (each thread waits: producers need no
       // barrier among themselves)
