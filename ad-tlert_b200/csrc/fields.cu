@@ -63,7 +63,13 @@ __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
 // by system (fields of each system) or by wavenumber (the primary field shared by all models).
 __global__ void spmm_kernel(SpmmArgs a) {
   chain_wait();
-  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x
+  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x. A block's
+  // entries cover a few consecutive dofs; their CSR columns and values are staged in shared
+  // memory first, so each thread's product issues only its independent x loads (the slot order,
+  // and so every sum, is that of the CSR rows).
+  constexpr int kSlots = 1024;
+  __shared__ int scol[kSlots];
+  __shared__ double sval[kSlots];
   const int NE = a.N * a.E;
   for (int t = blockIdx.y; t < a.systems; t += gridDim.y) {
     const int w = t % a.W, s = t / a.W;
@@ -72,17 +78,34 @@ __global__ void spmm_kernel(SpmmArgs a) {
     const double* rho = a.rho ? a.rho + (int64_t)s * a.E : nullptr;
     const double* base = a.base ? a.base + (int64_t)w * NE : nullptr;
     double* out = a.out + (int64_t)t * NE;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NE; i += gridDim.x * blockDim.x) {
+    for (int first = blockIdx.x * blockDim.x; first < NE; first += gridDim.x * blockDim.x) {
+      const int last = min(first + (int)blockDim.x, NE) - 1;
+      const int s0 = a.csr_ptr[first / a.E], s1 = a.csr_ptr[last / a.E + 1];
+      const bool staged = s1 - s0 <= kSlots;  // block-uniform
+      __syncthreads();  // the previous range's slots have been read
+      if (staged)
+        for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x) {
+          scol[k] = a.csr_col[s0 + k];
+          sval[k] = v[s0 + k];
+        }
+      __syncthreads();
+      const int i = first + threadIdx.x;
+      if (i >= NE) continue;
       const int n = i / a.E, e = i - n * a.E;
+      const int b = a.csr_ptr[n], end = a.csr_ptr[n + 1];
       double acc = 0.0;
       if (a.x_double) {
-        const double* x = (const double*)a.x + xo;
-        for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
-          acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E + e];
+        const double* x = (const double*)a.x + xo + e;
+        if (staged)
+          for (int slot = b - s0; slot < end - s0; ++slot) acc += sval[slot] * x[(int64_t)scol[slot] * a.E];
+        else
+          for (int slot = b; slot < end; ++slot) acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E];
       } else {
-        const float* x = (const float*)a.x + xo;
-        for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
-          acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E + e];
+        const float* x = (const float*)a.x + xo + e;
+        if (staged)
+          for (int slot = b - s0; slot < end - s0; ++slot) acc += sval[slot] * (double)x[(int64_t)scol[slot] * a.E];
+        else
+          for (int slot = b; slot < end; ++slot) acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E];
       }
       double coef = a.scale;
       if (rho) coef *= rho[e];

@@ -461,11 +461,11 @@ __device__ void store_tile(double (&acc)[4][4], const Micro& u, double* C, int64
 // P <- P^-1, R <- P^-1 R, L <- -L P^-1, S <- S - L P^-1 R. Every thread holds a fixed set of
 // augmented entries in registers (rows tr + 8 r, columns tc + 32 c; a panel's rows are pass
 // r = k0 / 8 of the 8 row groups). A step publishes the panel rows (with the identity in the
-// panel columns) and columns to one of two buffers, then one barrier; every warp inverts P
-// itself, forms C = L P^-1 for its own rows (C = -P^-1 on the panel rows, which start from
-// zero), and updates its entries by a <- a - C R. Stored: G_j, Z_p, V_q = Z_q^T, copies of the
-// couplings (for the Schur updates) and the fill A[q,p] = -A[q,j] Z_p. A non-positive pivot
-// becomes NaN, which reaches every result of the system.
+// panel columns) and columns to one of two buffers, then a barrier; warp 0 inverts P, then a
+// second barrier; every warp forms C = L P^-1 for its own rows (C = -P^-1 on the panel rows,
+// which start from zero), and updates its entries by a <- a - C R. Stored: G_j, Z_p,
+// V_q = Z_q^T, copies of the couplings (for the Schur updates) and the fill A[q,p] = -A[q,j] Z_p.
+// A non-positive pivot becomes NaN, which reaches every result of the system.
 template <int MAXM, int WCOL = 3 * MAXM>
 __global__ void __launch_bounds__(kSolverThreads, MAXM <= 48 ? 2 : 1)
 invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int* __restrict__ csr_ptr,
@@ -481,7 +481,7 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
   double* aug = sm;                             // [MAXM][LDA]
   double* rbuf = aug + MAXM * LDA;              // panel rows      [2][PB][W3]
   double* lbuf = rbuf + 2 * PB * W3;            // panel columns   [2][MAXM][PB + 1]
-  double* pinv_all = lbuf + 2 * MAXM * (PB + 1);  // per warp P^-1 [8][PB][PB]
+  double* pinv_all = lbuf + 2 * MAXM * (PB + 1);  // P^-1 [PB][PB] (room for 8)
   double* c_all = pinv_all + 8 * PB * PB;       // per warp C      [8][RP][PB]
   const int64_t* t = tasks + (int64_t)(task_begin + blockIdx.x) * T_FIELDS;
   const double* val = values + (int64_t)blockIdx.y * nnz;
@@ -525,7 +525,7 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
 
   // 3. block Gauss-Jordan in registers
   const int tc = threadIdx.x & 31, tr = threadIdx.x >> 5;
-  double* pinv = pinv_all + tr * PB * PB;
+  double* pinv = pinv_all;  // P^-1 of the current panel (written by warp 0)
   double* cw = c_all + tr * RP * PB;
   double a[RP][CP];
 #pragma unroll
@@ -567,9 +567,9 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
             cols[i * (PB + 1) + s] = (s < (unsigned)nb && i < mj) ? a[r][c] : 0.0;
           }
     __syncthreads();
-    // (b) P^-1 by every warp: lane 4 v + h holds row v, columns 2 h and 2 h + 1 (the padding
-    //     beyond nb is the identity)
-    {
+    // (b) P^-1 by warp 0 (the other warps wait at the barrier below instead of repeating it):
+    //     lane 4 v + h holds row v, columns 2 h and 2 h + 1 (the padding beyond nb is the identity)
+    if (tr == 0) {
       const int v = tc >> 2, h = tc & 3;
       double x0 = (v < nb && 2 * h < nb) ? cols[(k0 + v) * (PB + 1) + 2 * h] : (v == 2 * h ? 1.0 : 0.0);
       double x1 = (v < nb && 2 * h + 1 < nb) ? cols[(k0 + v) * (PB + 1) + 2 * h + 1] : (v == 2 * h + 1 ? 1.0 : 0.0);
@@ -592,7 +592,7 @@ invert_level_kernel(const int64_t* __restrict__ tasks, int task_begin, const int
       }
       *reinterpret_cast<double2*>(pinv + v * PB + 2 * h) = make_double2(x0, x1);
     }
-    __syncwarp();
+    __syncthreads();
     // (c) C for this warp's rows: L P^-1, or -P^-1 on the panel row
     for (int e = tc; e < RP * PB; e += 32) {
       const int r = e / PB, u = e - r * PB, i = tr + 8 * r;
@@ -1717,8 +1717,8 @@ void solve_levels(adt_plan* p, int systems, int nrhs, const double* factors, dou
   for (int level = p->levels - 1; level >= 0; --level) {
     const int t0 = p->level_begin[level], t1 = p->level_begin[level + 1];
     const int strip = strip_for<MAXM>((t1 - t0) * systems, nrhs, (int64_t)p->strip_fill * p->sms);
-    launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads, backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs,
-                                                              rhs_stride, nrhs, strip);
+    launch_chained(backward_level_kernel<MAXM>, dim3(t1 - t0, systems, (nrhs + strip - 1) / strip), kSolverThreads,
+                   backward_smem<MAXM>(), s, p->tasks, t0, factors, p->factor_stride, rhs, rhs_stride, nrhs, strip);
     p->launches++;
   }
 }
