@@ -277,6 +277,26 @@ def _to_host(tensor: Tensor) -> Tensor:
     return out
 
 
+def _widened_to_host(tensor: Tensor, dtype: torch.dtype = torch.float64, chunk_bytes: int = 256 << 20) -> Tensor:
+    """Device matrix -> page-locked CPU matrix of a wider dtype, widened on the device a block of
+    rows at a time, so the device holds at most ``chunk_bytes`` of the wide copy beside the
+    original (a whole-matrix widening would need three times the float32 matrix)."""
+
+    rows, columns = int(tensor.shape[0]), int(tensor.shape[1])
+    out = torch.empty(tensor.shape, dtype=dtype, pin_memory=True)
+    step = max(1, chunk_bytes // max(1, columns * (torch.finfo(dtype).bits // 8)))
+    buffers = []
+    for r0 in range(0, rows, step):
+        wide = tensor[r0:r0 + step].to(dtype)
+        out[r0:r0 + step].copy_(wide, non_blocking=True)
+        buffers.append(wide)  # kept alive until the copies finish
+        if len(buffers) > 2:  # at most two chunks in flight
+            torch.cuda.current_stream(tensor.device).synchronize()
+            buffers = buffers[-1:]
+    torch.cuda.current_stream(tensor.device).synchronize()
+    return out
+
+
 def _checked_to_host(tensor: Tensor, context: str) -> Tensor:
     """``_to_host`` with the finiteness check done on the device, queued before the copy, so a
     large result is never scanned on the host."""
@@ -775,7 +795,7 @@ class ERTForward2p5D:
             include_robin_boundary_derivative=include_robin_boundary_derivative,
             normal_sensitivity=normal_sensitivity, jacobian_cell_parameter_ids=jacobian_cell_parameter_ids,
             jacobian_parameter_count=jacobian_parameter_count)
-        return response, _to_host(jacobian.to(self.dtype))  # widened on the device: exact, and cheaper
+        return response, _widened_to_host(jacobian, self.dtype)  # widened on the device: exact, and cheaper
 
     def _solve_with_jacobian_device(self, conductivity, currents=1.0, *, batch_size=None,
                                     include_robin_boundary_derivative: bool = False, normal_sensitivity: bool = True,
@@ -818,7 +838,7 @@ class ERTForward2p5D:
             if columns is None:
                 host = self._jacobian_to_host(fields)
             else:  # float64 results (terrain) are widened on the device, not over the host's memory
-                host = _to_host(self._jacobian_device(fields, columns).to(self.dtype))
+                host = _widened_to_host(self._jacobian_device(fields, columns), self.dtype)
         return host.to(self.dtype)
 
     def _jacobian_to_host(self, fields: _Fields) -> Tensor:

@@ -2,7 +2,8 @@
 
 ``d log(rhoa) / d log(rho) = k J_R (-sigma) / rhoa``: the row factor k / rhoa and the column
 factor -sigma are applied by one kernel while the Jacobian is still on the device, and the
-result is widened to float64 there, so only the final matrix crosses to the host.
+result is widened to float64 there a block of rows at a time, so only the final matrix crosses
+to the host and the device never holds a whole float64 copy.
 """
 
 from __future__ import annotations
@@ -11,7 +12,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .ert2p5d import _to_host
+from .ert2p5d import _widened_to_host
 
 
 def log_response_and_jacobian(operator, conductivity, *, chain=None, **solve_kwargs) -> tuple[np.ndarray, np.ndarray]:
@@ -35,5 +36,5 @@ def log_response_and_jacobian(operator, conductivity, *, chain=None, **solve_kwa
     lib = _native.load_library()
     _native.check(lib.adt_scale_rows_columns(_native.ptr(jacobian), rows, columns, _native.ptr(row), _native.ptr(column),
                                              _native.stream_handle(device)), None, "adt_scale_rows_columns")
-    # widened to float64 on the device (exact), so the host receives the final array
-    return np.log(np.asarray(response.apparent_resistivity, dtype=float)), _to_host(jacobian.to(torch.float64)).numpy()
+    # widened to float64 on the device (exact) in row blocks, so the host receives the final array
+    return np.log(np.asarray(response.apparent_resistivity, dtype=float)), _widened_to_host(jacobian).numpy()
