@@ -63,13 +63,7 @@ __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
 // by system (fields of each system) or by wavenumber (the primary field shared by all models).
 __global__ void spmm_kernel(SpmmArgs a) {
   chain_wait();
-  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x. A block's
-  // entries cover a few consecutive dofs; their CSR columns and values are staged in shared
-  // memory first, so each thread's product issues only its independent x loads (the slot order,
-  // and so every sum, is that of the CSR rows).
-  constexpr int kSlots = 1024;
-  __shared__ int scol[kSlots];
-  __shared__ double sval[kSlots];
+  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x
   const int NE = a.N * a.E;
   for (int t = blockIdx.y; t < a.systems; t += gridDim.y) {
     const int w = t % a.W, s = t / a.W;
@@ -78,34 +72,17 @@ __global__ void spmm_kernel(SpmmArgs a) {
     const double* rho = a.rho ? a.rho + (int64_t)s * a.E : nullptr;
     const double* base = a.base ? a.base + (int64_t)w * NE : nullptr;
     double* out = a.out + (int64_t)t * NE;
-    for (int first = blockIdx.x * blockDim.x; first < NE; first += gridDim.x * blockDim.x) {
-      const int last = min(first + (int)blockDim.x, NE) - 1;
-      const int s0 = a.csr_ptr[first / a.E], s1 = a.csr_ptr[last / a.E + 1];
-      const bool staged = s1 - s0 <= kSlots;  // block-uniform
-      __syncthreads();  // the previous range's slots have been read
-      if (staged)
-        for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x) {
-          scol[k] = a.csr_col[s0 + k];
-          sval[k] = v[s0 + k];
-        }
-      __syncthreads();
-      const int i = first + threadIdx.x;
-      if (i >= NE) continue;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NE; i += gridDim.x * blockDim.x) {
       const int n = i / a.E, e = i - n * a.E;
-      const int b = a.csr_ptr[n], end = a.csr_ptr[n + 1];
       double acc = 0.0;
       if (a.x_double) {
-        const double* x = (const double*)a.x + xo + e;
-        if (staged)
-          for (int slot = b - s0; slot < end - s0; ++slot) acc += sval[slot] * x[(int64_t)scol[slot] * a.E];
-        else
-          for (int slot = b; slot < end; ++slot) acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E];
+        const double* x = (const double*)a.x + xo;
+        for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
+          acc += v[slot] * x[(int64_t)a.csr_col[slot] * a.E + e];
       } else {
-        const float* x = (const float*)a.x + xo + e;
-        if (staged)
-          for (int slot = b - s0; slot < end - s0; ++slot) acc += sval[slot] * (double)x[(int64_t)scol[slot] * a.E];
-        else
-          for (int slot = b; slot < end; ++slot) acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E];
+        const float* x = (const float*)a.x + xo;
+        for (int slot = a.csr_ptr[n]; slot < a.csr_ptr[n + 1]; ++slot)
+          acc += v[slot] * (double)x[(int64_t)a.csr_col[slot] * a.E + e];
       }
       double coef = a.scale;
       if (rho) coef *= rho[e];
@@ -138,33 +115,37 @@ __global__ void total_kernel(const double* x, const double* primary, const doubl
 }
 
 // Electrode potentials pot[s][e][r] = sum_k wr_k sum_w weight_w u_w[dof_rk][e] of every model into
-// a padded (E+1) x (E+1) table (slot E: the zero remote row and column), one thread per entry.
+// a padded (E+1) x (E+1) table (slot E: the zero remote row and column), one warp per entry: its
+// lanes take the (k, w) terms, summed by a fixed shuffle tree (repeatable).
 // Replaces _integrate + the electrode product of _normal_reciprocal (ert2p5d.py:560-582).
 __global__ void potentials_kernel(MeasureArgs a, int models, double* pot) {
   chain_wait();
-  const int E1 = a.E + 1;
+  const int E1 = a.E + 1, lane = threadIdx.x & 31;
   const int64_t total = (int64_t)models * E1 * E1;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int terms = a.RW * a.W;
+  for (int64_t idx = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); idx < total; idx += warps) {
     const int s = (int)(idx / (E1 * E1));
     const int rem = (int)(idx - (int64_t)s * E1 * E1);
     const int r = rem / E1, e = rem - r * E1;  // pot[s][e][r] stored at [s][r][e]: e fastest
     double acc = 0.0;
     if (r < a.E && e < a.E) {
       const int64_t fo = (int64_t)s * a.W * a.N * a.E;
-      for (int k = 0; k < a.RW; ++k) {
+      for (int item = lane; item < terms; item += 32) {
+        const int k = item / a.W, w = item - k * a.W;
         const int dof = a.rcv_dofs[r * a.RW + k];
         if (dof < 0) continue;
-        double integ = 0.0;
-        for (int w = 0; w < a.W; ++w) {
-          const int64_t i = fo + ((int64_t)w * a.N + dof) * a.E + e;
-          integ += a.weights[w] * (a.f_double ? ((const double*)a.fields)[i] : (double)((const float*)a.fields)[i]);
-        }
-        acc += a.rcv_w[r * a.RW + k] * integ;
+        const int64_t i = fo + ((int64_t)w * a.N + dof) * a.E + e;
+        const double f = a.f_double ? ((const double*)a.fields)[i] : (double)((const float*)a.fields)[i];
+        acc += a.rcv_w[r * a.RW + k] * (a.weights[w] * f);
       }
-      if (a.potentials) a.potentials[((int64_t)s * a.E + e) * a.E + r] = acc;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
     }
-    pot[idx] = acc;
+    if (lane == 0) {
+      if (a.potentials && r < a.E && e < a.E) a.potentials[((int64_t)s * a.E + e) * a.E + r] = acc;
+      pot[idx] = acc;
+    }
   }
 }
 

@@ -104,7 +104,8 @@ extern "C" adt_status adt_measure_static(adt_plan* p, const float* fields, int32
   a.D = p->D;
   a.combine = 0;
   cudaStream_t s = (cudaStream_t)stream;
-  adt::launch_chained(adt::potentials_kernel, grid_for((int64_t)need, p->sms), 256, 0, s, a, models, table);
+  adt::launch_chained(adt::potentials_kernel, grid_for((int64_t)need * 32, p->sms), 256, 0, s, a, models,
+                      table);  // a warp per entry
   adt::launch_chained(adt::transfers_kernel, grid_for((int64_t)models * p->D, p->sms), 256, 0, s, a, models, table);
   p->launches += 2;
   return adt::check_launch(p, "static measure");

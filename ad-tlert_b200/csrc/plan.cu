@@ -204,7 +204,7 @@ void launch_measure(adt_plan* p, const TF* fields, int models, double* normal, d
     if (cudaMalloc(&p->pot, need * sizeof(double)) != cudaSuccess) return;
     p->pot_count = need;
   }
-  launch_chained(potentials_kernel, grid_for((int64_t)need), 256, 0, s, a, models, p->pot);
+  launch_chained(potentials_kernel, grid_for((int64_t)need * 32), 256, 0, s, a, models, p->pot);  // warp per entry
   launch_chained(transfers_kernel, grid_for((int64_t)models * p->D), 256, 0, s, a, models, p->pot);
   p->launches += 2;
 }
