@@ -14,8 +14,20 @@ namespace adt {
 //   sigma_parent(cell(b)) * alpha_w[b] * Mb[b][ij]       (mixed boundary, if robin)
 // for systems t = model * W + w. Replaces _assemble + GroupSum (adtlert/forward/ert2p5d.py:275-314,
 // adtlert/forward/kernels.py:30-85).
+__device__ __forceinline__ double source_resistivity(const float* sigma, int Cm, int E, int idx, const int* ptr,
+                                                     const int* cells) {
+  const int s = idx / E, e = idx % E;
+  double acc = 0.0;
+  for (int i = ptr[e]; i < ptr[e + 1]; ++i) acc -= log((double)sigma[(int64_t)s * Cm + cells[i]]);
+  const int n = ptr[e + 1] - ptr[e];
+  return n > 0 ? exp(acc / n) : 1.0;
+}
+
 __global__ void assemble_kernel(AssembleArgs a) {
   chain_wait();
+  if (a.rho)  // the source resistivities ride along with the assembly (one launch fewer)
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < a.models * a.E; idx += gridDim.x * blockDim.x)
+      a.rho[idx] = source_resistivity(a.sigma, a.Cm, a.E, idx, a.src_ptr, a.src_cells);
   const int64_t total = (int64_t)a.systems * a.nnz;
   for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {
@@ -51,11 +63,7 @@ __global__ void source_rho_kernel(const float* sigma, int Cm, int E, int models,
   chain_wait();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= models * E) return;
-  const int s = idx / E, e = idx % E;
-  double acc = 0.0;
-  for (int i = ptr[e]; i < ptr[e + 1]; ++i) acc -= log((double)sigma[(int64_t)s * Cm + cells[i]]);
-  const int n = ptr[e + 1] - ptr[e];
-  rho[idx] = n > 0 ? exp(acc / n) : 1.0;
+  rho[idx] = source_resistivity(sigma, Cm, E, idx, ptr, cells);
 }
 
 // out[t][n][e] = base[w][n][e] + coef(t,e) * sum_{slot in row n} values[t][slot] x[src(t)][col][e]
@@ -97,19 +105,32 @@ __global__ void spmm_kernel(SpmmArgs a) {
 __global__ void total_kernel(const double* x, const double* primary, const double* rho, int W,
                              int N, int E, int systems, float* fields) {
   chain_wait();
-  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x
+  // systems over blockIdx.y, the (dof, electrode) entries of a system over blockIdx.x; with E a
+  // multiple of 4, four consecutive electrodes of one dof per thread (vector loads and store)
   const int NE = N * E;
+  const bool quad = (E & 3) == 0;
   for (int t = blockIdx.y; t < systems; t += gridDim.y) {
     const int w = t % W, s = t / W;
     const double* xs = x + (int64_t)t * NE;
+    const double* up = primary ? primary + (int64_t)w * NE : nullptr;
+    const double* rs = rho ? rho + (int64_t)s * E : nullptr;
     float* out = fields + (int64_t)t * NE;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NE; i += gridDim.x * blockDim.x) {
-      if (primary) {
-        const int e = i % E;
-        out[i] = (float)(xs[i] + rho[s * E + e] * primary[(int64_t)w * NE + i]);
-      } else {
-        out[i] = (float)xs[i];
+    if (quad) {
+      for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < NE / 4; q += gridDim.x * blockDim.x) {
+        const int i = 4 * q, e = i % E;
+        const double2 x0 = *reinterpret_cast<const double2*>(xs + i), x1 = *reinterpret_cast<const double2*>(xs + i + 2);
+        double v[4] = {x0.x, x0.y, x1.x, x1.y};
+        if (up) {
+          const double2 u0 = *reinterpret_cast<const double2*>(up + i), u1 = *reinterpret_cast<const double2*>(up + i + 2);
+          const double u[4] = {u0.x, u0.y, u1.x, u1.y};
+#pragma unroll
+          for (int k = 0; k < 4; ++k) v[k] = v[k] + rs[e + k] * u[k];
+        }
+        *reinterpret_cast<float4*>(out + i) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
       }
+    } else {
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NE; i += gridDim.x * blockDim.x)
+        out[i] = up ? (float)(xs[i] + rs[i % E] * up[i]) : (float)xs[i];
     }
   }
 }

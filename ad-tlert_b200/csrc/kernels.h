@@ -22,6 +22,11 @@ struct AssembleArgs {
   int systems, nnz, W, C, Cm, K2, BL2, Nb, robin;
   int identity;    // add the unit diagonal of fixed dofs (system matrices, not derivatives)
   int w0;          // wavenumber of system 0 (systems cover wavenumbers w0 .. w0 + W - 1)
+  // optional: source resistivities rho[s][e] of the models, computed by the same launch
+  double* rho = nullptr;
+  const int* src_ptr = nullptr;
+  const int* src_cells = nullptr;
+  int models = 0, E = 0;
 };
 
 struct SpmmArgs {

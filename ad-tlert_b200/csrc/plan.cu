@@ -141,10 +141,18 @@ AssembleArgs assemble_args(adt_plan* p, const float* sigma, int systems, double*
   return a;
 }
 
-// System matrices (identity = true: unit diagonals on fixed dofs) or their sigma-derivatives.
+// System matrices (identity = true: unit diagonals on fixed dofs) or their sigma-derivatives;
+// with `rho`, the same launch also writes the source resistivities of the `models` models.
 void launch_assemble(adt_plan* p, const float* sigma, int systems, double* values, bool robin,
-                     bool identity, cudaStream_t s) {
+                     bool identity, cudaStream_t s, double* rho = nullptr, int models = 0) {
   AssembleArgs a = assemble_args(p, sigma, systems, values, robin, identity);
+  if (rho) {
+    a.rho = rho;
+    a.src_ptr = p->src_ptr;
+    a.src_cells = p->src_cells;
+    a.models = models;
+    a.E = p->E;
+  }
   launch_chained(assemble_kernel, grid_for((int64_t)systems * p->nnz), 256, 0, s, a);
   p->launches++;
 }
@@ -606,10 +614,7 @@ adt_status adt_factorize_fields(adt_plan* p, int32_t slot, const float* sigma, i
       return fail(p, ADT_OOM, "field right-hand side allocation failed");
     sl.rhs_capacity = systems;
   }
-  launch_assemble(p, sigma, systems, sl.values, true, true, s);
-  launch_chained(source_rho_kernel, grid_for((int64_t)models * p->E), 256, 0, s, sigma, p->Cm, p->E, models,
-                 p->src_ptr, p->src_cells, sl.rho);
-  p->launches++;
+  launch_assemble(p, sigma, systems, sl.values, true, true, s, sl.rho, models);  // + source resistivities
   // rhs = A(1) u_p - rho A(sigma) u_p, forward-reduced level by level with the factorization
   launch_spmm<double>(p, sl.values, false, p->primary, false, sl.rho, p->refrhs, -1.0, systems, sl.rhs, s);
   st = factorize_systems_rhs(p, systems, sl.values, sl.factors, sl.rhs, p->E, s);
