@@ -337,11 +337,14 @@ class WindowedInversion:
         models = self._clip(initial_log.to(self.device, torch.float64)).contiguous()
         start, bound = (models, None) if screen is None else screen.window_start(self, observed, models, previous)
         predicted, J = self.linearize(start)
-        if bound is not None and float(self.objective(start, predicted, observed, weights)) > bound:
+        warm = bound is not None
+        if warm and float(self.objective(start, predicted, observed, weights)) > bound:
             screen.reject_start()  # the FEM does not confirm the screened start
             predicted, J = self.linearize(models)
+            warm = False
         else:
             models = start
+        stall = getattr(screen, "stall_tolerance", None) if warm else None
         result = WindowResult(models, predicted, [])
         scale = max(math.sqrt(models.numel()), 1.0)
         for _ in range(s.max_iterations):
@@ -381,6 +384,11 @@ class WindowedInversion:
                 break
             if math.sqrt(step_sq) / scale < s.step_tolerance:
                 result.stop_reason = "step_tolerance"
+                break
+            if stall is not None and len(result.chi2) >= 2 and \
+                    abs(result.chi2[-1] - result.chi2[-2]) <= stall * result.chi2[-2]:
+                result.stop_reason = "chi2_stalled"  # warm-started windows only (see SurrogateScreen)
+                screen.counts["stalled_windows"] += 1
                 break
         result.log_models, result.predicted_log = models, predicted
         return result
