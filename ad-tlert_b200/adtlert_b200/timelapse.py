@@ -345,6 +345,7 @@ class WindowedInversion:
         else:
             models = start
         stall = getattr(screen, "stall_tolerance", None) if warm else None
+        decrease_tolerance = getattr(screen, "objective_tolerance", None) if warm else None
         result = WindowResult(models, predicted, [])
         scale = max(math.sqrt(models.numel()), 1.0)
         for _ in range(s.max_iterations):
@@ -357,6 +358,7 @@ class WindowedInversion:
             candidate = self._clip(models + s.step_length * delta).contiguous()
             step = candidate - models
             accepted = None
+            decrease = None  # the step's predicted relative objective decrease (FEM line search)
             if screen is not None and s.line_search:
                 accepted = screen.screened_step(self, models, step, candidate, predicted, observed, weights, result)
             if accepted is None:
@@ -364,7 +366,9 @@ class WindowedInversion:
                 tau = 1.0
                 if s.line_search:
                     residual1 = weights * (candidate_predicted - predicted)
-                    tau = line_search_tau(self.quadratic(models, step, residual0, residual1))
+                    a0, a1, a2 = self.quadratic(models, step, residual0, residual1)
+                    tau = line_search_tau((a0, a1, a2))
+                    decrease = -(2.0 * a1 * tau + a2 * tau * tau) / a0 if a0 > 0.0 else None
                     step = tau * step
                 if tau < 0.95:
                     models = self._clip(models + step).contiguous()
@@ -389,6 +393,11 @@ class WindowedInversion:
                     abs(result.chi2[-1] - result.chi2[-2]) <= stall * result.chi2[-2]:
                 result.stop_reason = "chi2_stalled"  # warm-started windows only (see SurrogateScreen)
                 screen.counts["stalled_windows"] += 1
+                break
+            if decrease_tolerance is not None and decrease is not None and len(result.chi2) >= 2 and \
+                    decrease < decrease_tolerance:
+                result.stop_reason = "objective_converged"  # warm-started windows only (see SurrogateScreen)
+                screen.counts["converged_windows"] += 1
                 break
         result.log_models, result.predicted_log = models, predicted
         return result
