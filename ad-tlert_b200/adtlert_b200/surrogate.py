@@ -343,17 +343,23 @@ class SurrogateScreen:
     constant to 1e-4). It also stops after its second or later step when the line search's
     quadratic predicts that step lowered the objective by less than ``objective_tolerance``
     (relative): from a warm start the first step lowers the objective by ~3 %, the second by
-    0.01-0.2 %, later ones by less than 1e-4 (measured on the same run). The windows started from
-    the reference's models keep the reference's stop rules only.
+    0.01-0.2 %, later ones by less than 1e-4 (measured on the same run). Its Gauss-Newton steps
+    run at most ``cgls_iterations`` CGLS iterations instead of the settings' count: measured on the
+    same run with 60, 40, 30, 20, 15 and 10, the final chi2 and the ρa error stayed within 0.3 %
+    of the 60-iteration run for every count, 30 kept its Gauss-Newton iterations per window
+    (2.30 against 2.27) and fewer added iterations. The windows started from the reference's
+    models keep the reference's stop rules and CGLS count.
     """
 
     def __init__(self, surrogate: Surrogate | None, *, warm_start: bool = True, line_search: bool = False,
-                 stall_tolerance: float | None = 1.0e-4, objective_tolerance: float | None = 1.0e-3) -> None:
+                 stall_tolerance: float | None = 1.0e-4, objective_tolerance: float | None = 1.0e-3,
+                 cgls_iterations: int | None = 30) -> None:
         self.surrogate = surrogate
         self.warm_start = warm_start
         self.line_search = line_search
         self.stall_tolerance = stall_tolerance
         self.objective_tolerance = objective_tolerance
+        self.cgls_iterations = cgls_iterations
         self.counts = {"line_search_screened": 0, "line_search_fallbacks": 0, "warm_starts": 0,
                        "warm_start_fallbacks": 0, "surrogate_batches": 0, "stalled_windows": 0,
                        "converged_windows": 0}

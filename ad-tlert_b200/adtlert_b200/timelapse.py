@@ -256,8 +256,10 @@ class WindowedInversion:
         base = self._workspace.data_ptr()
         return (base + 255) & ~255, self._workspace.numel() - ((-base) % 256)
 
-    def gauss_newton_step(self, J: Tensor, weights: Tensor, rhs: Tensor, models: Tensor) -> Tensor:
-        """CGLS solution (T, C) float64 of the linearized window system (adt_gn_step)."""
+    def gauss_newton_step(self, J: Tensor, weights: Tensor, rhs: Tensor, models: Tensor,
+                          iterations: int | None = None) -> Tensor:
+        """CGLS solution (T, C) float64 of the linearized window system (adt_gn_step), with at most
+        ``iterations`` CGLS iterations (default: the settings' ``cgls_max_iterations``)."""
 
         f, s = self.forward, self.settings
         T = int(models.shape[0])
@@ -268,7 +270,8 @@ class WindowedInversion:
         _native.check(f._lib.adt_gn_step(
             f._plan, _native.ptr(J), T, f.D, f.C, _native.ptr(weights), _native.ptr(rhs), _native.ptr(models),
             _native.ptr(ptr), _native.ptr(cells), _native.ptr(w2), float(s.regularization),
-            float(s.temporal_regularization), int(s.cgls_max_iterations), float(s.cgls_tolerance),
+            float(s.temporal_regularization), int(s.cgls_max_iterations if iterations is None else iterations),
+            float(s.cgls_tolerance),
             _native.ptr(step), address, size, self.multiprocessors, f._stream()), f._plan, "adt_gn_step")
         return step
 
@@ -346,11 +349,12 @@ class WindowedInversion:
             models = start
         stall = getattr(screen, "stall_tolerance", None) if warm else None
         decrease_tolerance = getattr(screen, "objective_tolerance", None) if warm else None
+        cgls_iterations = getattr(screen, "cgls_iterations", None) if warm else None
         result = WindowResult(models, predicted, [])
         scale = max(math.sqrt(models.numel()), 1.0)
         for _ in range(s.max_iterations):
             residual0 = weights * (predicted - observed)
-            delta = self.gauss_newton_step(J, weights, (-residual0).contiguous(), models)
+            delta = self.gauss_newton_step(J, weights, (-residual0).contiguous(), models, cgls_iterations)
             if s.max_log_step is not None:
                 largest = float(delta.abs().max())
                 if largest > s.max_log_step:

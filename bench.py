@@ -1251,8 +1251,11 @@ def run_timelapse(args, rank: int, world: int) -> dict | None:
             report["series_rhoa_rms_rel_error"] = float(np.sqrt(np.mean(series_error ** 2)))
             report["series_rhoa_max_rel_error"] = float(np.abs(series_error).max())
             fem_line = {"value": total_windows / f_s, "misfit": f_misfit}
+            rules = {"warm_start_stop_rules": {"stall_tolerance": screen.stall_tolerance,
+                                               "objective_tolerance": screen.objective_tolerance,
+                                               "cgls_iterations": screen.cgls_iterations}}
             screened_line = (s_s, s_wall, s_launches + surrogate.mlp.launches - launches_before, s_misfit, report,
-                             screen.counts, iterations, s_predicted, fem_line)
+                             dict(screen.counts, **rules), iterations, s_predicted, fem_line)
     if rank != 0:
         return None
     line = {
