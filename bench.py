@@ -118,7 +118,7 @@ def barrier(world: int) -> None:
 
 
 class ClockSampler:
-    """SM clock and throttle reasons sampled every 10 ms through NVML (read-only queries) while
+    """SM clock and throttle reasons sampled every `period_s` through NVML (read-only queries) while
     the GPU works: the sampler is started before the warm-up steps and stopped after the timed
     steps. The GPU is addressed by its PCI bus id, so the samples belong to the device torch
     uses whatever CUDA_VISIBLE_DEVICES or the CUDA device ordering is. Falls back to nvidia-smi
@@ -198,7 +198,7 @@ class ClockSampler:
         reasons = sorted({name for _, _, mask in self.samples for name, bit in self.REASONS if mask & bit})
         return {"sm_mhz": statistics.median(s for s, _, _ in self.samples), "sm_max_mhz": float(self.samples[0][1]),
                 "reasons": reasons, "samples": len(self.samples), "pci_bus_id": self.pci,
-                "window": "warm-up and timed steps, 10 ms NVML samples"}
+                "window": f"warm-up and timed steps, {1e3 * self.period_s:g} ms NVML samples"}
 
 
 def measured_peaks() -> dict:
@@ -790,7 +790,7 @@ def run_b200(args, rank: int, world: int) -> dict | None:
             fn(i)
 
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(device.index) as clocks:
+    with ClockSampler(device.index, period_s=0.002) as clocks:  # ~1 ms steps: sample densely
         for i in range(args.warmup):
             step(i)
         torch.cuda.synchronize(device)
