@@ -343,17 +343,19 @@ class SurrogateScreen:
     constant to 1e-4). It also stops after its second or later step when the line search's
     quadratic predicts that step lowered the objective by less than ``objective_tolerance``
     (relative): from a warm start the first step lowers the objective by ~3 %, the second by
-    0.01-0.2 %, later ones by less than 1e-4 (measured on the same run). Its Gauss-Newton steps
-    run at most ``cgls_iterations`` CGLS iterations instead of the settings' count: measured on the
-    same run with 60, 40, 30, 20, 15 and 10, the final chi2 and the ρa error stayed within 0.3 %
-    of the 60-iteration run for every count, 30 kept its Gauss-Newton iterations per window
-    (2.30 against 2.27) and fewer added iterations. The windows started from the reference's
-    models keep the reference's stop rules and CGLS count.
+    0.01-0.2 %, later ones by less than 1e-4 (measured on the same run), so 3e-3 ends most warm
+    windows after their second step. Its Gauss-Newton steps run at most ``cgls_iterations`` CGLS
+    iterations instead of the settings' count: a step from next to the solution needs no fully
+    converged inner solve. Measured on the same run, the final chi2 and the ρa error stayed
+    within 0.6 % of the plain run's for every pair swept (objective tolerance 1e-3, 3e-3, 1e-2;
+    CGLS 60 down to 10), and (3e-3, 20) gave the most windows per second among the pairs that
+    kept about two iterations per window. The windows started from the reference's models keep
+    the reference's stop rules and CGLS count.
     """
 
     def __init__(self, surrogate: Surrogate | None, *, warm_start: bool = True, line_search: bool = False,
-                 stall_tolerance: float | None = 1.0e-4, objective_tolerance: float | None = 1.0e-3,
-                 cgls_iterations: int | None = 30) -> None:
+                 stall_tolerance: float | None = 1.0e-4, objective_tolerance: float | None = 3.0e-3,
+                 cgls_iterations: int | None = 20) -> None:
         self.surrogate = surrogate
         self.warm_start = warm_start
         self.line_search = line_search
