@@ -1320,7 +1320,8 @@ def cgls_roofline(inversion, observed, initial, index: int, device, reps: int = 
     obs = torch.as_tensor(np.log(observed[index:index + 3]), dtype=torch.float64, device=device)
     weights = torch.full_like(predicted, 1.0 / cold.settings.data_std)
     rhs = (-(weights * (predicted - obs))).contiguous()
-    cold.gauss_newton_step(J, weights, rhs, models)
+    with torch.cuda.nvtx.range("untimed_gn_step"):  # the step profiling captures select (ncu --nvtx)
+        cold.gauss_newton_step(J, weights, rhs, models)
     iterations = cold.cgls_iterations()
     stream = torch.cuda.current_stream(device)
     begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1335,14 +1336,21 @@ def cgls_roofline(inversion, observed, initial, index: int, device, reps: int = 
     algorithmic = passes * J.numel() * J.element_size()
     peaks = measured_peaks()
     achieved = algorithmic / step_s / 1e9
+    traffic = None
+    path = ROOT / "profiles" / "traffic_cgls.json"
+    if path.exists():  # DRAM bytes of one captured adt_gn_step, scaled to this step's data passes
+        captured = json.loads(path.read_text())["adt_gn_step"]
+        traffic = captured["dram_bytes"] * passes / (captured["cgls_iterations"] + 1)
     return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "normal_data_kernel (CGLS step)",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": "normal_data_kernel (CGLS step)",
             "algorithmic_bytes_per_launch": algorithmic, "launch_ms": step_s * 1e3, "cgls_iterations": iterations,
             "jacobian_bytes": J.numel() * J.element_size(), "peak_source": peaks["source"],
             "note": "one adt_gn_step = A^T b pass + one data pass per CGLS iteration (each reads the window's "
                     "Jacobians once) + the reduce and update kernels; the first two models' Jacobians are "
                     "loaded evict-last so they stay in the 126 MB L2 between passes, hence achieved can pass "
-                    "the HBM copy peak"}
+                    "the HBM copy peak; traffic = DRAM bytes of one step captured by ncu (profiles/"
+                    "traffic_cgls.json; ncu empties the caches before each launch, so every pass reads all three "
+                    "Jacobians there), scaled to this step's passes"}
 
 
 def timelapse_cpu_baseline(nodes, cells, electrodes, rows, observed, initial, iterations_per_window: float) -> dict:
