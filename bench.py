@@ -1117,7 +1117,9 @@ def timelapse_config(windows, world, D, C) -> dict:
     return {
         "workload": f"time-lapse Gauss-Newton inversion: {TIMELAPSE_STEPS} steps on the 2.5D flat section ({C} cells, "
                     f"{D} rows, 17 wavenumbers), {windows} windows of 3 steps, first-order spatial (50) and temporal "
-                    f"(10) smoothness, CGLS 60 iterations, line search, at most 15 iterations per window",
+                    f"(10) smoothness, CGLS 60 iterations, line search, at most 15 iterations per window (the "
+                    f"reference's settings; a window the surrogate screen starts warm adds the screen's stop rules "
+                    f"and CGLS count, reported under screening.warm_start_stop_rules)",
         "windows": windows,
         "steps": TIMELAPSE_STEPS,
         "cells": C,
