@@ -13,7 +13,10 @@
 // s -= alpha A^T A p, gamma' = s.s, stop when gamma' / gamma_0 < tolerance, p = s + (gamma' /
 // gamma) p. The reference keeps r = b - A x and recomputes s = A^T r; here s follows its own
 // recurrence, which is the same sequence in exact arithmetic and lets one pass over J per
-// iteration produce both ||A p||^2 = p.(A^T A p) and A^T A p.
+// iteration produce both ||A p||^2 = p.(A^T A p) and A^T A p. With u = A^T A p, the new
+// gamma' = (s - alpha u).(s - alpha u) = s.s - 2 alpha s.u + alpha^2 u.u comes from dot products
+// of the iteration's own s and u (no recurrence over iterations), so one update kernel finishes
+// the iteration.
 //
 // Kernels of one iteration (all chained on the caller's stream; a device flag set when the
 // iteration stops turns the rest of the launched iterations into no-ops, so the host never waits
@@ -23,10 +26,11 @@
 //                        in float64 registers; written once per block (normal_data_kernel: the
 //                        same with register loads, where p_t and the ring exceed shared memory).
 //   normal_reduce_kernel u = sum of the block partials (fixed order) + ls L p_t + lt T^T T p,
-//                        with L = R^T R from neighbour lists; block partials of p.u.
-//   cgls_alpha_kernel    alpha = gamma / p.u, x += alpha p, s -= alpha u; block partials of s.s.
-//   cgls_beta_kernel     gamma' = s.s, the stop test, beta = gamma' / gamma, p = s + beta p.
-// The last two run on every block; each block sums the partials it needs itself, in one order.
+//                        with L = R^T R from neighbour lists; block partials of p.u, s.u, u.u
+//                        and s.s.
+//   cgls_update_kernel   gamma = s.s, alpha = gamma / p.u, gamma' from the sums above, the stop
+//                        test; x += alpha p, s -= alpha u, p = s + (gamma' / gamma) p. Every
+//                        block sums the partials itself, in one order.
 // Every reduction runs in a fixed order, so a step is bitwise repeatable.
 #include <algorithm>
 
@@ -45,11 +49,14 @@ constexpr int kMaxVec = 8;  // float4 per thread of the data pass: C <= 4 * 512 
 constexpr int kRingSlots = 4;  // most rows of J in the shared-memory ring of one data-pass block
 constexpr uint32_t kRingWaitLimit = 1u << 22;  // mbarrier polls before a ring wait gives up
 constexpr size_t kL2ResidentBytes = 96u << 20;  // J bytes loaded evict-last (kept in L2 between passes)
+constexpr int kDots = 4;  // dot products per reduce block: p.u, s.u, u.u, s.s
 
 // Per-step device state. The host clears it before a step; `error` is raised by a data pass that
-// gave up waiting for its row copies (the step is then NaN). gamma = s.s alternates between two
-// slots by iteration parity, so the blocks of one kernel read the old value while block 0 writes
-// the new one.
+// gave up waiting for its row copies (the step is then NaN). `done` is 0 while the iterations
+// run, else 1 + the first iteration that must not run: the update kernel of the stopping
+// iteration sets it while its own other blocks still finish that iteration, and every later
+// kernel returns at once. gamma0 is s.s of the start (the stop test's reference); gamma[it & 1]
+// records iteration it's gamma' (nothing on the device reads it back).
 struct CglsState {
   int done;
   int iterations;
@@ -65,8 +72,7 @@ struct Workspace {
   double* p;
   double* u;
   double* partial;
-  double* dots;     // per-block partials of p.u (reduce kernel)
-  double* squares;  // per-block partials of s.s (alpha kernel)
+  double* dots;     // per-block partials of p.u, s.u, u.u and s.s (reduce kernel), kDots arrays
   int ctas_per_model;
   int reduce_blocks;
   int update_blocks;
@@ -100,8 +106,7 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
   char* p = take(n * sizeof(double));
   char* u = take(n * sizeof(double));
   char* partial = take((size_t)T * per * C * sizeof(double));
-  char* dots = take((size_t)reduce_blocks * sizeof(double));
-  char* squares = take((size_t)update_blocks * sizeof(double));
+  char* dots = take((size_t)kDots * reduce_blocks * sizeof(double));
   (void)D;
   if (w) {
     w->state = reinterpret_cast<CglsState*>(state);
@@ -110,7 +115,6 @@ size_t workspace_layout(int T, int D, int C, int sms, Workspace* w, char* base) 
     w->u = reinterpret_cast<double*>(u);
     w->partial = reinterpret_cast<double*>(partial);
     w->dots = reinterpret_cast<double*>(dots);
-    w->squares = reinterpret_cast<double*>(squares);
     w->ctas_per_model = per;
     w->reduce_blocks = reduce_blocks;
     w->update_blocks = update_blocks;
@@ -400,33 +404,20 @@ __device__ __forceinline__ double block_sum(double value, double* shared) {
   return total;
 }
 
-// Sum of `count` values in a fixed order (lane l adds values l, l + 32, ..., then a butterfly),
-// identical in every block that calls it; the result is returned to every thread of the block.
-__device__ __forceinline__ double ordered_sum(const double* __restrict__ values, int count, double* shared_total) {
-  if (threadIdx.x < 32) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < count; i += 32) v += values[i];
-#pragma unroll
-    for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_xor_sync(0xffffffffu, v, offset);
-    if (threadIdx.x == 0) *shared_total = v;
-  }
-  __syncthreads();
-  return *shared_total;
-}
-
 // u = (sum of the data partials) + spatial L v_t + temporal T^T T v, kReduceColumns elements (t, c)
 // per block, the data partials of each summed by kReduceGroups threads (every kReduceGroups-th
-// partial) and the group sums added in group order; with `dot_with`, per-block partials of
-// dot_with . u. `partial` may be null (regularizer only).
+// partial) and the group sums added in group order; with `dot_with` (v = p) and `s_vec`, the
+// block's partials of p.u, s.u, u.u and s.s into dots[k * gridDim.x + block], k = 0 .. 3.
+// `partial` may be null (regularizer only).
 __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
     const double* __restrict__ partial, int ctas_per_model, int T, int C, const double* __restrict__ v,
     const int* __restrict__ nbr_ptr, const int* __restrict__ nbr_cell, const double* __restrict__ nbr_w2,
-    double spatial, double temporal, const double* __restrict__ dot_with, double* __restrict__ u,
-    double* __restrict__ dots, const CglsState* __restrict__ state) {
+    double spatial, double temporal, const double* __restrict__ dot_with, const double* __restrict__ s_vec,
+    double* __restrict__ u, double* __restrict__ dots, const CglsState* __restrict__ state) {
   adt::chain_wait();
   if (state != nullptr && state->done) return;
   __shared__ double group_sum[kReduceGroups - 1][kReduceColumns];
-  __shared__ double shared[kReduceColumns / 32];
+  __shared__ double shared[kDots][kReduceColumns / 32];
   const int64_t n = (int64_t)T * C;
   const int column = threadIdx.x % kReduceColumns, group = threadIdx.x / kReduceColumns;
   const int64_t i = (int64_t)blockIdx.x * kReduceColumns + column;
@@ -440,7 +431,7 @@ __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
   if (group > 0) return;
 #pragma unroll
   for (int g = 0; g < kReduceGroups - 1; ++g) sum += group_sum[g][column];
-  double product = 0.0;
+  double product[kDots] = {0.0, 0.0, 0.0, 0.0};
   if (i < n) {
     const double* vt = v + (size_t)t * C;
     const double vc = vt[c];
@@ -451,18 +442,27 @@ __global__ void __launch_bounds__(kReduceThreads) normal_reduce_kernel(
     if (t < T - 1) tt += vc - v[i + C];
     const double value = sum + spatial * lap + temporal * tt;
     u[i] = value;
-    if (dot_with != nullptr) product = dot_with[i] * value;
+    if (dot_with != nullptr) {
+      const double si = s_vec[i];
+      product[0] = dot_with[i] * value;
+      product[1] = si * value;
+      product[2] = value * value;
+      product[3] = si * si;
+    }
   }
   if (dot_with != nullptr) {  // the first kReduceColumns threads (the other groups have left): named barrier
 #pragma unroll
-    for (int offset = 16; offset > 0; offset >>= 1) product += __shfl_xor_sync(0xffffffffu, product, offset);
-    if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = product;
+    for (int k = 0; k < kDots; ++k) {
+#pragma unroll
+      for (int offset = 16; offset > 0; offset >>= 1) product[k] += __shfl_xor_sync(0xffffffffu, product[k], offset);
+      if ((threadIdx.x & 31) == 0) shared[k][threadIdx.x >> 5] = product[k];
+    }
     asm volatile("bar.sync 1, %0;\n" ::"n"(kReduceColumns) : "memory");
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < kDots) {
       double total = 0.0;
 #pragma unroll
-      for (int w = 0; w < kReduceColumns / 32; ++w) total += shared[w];
-      dots[blockIdx.x] = total;
+      for (int w = 0; w < kReduceColumns / 32; ++w) total += shared[threadIdx.x][w];
+      dots[threadIdx.x * gridDim.x + blockIdx.x] = total;
     }
   }
 }
@@ -485,64 +485,57 @@ __global__ void __launch_bounds__(kStartThreads) cgls_start_kernel(CglsState* st
   if (threadIdx.x == 0) {
     st->gamma[0] = gamma;
     st->gamma0 = gamma;
-    st->done = gamma > 0.0 ? 0 : 1;
+    st->done = gamma > 0.0 ? 0 : 1;  // 1: iteration 0 must not run
     st->iterations = 0;
   }
 }
 
-// Iteration `it`, first half: alpha = gamma / p.u (p.u summed from the reduce partials by every
-// block in the same order), x += alpha p, s -= alpha u, per-block partials of s.s.
-__global__ void __launch_bounds__(kUpdateThreads) cgls_alpha_kernel(CglsState* st, int it, int64_t n,
-                                                                    const double* __restrict__ dots, int dot_count,
-                                                                    double* __restrict__ x, double* __restrict__ s,
-                                                                    const double* __restrict__ p,
-                                                                    const double* __restrict__ u,
-                                                                    double* __restrict__ squares) {
+// Iteration `it`: gamma = s.s, alpha = gamma / p.u, gamma' = s.s - 2 alpha s.u + alpha^2 u.u
+// (every block sums the reduce partials in the same order), x += alpha p, s -= alpha u; unless
+// the stop test holds (gamma' / gamma_0 < tolerance, or gamma' <= 0), p = s + (gamma' / gamma) p.
+// p.u <= 0 stops before the update, as the reference's `denominator <= 0` does.
+__global__ void __launch_bounds__(kUpdateThreads) cgls_update_kernel(CglsState* st, int it, int64_t n,
+                                                                     const double* __restrict__ dots, int dot_count,
+                                                                     double* __restrict__ x, double* __restrict__ s,
+                                                                     double* __restrict__ p,
+                                                                     const double* __restrict__ u, double tolerance) {
   adt::chain_wait();
-  if (st->done) return;  // set by an earlier kernel, or below by block 0 for the same reason
-  __shared__ double total, shared[kUpdateThreads / 32];
-  const double pu = ordered_sum(dots, dot_count, &total);
+  const int done = st->done;
+  if (done != 0 && done - 1 <= it) return;  // an earlier iteration stopped
+  __shared__ double totals[kDots];
+  // warp k sums the partials of product k in one fixed order (lane l adds partials l, l + 32, ...,
+  // then a butterfly), the same in every block
+  if (threadIdx.x < 32 * kDots) {
+    const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+    const double* values = dots + (size_t)k * dot_count;
+    double v = 0.0;
+    for (int j = lane; j < dot_count; j += 32) v += values[j];
+#pragma unroll
+    for (int offset = 16; offset > 0; offset >>= 1) v += __shfl_xor_sync(0xffffffffu, v, offset);
+    if (lane == 0) totals[k] = v;
+  }
+  __syncthreads();
+  const double pu = totals[0], su = totals[1], uu = totals[2], gamma = totals[3];
   if (!(pu > 0.0)) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->done = 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->done = it + 1;
     return;
   }
-  const double alpha = st->gamma[it & 1] / pu;
+  const double alpha = gamma / pu;
+  const double gamma_new = gamma - 2.0 * alpha * su + alpha * alpha * uu;
+  const bool stop = !(gamma_new > 0.0) || gamma_new / st->gamma0 < tolerance;
+  const double beta = gamma_new / gamma;
   const int64_t i = (int64_t)blockIdx.x * kUpdateThreads + threadIdx.x;
-  double square = 0.0;
   if (i < n) {
     x[i] += alpha * p[i];
     const double si = s[i] - alpha * u[i];
     s[i] = si;
-    square = si * si;
+    if (!stop) p[i] = si + beta * p[i];
   }
-  const double block_total = block_sum<kUpdateThreads>(square, shared);
-  if (threadIdx.x == 0) {
-    squares[blockIdx.x] = block_total;
-    if (blockIdx.x == 0) st->iterations += 1;
-  }
-}
-
-// Iteration `it`, second half: gamma' = s.s (every block sums the partials in the same order),
-// stop when gamma' / gamma_0 < tolerance, else beta = gamma' / gamma and p = s + beta p.
-__global__ void __launch_bounds__(kUpdateThreads) cgls_beta_kernel(CglsState* st, int it, int64_t n,
-                                                                   const double* __restrict__ squares, int count,
-                                                                   const double* __restrict__ s,
-                                                                   double* __restrict__ p, double tolerance) {
-  adt::chain_wait();
-  if (st->done) return;
-  __shared__ double total;
-  const double gamma_new = ordered_sum(squares, count, &total);
-  const bool stop = !(gamma_new > 0.0) || gamma_new / st->gamma0 < tolerance;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (stop)
-      st->done = 1;
-    else
-      st->gamma[(it + 1) & 1] = gamma_new;
+    st->iterations += 1;
+    st->gamma[it & 1] = gamma_new;
+    if (stop) st->done = it + 2;
   }
-  if (stop) return;
-  const double beta = gamma_new / st->gamma[it & 1];
-  const int64_t i = (int64_t)blockIdx.x * kUpdateThreads + threadIdx.x;
-  if (i < n) p[i] = s[i] + beta * p[i];
 }
 
 template <int VEC>
@@ -641,8 +634,8 @@ extern "C" adt_status adt_gn_step(adt_plan* p, const float* jacobian, int32_t st
   data_pass(p, jacobian, steps, rows, columns, data_weights, w.p, data_rhs, w, false, s);
   adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s, (const double*)w.partial,
                       w.ctas_per_model, (int)steps, (int)columns, models, neighbour_ptr, neighbour_cells,
-                      neighbour_weights, -spatial, -temporal, (const double*)nullptr, w.u, w.dots,
-                      (const CglsState*)nullptr);
+                      neighbour_weights, -spatial, -temporal, (const double*)nullptr, (const double*)nullptr, w.u,
+                      w.dots, (const CglsState*)nullptr);
   adt::launch_chained(cgls_start_kernel, dim3(1), dim3(kStartThreads), 0, s, w.state, n, (const double*)w.u, step,
                       w.s, w.p);
   p->launches += 3;
@@ -650,14 +643,11 @@ extern "C" adt_status adt_gn_step(adt_plan* p, const float* jacobian, int32_t st
     data_pass(p, jacobian, steps, rows, columns, data_weights, w.p, nullptr, w, true, s);
     adt::launch_chained(normal_reduce_kernel, dim3(w.reduce_blocks), dim3(kReduceThreads), 0, s,
                         (const double*)w.partial, w.ctas_per_model, (int)steps, (int)columns, (const double*)w.p,
-                        neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal, (const double*)w.p, w.u,
-                        w.dots, (const CglsState*)w.state);
-    adt::launch_chained(cgls_alpha_kernel, dim3(w.update_blocks), dim3(kUpdateThreads), 0, s, w.state, it, n,
-                        (const double*)w.dots, w.reduce_blocks, step, w.s, (const double*)w.p, (const double*)w.u,
-                        w.squares);
-    adt::launch_chained(cgls_beta_kernel, dim3(w.update_blocks), dim3(kUpdateThreads), 0, s, w.state, it, n,
-                        (const double*)w.squares, w.update_blocks, (const double*)w.s, w.p, tolerance);
-    p->launches += 4;
+                        neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal, (const double*)w.p,
+                        (const double*)w.s, w.u, w.dots, (const CglsState*)w.state);
+    adt::launch_chained(cgls_update_kernel, dim3(w.update_blocks), dim3(kUpdateThreads), 0, s, w.state, it, n,
+                        (const double*)w.dots, w.reduce_blocks, step, w.s, w.p, (const double*)w.u, tolerance);
+    p->launches += 3;
   }
   return adt::check_launch(p, "gauss-newton step");
 }
@@ -672,7 +662,7 @@ extern "C" adt_status adt_gn_regularize(adt_plan* p, int32_t steps, int32_t colu
   const int64_t n = (int64_t)steps * columns;
   adt::launch_chained(normal_reduce_kernel, dim3((unsigned)reduce_grid(n)), dim3(kReduceThreads), 0,
                       (cudaStream_t)stream, (const double*)nullptr, 0, (int)steps, (int)columns, models, neighbour_ptr, neighbour_cells, neighbour_weights, spatial, temporal,
-                      (const double*)nullptr, out, (double*)nullptr, (const CglsState*)nullptr);
+                      (const double*)nullptr, (const double*)nullptr, out, (double*)nullptr, (const CglsState*)nullptr);
   p->launches += 1;
   return adt::check_launch(p, "gauss-newton regularizer");
 }
