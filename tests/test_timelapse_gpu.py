@@ -93,6 +93,32 @@ def test_device_cgls_matches_the_oracle(small, golden):
     assert abs(ours - theirs) / theirs < 1e-4, (ours, theirs)
 
 
+def test_device_cgls_stop_rule(small, golden):
+    """A loose tolerance stops the device CGLS early (the reference's 1e-12 never does): the step
+    equals the oracle's with the same tolerance, and bitwise the device's own run truncated at the
+    same iteration count, so every block finished the stopping iteration's update."""
+
+    op, inputs = small
+    nodes, cells = inputs["nodes"], inputs["cells"]
+    observed, initial = golden["observed_log"][:3], golden["initial_log"][:3]
+    settings = _settings(golden, cgls_tolerance=1.0e-3)
+    step, expected, _, _ = _compare_steps(op, nodes, cells, settings, observed, initial)
+    assert_close(step, expected, 1e-5, "CGLS step stopped by the tolerance")
+    inv = WindowedInversion(op, settings)
+    models = inv._clip(torch.as_tensor(initial, dtype=torch.float64, device="cuda")).contiguous()
+    predicted, J = inv.linearize(models)
+    obs = torch.as_tensor(observed, dtype=torch.float64, device="cuda")
+    weights = torch.full_like(predicted, 1.0 / settings.data_std)
+    rhs = (-(weights * (predicted - obs))).contiguous()
+    stopped = inv.gauss_newton_step(J, weights, rhs, models).cpu().numpy()
+    count = inv.cgls_iterations()
+    assert 0 < count < settings.cgls_max_iterations, count
+    full = WindowedInversion(op, _settings(golden))
+    truncated = full.gauss_newton_step(J, weights, rhs, models, iterations=count).cpu().numpy()
+    assert full.cgls_iterations() == count
+    assert np.array_equal(stopped, truncated)
+
+
 def test_device_cgls_on_the_benchmark_section():
     nodes, cells, electrodes, rows = synthetic.flat_section()
     op = ERTForward2p5D(Mesh.from_arrays(nodes, cells), Survey.from_arrays(electrodes, rows))
